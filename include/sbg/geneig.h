@@ -1,0 +1,184 @@
+/*
+ * sbg/geneig.h — C ABI of the B200 batched Hermitian-definite generalized eigensolver
+ *
+ *     A x = lambda B x,   A Hermitian (may be indefinite), B Hermitian positive definite,
+ *
+ * for batches of complex128 n x n pairs, the spin-wave pairs Sunny.jl produces per q-point.
+ * Drop-in for the launchers of riteshbhirud/sunny-batched-geneig:
+ *   - the fixed n = 54 C ABI of src/geneig_fixed.cu (same names, signatures, layout), and
+ *   - the runtime-n NvrtcGeneigSolver of src/nvrtc/nvrtc_solver.hpp:99-145, exposed as an
+ *     opaque handle with the same construction options, launch / launch_chunked and getters.
+ *
+ * Conventions (identical to the reference):
+ *   - matrices are column-major, leading dimension n, pairs contiguous (stride n*n elements);
+ *   - A is read in full; only the lower triangle of B is read;
+ *   - W[b*n + i] ascending; column i of X is the eigenvector of W[b*n+i], X^H B X = I,
+ *     arbitrary phase per column;
+ *   - every call is asynchronous on the given stream; the caller owns all device buffers.
+ * Per-pair info (always written; the caller need not zero it):
+ *   0            success
+ *   1 .. n       the tridiagonal QL failed to converge (that many off-diagonals left),
+ *                the zheev/zhegv convention
+ *   n + i        the leading minor of order i of B is not positive definite (also NaN/Inf
+ *                on B's diagonal path), the zhegv convention; W and X of that pair are NaN.
+ *   The staged Cholesky / reduction launchers report the zpotrf convention (i, not n + i).
+ *   The first failing stage wins (the reference's heev could overwrite a potrf failure).
+ */
+#ifndef SBG_GENEIG_H
+#define SBG_GENEIG_H
+
+#include <stddef.h>
+#include <cuComplex.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum {
+    SBG_OK = 0,
+    SBG_ERR_INVALID_VALUE = 1,   /* bad n, batch, pointer or option */
+    SBG_ERR_CUDA = 2,            /* a CUDA runtime call failed (see sbg_last_error) */
+    SBG_ERR_NO_MEMORY = 3,       /* device workspace allocation failed */
+    SBG_ERR_UNSUPPORTED = 4,     /* n outside the supported range for this form */
+    SBG_ERR_CAPTURING = 5,       /* workspace growth needed while the stream is being captured */
+    SBG_ERR_INTERNAL = 6         /* a C++ exception escaped (message in sbg_last_error) */
+} sbg_status;
+
+const char* sbg_status_string(int status);
+/* Message of the last failed call on this host thread ("" if none). */
+const char* sbg_last_error(void);
+
+/* ------------------------------------------------------------------ fixed n = 54 drop-in */
+/* Replaces src/geneig_fixed.cu:474-492: full solve of batch_size pairs. */
+void geneig_full_n54_batched_launch(const cuDoubleComplex* d_H, const cuDoubleComplex* d_S,
+                                    double* d_W, cuDoubleComplex* d_U, int* d_info,
+                                    int batch_size, cudaStream_t stream);
+/* Replace src/geneig_fixed.cu:494-497 (block size and dynamic shared memory of the
+ * largest stage kernel of the batched solve). */
+unsigned int geneig_full_n54_batched_block_dim_x(void);
+unsigned int geneig_full_n54_batched_shared_mem_bytes(void);
+
+/* Staged twins (debug / validation entry points, src/geneig_fixed.cu:106-152, 166-227,
+ * 247-325, 339-405, 516-592).  The single-matrix ones process exactly one pair. */
+/* geneig_fixed.cu:134-152: L = chol(S), lower, strict upper zeroed; info = zpotrf's. */
+void chol_n54_launch(const cuDoubleComplex* d_S, cuDoubleComplex* d_L, int* d_info,
+                     cudaStream_t stream);
+unsigned int chol_n54_block_dim_x(void);
+unsigned int chol_n54_shared_mem_bytes(void);
+/* geneig_fixed.cu:208-227: M = L^{-1} H L^{-H}, lower, strict upper zeroed. */
+void geneig_reduce_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComplex* d_S,
+                              cuDoubleComplex* d_M, int* d_info, cudaStream_t stream);
+unsigned int geneig_reduce_n54_block_dim_x(void);
+unsigned int geneig_reduce_n54_shared_mem_bytes(void);
+/* geneig_fixed.cu:302-325: W, V = eig(M) (V: eigenvectors of the reduced matrix). */
+void geneig_reduce_eig_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComplex* d_S,
+                                  double* d_W, cuDoubleComplex* d_V, int* d_info,
+                                  cudaStream_t stream);
+unsigned int geneig_reduce_eig_n54_block_dim_x(void);
+unsigned int geneig_reduce_eig_n54_shared_mem_bytes(void);
+/* Introspection twins of geneig_fixed.cu:320-324: shared memory of the Cholesky/reduction
+ * stage, of the eigensolve stage, and the per-pair device workspace (complex128 elements). */
+unsigned int geneig_reduce_eig_n54_chol_smem_bytes(void);
+unsigned int geneig_reduce_eig_n54_heev_smem_bytes(void);
+unsigned int geneig_reduce_eig_n54_heev_workspace(void);
+/* geneig_fixed.cu:385-405: full solve of one pair. */
+void geneig_full_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComplex* d_S,
+                            double* d_W, cuDoubleComplex* d_U, int* d_info, cudaStream_t stream);
+unsigned int geneig_full_n54_block_dim_x(void);
+unsigned int geneig_full_n54_shared_mem_bytes(void);
+/* geneig_fixed.cu:569-592: from (L, M) (lower triangles read) -> W, U = L^{-H} eigvecs(M). */
+void geneig_finish_n54_launch(const cuDoubleComplex* d_L, const cuDoubleComplex* d_M,
+                              double* d_W, cuDoubleComplex* d_U, int* d_info, int batch_size,
+                              cudaStream_t stream);
+unsigned int geneig_finish_n54_block_dim_x(void);
+unsigned int geneig_finish_n54_shared_mem_bytes(void);
+
+/* ------------------------------------------------------------------ runtime-n solver */
+/* Mirrors NvrtcGeneigSolver (src/nvrtc/nvrtc_solver.hpp:81-217).  The reference JIT-compiles
+ * a kernel per (n, pairs per CTA, block size); here every kernel is compiled ahead of time
+ * for sm_100a and construction only selects a schedule (and, with SBG_TUNING_AUTOTUNE,
+ * measures the candidates and persists the winner). */
+typedef struct sbg_solver sbg_solver;
+
+enum { SBG_TUNING_SUGGESTED = 0, SBG_TUNING_AUTOTUNE = 1 };            /* TuningMode, hpp:38 */
+enum { SBG_CACHE_AUTO = 0, SBG_CACHE_NO_DISK = 1, SBG_CACHE_NONE = 2 }; /* CacheMode, hpp:46 */
+enum { SBG_PRECISION_FP64 = 0, SBG_PRECISION_MIXED = 1 };
+
+typedef struct {
+    int batches_per_block;    /* pairs per CTA of the QL stage; 0 = auto (ctor arg, hpp:99) */
+    int force_block_dim_x;    /* threads per CTA of the reduce/back stages; 0 = auto (hpp:100) */
+    int tuning_mode;          /* SBG_TUNING_*  (hpp:101) */
+    int cache_mode;           /* SBG_CACHE_*   (hpp:102) */
+    int precision;            /* SBG_PRECISION_FP64 (plain drop-in) or SBG_PRECISION_MIXED */
+    int refine_steps;         /* mixed form: Ogita-Aishima steps, 0 = default (2) */
+    int workspace_pairs;      /* pairs per internal chunk; 0 = default */
+} sbg_solver_options;
+
+void sbg_solver_options_init(sbg_solver_options* opts);
+/* NvrtcGeneigSolver ctor (nvrtc_solver.cpp:927-1047). opts may be NULL. */
+int sbg_solver_create(int n, int device_id, const sbg_solver_options* opts, sbg_solver** out);
+int sbg_solver_destroy(sbg_solver* s);
+/* NvrtcGeneigSolver::launch (nvrtc_solver.cpp:1063-1076).  Any batch >= 0; no multiple-of-
+ * pairs-per-CTA restriction (the reference's partial last block was unchecked). */
+int sbg_solver_launch(sbg_solver* s, const cuDoubleComplex* d_A, const cuDoubleComplex* d_B,
+                      double* d_W, cuDoubleComplex* d_X, int* d_info, int batch,
+                      cudaStream_t stream);
+/* NvrtcGeneigSolver::launch_chunked (nvrtc_solver.cpp:1078-1107): round-robin chunks of
+ * chunk_size pairs over num_streams streams, no synchronisation between chunks. */
+int sbg_solver_launch_chunked(sbg_solver* s, const cuDoubleComplex* d_A,
+                              const cuDoubleComplex* d_B, double* d_W, cuDoubleComplex* d_X,
+                              int* d_info, int total, int chunk_size, int num_streams,
+                              const cudaStream_t* streams);
+/* Pre-sizes the internal workspace (pairs per chunk, number of stream slots) so later
+ * launches never allocate (required before capturing a launch into a CUDA graph). */
+int sbg_solver_reserve(sbg_solver* s, int pairs, int stream_slots);
+/* End-to-end solve of HOST-resident pairs: chunks of chunk_size pairs are copied to the
+ * device, solved and copied back, round-robin over num_streams internal streams so the
+ * copies of one chunk overlap the kernels of another (the chunked multi-stream idea of
+ * launch_chunked, nvrtc_solver.cpp:1078-1107, applied to host<->device traffic).
+ * Synchronous: returns once W, X and info are on the host.  Host buffers should be
+ * page-locked (cudaHostAlloc) for the copies to overlap.  Device staging buffers are
+ * owned by the solver and grow on demand. */
+int sbg_solver_solve_host(sbg_solver* s, const cuDoubleComplex* h_A, const cuDoubleComplex* h_B,
+                          double* h_W, cuDoubleComplex* h_X, int* h_info, int batch,
+                          int chunk_size, int num_streams);
+
+/* Per-stage timing: when enabled, every launch records CUDA events around each stage
+ * kernel on the launch stream.  sbg_solver_read_stage_times synchronizes on them and
+ * returns, per stage (0 = Cholesky + reduction + tridiagonalisation, 1 = tridiagonal
+ * eigensolve (QL, or QL + refinement for the mixed form), 2 = back-transform), the summed
+ * milliseconds and the number of kernel launches, then clears the record. */
+int sbg_solver_enable_stage_timing(sbg_solver* s, int enable);
+int sbg_solver_read_stage_times(sbg_solver* s, double* ms_out3, int* launches_out3);
+
+/* Device bytes of workspace per pair for a given n and precision. */
+size_t sbg_workspace_bytes_per_pair(int n, int precision);
+
+/* Getters (nvrtc_solver.hpp:128-145). */
+int sbg_solver_matrix_size(const sbg_solver* s);
+int sbg_solver_batches_per_block(const sbg_solver* s);
+int sbg_solver_block_dim_x(const sbg_solver* s);
+unsigned int sbg_solver_shared_mem_bytes(const sbg_solver* s);
+int sbg_solver_was_autotuned(const sbg_solver* s);
+int sbg_solver_autotune_sweep_ran(const sbg_solver* s);
+/* "in-process", "disk" or "compile" (here: "measured") — which layer supplied the schedule. */
+const char* sbg_solver_cache_layer_used(const sbg_solver* s);
+int sbg_solver_precision(const sbg_solver* s);
+
+/* Largest n each form supports on this device (shared-memory bound). */
+int sbg_max_n(int precision);
+
+/* Autotune table (the analogue of the reference's on-disk cubin cache,
+ * nvrtc_solver.cpp:403-431): path of this device's table file, written into buf.
+ * Directory: $SUNNY_GENEIG_CACHE_DIR, else $XDG_CACHE_HOME/sunny_geneig_b200, else
+ * $HOME/.cache/sunny_geneig_b200. */
+int sbg_tuning_table_path(int device_id, char* buf, size_t buflen);
+/* Forgets the in-process autotune memo (the next autotuned construction reads the file). */
+int sbg_tuning_forget_in_process(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SBG_GENEIG_H */

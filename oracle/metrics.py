@@ -1,0 +1,126 @@
+"""Parity metrics between a candidate solve and the LAPACK oracle.
+
+TEST INFRASTRUCTURE ONLY (the checker; the product never imports it).
+
+Inputs are flat column-major pairs, shape (batch, n*n) complex128, and
+eigenvalues (batch, n).  Metrics follow the reference's tests:
+  * eig_rel_ref  = max_i |W_g - W_r| / max(|W_r|, 1)      tests/test_full_batched_n54.cpp:95-99
+  * phase_err    = max_i 1 - |u_g^H S u_r| over columns whose eigenvalue gap to
+                   its neighbours is >= degen_gap            tests/test_full_batched_n54.cpp:100-113
+and add the gates the B200 build is held to:
+  * eig_rel      = max_i |W_g - W_r| / |W_r|                (pure relative error)
+  * residual     = ||A X - B X diag(W)||_F / (||A||_F ||X||_F)
+  * orth         = max |X^H B X - I|
+  * cluster_sin  = largest sine of the B-principal angle between candidate and
+                   oracle invariant subspaces, over clusters of eigenvalues
+                   closer than cluster_gap * max(|lambda|, 1).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def as_mats(M, n: int) -> np.ndarray:
+    """(batch, n*n) column-major -> (batch, n, n) with [b, i, j] = M(i, j)."""
+    M = np.asarray(M)
+    return M.reshape(-1, n, n).transpose(0, 2, 1)
+
+
+def from_mats(M) -> np.ndarray:
+    M = np.asarray(M)
+    b, n, _ = M.shape
+    return np.ascontiguousarray(M.transpose(0, 2, 1)).reshape(b, n * n)
+
+
+def eig_rel_ref(Wg, Wr) -> np.ndarray:
+    Wg = np.asarray(Wg, np.float64)
+    Wr = np.asarray(Wr, np.float64)
+    return np.max(np.abs(Wg - Wr) / np.maximum(np.abs(Wr), 1.0), axis=-1)
+
+
+def eig_rel(Wg, Wr) -> np.ndarray:
+    Wg = np.asarray(Wg, np.float64)
+    Wr = np.asarray(Wr, np.float64)
+    den = np.abs(Wr)
+    den = np.where(den == 0.0, 1.0, den)
+    return np.max(np.abs(Wg - Wr) / den, axis=-1)
+
+
+def nondegenerate_mask(Wr, degen_gap: float = 1e-6) -> np.ndarray:
+    Wr = np.asarray(Wr, np.float64)
+    d = np.abs(np.diff(Wr, axis=-1))
+    inf = np.full(Wr.shape[:-1] + (1,), np.inf)
+    left = np.concatenate([inf, d], axis=-1)
+    right = np.concatenate([d, inf], axis=-1)
+    return np.minimum(left, right) >= degen_gap
+
+
+def phase_err(S, Ug, Ur, Wr, n: int, degen_gap: float = 1e-6) -> np.ndarray:
+    Sm = as_mats(S, n)
+    G = as_mats(Ug, n)
+    R = as_mats(Ur, n)
+    SR = Sm @ R
+    inner = np.einsum("bki,bki->bi", G.conj(), SR)
+    err = 1.0 - np.abs(inner)
+    mask = nondegenerate_mask(Wr, degen_gap)
+    err = np.where(mask, err, 0.0)
+    return err.max(axis=-1)
+
+
+def residual(A, B, X, W, n: int) -> np.ndarray:
+    Am = as_mats(A, n)
+    Bm = as_mats(B, n)
+    Xm = as_mats(X, n)
+    R = Am @ Xm - (Bm @ Xm) * np.asarray(W)[:, None, :]
+    num = np.linalg.norm(R, axis=(1, 2))
+    den = np.linalg.norm(Am, axis=(1, 2)) * np.linalg.norm(Xm, axis=(1, 2))
+    return num / np.where(den == 0.0, 1.0, den)
+
+
+def orth(B, X, n: int) -> np.ndarray:
+    Bm = as_mats(B, n)
+    Xm = as_mats(X, n)
+    G = Xm.conj().transpose(0, 2, 1) @ Bm @ Xm
+    G = G - np.eye(n)[None]
+    return np.abs(G).reshape(G.shape[0], -1).max(axis=-1)
+
+
+def clusters(w, cluster_gap: float):
+    """Index ranges [lo, hi) of runs whose neighbour gaps are < cluster_gap*max(|w|,1)."""
+    out = []
+    lo = 0
+    n = len(w)
+    for i in range(1, n + 1):
+        if i == n or abs(w[i] - w[i - 1]) >= cluster_gap * max(abs(w[i]), abs(w[i - 1]), 1.0):
+            if i - lo > 1:
+                out.append((lo, i))
+            lo = i
+    return out
+
+
+def cluster_sin(B, Xg, Xr, Wr, n: int, cluster_gap: float = 1e-6) -> np.ndarray:
+    """Largest B-principal-angle sine between candidate and oracle cluster subspaces."""
+    Bm = as_mats(B, n)
+    G = as_mats(Xg, n)
+    R = as_mats(Xr, n)
+    Wr = np.asarray(Wr)
+    out = np.zeros(G.shape[0])
+    for b in range(G.shape[0]):
+        for lo, hi in clusters(Wr[b], cluster_gap):
+            M = R[b][:, lo:hi].conj().T @ Bm[b] @ G[b][:, lo:hi]
+            s = np.linalg.svd(M, compute_uv=False)
+            smin = min(1.0, float(s.min()))
+            out[b] = max(out[b], float(np.sqrt(max(0.0, 1.0 - smin * smin))))
+    return out
+
+
+def summarize(A, B, Wg, Xg, Wr, Xr, n: int, degen_gap: float = 1e-6) -> dict:
+    """All parity figures over a batch, as maxima (floats)."""
+    return dict(
+        eig_rel_ref=float(eig_rel_ref(Wg, Wr).max(initial=0.0)),
+        eig_rel=float(eig_rel(Wg, Wr).max(initial=0.0)),
+        phase_err=float(phase_err(B, Xg, Xr, Wr, n, degen_gap).max(initial=0.0)),
+        residual=float(residual(A, B, Xg, Wg, n).max(initial=0.0)),
+        orth=float(orth(B, Xg, n).max(initial=0.0)),
+        cluster_sin=float(cluster_sin(B, Xg, Xr, Wr, n, degen_gap).max(initial=0.0)),
+    )

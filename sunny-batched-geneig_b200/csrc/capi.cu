@@ -1,0 +1,536 @@
+// C ABI of the batched generalized eigensolver: the fixed n = 54 drop-in of
+// src/geneig_fixed.cu and the runtime-n solver handle that mirrors
+// NvrtcGeneigSolver (src/nvrtc/nvrtc_solver.hpp).  Every entry point catches
+// C++ exceptions and maps failures to sbg_status codes; the reference's void
+// launchers keep their void signatures and report through sbg_last_error() and
+// the CUDA error state.
+#include "sbg/geneig.h"
+#include "kernels.cuh"
+#include "tuning.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw Error(e == cudaErrorMemoryAllocation ? SBG_ERR_NO_MEMORY : SBG_ERR_CUDA,
+                    std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return SBG_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.status;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return SBG_ERR_INTERNAL;
+    } catch (...) {
+        g_last_error = "unknown exception";
+        return SBG_ERR_INTERNAL;
+    }
+}
+
+// Device workspace of one stream slot; grows on demand, never during capture.
+struct Slot {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int capacity = 0;
+};
+
+int default_chunk_pairs(int n) {
+    const size_t per = sbg::workspace_bytes_per_pair(n);
+    const size_t target = size_t(1) << 30;     // about 1 GiB of scratch per stream slot
+    size_t pairs = target / std::max<size_t>(per, 1);
+    pairs = std::min<size_t>(std::max<size_t>(pairs, 1024), 65536);
+    return static_cast<int>(pairs);
+}
+
+}  // namespace
+
+struct sbg_solver {
+    int n = 0;
+    int device = 0;
+    int precision = SBG_PRECISION_FP64;
+    int refine_steps = 2;
+    int chunk_pairs = 0;
+    sbg::Schedule sched;
+    bool autotuned = false;
+    bool sweep_ran = false;
+    const char* layer = "compile";
+    std::mutex mu;
+    std::vector<Slot> slots;
+    // staging buffers of the host-buffer path, one per internal stream
+    struct Staging { void* A = nullptr; void* B = nullptr; void* X = nullptr; void* W = nullptr; void* info = nullptr;
+                     int capacity = 0; cudaStream_t stream = nullptr; };
+    std::vector<Staging> staging;
+    // per-stage event timing
+    bool timing = false;
+    struct StageEvents { int stage; int kernels; cudaEvent_t a, b; };
+    std::vector<StageEvents> stage_events;
+
+    ~sbg_solver() {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        for (auto& s : slots) if (s.ptr) cudaFree(s.ptr);
+        for (auto& st : staging) {
+            if (st.stream) cudaStreamDestroy(st.stream);
+            for (void* p : {st.A, st.B, st.X, st.W, st.info}) if (p) cudaFree(p);
+        }
+        for (auto& e : stage_events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+        cudaSetDevice(prev);
+    }
+
+    void stage_begin(cudaStream_t stream, cudaEvent_t* a) {
+        *a = nullptr;
+        if (!timing) return;
+        check_cuda(cudaEventCreate(a), "cudaEventCreate");
+        check_cuda(cudaEventRecord(*a, stream), "cudaEventRecord");
+    }
+    void stage_end(cudaStream_t stream, cudaEvent_t a, int stage, int kernels) {
+        if (!timing || !a) return;
+        cudaEvent_t b;
+        check_cuda(cudaEventCreate(&b), "cudaEventCreate");
+        check_cuda(cudaEventRecord(b, stream), "cudaEventRecord");
+        std::lock_guard<std::mutex> lock(mu);
+        stage_events.push_back({stage, kernels, a, b});
+    }
+
+    sbg::Workspace workspace(int slot_idx, int pairs, cudaStream_t stream) {
+        std::lock_guard<std::mutex> lock(mu);
+        if (static_cast<int>(slots.size()) <= slot_idx) slots.resize(slot_idx + 1);
+        Slot& s = slots[slot_idx];
+        if (s.capacity < pairs) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (stream) check_cuda(cudaStreamIsCapturing(stream, &cs), "cudaStreamIsCapturing");
+            if (cs != cudaStreamCaptureStatusNone)
+                throw Error(SBG_ERR_CAPTURING, "workspace must grow while the stream is capturing; "
+                                               "call sbg_solver_reserve before capture");
+            if (s.ptr) { check_cuda(cudaFree(s.ptr), "cudaFree"); s.ptr = nullptr; s.capacity = 0; }
+            const size_t bytes = sbg::workspace_bytes_per_pair(n) * static_cast<size_t>(pairs) + 5 * 256;
+            check_cuda(cudaMalloc(&s.ptr, bytes), "cudaMalloc(workspace)");
+            s.bytes = bytes;
+            s.capacity = pairs;
+        }
+        return sbg::carve_workspace(s.ptr, n, s.capacity);
+    }
+
+    // One chunk of at most chunk_pairs pairs through the three stages.
+    void run_chunk(const double2* A, const double2* B, double* W, double2* X, int* info, int cnt,
+                   const sbg::Workspace& ws, cudaStream_t stream) {
+        cudaEvent_t ev;
+        stage_begin(stream, &ev);
+        check_cuda(sbg::launch_reduce(sbg::kReduceFull, A, B, n, cnt, ws, nullptr, info,
+                                      sched.reduce_threads, stream), "reduce kernel");
+        stage_end(stream, ev, 0, 1);
+        stage_begin(stream, &ev);
+        if (precision == SBG_PRECISION_MIXED)
+            check_cuda(sbg::launch_tridiag_mixed(n, cnt, ws, W, X, info, refine_steps, sched.ql_warps,
+                                                 sched.refine_threads, stream), "mixed eigensolve kernels");
+        else
+            check_cuda(sbg::launch_tridiag_ql(n, cnt, ws, W, X, info, sched.ql_warps, stream), "QL kernel");
+        stage_end(stream, ev, 1, precision == SBG_PRECISION_MIXED ? 2 : 1);
+        stage_begin(stream, &ev);
+        check_cuda(sbg::launch_back(sbg::kBackFull, n, cnt, ws, X, info, sched.back_threads, stream),
+                   "back-transform kernel");
+        stage_end(stream, ev, 2, 1);
+    }
+
+    void solve_host(const double2* hA, const double2* hB, double* hW, double2* hX, int* hinfo, int batch,
+                    int chunk, int nstreams) {
+        if (batch < 0 || chunk <= 0 || nstreams <= 0) throw Error(SBG_ERR_INVALID_VALUE, "bad solve_host arguments");
+        if (batch == 0) return;
+        if (!hA || !hB || !hW || !hX || !hinfo) throw Error(SBG_ERR_INVALID_VALUE, "null host pointer");
+        chunk = std::min(chunk, batch);
+        const size_t nn = static_cast<size_t>(n) * n;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            if (static_cast<int>(staging.size()) < nstreams) staging.resize(nstreams);
+            for (int i = 0; i < nstreams; ++i) {
+                Staging& st = staging[i];
+                if (!st.stream) check_cuda(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+                if (st.capacity < chunk) {
+                    for (void** p : {&st.A, &st.B, &st.X, &st.W, &st.info}) if (*p) { cudaFree(*p); *p = nullptr; }
+                    check_cuda(cudaMalloc(&st.A, 16 * nn * chunk), "cudaMalloc(staging)");
+                    check_cuda(cudaMalloc(&st.B, 16 * nn * chunk), "cudaMalloc(staging)");
+                    check_cuda(cudaMalloc(&st.X, 16 * nn * chunk), "cudaMalloc(staging)");
+                    check_cuda(cudaMalloc(&st.W, 8 * static_cast<size_t>(n) * chunk), "cudaMalloc(staging)");
+                    check_cuda(cudaMalloc(&st.info, 4 * static_cast<size_t>(chunk)), "cudaMalloc(staging)");
+                    st.capacity = chunk;
+                }
+            }
+        }
+        int idx = 0;
+        for (int off = 0; off < batch; off += chunk, ++idx) {
+            const int cnt = std::min(chunk, batch - off);
+            Staging& st = staging[idx % nstreams];
+            check_cuda(cudaMemcpyAsync(st.A, hA + nn * off, 16 * nn * cnt, cudaMemcpyHostToDevice, st.stream), "H2D A");
+            check_cuda(cudaMemcpyAsync(st.B, hB + nn * off, 16 * nn * cnt, cudaMemcpyHostToDevice, st.stream), "H2D B");
+            launch(static_cast<double2*>(st.A), static_cast<double2*>(st.B), static_cast<double*>(st.W),
+                   static_cast<double2*>(st.X), static_cast<int*>(st.info), cnt, st.stream, idx % nstreams);
+            check_cuda(cudaMemcpyAsync(hX + nn * off, st.X, 16 * nn * cnt, cudaMemcpyDeviceToHost, st.stream), "D2H X");
+            check_cuda(cudaMemcpyAsync(hW + static_cast<size_t>(n) * off, st.W, 8 * static_cast<size_t>(n) * cnt,
+                                       cudaMemcpyDeviceToHost, st.stream), "D2H W");
+            check_cuda(cudaMemcpyAsync(hinfo + off, st.info, 4 * static_cast<size_t>(cnt), cudaMemcpyDeviceToHost,
+                                       st.stream), "D2H info");
+        }
+        for (int i = 0; i < nstreams; ++i) check_cuda(cudaStreamSynchronize(staging[i].stream), "cudaStreamSynchronize");
+    }
+
+    void launch(const double2* A, const double2* B, double* W, double2* X, int* info, int batch,
+                cudaStream_t stream, int slot_idx = 0) {
+        if (batch < 0) throw Error(SBG_ERR_INVALID_VALUE, "batch < 0");
+        if (batch == 0) return;
+        if (!A || !B || !W || !X || !info) throw Error(SBG_ERR_INVALID_VALUE, "null device pointer");
+        const size_t nn = static_cast<size_t>(n) * n;
+        const int cap = std::min(batch, chunk_pairs);
+        sbg::Workspace ws = workspace(slot_idx, cap, stream);
+        for (int off = 0; off < batch; off += ws.capacity) {
+            const int cnt = std::min(ws.capacity, batch - off);
+            run_chunk(A + nn * off, B + nn * off, W + static_cast<size_t>(n) * off, X + nn * off, info + off,
+                      cnt, ws, stream);
+        }
+    }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) check_cuda(cudaSetDevice(dev), "cudaSetDevice");
+    }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+int supported_max_n(int precision) {
+    const size_t lim = static_cast<size_t>(sbg::max_smem_optin());
+    int best = 0;
+    for (int n = 1; n <= 256; ++n) {
+        size_t need = std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, n), sbg::back_smem_bytes(n));
+        need = std::max(need, sbg::tridiag_smem_bytes(n, 1, precision == SBG_PRECISION_MIXED));
+        if (precision == SBG_PRECISION_MIXED) need = std::max(need, sbg::refine_smem_bytes(n, 128));
+        if (need <= lim) best = n;
+    }
+    return best;
+}
+
+void create_solver(int n, int device, const sbg_solver_options* o, sbg_solver** out) {
+    if (!out) throw Error(SBG_ERR_INVALID_VALUE, "out == NULL");
+    *out = nullptr;
+    sbg_solver_options opts;
+    sbg_solver_options_init(&opts);
+    if (o) opts = *o;
+    if (n < 1) throw Error(SBG_ERR_INVALID_VALUE, "n must be >= 1");
+    if (opts.precision != SBG_PRECISION_FP64 && opts.precision != SBG_PRECISION_MIXED)
+        throw Error(SBG_ERR_INVALID_VALUE, "unknown precision");
+    int ndev = 0;
+    check_cuda(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+    if (device < 0 || device >= ndev) throw Error(SBG_ERR_INVALID_VALUE, "device_id out of range");
+    DeviceGuard g(device);
+    if (n > supported_max_n(opts.precision))
+        throw Error(SBG_ERR_UNSUPPORTED, "n = " + std::to_string(n) + " exceeds the single-CTA limit (" +
+                                             std::to_string(supported_max_n(opts.precision)) + ")");
+    std::unique_ptr<sbg_solver> s(new sbg_solver);
+    s->n = n;
+    s->device = device;
+    s->precision = opts.precision;
+    s->refine_steps = opts.refine_steps > 0 ? opts.refine_steps : 3;
+    s->chunk_pairs = opts.workspace_pairs > 0 ? opts.workspace_pairs : default_chunk_pairs(n);
+    sbg::TuneRequest req;
+    req.n = n;
+    req.device = device;
+    req.precision = opts.precision;
+    req.force_threads = opts.force_block_dim_x;
+    req.force_ql_warps = opts.batches_per_block;
+    req.autotune = opts.tuning_mode == SBG_TUNING_AUTOTUNE;
+    req.cache_mode = opts.cache_mode;
+    sbg::TuneResult tr = sbg::select_schedule(req);
+    s->sched = tr.sched;
+    s->autotuned = tr.autotuned;
+    s->sweep_ran = tr.sweep_ran;
+    s->layer = tr.layer;
+    *out = s.release();
+}
+
+// Process-wide n = 54 FP64 solver per device, used by the fixed-size drop-in.
+sbg_solver* default_n54_solver() {
+    static std::mutex mu;
+    static std::map<int, sbg_solver*> solvers;
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = solvers.find(dev);
+    if (it != solvers.end()) return it->second;
+    sbg_solver* s = nullptr;
+    create_solver(54, dev, nullptr, &s);
+    solvers[dev] = s;       // lives until process exit
+    return s;
+}
+
+void report_void(int status) {
+    if (status != SBG_OK) std::fprintf(stderr, "[sbg] %s\n", g_last_error.c_str());
+}
+
+const double2* c2(const cuDoubleComplex* p) { return reinterpret_cast<const double2*>(p); }
+double2* c2(cuDoubleComplex* p) { return reinterpret_cast<double2*>(p); }
+
+}  // namespace
+
+extern "C" {
+
+const char* sbg_status_string(int status) {
+    switch (status) {
+        case SBG_OK: return "ok";
+        case SBG_ERR_INVALID_VALUE: return "invalid value";
+        case SBG_ERR_CUDA: return "CUDA error";
+        case SBG_ERR_NO_MEMORY: return "out of device memory";
+        case SBG_ERR_UNSUPPORTED: return "unsupported size";
+        case SBG_ERR_CAPTURING: return "workspace growth during stream capture";
+        case SBG_ERR_INTERNAL: return "internal error";
+        default: return "unknown status";
+    }
+}
+
+const char* sbg_last_error(void) { return g_last_error.c_str(); }
+
+void sbg_solver_options_init(sbg_solver_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->tuning_mode = SBG_TUNING_SUGGESTED;
+    o->cache_mode = SBG_CACHE_AUTO;
+    o->precision = SBG_PRECISION_FP64;
+}
+
+int sbg_solver_create(int n, int device_id, const sbg_solver_options* opts, sbg_solver** out) {
+    return guarded([&] { create_solver(n, device_id, opts, out); });
+}
+
+int sbg_solver_destroy(sbg_solver* s) {
+    return guarded([&] { delete s; });
+}
+
+int sbg_solver_launch(sbg_solver* s, const cuDoubleComplex* d_A, const cuDoubleComplex* d_B, double* d_W,
+                      cuDoubleComplex* d_X, int* d_info, int batch, cudaStream_t stream) {
+    return guarded([&] {
+        if (!s) throw Error(SBG_ERR_INVALID_VALUE, "solver == NULL");
+        DeviceGuard g(s->device);
+        s->launch(c2(d_A), c2(d_B), d_W, c2(d_X), d_info, batch, stream);
+    });
+}
+
+int sbg_solver_launch_chunked(sbg_solver* s, const cuDoubleComplex* d_A, const cuDoubleComplex* d_B,
+                              double* d_W, cuDoubleComplex* d_X, int* d_info, int total, int chunk_size,
+                              int num_streams, const cudaStream_t* streams) {
+    return guarded([&] {
+        if (!s) throw Error(SBG_ERR_INVALID_VALUE, "solver == NULL");
+        if (total < 0) throw Error(SBG_ERR_INVALID_VALUE, "total < 0");
+        if (total == 0) return;
+        if (chunk_size <= 0) throw Error(SBG_ERR_INVALID_VALUE, "launch_chunked: chunk_size must be > 0");
+        if (num_streams <= 0 || !streams)
+            throw Error(SBG_ERR_INVALID_VALUE, "launch_chunked: need num_streams > 0 streams");
+        DeviceGuard g(s->device);
+        const size_t nn = static_cast<size_t>(s->n) * s->n;
+        int idx = 0;
+        for (int off = 0; off < total; off += chunk_size, ++idx) {
+            const int cnt = std::min(chunk_size, total - off);
+            const int slot = idx % num_streams;     // one workspace per stream: chunks in flight never share
+            s->launch(c2(d_A) + nn * off, c2(d_B) + nn * off, d_W + static_cast<size_t>(s->n) * off,
+                      c2(d_X) + nn * off, d_info + off, cnt, streams[slot], slot);
+        }
+    });
+}
+
+int sbg_solver_solve_host(sbg_solver* s, const cuDoubleComplex* h_A, const cuDoubleComplex* h_B, double* h_W,
+                          cuDoubleComplex* h_X, int* h_info, int batch, int chunk_size, int num_streams) {
+    return guarded([&] {
+        if (!s) throw Error(SBG_ERR_INVALID_VALUE, "solver == NULL");
+        DeviceGuard g(s->device);
+        s->solve_host(c2(h_A), c2(h_B), h_W, c2(h_X), h_info, batch, chunk_size, num_streams);
+    });
+}
+
+int sbg_solver_enable_stage_timing(sbg_solver* s, int enable) {
+    return guarded([&] {
+        if (!s) throw Error(SBG_ERR_INVALID_VALUE, "solver == NULL");
+        s->timing = enable != 0;
+    });
+}
+
+int sbg_solver_read_stage_times(sbg_solver* s, double* ms, int* launches) {
+    return guarded([&] {
+        if (!s || !ms || !launches) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
+        DeviceGuard g(s->device);
+        std::vector<sbg_solver::StageEvents> evs;
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            evs.swap(s->stage_events);
+        }
+        for (int k = 0; k < 3; ++k) { ms[k] = 0.0; launches[k] = 0; }
+        for (auto& e : evs) {
+            check_cuda(cudaEventSynchronize(e.b), "cudaEventSynchronize");
+            float t = 0.f;
+            check_cuda(cudaEventElapsedTime(&t, e.a, e.b), "cudaEventElapsedTime");
+            ms[e.stage] += t;
+            launches[e.stage] += e.kernels;
+            cudaEventDestroy(e.a);
+            cudaEventDestroy(e.b);
+        }
+    });
+}
+
+int sbg_solver_reserve(sbg_solver* s, int pairs, int stream_slots) {
+    return guarded([&] {
+        if (!s || pairs < 0 || stream_slots < 1) throw Error(SBG_ERR_INVALID_VALUE, "bad reserve arguments");
+        DeviceGuard g(s->device);
+        const int cap = std::min(std::max(pairs, 1), s->chunk_pairs);
+        for (int i = 0; i < stream_slots; ++i) s->workspace(i, cap, nullptr);
+    });
+}
+
+size_t sbg_workspace_bytes_per_pair(int n, int /*precision*/) {
+    return n > 0 ? sbg::workspace_bytes_per_pair(n) : 0;
+}
+
+int sbg_solver_matrix_size(const sbg_solver* s) { return s ? s->n : 0; }
+int sbg_solver_batches_per_block(const sbg_solver* s) { return s ? s->sched.ql_warps : 0; }
+int sbg_solver_block_dim_x(const sbg_solver* s) { return s ? s->sched.reduce_threads : 0; }
+unsigned int sbg_solver_shared_mem_bytes(const sbg_solver* s) {
+    if (!s) return 0;
+    size_t m = std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, s->n), sbg::back_smem_bytes(s->n));
+    return static_cast<unsigned>(m);
+}
+int sbg_solver_was_autotuned(const sbg_solver* s) { return s ? s->autotuned : 0; }
+int sbg_solver_autotune_sweep_ran(const sbg_solver* s) { return s ? s->sweep_ran : 0; }
+const char* sbg_solver_cache_layer_used(const sbg_solver* s) { return s ? s->layer : ""; }
+int sbg_solver_precision(const sbg_solver* s) { return s ? s->precision : -1; }
+
+int sbg_tuning_table_path(int device_id, char* buf, size_t buflen) {
+    return guarded([&] {
+        if (!buf || buflen == 0) throw Error(SBG_ERR_INVALID_VALUE, "buffer");
+        const std::string p = sbg::tuning_table_path(device_id);
+        if (p.size() + 1 > buflen) throw Error(SBG_ERR_INVALID_VALUE, "buffer too small");
+        std::memcpy(buf, p.c_str(), p.size() + 1);
+    });
+}
+
+int sbg_tuning_forget_in_process(void) {
+    return guarded([&] { sbg::forget_in_process(); });
+}
+
+int sbg_max_n(int precision) {
+    int r = 0;
+    guarded([&] { r = supported_max_n(precision); });
+    return r;
+}
+
+// ------------------------------------------------------------------ fixed n = 54 drop-in
+
+void geneig_full_n54_batched_launch(const cuDoubleComplex* d_H, const cuDoubleComplex* d_S, double* d_W,
+                                    cuDoubleComplex* d_U, int* d_info, int batch_size, cudaStream_t stream) {
+    report_void(guarded([&] {
+        if (batch_size <= 0) return;
+        default_n54_solver()->launch(c2(d_H), c2(d_S), d_W, c2(d_U), d_info, batch_size, stream);
+    }));
+}
+unsigned int geneig_full_n54_batched_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads; }
+unsigned int geneig_full_n54_batched_shared_mem_bytes(void) {
+    return static_cast<unsigned>(std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, 54), sbg::back_smem_bytes(54)));
+}
+
+void chol_n54_launch(const cuDoubleComplex* d_S, cuDoubleComplex* d_L, int* d_info, cudaStream_t stream) {
+    report_void(guarded([&] {
+        sbg::Workspace none;
+        check_cuda(sbg::launch_reduce(sbg::kReduceChol, nullptr, c2(d_S), 54, 1, none, c2(d_L), d_info,
+                                      sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads, stream),
+                   "chol kernel");
+    }));
+}
+unsigned int chol_n54_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads; }
+unsigned int chol_n54_shared_mem_bytes(void) { return static_cast<unsigned>(sbg::reduce_smem_bytes(sbg::kReduceChol, 54)); }
+
+void geneig_reduce_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComplex* d_S, cuDoubleComplex* d_M,
+                              int* d_info, cudaStream_t stream) {
+    report_void(guarded([&] {
+        sbg::Workspace none;
+        check_cuda(sbg::launch_reduce(sbg::kReduceHegst, c2(d_H), c2(d_S), 54, 1, none, c2(d_M), d_info,
+                                      sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads, stream),
+                   "reduce kernel");
+    }));
+}
+unsigned int geneig_reduce_n54_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads; }
+unsigned int geneig_reduce_n54_shared_mem_bytes(void) { return static_cast<unsigned>(sbg::reduce_smem_bytes(sbg::kReduceHegst, 54)); }
+
+void geneig_reduce_eig_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComplex* d_S, double* d_W,
+                                  cuDoubleComplex* d_V, int* d_info, cudaStream_t stream) {
+    report_void(guarded([&] {
+        sbg_solver* s = default_n54_solver();
+        sbg::Workspace ws = s->workspace(0, 1, stream);
+        check_cuda(sbg::launch_reduce(sbg::kReduceFull, c2(d_H), c2(d_S), 54, 1, ws, nullptr, d_info,
+                                      s->sched.reduce_threads, stream), "reduce kernel");
+        check_cuda(sbg::launch_tridiag_ql(54, 1, ws, d_W, c2(d_V), d_info, s->sched.ql_warps, stream), "QL kernel");
+        check_cuda(sbg::launch_back(sbg::kBackQOnly, 54, 1, ws, c2(d_V), d_info, s->sched.back_threads, stream),
+                   "back kernel");
+    }));
+}
+unsigned int geneig_reduce_eig_n54_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads; }
+unsigned int geneig_reduce_eig_n54_shared_mem_bytes(void) { return geneig_full_n54_batched_shared_mem_bytes(); }
+unsigned int geneig_reduce_eig_n54_chol_smem_bytes(void) { return static_cast<unsigned>(sbg::reduce_smem_bytes(sbg::kReduceFull, 54)); }
+unsigned int geneig_reduce_eig_n54_heev_smem_bytes(void) {
+    return static_cast<unsigned>(sbg::tridiag_smem_bytes(54, sbg::default_schedule(54, SBG_PRECISION_FP64).ql_warps, false));
+}
+unsigned int geneig_reduce_eig_n54_heev_workspace(void) {
+    return static_cast<unsigned>(sbg::workspace_bytes_per_pair(54) / 16);
+}
+
+void geneig_full_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComplex* d_S, double* d_W,
+                            cuDoubleComplex* d_U, int* d_info, cudaStream_t stream) {
+    geneig_full_n54_batched_launch(d_H, d_S, d_W, d_U, d_info, 1, stream);
+}
+unsigned int geneig_full_n54_block_dim_x(void) { return geneig_full_n54_batched_block_dim_x(); }
+unsigned int geneig_full_n54_shared_mem_bytes(void) { return geneig_full_n54_batched_shared_mem_bytes(); }
+
+void geneig_finish_n54_launch(const cuDoubleComplex* d_L, const cuDoubleComplex* d_M, double* d_W,
+                              cuDoubleComplex* d_U, int* d_info, int batch_size, cudaStream_t stream) {
+    report_void(guarded([&] {
+        if (batch_size <= 0) return;
+        sbg_solver* s = default_n54_solver();
+        const size_t nn = 54 * 54;
+        const int cap = std::min(batch_size, s->chunk_pairs);
+        sbg::Workspace ws = s->workspace(0, cap, stream);
+        for (int off = 0; off < batch_size; off += ws.capacity) {
+            const int cnt = std::min(ws.capacity, batch_size - off);
+            check_cuda(sbg::launch_reduce(sbg::kReduceFromLM, c2(d_M) + nn * off, c2(d_L) + nn * off, 54, cnt, ws,
+                                          nullptr, d_info + off, s->sched.reduce_threads, stream), "reduce kernel");
+            check_cuda(sbg::launch_tridiag_ql(54, cnt, ws, d_W + 54 * off, c2(d_U) + nn * off, d_info + off,
+                                              s->sched.ql_warps, stream), "QL kernel");
+            check_cuda(sbg::launch_back(sbg::kBackFull, 54, cnt, ws, c2(d_U) + nn * off, d_info + off,
+                                        s->sched.back_threads, stream), "back kernel");
+        }
+    }));
+}
+unsigned int geneig_finish_n54_block_dim_x(void) { return geneig_full_n54_batched_block_dim_x(); }
+unsigned int geneig_finish_n54_shared_mem_bytes(void) { return geneig_full_n54_batched_shared_mem_bytes(); }
+
+}  // extern "C"

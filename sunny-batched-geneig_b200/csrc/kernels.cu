@@ -1,0 +1,467 @@
+// Stage kernels of the batched generalized eigensolve and their launchers.
+//
+//   k_reduce   one CTA per pair: TMA bulk-copy A and the lower triangle of B into
+//              shared memory, potrf, C = L^{-1} A L^{-H}, Householder
+//              tridiagonalisation; writes L, the reflectors and (d, e, tau).
+//   k_tridiag  one warp per pair: implicit QL on (d, e) with the rotations
+//              accumulated into Z (shared memory), eigenvalues ascending -> W,
+//              Z -> the caller's X buffer.
+//   k_back     one CTA per pair: X = L^{-H} Q Z in shared memory, written over Z.
+//
+// The split follows where the work is latency bound: the QL recurrence is a
+// dependent scalar chain per pair, so it runs with many pairs per SM (only Z is
+// resident), while the BLAS2/BLAS3-shaped stages run a CTA per pair.
+#include "kernels.cuh"
+#include "stages.cuh"
+
+#include <mutex>
+
+namespace sbg {
+
+namespace {
+
+__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Shared-memory carve-up of k_reduce.
+struct ReduceSmem {
+    size_t Ls, As, invd, vbuf, pbuf, wbuf, sh, d, e, tau, bar, total;
+    __host__ __device__ ReduceSmem(int n) {
+        const size_t ld = static_cast<size_t>(tile_ld(n));
+        size_t o = 0;
+        Ls = o;   o += 16 * ld * n;
+        As = o;   o += 16 * ld * n;
+        invd = o; o += align_up(8 * n, 16);
+        vbuf = o; o += 16 * n;
+        pbuf = o; o += 32 * n;
+        wbuf = o; o += 16 * n;
+        sh = o;   o += 32;
+        d = o;    o += align_up(8 * n, 16);
+        e = o;    o += align_up(8 * n, 16);
+        tau = o;  o += 16 * n;
+        bar = o;  o += 16;
+        total = o;
+    }
+};
+
+struct BackSmem {
+    size_t LVs, Ys, invd, tau, bar, total;
+    __host__ __device__ BackSmem(int n) {
+        const size_t ld = static_cast<size_t>(tile_ld(n));
+        size_t o = 0;
+        LVs = o;  o += 16 * ld * n;
+        Ys = o;   o += 16 * ld * n;
+        invd = o; o += align_up(8 * n, 16);
+        tau = o;  o += 16 * n;
+        bar = o;  o += 16;
+        total = o;
+    }
+};
+
+template <typename R>
+__host__ __device__ inline size_t tridiag_warp_bytes(int n) {
+    return align_up(sizeof(R) * (static_cast<size_t>(n) * tile_ld(n) + 2 * n), 16);
+}
+
+__host__ __device__ inline int pick_group(int threads, int n) {
+    int g = 1;
+    while (g < 32 && threads / (2 * g) >= n) g *= 2;
+    return g;
+}
+
+// Waits for the bulk copies of this CTA; on the (never expected) timeout it flags
+// the pair and waits once more, bounded, so no copy lands after the CTA exits.
+__device__ inline bool wait_copies(uint64_t* bar, int* info_word) {
+    if (mbar_wait_bounded(bar, 0, kMaxPolls)) return true;
+    if (threadIdx.x == 0 && info_word) atomicOr(info_word, kInfoCopyTimeout);
+    mbar_wait_bounded(bar, 0, kMaxPolls);
+    return false;
+}
+
+// ----------------------------------------------------------------------------- k_reduce
+template <int T>
+__global__ void __launch_bounds__(T) k_reduce(int mode, const double2* __restrict__ A,
+                                              const double2* __restrict__ B, int n, int batch,
+                                              Workspace ws, double2* __restrict__ out,
+                                              int* __restrict__ info) {
+    const int b = blockIdx.x;
+    if (b >= batch) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const ReduceSmem lay(n);
+    const int ld = tile_ld(n);
+    double2* Ls = reinterpret_cast<double2*>(smem + lay.Ls);
+    double2* As = reinterpret_cast<double2*>(smem + lay.As);
+    double* invd = reinterpret_cast<double*>(smem + lay.invd);
+    double2* vbuf = reinterpret_cast<double2*>(smem + lay.vbuf);
+    double2* pbuf = reinterpret_cast<double2*>(smem + lay.pbuf);
+    double2* wbuf = reinterpret_cast<double2*>(smem + lay.wbuf);
+    double2* sh = reinterpret_cast<double2*>(smem + lay.sh);
+    double* d_s = reinterpret_cast<double*>(smem + lay.d);
+    double* e_s = reinterpret_cast<double*>(smem + lay.e);
+    double2* tau_s = reinterpret_cast<double2*>(smem + lay.tau);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + lay.bar);
+
+    const int tid = threadIdx.x;
+    const size_t mat = static_cast<size_t>(n) * n;
+    const double2* Ab = A + mat * b;     // A, or M in kReduceFromLM
+    const double2* Bb = B + mat * b;     // B, or L in kReduceFromLM
+    const bool need_a = mode != kReduceChol;
+
+    // ---- stage the pair into shared memory: B (lower part of each column) and A
+    if (tid == 0) { mbar_init(bar, 1); fence_mbar_init(); }
+    __syncthreads();
+    if (tid < 32) {
+        if (tid == 0) {
+            uint32_t bytes = static_cast<uint32_t>(16 * (static_cast<size_t>(n) * (n + 1) / 2));
+            if (need_a) bytes += static_cast<uint32_t>(16 * mat);
+            mbar_arrive_expect_tx(bar, bytes);
+        }
+        __syncwarp();
+        for (int j = tid; j < n; j += 32) {
+            bulk_g2s(Ls + j + static_cast<size_t>(j) * ld, Bb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
+            if (need_a) bulk_g2s(As + static_cast<size_t>(j) * ld, Ab + static_cast<size_t>(j) * n, 16u * n, bar);
+        }
+    }
+    wait_copies(bar, info + b);
+
+    const int G = pick_group(T, n);
+    int st = 0;
+    if (mode == kReduceFromLM) {
+        for (int i = tid; i < n; i += T) invd[i] = 1.0 / Ls[i + i * ld].x;
+        __syncthreads();
+    } else {
+        st = potrf_lower(Ls, ld, n, invd);
+    }
+    if (st != 0) {
+        if (tid == 0) info[b] = (mode == kReduceFull) ? n + st : st;
+        return;
+    }
+    if (mode == kReduceChol) {
+        for (size_t idx = tid; idx < mat; idx += T) {
+            const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
+            out[mat * b + idx] = (i >= j) ? Ls[i + j * ld] : make_double2(0.0, 0.0);
+        }
+        if (tid == 0) info[b] = 0;
+        return;
+    }
+    if (mode != kReduceFromLM) {
+        trsm_left_lower(Ls, ld, invd, As, ld, n, G);
+        __syncthreads();
+        trsm_right_lowerH(Ls, ld, invd, As, ld, n, G);
+        __syncthreads();
+    }
+    if (mode == kReduceHegst) {
+        for (size_t idx = tid; idx < mat; idx += T) {
+            const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
+            double2 v = make_double2(0.0, 0.0);
+            if (i >= j) { v = As[i + j * ld]; if (i == j) v.y = 0.0; }
+            out[mat * b + idx] = v;
+        }
+        if (tid == 0) info[b] = 0;
+        return;
+    }
+    // ---- tridiagonalise C, then store L (lower) and the reflectors (rows, upper) in one tile
+    hetrd_lower(As, ld, n, d_s, e_s, tau_s, vbuf, pbuf, wbuf, sh);
+    double2* LVg = ws.LV + mat * b;
+    for (size_t idx = tid; idx < mat; idx += T) {
+        const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
+        double2 v = make_double2(0.0, 0.0);
+        if (i >= j) v = Ls[i + j * ld];
+        else if (j >= i + 2) v = As[j + i * ld];       // LV(i, j) = v_i(j)
+        LVg[idx] = v;
+    }
+    for (int i = tid; i < n; i += T) {
+        ws.d[static_cast<size_t>(n) * b + i] = d_s[i];
+        ws.e[static_cast<size_t>(n) * b + i] = e_s[i];
+        ws.tau[static_cast<size_t>(n) * b + i] = (i + 1 < n) ? tau_s[i] : make_double2(0.0, 0.0);
+    }
+    if (tid == 0) info[b] = 0;
+}
+
+// ----------------------------------------------------------------------------- k_tridiag
+// R = double: the plain path, Z (double) -> X region, W final.
+// R = float : the mixed path's first half, Z (float) -> X region, W provisional.
+template <typename R>
+__global__ void k_tridiag(int n, int batch, Workspace ws, double* __restrict__ W,
+                          double2* __restrict__ X, int* __restrict__ info) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (b >= batch) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int ldz = tile_ld(n);
+    R* Z = reinterpret_cast<R*>(smem + tridiag_warp_bytes<R>(n) * warp);
+    R* d = Z + static_cast<size_t>(n) * ldz;
+    R* e = d + n;
+    const size_t mat = static_cast<size_t>(n) * n;
+    R* Zg = reinterpret_cast<R*>(X + mat * b);
+    double* Wb = W + static_cast<size_t>(n) * b;
+    if (info[b] != 0) {
+        for (int i = lane; i < n; i += 32) Wb[i] = __longlong_as_double(0x7ff8000000000000ll);
+        return;
+    }
+    for (int i = lane; i < n; i += 32) {
+        d[i] = static_cast<R>(ws.d[static_cast<size_t>(n) * b + i]);
+        e[i] = static_cast<R>(ws.e[static_cast<size_t>(n) * b + i]);
+    }
+    for (int r = lane; r < n; r += 32)
+        for (int c = 0; c < n; ++c) Z[r * ldz + c] = (r == c) ? R(1) : R(0);
+    __syncwarp();
+    const int unconv = tridiag_ql<R>(n, d, e, Z, ldz);
+    for (int i = lane; i < n; i += 32) Wb[i] = static_cast<double>(d[i]);
+    for (size_t idx = lane; idx < mat; idx += 32) {
+        const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
+        Zg[idx] = Z[r * ldz + c];
+    }
+    if (lane == 0 && unconv) info[b] = unconv;
+}
+
+// ----------------------------------------------------------------------------- k_refine
+// Mixed path, second half: FP64 Ogita-Aishima refinement of the FP32 tridiagonal
+// eigenpairs.  Reads Z (float, column-major) from the X region and (d, e) from
+// the workspace; writes the refined Z (double) over it and W.
+struct RefineSmem {
+    size_t Z0, Z1, TZ, Rm, Sm, d, e, lam, red, total;
+    __host__ __device__ RefineSmem(int n, int nwarps) {
+        const size_t tile = align_up(8 * static_cast<size_t>(n) * tile_ld(n), 16);
+        size_t o = 0;
+        Z0 = o; o += tile;
+        Z1 = o; o += tile;
+        TZ = o; o += tile;
+        Rm = o; o += tile;
+        Sm = o; o += tile;
+        d = o;  o += align_up(8 * n, 16);
+        e = o;  o += align_up(8 * n, 16);
+        lam = o; o += align_up(8 * n, 16);
+        red = o; o += 32 * nwarps;
+        total = o;
+    }
+};
+
+template <int T>
+__global__ void __launch_bounds__(T) k_refine(int n, int batch, Workspace ws, double* __restrict__ W,
+                                              double2* __restrict__ X, int* __restrict__ info,
+                                              int max_steps) {
+    const int b = blockIdx.x;
+    if (b >= batch) return;
+    if (info[b] > n || info[b] < 0) return;          // B not positive definite: W already NaN
+    extern __shared__ __align__(16) unsigned char smem[];
+    const RefineSmem lay(n, T / 32);
+    const int ld = tile_ld(n), tid = threadIdx.x;
+    double* Za = reinterpret_cast<double*>(smem + lay.Z0);
+    double* Zb = reinterpret_cast<double*>(smem + lay.Z1);
+    double* TZ = reinterpret_cast<double*>(smem + lay.TZ);
+    double* Rm = reinterpret_cast<double*>(smem + lay.Rm);
+    double* Sm = reinterpret_cast<double*>(smem + lay.Sm);
+    double* dT = reinterpret_cast<double*>(smem + lay.d);
+    double* eT = reinterpret_cast<double*>(smem + lay.e);
+    double* lam = reinterpret_cast<double*>(smem + lay.lam);
+    double* red = reinterpret_cast<double*>(smem + lay.red);
+    const size_t mat = static_cast<size_t>(n) * n;
+    const float* Z32 = reinterpret_cast<const float*>(X + mat * b);
+    for (size_t idx = tid; idx < mat; idx += T) {
+        const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
+        Za[r + c * ld] = static_cast<double>(Z32[idx]);
+    }
+    for (int i = tid; i < n; i += T) {
+        dT[i] = ws.d[static_cast<size_t>(n) * b + i];
+        eT[i] = ws.e[static_cast<size_t>(n) * b + i];
+    }
+    __syncthreads();
+    for (int step = 0; step < max_steps; ++step) {
+        const double em = oa_refine_step<2>(n, dT, eT, Za, ld, TZ, Rm, Sm, Zb, lam, red);
+        double* t = Za; Za = Zb; Zb = t;
+        if (em < 1e-15) break;                       // uniform: em is the same on every thread
+    }
+    // ascending order (the FP32 order can differ for near-equal eigenvalues)
+    if (tid == 0) {
+        for (int i = 0; i + 1 < n; ++i) {
+            int k = i;
+            for (int j = i + 1; j < n; ++j) if (lam[j] < lam[k]) k = j;
+            red[0] = 0.0;
+            if (k != i) { const double t = lam[i]; lam[i] = lam[k]; lam[k] = t; }
+            reinterpret_cast<int*>(TZ)[i] = k;       // swap record
+        }
+    }
+    __syncthreads();
+    for (int i = 0; i + 1 < n; ++i) {
+        const int k = reinterpret_cast<int*>(TZ)[i];
+        if (k != i) for (int r = tid; r < n; r += T) { const double t = Za[r + i * ld]; Za[r + i * ld] = Za[r + k * ld]; Za[r + k * ld] = t; }
+        __syncthreads();
+    }
+    double* Zg = reinterpret_cast<double*>(X + mat * b);
+    for (size_t idx = tid; idx < mat; idx += T) {
+        const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
+        Zg[idx] = Za[r + c * ld];
+    }
+    for (int i = tid; i < n; i += T) W[static_cast<size_t>(n) * b + i] = lam[i];
+}
+
+// ----------------------------------------------------------------------------- k_back
+template <int T>
+__global__ void __launch_bounds__(T) k_back(int mode, int n, int batch, Workspace ws,
+                                            double2* __restrict__ X, const int* __restrict__ info) {
+    const int b = blockIdx.x;
+    if (b >= batch) return;
+    const size_t mat = static_cast<size_t>(n) * n;
+    double2* Xb = X + mat * b;
+    const int tid = threadIdx.x;
+    if (info[b] > n || info[b] < 0) {     // B not positive definite: nothing to transform
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        for (size_t idx = tid; idx < mat; idx += T) Xb[idx] = make_double2(nan, nan);
+        return;
+    }
+    extern __shared__ __align__(16) unsigned char smem[];
+    const BackSmem lay(n);
+    const int ld = tile_ld(n);
+    double2* LVs = reinterpret_cast<double2*>(smem + lay.LVs);
+    double2* Ys = reinterpret_cast<double2*>(smem + lay.Ys);
+    double* invd = reinterpret_cast<double*>(smem + lay.invd);
+    double2* tau_s = reinterpret_cast<double2*>(smem + lay.tau);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + lay.bar);
+
+    const double2* LVg = ws.LV + mat * b;
+    if (tid == 0) { mbar_init(bar, 1); fence_mbar_init(); }
+    __syncthreads();
+    if (tid < 32) {
+        if (tid == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(16 * mat));
+        __syncwarp();
+        for (int j = tid; j < n; j += 32)
+            bulk_g2s(LVs + static_cast<size_t>(j) * ld, LVg + static_cast<size_t>(j) * n, 16u * n, bar);
+    }
+    const double* Zg = reinterpret_cast<const double*>(Xb);
+    for (size_t idx = tid; idx < mat; idx += T) {
+        const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
+        Ys[r + c * ld] = make_double2(Zg[idx], 0.0);
+    }
+    for (int i = tid; i < n; i += T) tau_s[i] = ws.tau[static_cast<size_t>(n) * b + i];
+    wait_copies(bar, nullptr);
+    for (int i = tid; i < n; i += T) invd[i] = 1.0 / LVs[i + i * ld].x;
+    __syncthreads();
+    const int G = pick_group(T, n);
+    apply_q_left<double>(LVs, ld, tau_s, Ys, ld, n, G);
+    __syncthreads();
+    if (mode == kBackFull) {
+        trsm_left_lowerH(LVs, ld, invd, Ys, ld, n, G);
+        __syncthreads();
+    }
+    for (size_t idx = tid; idx < mat; idx += T) {
+        const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
+        Xb[idx] = Ys[r + c * ld];
+    }
+}
+
+template <class K>
+void set_max_smem_once(K kernel, std::once_flag& flag) {
+    std::call_once(flag, [&]() {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem_optin());
+    });
+}
+
+}  // namespace
+
+// ============================================================================== host side
+
+size_t workspace_bytes_per_pair(int n) {
+    const size_t nn = static_cast<size_t>(n) * n;
+    return 16 * nn + 16 * n + 8 * n * 2;
+}
+
+Workspace carve_workspace(void* base, int n, int capacity) {
+    Workspace w;
+    w.n = n;
+    w.capacity = capacity;
+    const size_t nn = static_cast<size_t>(n) * n, cap = static_cast<size_t>(capacity);
+    char* p = static_cast<char*>(base);
+    auto take = [&](size_t bytes) { char* q = p; p += align_up(bytes, 256); return q; };
+    w.LV = reinterpret_cast<double2*>(take(16 * nn * cap));
+    w.tau = reinterpret_cast<double2*>(take(16 * n * cap));
+    w.d = reinterpret_cast<double*>(take(8 * n * cap));
+    w.e = reinterpret_cast<double*>(take(8 * n * cap));
+    return w;
+}
+
+int max_smem_optin() {
+    static int value = [] {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        return v;
+    }();
+    return value;
+}
+
+size_t reduce_smem_bytes(int, int n) { return ReduceSmem(n).total; }
+size_t back_smem_bytes(int n) { return BackSmem(n).total; }
+size_t tridiag_smem_bytes(int n, int warps_per_cta, bool single) {
+    return (single ? tridiag_warp_bytes<float>(n) : tridiag_warp_bytes<double>(n)) * warps_per_cta;
+}
+
+cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, int batch,
+                          const Workspace& ws, double2* out, int* info, int threads, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    const size_t smem = reduce_smem_bytes(mode, n);
+    if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+    static std::once_flag f128, f256;
+    if (threads == 128) {
+        set_max_smem_once(k_reduce<128>, f128);
+        k_reduce<128><<<batch, 128, smem, stream>>>(mode, A, B, n, batch, ws, out, info);
+    } else {
+        set_max_smem_once(k_reduce<256>, f256);
+        k_reduce<256><<<batch, 256, smem, stream>>>(mode, A, B, n, batch, ws, out, info);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tridiag_ql(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                              int warps_per_cta, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    const size_t smem = tridiag_smem_bytes(n, warps_per_cta, false);
+    if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+    static std::once_flag f;
+    set_max_smem_once(k_tridiag<double>, f);
+    const int grid = (batch + warps_per_cta - 1) / warps_per_cta;
+    k_tridiag<double><<<grid, 32 * warps_per_cta, smem, stream>>>(n, batch, ws, W, X, info);
+    return cudaGetLastError();
+}
+
+size_t refine_smem_bytes(int n, int threads) { return RefineSmem(n, threads / 32).total; }
+
+cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                                 int refine_steps, int warps_per_cta, int refine_threads, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    const size_t smem = tridiag_smem_bytes(n, warps_per_cta, true);
+    const size_t rsmem = refine_smem_bytes(n, refine_threads);
+    if (smem > static_cast<size_t>(max_smem_optin()) || rsmem > static_cast<size_t>(max_smem_optin()))
+        return cudaErrorInvalidValue;
+    static std::once_flag f, f128, f256;
+    set_max_smem_once(k_tridiag<float>, f);
+    const int grid = (batch + warps_per_cta - 1) / warps_per_cta;
+    k_tridiag<float><<<grid, 32 * warps_per_cta, smem, stream>>>(n, batch, ws, W, X, info);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    if (refine_threads == 128) {
+        set_max_smem_once(k_refine<128>, f128);
+        k_refine<128><<<batch, 128, rsmem, stream>>>(n, batch, ws, W, X, info, refine_steps);
+    } else {
+        set_max_smem_once(k_refine<256>, f256);
+        k_refine<256><<<batch, 256, rsmem, stream>>>(n, batch, ws, W, X, info, refine_steps);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
+                        int threads, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    const size_t smem = back_smem_bytes(n);
+    if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+    static std::once_flag f128, f256;
+    if (threads == 128) {
+        set_max_smem_once(k_back<128>, f128);
+        k_back<128><<<batch, 128, smem, stream>>>(mode, n, batch, ws, X, info);
+    } else {
+        set_max_smem_once(k_back<256>, f256);
+        k_back<256><<<batch, 256, smem, stream>>>(mode, n, batch, ws, X, info);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace sbg

@@ -1,0 +1,58 @@
+// Kernel declarations and the workspace layout shared by the host launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+
+namespace sbg {
+
+// Per-pair scratch between the three stage kernels (struct of arrays over pairs).
+//   LV  n*n complex   column-major, ld = n: the Cholesky factor L in the lower
+//                     triangle (diagonal included) and the Householder vectors of
+//                     the tridiagonalisation along the rows above the
+//                     superdiagonal: LV(k, i) = v_k(i) for i >= k + 2
+//   tau n   complex   reflector scalars
+//   d,e n   real      tridiagonal diagonal / subdiagonal
+// The tridiagonal eigenvectors Z (n*n real) are written into the caller's X buffer,
+// which the back-transform kernel then overwrites with X in place.
+struct Workspace {
+    double2* LV = nullptr;
+    double2* tau = nullptr;
+    double* d = nullptr;
+    double* e = nullptr;
+    int capacity = 0;   // pairs
+    int n = 0;
+};
+
+size_t workspace_bytes_per_pair(int n);
+// Carves a Workspace for `capacity` pairs of size n out of `base` (256-byte aligned).
+Workspace carve_workspace(void* base, int n, int capacity);
+
+enum ReduceMode : int {
+    kReduceFull = 0,      // potrf + hegst + hetrd  -> ws.LV/tau/d/e
+    kReduceChol = 1,      // potrf only             -> out (L, strict upper zeroed)
+    kReduceHegst = 2,     // potrf + hegst          -> out (M lower, strict upper zeroed)
+    kReduceFromLM = 3,    // hetrd of a given M     -> ws (L copied in)
+};
+enum BackMode : int {
+    kBackFull = 0,        // X = L^{-H} Q Z
+    kBackQOnly = 1,       // V = Q Z (eigenvectors of the reduced matrix)
+};
+
+// Launchers (asynchronous on `stream`; return cudaSuccess or the launch error).
+cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, int batch,
+                          const Workspace& ws, double2* out, int* info, int threads, cudaStream_t stream);
+cudaError_t launch_tridiag_ql(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                              int warps_per_cta, cudaStream_t stream);
+cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                                 int refine_steps, int warps_per_cta, int refine_threads, cudaStream_t stream);
+cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
+                        int threads, cudaStream_t stream);
+
+size_t reduce_smem_bytes(int mode, int n);
+size_t tridiag_smem_bytes(int n, int warps_per_cta, bool single);
+size_t back_smem_bytes(int n);
+size_t refine_smem_bytes(int n, int threads);
+int max_smem_optin();
+
+}  // namespace sbg

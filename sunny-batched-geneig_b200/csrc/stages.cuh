@@ -1,0 +1,549 @@
+// Stage device functions of the generalized Hermitian-definite eigensolve
+//   A x = lambda B x,  B = L L^H,  C = L^{-1} A L^{-H} = Q T Q^H,  T Z = Z Lambda,
+//   X = L^{-H} Q Z.
+//
+// Each function runs on one CTA ("team") over tiles that live in shared memory
+// (column-major, leading dimension ld = n | 1 so row walks are bank-conflict
+// free).  The stage boundaries are the reference's (src/geneig_fixed.cu:455-464):
+// potrf on B, the two-sided triangular reduction, the Hermitian eigensolve and
+// the back substitution; the eigensolve is split into Householder
+// tridiagonalisation, implicit QL on the real tridiagonal, and the reflector
+// back-application.
+#pragma once
+
+#include "common.cuh"
+
+namespace sbg {
+
+// ============================================================================ potrf
+// In-place lower Cholesky of the tile L (only the lower triangle is read, as
+// zpotrf 'L'). Right-looking, one CTA barrier per column: in phase k every
+// thread updates the trailing lower triangle with the unscaled column k divided
+// by L_kk, and the scaling of column k itself is deferred to phase k+1, when no
+// thread reads it any more.  invd[k] receives 1 / L_kk.
+// Returns 0, or k+1 for the first leading minor that is not positive definite
+// (also for NaN), the zpotrf convention.  Reference: Cholesky54, geneig_fixed.cu:17-26.
+template <typename R>
+__device__ int potrf_lower(cplx<R>* L, int ld, int n, R* invd) {
+    using C = cplx<R>;
+    const int tid = threadIdx.x, T = blockDim.x;
+    R pd = R(0), pinv = R(0);
+    for (int k = 0; k < n; ++k) {
+        const R dkk = L[k + k * ld].x;
+        if (!(dkk > R(0))) return k + 1;           // uniform: every thread reads the same word
+        const R d = sqrt(dkk);
+        const R inv = R(1) / d;
+        const R invdd = inv * inv;
+        if (k > 0) {                                // deferred scaling of column k-1
+            for (int i = k + tid; i < n; i += T) L[i + (k - 1) * ld] = cscale(L[i + (k - 1) * ld], pinv);
+            if (tid == 0) L[(k - 1) + (k - 1) * ld] = mk<R>(pd, R(0));
+        }
+        if (tid == 0) invd[k] = inv;
+        const int m = n - k - 1;
+        const C* colk = L + k * ld;
+        for (int idx = tid; idx < m * m; idx += T) {
+            const int jj = idx / m, ii = idx - jj * m;
+            if (ii < jj) continue;
+            const int i = k + 1 + ii, j = k + 1 + jj;
+            const C lik = cscale(colk[i], invdd);
+            L[i + j * ld] = cfmsc(lik, colk[j], L[i + j * ld]);
+        }
+        __syncthreads();
+        pd = d; pinv = inv;
+    }
+    if (tid == 0) L[(n - 1) + (n - 1) * ld] = mk<R>(pd, R(0));
+    __syncthreads();
+    return 0;
+}
+
+// ============================================================================ trsm (left, lower, no-trans)
+// W <- L^{-1} W for the full n x n tile W (Trsm54Left, geneig_fixed.cu:33-45).
+// Columns are independent: G lanes of one warp share a column, lane g owning the
+// rows i = g (mod G); the solved entry of row k is broadcast by shuffle.
+template <typename R>
+__device__ void trsm_left_lower(const cplx<R>* L, int ldl, const R* invd, cplx<R>* W, int ldw, int n, int G) {
+    using C = cplx<R>;
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int cols_per_pass = T / G;
+    const int g = tid % G;
+    for (int jb = 0; jb < n; jb += cols_per_pass) {
+        const int j = jb + tid / G;
+        const bool valid = j < n;
+        C* w = W + (valid ? j : 0) * ldw;
+        for (int k = 0; k < n; ++k) {
+            const int owner = k % G;
+            C wk = mk<R>(R(0), R(0));
+            if (valid && owner == g) { wk = cscale(w[k], invd[k]); w[k] = wk; }
+            wk = cshfl(wk, owner, G);
+            if (valid) {
+                const C* lk = L + k * ldl;
+                int i0 = k + 1 + ((g - (k + 1)) % G + G) % G;
+                for (int i = i0; i < n; i += G) w[i] = cfms(lk[i], wk, w[i]);
+            }
+        }
+    }
+}
+
+// ============================================================================ trsm (right, lower, conj-trans)
+// W <- W L^{-H}, lower triangle only (Trsm54Right, geneig_fixed.cu:47-59; the
+// result is Hermitian so only C(i, k), k <= i, is formed).  Rows are
+// independent: G lanes share a row, lane g owning the columns kk = g (mod G).
+template <typename R>
+__device__ void trsm_right_lowerH(const cplx<R>* L, int ldl, const R* invd, cplx<R>* W, int ldw, int n, int G) {
+    using C = cplx<R>;
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int rows_per_pass = T / G;
+    const int g = tid % G;
+    const int warp_first = (tid & ~31) / G;             // first row slot of this warp in a pass
+    const int warp_rows = 32 / G;
+    for (int ib = 0; ib < n; ib += rows_per_pass) {
+        const int i = ib + tid / G;
+        const bool valid = i < n;
+        const int kmax = min(n - 1, ib + warp_first + warp_rows - 1);   // uniform per warp
+        for (int k = 0; k <= kmax; ++k) {
+            const int owner = k % G;
+            const bool act = valid && k <= i;
+            C ck = mk<R>(R(0), R(0));
+            if (act && owner == g) { ck = cscale(W[i + k * ldw], invd[k]); W[i + k * ldw] = ck; }
+            ck = cshfl(ck, owner, G);
+            if (act) {
+                int kk0 = k + 1 + ((g - (k + 1)) % G + G) % G;
+                for (int kk = kk0; kk <= i; kk += G)
+                    W[i + kk * ldw] = cfmsc(ck, L[kk + k * ldl], W[i + kk * ldw]);
+            }
+        }
+    }
+}
+
+// ============================================================================ hetrd (lower)
+// Householder reduction of the Hermitian tile A (lower triangle valid) to real
+// symmetric tridiagonal form T = Q^H A Q, Q = H_0 H_1 ... H_{n-2},
+// H_k = I - tau_k v_k v_k^H with v_k = (0_{k+1}, 1, A(k+2:n, k)) stored in place.
+// Outputs d[0:n], e[0:n-1] (real), tau[0:n-1].  The steps are LAPACK zhetd2's
+// (reflector as zlarfg, p = tau A22 v, w = p - tau/2 (p^H v) v,
+// A22 -= v w^H + w v^H); the team splits the Hermitian matvec into a row walk
+// over the lower part and a column walk over the mirrored upper part.
+// Scratch: vbuf, wbuf (n complex), pbuf (2n complex), sh (2 complex).
+template <typename R>
+__device__ void hetrd_lower(cplx<R>* A, int lda, int n, R* d, R* e, cplx<R>* tau,
+                            cplx<R>* vbuf, cplx<R>* pbuf, cplx<R>* wbuf, cplx<R>* sh) {
+    using C = cplx<R>;
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int k = 0; k + 1 < n; ++k) {
+        const int m = n - k - 1;
+        C* x = A + (k + 1) + k * lda;                    // x[0..m) = A(k+1:n, k)
+        if (warp == 0) {
+            R s2 = R(0);
+            for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
+            s2 = warp_sum(s2);
+            const C alpha = x[0];
+            C tk, scale;
+            R beta;
+            if (s2 == R(0) && alpha.y == R(0)) {
+                tk = mk<R>(R(0), R(0)); beta = alpha.x; scale = mk<R>(R(0), R(0));
+            } else {
+                const R nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
+                beta = alpha.x >= R(0) ? -nrm : nrm;
+                tk = mk<R>((beta - alpha.x) / beta, -alpha.y / beta);
+                const R ar = alpha.x - beta, ai = alpha.y;   // scale = 1 / (alpha - beta)
+                const R den = ar * ar + ai * ai;
+                scale = mk<R>(ar / den, -ai / den);
+            }
+            if (tk.x != R(0) || tk.y != R(0)) {
+                for (int i = 1 + lane; i < m; i += 32) {
+                    const C vi = cmul(x[i], scale);
+                    x[i] = vi; vbuf[i] = vi;
+                }
+            }
+            if (lane == 0) {
+                vbuf[0] = mk<R>(R(1), R(0));
+                sh[0] = tk;
+                e[k] = beta;
+                tau[k] = tk;
+            }
+        }
+        __syncthreads();
+        const C tk = sh[0];
+        if (tk.x == R(0) && tk.y == R(0)) {               // H_k = I; keep the diagonal real
+            if (tid == 0) A[(k + 1) + (k + 1) * lda].y = R(0);
+            __syncthreads();
+            continue;
+        }
+        C* A22 = A + (k + 1) + (k + 1) * lda;
+        // p partial sums: part 0 = sum_{j<=r} A22(r,j) v_j, part 1 = sum_{j>r} conj(A22(j,r)) v_j
+        for (int t = tid; t < 2 * m; t += T) {
+            const int part = t >= m, r = t - part * m;
+            C acc0 = mk<R>(R(0), R(0)), acc1 = mk<R>(R(0), R(0));
+            if (part == 0) {
+                int j = 0;
+                for (; j + 1 < r; j += 2) {
+                    acc0 = cfma(A22[r + j * lda], vbuf[j], acc0);
+                    acc1 = cfma(A22[r + (j + 1) * lda], vbuf[j + 1], acc1);
+                }
+                for (; j < r; ++j) acc0 = cfma(A22[r + j * lda], vbuf[j], acc0);
+                const R drr = A22[r + r * lda].x;
+                acc0.x = fma(drr, vbuf[r].x, acc0.x);
+                acc0.y = fma(drr, vbuf[r].y, acc0.y);
+            } else {
+                const C* col = A22 + r * lda;
+                int j = r + 1;
+                for (; j + 1 < m; j += 2) {
+                    acc0 = cfmac(col[j], vbuf[j], acc0);
+                    acc1 = cfmac(col[j + 1], vbuf[j + 1], acc1);
+                }
+                for (; j < m; ++j) acc0 = cfmac(col[j], vbuf[j], acc0);
+            }
+            pbuf[t] = cadd(acc0, acc1);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            // p = tau (part0 + part1); alpha2 = -tau/2 (p^H v); w = p + alpha2 v
+            C dot = mk<R>(R(0), R(0));
+            for (int r = lane; r < m; r += 32) {
+                const C p = cmul(tk, cadd(pbuf[r], pbuf[m + r]));
+                wbuf[r] = p;
+                dot = cfmac(p, vbuf[r], dot);
+            }
+            dot.x = warp_sum(dot.x);
+            dot.y = warp_sum(dot.y);
+            const C a2 = cscale(cmul(tk, dot), R(-0.5));
+            for (int r = lane; r < m; r += 32) wbuf[r] = cfma(a2, vbuf[r], wbuf[r]);
+        }
+        __syncthreads();
+        // A22 -= v w^H + w v^H on the lower triangle; thread (row r, column chunk c)
+        {
+            const int chunks = max(1, T / m);
+            const int cw = (m + chunks - 1) / chunks;
+            for (int t = tid; t < m * chunks; t += T) {
+                const int r = t % m, c = t / m;
+                const C vr = vbuf[r], wr = wbuf[r];
+                const int j0 = c * cw, j1 = min(r + 1, (c + 1) * cw);
+                for (int j = j0; j < j1; ++j) {
+                    C a = A22[r + j * lda];
+                    a = cfmsc(vr, wbuf[j], a);
+                    a = cfmsc(wr, vbuf[j], a);
+                    if (j == r) a.y = R(0);
+                    A22[r + j * lda] = a;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < n; i += T) d[i] = A[i + i * lda].x;
+    if (tid == 0 && n >= 1) e[n - 1] = R(0);
+    __syncthreads();
+}
+
+// ============================================================================ Q Z
+// Y <- Q Y with Q = H_0 ... H_{n-2} from hetrd_lower.  The reflectors are read
+// from the rows of the tile LV: component i >= k+2 of v_k sits at LV(k, i) (the
+// strict upper triangle above the superdiagonal, so one tile also holds L in its
+// lower triangle); v_k(k+1) = 1 is implicit.  Applied right to left; columns of
+// Y are independent, G lanes per column reduce v^H y by shuffle.
+template <typename R>
+__device__ void apply_q_left(const cplx<R>* LV, int ld, const cplx<R>* tau, cplx<R>* Y, int ldy, int n, int G) {
+    using C = cplx<R>;
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int cols_per_pass = T / G;
+    const int g = tid % G;
+    for (int jb = 0; jb < n; jb += cols_per_pass) {
+        const int j = jb + tid / G;
+        const bool valid = j < n;
+        C* y = Y + (valid ? j : 0) * ldy;
+        for (int k = n - 2; k >= 0; --k) {
+            const C tk = tau[k];
+            if (tk.x == R(0) && tk.y == R(0)) continue;      // uniform
+            const int m = n - k - 1;
+            const C* v = LV + k + (k + 1) * ld;               // v[i] = LV(k, k+1+i), v[0] = 1
+            C s = mk<R>(R(0), R(0));
+            if (valid) {
+                for (int i = g; i < m; i += G) {
+                    const C vi = (i == 0) ? mk<R>(R(1), R(0)) : v[i * ld];
+                    s = cfmac(vi, y[k + 1 + i], s);
+                }
+            }
+            s.x = group_sum(s.x, G);
+            s.y = group_sum(s.y, G);
+            s = cmul(tk, s);
+            if (valid) {
+                for (int i = g; i < m; i += G) {
+                    const C vi = (i == 0) ? mk<R>(R(1), R(0)) : v[i * ld];
+                    y[k + 1 + i] = cfms(vi, s, y[k + 1 + i]);
+                }
+            }
+        }
+    }
+}
+
+// ============================================================================ trsm (left, lower, conj-trans)
+// Y <- L^{-H} Y (Trsm54LeftConj, geneig_fixed.cu:63-75): backward substitution
+// per column, G lanes per column, lane g owning rows i = g (mod G).
+template <typename R>
+__device__ void trsm_left_lowerH(const cplx<R>* L, int ldl, const R* invd, cplx<R>* Y, int ldy, int n, int G) {
+    using C = cplx<R>;
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int cols_per_pass = T / G;
+    const int g = tid % G;
+    for (int jb = 0; jb < n; jb += cols_per_pass) {
+        const int j = jb + tid / G;
+        const bool valid = j < n;
+        C* y = Y + (valid ? j : 0) * ldy;
+        for (int k = n - 1; k >= 0; --k) {
+            const int owner = k % G;
+            C xk = mk<R>(R(0), R(0));
+            if (valid && owner == g) { xk = cscale(y[k], invd[k]); y[k] = xk; }
+            xk = cshfl(xk, owner, G);
+            if (valid) {
+                for (int i = g; i < k; i += G) y[i] = cfms(cconj(L[k + i * ldl]), xk, y[i]);
+            }
+        }
+    }
+}
+
+// ============================================================================ tridiagonal QL
+// Eigen-decomposition of the real symmetric tridiagonal (d, e) by implicit QL
+// with Wilkinson-type shifts, accumulating the rotations into Z (row-major,
+// Z[r * ldz + c], initialised to I by the caller).  One warp per problem: every
+// lane runs the same scalar recurrence (so no broadcast is needed) and applies
+// each rotation to the rows it owns (r = lane + 32 q).  The deflation test is
+// LAPACK dsteqr's relative one, |e_m|^2 <= eps^2 |d_m| |d_{m+1}| + safmin, and the
+// matrix is scaled to unit max-norm first (dsteqr scales only at the range
+// limits; scaling always keeps the single-precision variant safe).
+// Eigenvalues come back ascending with Z's columns permuted alike (dsteqr's
+// final selection sort).  Returns the number of off-diagonals that failed to
+// converge within 30 iterations per eigenvalue (0 on success).
+// d, e live in shared memory private to the warp; only lane 0 writes them.
+template <typename R>
+__device__ int tridiag_ql(int n, R* d, R* e, R* Z, int ldz) {
+    const int lane = threadIdx.x & 31;
+    const R eps = sizeof(R) == 8 ? R(1.1102230246251565e-16) : R(5.9604645e-08);
+    const R eps2 = eps * eps;
+    const R safmin = sizeof(R) == 8 ? R(2.2250738585072014e-308) : R(1.17549435e-38);
+    // scale to unit max-norm
+    R anorm = R(0);
+    for (int i = 0; i < n; ++i) anorm = fmax(anorm, fabs(d[i]));
+    for (int i = 0; i + 1 < n; ++i) anorm = fmax(anorm, fabs(e[i]));
+    if (!(anorm > R(0)) || !isfinite(anorm)) anorm = R(1);
+    const R sc = R(1) / anorm;
+    __syncwarp();
+    if (lane == 0) {
+        for (int i = 0; i < n; ++i) d[i] *= sc;
+        for (int i = 0; i + 1 < n; ++i) e[i] *= sc;
+        e[n - 1] = R(0);
+    }
+    __syncwarp();
+    int unconverged = 0;
+    const int maxit = 30;
+    for (int l = 0; l < n; ++l) {
+        int iter = 0;
+        for (;;) {
+            int m = l;
+            for (; m < n - 1; ++m) {
+                const R em = e[m];
+                if (em * em <= (eps2 * fabs(d[m])) * fabs(d[m + 1]) + safmin) break;
+            }
+            if (m == l) break;
+            if (iter == maxit) { ++unconverged; break; }
+            ++iter;
+            const R el = e[l], dl = d[l];
+            R g = (d[l + 1] - dl) / (R(2) * el);
+            R r = sqrt(fma(g, g, R(1)));
+            g = d[m] - dl + el / (g + copysign(r, g));
+            R s = R(1), c = R(1), p = R(0);
+            bool early = false;
+            for (int i = m - 1; i >= l; --i) {
+                const R ei = e[i];
+                const R f = s * ei, b = c * ei;
+                const R rr = fma(f, f, g * g);
+                if (rr == R(0)) {
+                    __syncwarp();
+                    if (lane == 0) { d[i + 1] -= p; e[m] = R(0); }
+                    __syncwarp();
+                    early = true;
+                    break;
+                }
+                const R ri = rsqrt(rr);
+                r = rr * ri;
+                s = f * ri;
+                c = g * ri;
+                const R di1 = d[i + 1];
+                g = di1 - p;
+                r = fma(d[i] - g, s, R(2) * c * b);
+                p = s * r;
+                __syncwarp();
+                if (lane == 0) { e[i + 1] = rr * ri; d[i + 1] = g + p; }
+                g = fma(c, r, -b);
+                // rotate columns i, i+1 of the rows this lane owns
+                for (int row = lane; row < n; row += 32) {
+                    R* zr = Z + row * ldz;
+                    const R zi = zr[i], zi1 = zr[i + 1];
+                    zr[i + 1] = fma(s, zi, c * zi1);
+                    zr[i] = fma(c, zi, -s * zi1);
+                }
+                __syncwarp();
+            }
+            if (early) continue;
+            __syncwarp();
+            if (lane == 0) { d[l] -= p; e[l] = g; e[m] = R(0); }
+            __syncwarp();
+        }
+    }
+    // sort ascending (selection sort, as dsteqr)
+    for (int i = 0; i + 1 < n; ++i) {
+        int k = i;
+        R pmin = d[i];
+        for (int j = i + 1; j < n; ++j) if (d[j] < pmin) { k = j; pmin = d[j]; }
+        if (k != i) {
+            __syncwarp();
+            if (lane == 0) { d[k] = d[i]; d[i] = pmin; }
+            for (int row = lane; row < n; row += 32) {
+                R* zr = Z + row * ldz;
+                const R t = zr[i]; zr[i] = zr[k]; zr[k] = t;
+            }
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+    if (lane == 0) for (int i = 0; i < n; ++i) d[i] *= anorm;
+    __syncwarp();
+    return unconverged;
+}
+
+// ============================================================================ Ogita-Aishima refinement
+// One refinement step for the eigen-decomposition of the real symmetric
+// tridiagonal T = tridiag(e, d, e) from an approximate eigenvector matrix Z
+// (column-major tile, ld), following Ogita & Aishima, "Iterative refinement for
+// symmetric eigenvalue decomposition" (Japan J. Indust. Appl. Math. 35, 2018),
+// Algorithm 1:
+//   R = I - Z^T Z,  S = Z^T T Z,  lam_i = S_ii / (1 - R_ii),
+//   delta = 2 (||S - diag(lam)|| + ||T|| ||R||)  (Frobenius norms bound the 2-norms),
+//   E_ij = (S_ij + lam_j R_ij) / (lam_j - lam_i)  if |lam_i - lam_j| > delta, else R_ij / 2,
+//   Z' = Z + Z E.
+// Every product runs in FP64.  TZ, Rm, Sm are n x n scratch tiles (same ld);
+// Znew receives Z'.  red is 4 doubles of scratch per warp.  Returns
+// max_{i != j} |E_ij| (the size of the correction), identical on every thread.
+template <int TB>
+__device__ double oa_refine_step(int n, const double* dT, const double* eT, const double* Z, int ld,
+                                 double* TZ, double* Rm, double* Sm, double* Znew, double* lam,
+                                 double* red) {
+    const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = T >> 5;
+    // TZ = T Z
+    for (int idx = tid; idx < n * n; idx += T) {
+        const int j = idx / n, i = idx - j * n;
+        const double* z = Z + j * ld;
+        double v = dT[i] * z[i];
+        if (i > 0) v = fma(eT[i - 1], z[i - 1], v);
+        if (i + 1 < n) v = fma(eT[i], z[i + 1], v);
+        TZ[i + j * ld] = v;
+    }
+    __syncthreads();
+    // Rm = I - Z^T Z, Sm = Z^T (T Z): TB x TB register tiles
+    const int nb = (n + TB - 1) / TB;
+    for (int blk = tid; blk < nb * nb; blk += T) {
+        const int bj = blk / nb, bi = blk - bj * nb;
+        double r[TB][TB], sacc[TB][TB];
+#pragma unroll
+        for (int a = 0; a < TB; ++a)
+#pragma unroll
+            for (int c = 0; c < TB; ++c) { r[a][c] = 0.0; sacc[a][c] = 0.0; }
+        int ci[TB], cj[TB];
+#pragma unroll
+        for (int a = 0; a < TB; ++a) { ci[a] = min(bi * TB + a, n - 1); cj[a] = min(bj * TB + a, n - 1); }
+        for (int k = 0; k < n; ++k) {
+            double zi[TB], zj[TB], tj[TB];
+#pragma unroll
+            for (int a = 0; a < TB; ++a) { zi[a] = Z[k + ci[a] * ld]; zj[a] = Z[k + cj[a] * ld]; tj[a] = TZ[k + cj[a] * ld]; }
+#pragma unroll
+            for (int a = 0; a < TB; ++a)
+#pragma unroll
+                for (int c = 0; c < TB; ++c) { r[a][c] = fma(zi[a], zj[c], r[a][c]); sacc[a][c] = fma(zi[a], tj[c], sacc[a][c]); }
+        }
+#pragma unroll
+        for (int a = 0; a < TB; ++a)
+#pragma unroll
+            for (int c = 0; c < TB; ++c) {
+                const int i = bi * TB + a, j = bj * TB + c;
+                if (i < n && j < n) {
+                    Rm[i + j * ld] = (i == j ? 1.0 : 0.0) - r[a][c];
+                    Sm[i + j * ld] = sacc[a][c];
+                }
+            }
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += T) lam[i] = Sm[i + i * ld] / (1.0 - Rm[i + i * ld]);
+    // Frobenius norms of S - diag(lam), R and T
+    double s_off = 0.0, r_n = 0.0, t_n = 0.0;
+    for (int idx = tid; idx < n * n; idx += T) {
+        const int j = idx / n, i = idx - j * n;
+        const double sv = Sm[i + j * ld], rv = Rm[i + j * ld];
+        if (i != j) s_off = fma(sv, sv, s_off);
+        r_n = fma(rv, rv, r_n);
+    }
+    for (int i = tid; i < n; i += T) {
+        t_n = fma(dT[i], dT[i], t_n);
+        if (i + 1 < n) t_n = fma(2.0 * eT[i], eT[i], t_n);
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += T) {
+        const double dv = Sm[i + i * ld] - lam[i];
+        s_off = fma(dv, dv, s_off);
+    }
+    s_off = warp_sum(s_off); r_n = warp_sum(r_n); t_n = warp_sum(t_n);
+    if (lane == 0) { red[4 * warp] = s_off; red[4 * warp + 1] = r_n; red[4 * warp + 2] = t_n; }
+    __syncthreads();
+    double S2 = 0.0, R2 = 0.0, T2 = 0.0;
+    for (int w = 0; w < nw; ++w) { S2 += red[4 * w]; R2 += red[4 * w + 1]; T2 += red[4 * w + 2]; }
+    const double delta = 2.0 * (sqrt(S2) + sqrt(T2) * sqrt(R2));
+    // E (over Sm)
+    double emax = 0.0;
+    for (int idx = tid; idx < n * n; idx += T) {
+        const int j = idx / n, i = idx - j * n;
+        const double rij = Rm[i + j * ld];
+        double eij;
+        const double gap = lam[j] - lam[i];
+        if (i != j && fabs(gap) > delta) eij = (Sm[i + j * ld] + lam[j] * rij) / gap;
+        else eij = 0.5 * rij;
+        if (i != j) emax = fmax(emax, fabs(eij));
+        TZ[i + j * ld] = eij;                  // E kept in TZ (T Z is no longer needed)
+    }
+    __syncthreads();
+    // Znew = Z + Z E
+    for (int blk = tid; blk < nb * nb; blk += T) {
+        const int bj = blk / nb, bi = blk - bj * nb;
+        double acc[TB][TB];
+        int ri[TB], cj[TB];
+#pragma unroll
+        for (int a = 0; a < TB; ++a) { ri[a] = min(bi * TB + a, n - 1); cj[a] = min(bj * TB + a, n - 1); }
+#pragma unroll
+        for (int a = 0; a < TB; ++a)
+#pragma unroll
+            for (int c = 0; c < TB; ++c) acc[a][c] = Z[ri[a] + cj[c] * ld];
+        for (int k = 0; k < n; ++k) {
+            double zr[TB], ek[TB];
+#pragma unroll
+            for (int a = 0; a < TB; ++a) { zr[a] = Z[ri[a] + k * ld]; ek[a] = TZ[k + cj[a] * ld]; }
+#pragma unroll
+            for (int a = 0; a < TB; ++a)
+#pragma unroll
+                for (int c = 0; c < TB; ++c) acc[a][c] = fma(zr[a], ek[c], acc[a][c]);
+        }
+#pragma unroll
+        for (int a = 0; a < TB; ++a)
+#pragma unroll
+            for (int c = 0; c < TB; ++c) {
+                const int i = bi * TB + a, j = bj * TB + c;
+                if (i < n && j < n) Znew[i + j * ld] = acc[a][c];
+            }
+    }
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) emax = fmax(emax, shfl_xor(emax, m));
+    if (lane == 0) red[4 * warp + 3] = emax;
+    __syncthreads();
+    double em = 0.0;
+    for (int w = 0; w < nw; ++w) em = fmax(em, red[4 * w + 3]);
+    __syncthreads();
+    return em;
+}
+
+}  // namespace sbg

@@ -1,0 +1,420 @@
+// Schedule selection and autotuning for the stage kernels (see tuning.h).
+#include "tuning.h"
+#include "kernels.cuh"
+#include "sbg/geneig.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <random>
+#include <sstream>
+#include <tuple>
+#include <vector>
+
+#include <sys/stat.h>
+#include <unistd.h>
+
+namespace sbg {
+
+namespace {
+
+constexpr const char* kTableMagic = "SBGTUNE";
+constexpr int kTableVersion = 1;
+constexpr const char* kLibVersion = "sbg-geneig-0.1";
+
+std::mutex g_mu;
+std::map<std::tuple<int, int, int>, Schedule> g_in_process;   // (device, n, precision)
+
+bool fits(int n, int precision, const Schedule& s) {
+    const size_t lim = static_cast<size_t>(max_smem_optin());
+    if (reduce_smem_bytes(kReduceFull, n) > lim || back_smem_bytes(n) > lim) return false;
+    if (tridiag_smem_bytes(n, s.ql_warps, precision == SBG_PRECISION_MIXED) > lim) return false;
+    if (precision == SBG_PRECISION_MIXED && refine_smem_bytes(n, s.refine_threads) > lim) return false;
+    return true;
+}
+
+uint64_t fnv1a(const std::string& s) {
+    uint64_t h = 1469598103934665603ull;
+    for (unsigned char c : s) { h ^= c; h *= 1099511628211ull; }
+    return h;
+}
+
+std::string device_key(int device) {
+    cudaDeviceProp p{};
+    cudaGetDeviceProperties(&p, device);
+    std::ostringstream o;
+    o << p.name << "|sm" << p.major << p.minor << "|" << p.multiProcessorCount << "|" << kLibVersion;
+    return o.str();
+}
+
+struct TableEntry { int n, precision; Schedule s; double us; };
+
+// Parses a table file; returns false (and leaves out empty) if it is missing,
+// truncated, foreign or fails its checksum.
+bool load_table(const std::string& path, const std::string& key, std::vector<TableEntry>& out) {
+    out.clear();
+    std::ifstream f(path);
+    if (!f) return false;
+    std::string line, body;
+    std::vector<std::string> lines;
+    while (std::getline(f, line)) lines.push_back(line);
+    if (lines.size() < 3) return false;
+    for (size_t i = 0; i + 1 < lines.size(); ++i) body += lines[i] + "\n";
+    {
+        std::istringstream cs(lines.back());
+        std::string tag, hex;
+        cs >> tag >> hex;
+        if (tag != "checksum") return false;
+        char buf[32];
+        std::snprintf(buf, sizeof(buf), "%016llx", static_cast<unsigned long long>(fnv1a(body)));
+        if (hex != buf) return false;
+    }
+    {
+        std::istringstream hs(lines[0]);
+        std::string magic;
+        int ver = 0;
+        hs >> magic >> ver;
+        if (magic != kTableMagic || ver != kTableVersion) return false;
+    }
+    if (lines[1] != "device " + key) return false;
+    for (size_t i = 2; i + 1 < lines.size(); ++i) {
+        std::istringstream es(lines[i]);
+        std::string tag;
+        TableEntry e{};
+        es >> tag >> e.n >> e.precision >> e.s.reduce_threads >> e.s.back_threads >> e.s.ql_warps >>
+            e.s.refine_threads >> e.us;
+        if (tag != "entry" || !es) { out.clear(); return false; }
+        out.push_back(e);
+    }
+    return true;
+}
+
+bool mkdirs(const std::string& dir) {
+    std::string cur;
+    std::istringstream ss(dir);
+    std::string part;
+    if (!dir.empty() && dir[0] == '/') cur = "/";
+    while (std::getline(ss, part, '/')) {
+        if (part.empty()) continue;
+        cur += part + "/";
+        if (mkdir(cur.c_str(), 0755) != 0 && errno != EEXIST) return false;
+    }
+    return true;
+}
+
+void save_table(const std::string& path, const std::string& key, const std::vector<TableEntry>& entries) {
+    const std::string dir = path.substr(0, path.find_last_of('/'));
+    if (!mkdirs(dir)) return;
+    std::ostringstream body;
+    body << kTableMagic << " " << kTableVersion << "\n";
+    body << "device " << key << "\n";
+    for (const auto& e : entries)
+        body << "entry " << e.n << " " << e.precision << " " << e.s.reduce_threads << " " << e.s.back_threads << " "
+             << e.s.ql_warps << " " << e.s.refine_threads << " " << e.us << "\n";
+    const std::string b = body.str();
+    char buf[32];
+    std::snprintf(buf, sizeof(buf), "%016llx", static_cast<unsigned long long>(fnv1a(b)));
+    const std::string tmp = path + ".tmp." + std::to_string(getpid());
+    {
+        std::ofstream f(tmp, std::ios::trunc);
+        if (!f) return;
+        f << b << "checksum " << buf << "\n";
+        if (!f) { std::remove(tmp.c_str()); return; }
+    }
+    if (std::rename(tmp.c_str(), path.c_str()) != 0) std::remove(tmp.c_str());
+}
+
+// ------------------------------------------------------------------ measurement
+
+struct DevBuf {
+    void* p = nullptr;
+    explicit DevBuf(size_t bytes) { if (cudaMalloc(&p, bytes) != cudaSuccess) p = nullptr; }
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+
+// Synthetic tuning pairs: A = G + G^H, B = (n + 1) I + (H + H^H) / 4 (diagonally
+// dominant, so Hermitian positive definite), G, H complex normal.
+void make_pairs(int n, int count, std::vector<std::complex<double>>& A, std::vector<std::complex<double>>& B) {
+    std::mt19937_64 rng(0x5B6A7ull + n);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    const size_t nn = static_cast<size_t>(n) * n;
+    A.assign(nn * count, 0.0);
+    B.assign(nn * count, 0.0);
+    std::vector<std::complex<double>> G(nn), H(nn);
+    for (int b = 0; b < count; ++b) {
+        for (size_t i = 0; i < nn; ++i) { G[i] = {nd(rng), nd(rng)}; H[i] = {nd(rng), nd(rng)}; }
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                A[nn * b + i + j * n] = G[i + j * n] + std::conj(G[j + i * n]);
+                B[nn * b + i + j * n] = 0.25 * (H[i + j * n] + std::conj(H[j + i * n]));
+                if (i == j) B[nn * b + i + j * n] += double(n + 1);
+            }
+    }
+}
+
+template <class F>
+double median_ms(F&& launch, int reps, cudaStream_t st) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::vector<float> t;
+    launch();   // warm-up
+    for (int r = 0; r < reps; ++r) {
+        cudaEventRecord(e0, st);
+        launch();
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        t.push_back(ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::sort(t.begin(), t.end());
+    return t[t.size() / 2];
+}
+
+struct Bench {
+    int n, precision, count;
+    size_t nn;
+    DevBuf A, B, W, X, Z, info, wsbuf;
+    Workspace ws;
+    cudaStream_t st = nullptr;
+    Bench(int n_, int prec, int count_)
+        : n(n_), precision(prec), count(count_), nn(static_cast<size_t>(n_) * n_),
+          A(16 * nn * count_), B(16 * nn * count_), W(8 * static_cast<size_t>(n_) * count_), X(16 * nn * count_),
+          Z(16 * nn * count_), info(4 * static_cast<size_t>(count_)),
+          wsbuf(workspace_bytes_per_pair(n_) * count_ + 5 * 256) {
+        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        ws = carve_workspace(wsbuf.p, n, count);
+    }
+    ~Bench() { if (st) cudaStreamDestroy(st); }
+    bool ok() const { return A.p && B.p && W.p && X.p && Z.p && info.p && wsbuf.p; }
+    double2* a() { return static_cast<double2*>(A.p); }
+    double2* b() { return static_cast<double2*>(B.p); }
+    double* w() { return static_cast<double*>(W.p); }
+    double2* x() { return static_cast<double2*>(X.p); }
+    int* inf() { return static_cast<int*>(info.p); }
+    void eig(const Schedule& s) {
+        if (precision == SBG_PRECISION_MIXED)
+            launch_tridiag_mixed(n, count, ws, w(), x(), inf(), 3, s.ql_warps, s.refine_threads, st);
+        else
+            launch_tridiag_ql(n, count, ws, w(), x(), inf(), s.ql_warps, st);
+    }
+    void full(const Schedule& s) {
+        launch_reduce(kReduceFull, a(), b(), n, count, ws, nullptr, inf(), s.reduce_threads, st);
+        eig(s);
+        launch_back(kBackFull, n, count, ws, x(), inf(), s.back_threads, st);
+    }
+};
+
+// Host residual ||A x - lam B x||_inf / (||A||_F ||x||_2) for one column.
+double host_residual(int n, const std::complex<double>* A, const std::complex<double>* B,
+                     const std::complex<double>* x, double lam) {
+    double an = 0, xn = 0, r = 0;
+    for (int i = 0; i < n * n; ++i) an += std::norm(A[i]);
+    for (int i = 0; i < n; ++i) xn += std::norm(x[i]);
+    for (int i = 0; i < n; ++i) {
+        std::complex<double> ax = 0, bx = 0;
+        for (int j = 0; j < n; ++j) {
+            ax += A[i + j * n] * x[j];
+            const std::complex<double> bij = (i >= j) ? B[i + j * n] : std::conj(B[j + i * n]);
+            bx += bij * x[j];
+        }
+        r = std::max(r, std::abs(ax - lam * bx));
+    }
+    return r / (std::sqrt(an) * std::sqrt(xn));
+}
+
+bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double& best_us) {
+    const int count = std::max(512, std::min(4096, (1 << 22) / (n * n)));
+    Bench bench(n, precision, count);
+    if (!bench.ok()) return false;
+    std::vector<std::complex<double>> hA, hB;
+    make_pairs(n, count, hA, hB);
+    cudaMemcpy(bench.A.p, hA.data(), 16 * bench.nn * count, cudaMemcpyHostToDevice);
+    cudaMemcpy(bench.B.p, hB.data(), 16 * bench.nn * count, cudaMemcpyHostToDevice);
+    const Schedule base = default_schedule(n, precision);
+    const std::vector<int> thread_opts = req.force_threads ? std::vector<int>{req.force_threads} : std::vector<int>{128, 256};
+    const std::vector<int> warp_opts = req.force_ql_warps ? std::vector<int>{req.force_ql_warps} : std::vector<int>{1, 2, 4, 8};
+    Schedule win = base;
+    double t_total = 0.0;
+    // k_reduce
+    {
+        double bt = 1e30;
+        for (int t : thread_opts) {
+            double ms = median_ms([&] { launch_reduce(kReduceFull, bench.a(), bench.b(), n, count, bench.ws, nullptr,
+                                                      bench.inf(), t, bench.st); }, 3, bench.st);
+            if (ms < bt) { bt = ms; win.reduce_threads = t; }
+        }
+        t_total += bt;
+    }
+    // eigensolve of the tridiagonal (k_reduce's output stays valid in the workspace)
+    {
+        double bt = 1e30;
+        std::vector<int> refine_opts = precision == SBG_PRECISION_MIXED ? std::vector<int>{128, 256} : std::vector<int>{256};
+        for (int w : warp_opts)
+            for (int rt : refine_opts) {
+                Schedule s = win;
+                s.ql_warps = w;
+                s.refine_threads = rt;
+                if (!fits(n, precision, s)) continue;
+                double ms = median_ms([&] { bench.eig(s); }, 3, bench.st);
+                if (ms < bt) { bt = ms; win.ql_warps = w; win.refine_threads = rt; }
+            }
+        t_total += bt;
+    }
+    // k_back (restores Z before every run: the kernel overwrites it with X)
+    {
+        bench.eig(win);
+        cudaMemcpyAsync(bench.Z.p, bench.X.p, 16 * bench.nn * count, cudaMemcpyDeviceToDevice, bench.st);
+        double bt = 1e30;
+        for (int t : thread_opts) {
+            double ms = median_ms([&] {
+                cudaMemcpyAsync(bench.X.p, bench.Z.p, 16 * bench.nn * count, cudaMemcpyDeviceToDevice, bench.st);
+                launch_back(kBackFull, n, count, bench.ws, bench.x(), bench.inf(), t, bench.st);
+            }, 3, bench.st);
+            if (ms < bt) { bt = ms; win.back_threads = t; }
+        }
+        t_total += bt;
+    }
+    // validate the winner against the built-in schedule and against the residual
+    const int spot = std::min(count, 8);
+    std::vector<double> W0(static_cast<size_t>(n) * spot), W1(W0.size());
+    std::vector<std::complex<double>> X1(bench.nn * spot);
+    std::vector<int> I1(spot);
+    bench.full(base);
+    cudaMemcpyAsync(W0.data(), bench.W.p, 8 * W0.size(), cudaMemcpyDeviceToHost, bench.st);
+    bench.full(win);
+    cudaMemcpyAsync(W1.data(), bench.W.p, 8 * W1.size(), cudaMemcpyDeviceToHost, bench.st);
+    cudaMemcpyAsync(X1.data(), bench.X.p, 16 * X1.size(), cudaMemcpyDeviceToHost, bench.st);
+    cudaMemcpyAsync(I1.data(), bench.info.p, 4 * spot, cudaMemcpyDeviceToHost, bench.st);
+    if (cudaStreamSynchronize(bench.st) != cudaSuccess) return false;
+    bool valid = true;
+    for (int p = 0; p < spot && valid; ++p) {
+        if (I1[p] != 0) valid = false;
+        for (int i = 0; i < n && valid; ++i) {
+            const double w0 = W0[static_cast<size_t>(n) * p + i], w1 = W1[static_cast<size_t>(n) * p + i];
+            if (!(std::fabs(w1 - w0) <= 1e-11 * std::max(1.0, std::fabs(w0)))) valid = false;
+        }
+        for (int i = 0; i < n && valid; i += std::max(1, n / 4)) {
+            const double r = host_residual(n, hA.data() + bench.nn * p, hB.data() + bench.nn * p,
+                                           X1.data() + bench.nn * p + static_cast<size_t>(i) * n,
+                                           W1[static_cast<size_t>(n) * p + i]);
+            if (!(r <= 1e-12)) valid = false;
+        }
+    }
+    if (!valid) {
+        std::fprintf(stderr, "[sbg autotune] n=%d: winner failed validation, keeping the built-in schedule\n", n);
+        win = base;
+    }
+    best = win;
+    best_us = 1e3 * t_total / count;
+    std::fprintf(stderr, "[sbg autotune] n=%d precision=%d: reduce=%d back=%d ql_warps=%d refine=%d (%.3f us/pair)\n",
+                 n, precision, win.reduce_threads, win.back_threads, win.ql_warps, win.refine_threads, best_us);
+    return true;
+}
+
+}  // namespace
+
+Schedule default_schedule(int n, int precision) {
+    Schedule s;
+    s.reduce_threads = n > 24 ? 256 : 128;
+    s.back_threads = n > 24 ? 256 : 128;
+    s.refine_threads = n > 24 ? 256 : 128;
+    s.ql_warps = n <= 32 ? 8 : (n <= 64 ? 4 : 2);
+    while (s.ql_warps > 1 && !fits(n, precision, s)) s.ql_warps /= 2;
+    return s;
+}
+
+std::string tuning_cache_dir() {
+    if (const char* d = std::getenv("SUNNY_GENEIG_CACHE_DIR")) if (*d) return d;
+    if (const char* x = std::getenv("XDG_CACHE_HOME")) if (*x) return std::string(x) + "/sunny_geneig_b200";
+    if (const char* h = std::getenv("HOME")) if (*h) return std::string(h) + "/.cache/sunny_geneig_b200";
+    return "/tmp/sunny_geneig_b200";
+}
+
+std::string tuning_table_path(int device) {
+    cudaDeviceProp p{};
+    cudaGetDeviceProperties(&p, device);
+    std::string name = p.name;
+    for (char& c : name) if (!std::isalnum(static_cast<unsigned char>(c))) c = '_';
+    return tuning_cache_dir() + "/schedules_" + name + "_sm" + std::to_string(p.major * 10 + p.minor) + ".tbl";
+}
+
+void forget_in_process() {
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_in_process.clear();
+}
+
+TuneResult select_schedule(const TuneRequest& req) {
+    TuneResult r;
+    r.sched = default_schedule(req.n, req.precision);
+    if (req.force_threads) {
+        if (req.force_threads != 128 && req.force_threads != 256)
+            throw std::runtime_error("force_block_dim_x must be 128 or 256");
+        r.sched.reduce_threads = r.sched.back_threads = r.sched.refine_threads = req.force_threads;
+    }
+    if (req.force_ql_warps) {
+        if (req.force_ql_warps < 1 || req.force_ql_warps > 16) throw std::runtime_error("batches_per_block must be 1..16");
+        r.sched.ql_warps = req.force_ql_warps;
+        if (!fits(req.n, req.precision, r.sched))
+            throw std::runtime_error("batches_per_block=" + std::to_string(req.force_ql_warps) +
+                                     " exceeds the shared-memory budget for n=" + std::to_string(req.n));
+    }
+    if (!req.autotune) return r;
+    r.autotuned = true;
+    const auto key = std::make_tuple(req.device, req.n, req.precision);
+    const bool use_mem = req.cache_mode != SBG_CACHE_NONE;
+    const bool use_disk = req.cache_mode == SBG_CACHE_AUTO;
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (use_mem) {
+        auto it = g_in_process.find(key);
+        if (it != g_in_process.end()) { r.sched = it->second; r.layer = "in-process"; return r; }
+    }
+    const std::string dkey = device_key(req.device);
+    const std::string path = tuning_table_path(req.device);
+    std::vector<TableEntry> table;
+    bool table_ok = false;
+    if (use_disk) {
+        table_ok = load_table(path, dkey, table);
+        if (table_ok) {
+            for (const auto& e : table)
+                if (e.n == req.n && e.precision == req.precision && fits(req.n, req.precision, e.s)) {
+                    r.sched = e.s;
+                    r.layer = "disk";
+                    if (use_mem) g_in_process[key] = e.s;
+                    return r;
+                }
+        } else {
+            struct stat sb;
+            if (stat(path.c_str(), &sb) == 0)
+                std::fprintf(stderr, "[sbg autotune] ignoring unreadable or corrupt table %s\n", path.c_str());
+        }
+    }
+    Schedule best;
+    double us = 0;
+    if (!sweep(req.n, req.precision, req, best, us)) throw std::runtime_error("autotune sweep could not allocate");
+    r.sched = best;
+    r.sweep_ran = true;
+    r.layer = "measured";
+    if (use_mem) g_in_process[key] = best;
+    if (use_disk) {
+        if (!table_ok) table.clear();
+        table.erase(std::remove_if(table.begin(), table.end(),
+                                   [&](const TableEntry& e) { return e.n == req.n && e.precision == req.precision; }),
+                    table.end());
+        table.push_back({req.n, req.precision, best, us});
+        save_table(path, dkey, table);
+    }
+    return r;
+}
+
+}  // namespace sbg

@@ -1,0 +1,264 @@
+"""B200 batched complex Hermitian-definite generalized eigensolver, A x = lambda B x.
+
+Python host side over the C ABI (include/sbg/geneig.h).  Device buffers are
+torch CUDA tensors, laid out as the reference's launchers expect
+(src/geneig_fixed.cu:474-492, src/nvrtc/nvrtc_solver.hpp:112-120):
+pairs contiguous, each n x n matrix column-major with leading dimension n.  The
+Python functions take and return flat per-pair tensors of shape (batch, n*n)
+(complex128) in that column-major order; ``to_colmajor`` / ``from_colmajor``
+convert from / to (batch, n, n) row-indexed tensors.
+
+    solver = sbg.Solver(54, precision="fp64")          # NvrtcGeneigSolver(54, 0)
+    solver.launch(dA, dB, dW, dX, dinfo)               # ::launch(...)
+    W, X, info = sbg.solve(A, B)                        # host or device inputs
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import SolverOptions, load
+
+__all__ = [
+    "Solver", "SolverError", "solve", "to_colmajor", "from_colmajor", "max_n",
+    "geneig_full_n54_batched", "chol_n54", "reduce_n54", "reduce_eig_n54", "full_n54", "finish_n54",
+    "PRECISIONS", "fixed_n54_introspection", "tuning_table_path", "tuning_forget_in_process",
+]
+
+PRECISIONS = {"fp64": 0, "mixed": 1}
+_TUNING = {"suggested": 0, "autotune": 1}
+_CACHE = {"auto": 0, "no_disk": 1, "none": 2}
+
+
+class SolverError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        lib = load()
+        msg = lib.sbg_last_error().decode() or lib.sbg_status_string(status).decode()
+        super().__init__(f"{where}: {lib.sbg_status_string(status).decode()} ({msg})")
+        self.status = status
+
+
+def _check(status: int, where: str) -> None:
+    if status != 0:
+        raise SolverError(status, where)
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def to_colmajor(M: torch.Tensor) -> torch.Tensor:
+    """(batch, n, n) with [b, i, j] = M(i, j)  ->  (batch, n*n) column-major."""
+    b, n, _ = M.shape
+    return M.transpose(-1, -2).contiguous().reshape(b, n * n)
+
+
+def from_colmajor(M: torch.Tensor, n: int) -> torch.Tensor:
+    return M.reshape(-1, n, n).transpose(-1, -2)
+
+
+def max_n(precision: str = "fp64") -> int:
+    return int(load().sbg_max_n(PRECISIONS[precision]))
+
+
+def _check_pair_buffers(n, A, B, W, X, info):
+    for name, t, dt in (("A", A, torch.complex128), ("B", B, torch.complex128), ("W", W, torch.float64),
+                        ("X", X, torch.complex128), ("info", info, torch.int32)):
+        if not t.is_cuda:
+            raise ValueError(f"{name} must be a CUDA tensor")
+        if t.dtype != dt:
+            raise ValueError(f"{name} must be {dt}, got {t.dtype}")
+        if not t.is_contiguous():
+            raise ValueError(f"{name} must be contiguous")
+    batch = info.numel()
+    for name, t, per in (("A", A, n * n), ("B", B, n * n), ("W", W, n), ("X", X, n * n)):
+        if t.numel() != batch * per:
+            raise ValueError(f"{name} has {t.numel()} elements, expected {batch * per} for batch {batch}")
+    return batch
+
+
+class Solver:
+    """Runtime-n solver handle (mirrors NvrtcGeneigSolver, src/nvrtc/nvrtc_solver.hpp:81-217).
+
+    batches_per_block: pairs per CTA of the QL stage (0 = auto).
+    block_dim: threads per CTA of the CTA-per-pair stages, 128 or 256 (0 = auto).
+    tuning: "suggested" (built-in schedule) or "autotune" (measured, persisted).
+    cache: "auto" | "no_disk" | "none" (the autotune table's layers).
+    precision: "fp64" (the plain drop-in) or "mixed" (FP32 tridiagonal eigensolve +
+    FP64 Ogita-Aishima refinement).
+    """
+
+    def __init__(self, n: int, device: int = 0, *, precision: str = "fp64", batches_per_block: int = 0,
+                 block_dim: int = 0, tuning: str = "suggested", cache: str = "auto", refine_steps: int = 0,
+                 workspace_pairs: int = 0):
+        lib = load()
+        opts = SolverOptions()
+        lib.sbg_solver_options_init(ctypes.byref(opts))
+        opts.batches_per_block = batches_per_block
+        opts.force_block_dim_x = block_dim
+        opts.tuning_mode = _TUNING[tuning]
+        opts.cache_mode = _CACHE[cache]
+        opts.precision = PRECISIONS[precision]
+        opts.refine_steps = refine_steps
+        opts.workspace_pairs = workspace_pairs
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(device):
+            _check(lib.sbg_solver_create(n, device, ctypes.byref(opts), ctypes.byref(handle)), "sbg_solver_create")
+        self._h = handle
+        self._lib = lib
+        self.n = n
+        self.device = device
+        self.precision = precision
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.sbg_solver_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def launch(self, A, B, W, X, info, stream=None) -> None:
+        """Full solve of the pairs in A, B (device tensors) into W, X, info."""
+        batch = _check_pair_buffers(self.n, A, B, W, X, info)
+        _check(self._lib.sbg_solver_launch(self._h, _ptr(A), _ptr(B), _ptr(W), _ptr(X), _ptr(info), batch,
+                                           _stream(stream)), "sbg_solver_launch")
+
+    def launch_chunked(self, A, B, W, X, info, chunk_size: int, streams) -> None:
+        """Round-robin chunks over several streams (NvrtcGeneigSolver::launch_chunked)."""
+        batch = _check_pair_buffers(self.n, A, B, W, X, info)
+        arr = (ctypes.c_void_p * len(streams))(*[s.cuda_stream for s in streams])
+        _check(self._lib.sbg_solver_launch_chunked(self._h, _ptr(A), _ptr(B), _ptr(W), _ptr(X), _ptr(info), batch,
+                                                   chunk_size, len(streams), arr), "sbg_solver_launch_chunked")
+
+    def solve_host(self, A, B, W, X, info, chunk_size: int = 16384, num_streams: int = 2) -> None:
+        """End-to-end solve of host (ideally pinned) CPU tensors; synchronous."""
+        for name, t, dt in (("A", A, torch.complex128), ("B", B, torch.complex128), ("W", W, torch.float64),
+                            ("X", X, torch.complex128), ("info", info, torch.int32)):
+            if t.is_cuda or t.dtype != dt or not t.is_contiguous():
+                raise ValueError(f"{name} must be a contiguous host {dt} tensor")
+        batch = info.numel()
+        _check(self._lib.sbg_solver_solve_host(self._h, _ptr(A), _ptr(B), _ptr(W), _ptr(X), _ptr(info), batch,
+                                               chunk_size, num_streams), "sbg_solver_solve_host")
+
+    def enable_stage_timing(self, enable: bool = True) -> None:
+        _check(self._lib.sbg_solver_enable_stage_timing(self._h, int(enable)), "sbg_solver_enable_stage_timing")
+
+    def read_stage_times(self):
+        """{stage: (ms, kernel launches)} for stages reduce, eig, back since the last read."""
+        ms = (ctypes.c_double * 3)()
+        nl = (ctypes.c_int * 3)()
+        _check(self._lib.sbg_solver_read_stage_times(self._h, ms, nl), "sbg_solver_read_stage_times")
+        return {k: (ms[i], nl[i]) for i, k in enumerate(("reduce", "eig", "back"))}
+
+    def reserve(self, pairs: int, stream_slots: int = 1) -> None:
+        _check(self._lib.sbg_solver_reserve(self._h, pairs, stream_slots), "sbg_solver_reserve")
+
+    @property
+    def batches_per_block(self) -> int:
+        return int(self._lib.sbg_solver_batches_per_block(self._h))
+
+    @property
+    def block_dim_x(self) -> int:
+        return int(self._lib.sbg_solver_block_dim_x(self._h))
+
+    @property
+    def shared_mem_bytes(self) -> int:
+        return int(self._lib.sbg_solver_shared_mem_bytes(self._h))
+
+    @property
+    def was_autotuned(self) -> bool:
+        return bool(self._lib.sbg_solver_was_autotuned(self._h))
+
+    @property
+    def autotune_sweep_ran(self) -> bool:
+        return bool(self._lib.sbg_solver_autotune_sweep_ran(self._h))
+
+    @property
+    def cache_layer_used(self) -> str:
+        return self._lib.sbg_solver_cache_layer_used(self._h).decode()
+
+
+def solve(A, B, *, precision: str = "fp64", device: int = 0, solver: Solver | None = None, stream=None):
+    """Solves every pair of A, B ((batch, n*n) column-major complex128, host or device).
+
+    Host inputs are copied to the device and the results copied back (the
+    end-to-end path); device inputs stay on the device.  Returns (W, X, info).
+    """
+    host = not (isinstance(A, torch.Tensor) and A.is_cuda)
+    A = torch.as_tensor(A)
+    B = torch.as_tensor(B)
+    batch, nn = A.shape
+    n = int(round(nn ** 0.5))
+    if n * n != nn or B.shape != A.shape:
+        raise ValueError("A and B must both be (batch, n*n)")
+    dev = torch.device("cuda", device)
+    if solver is None:
+        solver = Solver(n, device, precision=precision)
+    dA = A.to(dev, non_blocking=True)
+    dB = B.to(dev, non_blocking=True)
+    dW = torch.empty((batch, n), dtype=torch.float64, device=dev)
+    dX = torch.empty((batch, nn), dtype=torch.complex128, device=dev)
+    dinfo = torch.empty(batch, dtype=torch.int32, device=dev)
+    solver.launch(dA, dB, dW, dX, dinfo, stream=stream)
+    if host:
+        return dW.cpu(), dX.cpu(), dinfo.cpu()
+    return dW, dX, dinfo
+
+
+# ------------------------------------------------------------------ fixed n = 54 drop-in
+
+def geneig_full_n54_batched(A, B, W, X, info, stream=None) -> None:
+    """geneig_full_n54_batched_launch (src/geneig_fixed.cu:474-492)."""
+    batch = _check_pair_buffers(54, A, B, W, X, info)
+    load().geneig_full_n54_batched_launch(_ptr(A), _ptr(B), _ptr(W), _ptr(X), _ptr(info), batch, _stream(stream))
+
+
+def chol_n54(S, L, info, stream=None) -> None:
+    load().chol_n54_launch(_ptr(S), _ptr(L), _ptr(info), _stream(stream))
+
+
+def reduce_n54(H, S, M, info, stream=None) -> None:
+    load().geneig_reduce_n54_launch(_ptr(H), _ptr(S), _ptr(M), _ptr(info), _stream(stream))
+
+
+def reduce_eig_n54(H, S, W, V, info, stream=None) -> None:
+    load().geneig_reduce_eig_n54_launch(_ptr(H), _ptr(S), _ptr(W), _ptr(V), _ptr(info), _stream(stream))
+
+
+def full_n54(H, S, W, U, info, stream=None) -> None:
+    load().geneig_full_n54_launch(_ptr(H), _ptr(S), _ptr(W), _ptr(U), _ptr(info), _stream(stream))
+
+
+def finish_n54(L, M, W, U, info, batch: int, stream=None) -> None:
+    load().geneig_finish_n54_launch(_ptr(L), _ptr(M), _ptr(W), _ptr(U), _ptr(info), batch, _stream(stream))
+
+
+def fixed_n54_introspection() -> dict:
+    lib = load()
+    names = [k for k in _lib.SIGNATURES if k.endswith(("_block_dim_x", "_shared_mem_bytes", "_smem_bytes", "_workspace"))
+             and "n54" in k]
+    return {k: int(getattr(lib, k)()) for k in names}
+
+
+def tuning_table_path(device: int = 0) -> str:
+    buf = ctypes.create_string_buffer(4096)
+    _check(load().sbg_tuning_table_path(device, buf, len(buf)), "sbg_tuning_table_path")
+    return buf.value.decode()
+
+
+def tuning_forget_in_process() -> None:
+    _check(load().sbg_tuning_forget_in_process(), "sbg_tuning_forget_in_process")
