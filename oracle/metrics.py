@@ -9,6 +9,7 @@ eigenvalues (batch, n).  Metrics follow the reference's tests:
                    its neighbours is >= degen_gap            tests/test_full_batched_n54.cpp:100-113
 and add the gates the B200 build is held to:
   * eig_rel      = max_i |W_g - W_r| / |W_r|                (pure relative error)
+  * eig_rel_norm = max_i |W_g - W_r| / max_j |W_r|          (norm-wise relative error)
   * residual     = ||A X - B X diag(W)||_F / (||A||_F ||X||_F)
   * orth         = max |X^H B X - I|
   * cluster_sin  = largest sine of the B-principal angle between candidate and
@@ -44,6 +45,15 @@ def eig_rel(Wg, Wr) -> np.ndarray:
     den = np.abs(Wr)
     den = np.where(den == 0.0, 1.0, den)
     return np.max(np.abs(Wg - Wr) / den, axis=-1)
+
+
+def eig_rel_norm(Wg, Wr) -> np.ndarray:
+    """max_i |W_g - W_r| / max_j |W_r| (norm-wise relative error per pair)."""
+    Wg = np.asarray(Wg, np.float64)
+    Wr = np.asarray(Wr, np.float64)
+    den = np.abs(Wr).max(axis=-1)
+    den = np.where(den == 0.0, 1.0, den)
+    return np.abs(Wg - Wr).max(axis=-1) / den
 
 
 def nondegenerate_mask(Wr, degen_gap: float = 1e-6) -> np.ndarray:
@@ -119,6 +129,7 @@ def summarize(A, B, Wg, Xg, Wr, Xr, n: int, degen_gap: float = 1e-6) -> dict:
     return dict(
         eig_rel_ref=float(eig_rel_ref(Wg, Wr).max(initial=0.0)),
         eig_rel=float(eig_rel(Wg, Wr).max(initial=0.0)),
+        eig_rel_norm=float(eig_rel_norm(Wg, Wr).max(initial=0.0)),
         phase_err=float(phase_err(B, Xg, Xr, Wr, n, degen_gap).max(initial=0.0)),
         residual=float(residual(A, B, Xg, Wg, n).max(initial=0.0)),
         orth=float(orth(B, Xg, n).max(initial=0.0)),

@@ -145,11 +145,13 @@ struct sbg_solver {
         stage_end(stream, ev, 0, 1);
         stage_begin(stream, &ev);
         if (precision == SBG_PRECISION_MIXED)
-            check_cuda(sbg::launch_tridiag_mixed(n, cnt, ws, W, X, info, refine_steps, sched.ql_warps,
-                                                 sched.refine_threads, stream), "mixed eigensolve kernels");
+            check_cuda(sbg::launch_tridiag_mixed(n, cnt, ws, W, X, info, refine_steps, sched.chain_threads,
+                                                 sched.ql_warps, sched.refine_threads, stream),
+                       "mixed eigensolve kernels");
         else
-            check_cuda(sbg::launch_tridiag_ql(n, cnt, ws, W, X, info, sched.ql_warps, stream), "QL kernel");
-        stage_end(stream, ev, 1, precision == SBG_PRECISION_MIXED ? 2 : 1);
+            check_cuda(sbg::launch_ql_logged(n, cnt, ws, W, X, info, false, sched.chain_threads, sched.ql_warps,
+                                             stream), "QL kernels");
+        stage_end(stream, ev, 1, precision == SBG_PRECISION_MIXED ? 3 : 2);
         stage_begin(stream, &ev);
         check_cuda(sbg::launch_back(sbg::kBackFull, n, cnt, ws, X, info, sched.back_threads, stream),
                    "back-transform kernel");
@@ -229,7 +231,8 @@ int supported_max_n(int precision) {
     int best = 0;
     for (int n = 1; n <= 256; ++n) {
         size_t need = std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, n), sbg::back_smem_bytes(n));
-        need = std::max(need, sbg::tridiag_smem_bytes(n, 1, precision == SBG_PRECISION_MIXED));
+        need = std::max(need, sbg::ql_apply_smem_bytes(n, 1, precision == SBG_PRECISION_MIXED));
+        need = std::max(need, sbg::ql_chain_smem_bytes(n, 32, precision == SBG_PRECISION_MIXED));
         if (precision == SBG_PRECISION_MIXED) need = std::max(need, sbg::refine_smem_bytes(n, 128));
         if (need <= lim) best = n;
     }
@@ -489,7 +492,8 @@ void geneig_reduce_eig_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComp
         sbg::Workspace ws = s->workspace(0, 1, stream);
         check_cuda(sbg::launch_reduce(sbg::kReduceFull, c2(d_H), c2(d_S), 54, 1, ws, nullptr, d_info,
                                       s->sched.reduce_threads, stream), "reduce kernel");
-        check_cuda(sbg::launch_tridiag_ql(54, 1, ws, d_W, c2(d_V), d_info, s->sched.ql_warps, stream), "QL kernel");
+        check_cuda(sbg::launch_ql_logged(54, 1, ws, d_W, c2(d_V), d_info, false, s->sched.chain_threads,
+                                         s->sched.ql_warps, stream), "QL kernels");
         check_cuda(sbg::launch_back(sbg::kBackQOnly, 54, 1, ws, c2(d_V), d_info, s->sched.back_threads, stream),
                    "back kernel");
     }));
@@ -498,7 +502,7 @@ unsigned int geneig_reduce_eig_n54_block_dim_x(void) { return sbg::default_sched
 unsigned int geneig_reduce_eig_n54_shared_mem_bytes(void) { return geneig_full_n54_batched_shared_mem_bytes(); }
 unsigned int geneig_reduce_eig_n54_chol_smem_bytes(void) { return static_cast<unsigned>(sbg::reduce_smem_bytes(sbg::kReduceFull, 54)); }
 unsigned int geneig_reduce_eig_n54_heev_smem_bytes(void) {
-    return static_cast<unsigned>(sbg::tridiag_smem_bytes(54, sbg::default_schedule(54, SBG_PRECISION_FP64).ql_warps, false));
+    return static_cast<unsigned>(sbg::ql_apply_smem_bytes(54, sbg::default_schedule(54, SBG_PRECISION_FP64).ql_warps, false));
 }
 unsigned int geneig_reduce_eig_n54_heev_workspace(void) {
     return static_cast<unsigned>(sbg::workspace_bytes_per_pair(54) / 16);
@@ -523,8 +527,8 @@ void geneig_finish_n54_launch(const cuDoubleComplex* d_L, const cuDoubleComplex*
             const int cnt = std::min(ws.capacity, batch_size - off);
             check_cuda(sbg::launch_reduce(sbg::kReduceFromLM, c2(d_M) + nn * off, c2(d_L) + nn * off, 54, cnt, ws,
                                           nullptr, d_info + off, s->sched.reduce_threads, stream), "reduce kernel");
-            check_cuda(sbg::launch_tridiag_ql(54, cnt, ws, d_W + 54 * off, c2(d_U) + nn * off, d_info + off,
-                                              s->sched.ql_warps, stream), "QL kernel");
+            check_cuda(sbg::launch_ql_logged(54, cnt, ws, d_W + 54 * off, c2(d_U) + nn * off, d_info + off, false,
+                                             s->sched.chain_threads, s->sched.ql_warps, stream), "QL kernels");
             check_cuda(sbg::launch_back(sbg::kBackFull, 54, cnt, ws, c2(d_U) + nn * off, d_info + off,
                                         s->sched.back_threads, stream), "back kernel");
         }

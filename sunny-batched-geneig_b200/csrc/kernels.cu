@@ -14,6 +14,7 @@
 #include "kernels.cuh"
 #include "stages.cuh"
 
+#include <cstdlib>
 #include <mutex>
 
 namespace sbg {
@@ -295,6 +296,146 @@ __global__ void __launch_bounds__(T) k_refine(int n, int batch, Workspace ws, do
     for (int i = tid; i < n; i += T) W[static_cast<size_t>(n) * b + i] = lam[i];
 }
 
+// ----------------------------------------------------------------------------- k_ql_chain
+// One THREAD per pair: the scalar QL recurrence with (d, e) in shared memory
+// interleaved over the CTA, rotations appended to the pair's log.  All 32 lanes of
+// a warp do useful work, so the FP64 pipe runs the chains of 32 pairs at once.
+template <typename R>
+__global__ void k_ql_chain(int n, int batch, Workspace ws, double* __restrict__ W, int* __restrict__ info) {
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int b = blockIdx.x * T + tid;
+    extern __shared__ __align__(16) unsigned char smem[];
+    R* d = reinterpret_cast<R*>(smem) + tid;
+    R* e = reinterpret_cast<R*>(smem) + static_cast<size_t>(n) * T + tid;
+    if (b >= batch) return;
+    double* Wb = W + static_cast<size_t>(n) * b;
+    cplx<R>* log = reinterpret_cast<cplx<R>*>(ws.log) + static_cast<size_t>(ws.log_cap) * b;
+    ws.flag[b] = 0;
+    if (info[b] != 0) {
+        for (int i = 0; i < n; ++i) Wb[i] = __longlong_as_double(0x7ff8000000000000ll);
+        log[0] = mk<R>(R(-1), R(0));
+        return;
+    }
+    for (int i = 0; i < n; ++i) {
+        d[i * T] = static_cast<R>(ws.d[static_cast<size_t>(n) * b + i]);
+        e[i * T] = static_cast<R>(ws.e[static_cast<size_t>(n) * b + i]);
+    }
+    const int r = ql_chain<R>(n, d, e, T, log, ws.log_cap, ws.perm + static_cast<size_t>(n) * b, Wb);
+    if (r < 0) ws.flag[b] = 1;
+    else if (r > 0) info[b] = r;
+}
+
+// ----------------------------------------------------------------------------- k_ql_apply
+// One warp per pair: Z = I, then every logged rotation applied to the rows the lane
+// owns (r = lane + 32 q), Z row-major in shared memory with an odd leading
+// dimension.  The log is read 32 entries at a time (one coalesced load, staged in
+// shared memory, read back by broadcast); within a sweep the rotation at column i
+// only needs z_i loaded, z_{i+1} being carried in a register.  Columns are written
+// out in the sorted order of the eigenvalues.  A pair whose log overflowed is
+// solved here by the warp-per-pair QL instead.
+template <typename R>
+__host__ __device__ inline size_t ql_apply_warp_bytes(int n) {
+    return align_up(sizeof(R) * static_cast<size_t>(n) * tile_ld(n), 16) + 2 * 32 * sizeof(cplx<R>) +
+           align_up(sizeof(R) * 2 * n, 16);
+}
+
+template <typename R>
+__global__ void k_ql_apply(int n, int batch, Workspace ws, double* __restrict__ W, double2* __restrict__ X,
+                           int* __restrict__ info) {
+    using C = cplx<R>;
+    constexpr int MAXQ = 3;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (b >= batch) return;
+    if (info[b] > n || info[b] < 0) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int ldz = tile_ld(n);
+    unsigned char* base = smem + ql_apply_warp_bytes<R>(n) * warp;
+    R* Z = reinterpret_cast<R*>(base);
+    C* stage = reinterpret_cast<C*>(base + align_up(sizeof(R) * static_cast<size_t>(n) * ldz, 16));
+    R* dd = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(stage) + 2 * 32 * sizeof(C));
+    R* ee = dd + n;
+    const size_t mat = static_cast<size_t>(n) * n;
+    for (int r = lane; r < n; r += 32)
+        for (int c = 0; c < n; ++c) Z[r * ldz + c] = (r == c) ? R(1) : R(0);
+    const int* perm = ws.perm + static_cast<size_t>(n) * b;
+    bool identity_perm = false;
+    if (ws.flag[b]) {
+        for (int i = lane; i < n; i += 32) {
+            dd[i] = static_cast<R>(ws.d[static_cast<size_t>(n) * b + i]);
+            ee[i] = static_cast<R>(ws.e[static_cast<size_t>(n) * b + i]);
+        }
+        __syncwarp();
+        const int unconv = tridiag_ql<R>(n, dd, ee, Z, ldz);
+        for (int i = lane; i < n; i += 32) W[static_cast<size_t>(n) * b + i] = static_cast<double>(dd[i]);
+        if (lane == 0 && unconv) info[b] = unconv;
+        identity_perm = true;
+    } else {
+        __syncwarp();
+        const C* log = reinterpret_cast<const C*>(ws.log) + static_cast<size_t>(ws.log_cap) * b;
+        int p = 0;                         // next entry to consume
+        int loaded = 0;                    // entries [loaded - 32, loaded) are staged in buf
+        int buf = 0;
+        C pre = log[lane];                 // prefetched batch
+        int remaining = 0, col = 0;
+        R carry[MAXQ];
+        bool done = false;
+        while (!done) {
+            // stage the prefetched batch, prefetch the next one
+            stage[buf * 32 + lane] = pre;
+            __syncwarp();
+            const int batch_base = loaded;
+            loaded += 32;
+            if (loaded < ws.log_cap) pre = log[min(loaded + lane, ws.log_cap - 1)];
+            for (int k = 0; k < 32 && !done; ++k, ++p) {
+                const C ent = stage[buf * 32 + k];
+                if (remaining == 0) {
+                    const int top = static_cast<int>(ent.x);
+                    if (top < 0) { done = true; break; }
+                    remaining = static_cast<int>(ent.y);
+                    col = top;
+#pragma unroll
+                    for (int q = 0; q < MAXQ; ++q) {
+                        const int r = lane + 32 * q;
+                        if (r < n) carry[q] = Z[r * ldz + col + 1];
+                    }
+                    continue;
+                }
+                const R c = ent.x, s = ent.y;
+#pragma unroll
+                for (int q = 0; q < MAXQ; ++q) {
+                    const int r = lane + 32 * q;
+                    if (r < n) {
+                        R* zr = Z + r * ldz;
+                        const R zi = zr[col], zi1 = carry[q];
+                        zr[col + 1] = fma(s, zi, c * zi1);
+                        carry[q] = fma(c, zi, -s * zi1);
+                    }
+                }
+                --col;
+                if (--remaining == 0) {
+#pragma unroll
+                    for (int q = 0; q < MAXQ; ++q) {
+                        const int r = lane + 32 * q;
+                        if (r < n) Z[r * ldz + col + 1] = carry[q];
+                    }
+                }
+            }
+            (void)batch_base;
+            __syncwarp();
+            buf ^= 1;
+            if (loaded >= ws.log_cap && !done) done = true;   // malformed log guard (never reached)
+        }
+        __syncwarp();
+    }
+    R* Zg = reinterpret_cast<R*>(X + mat * b);
+    for (size_t idx = lane; idx < mat; idx += 32) {
+        const int k = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(k) * n);
+        const int src = identity_perm ? k : perm[k];
+        Zg[idx] = Z[r * ldz + src];
+    }
+}
+
 // ----------------------------------------------------------------------------- k_back
 template <int T>
 __global__ void __launch_bounds__(T) k_back(int mode, int n, int batch, Workspace ws,
@@ -360,9 +501,19 @@ void set_max_smem_once(K kernel, std::once_flag& flag) {
 
 // ============================================================================== host side
 
+int ql_log_capacity(int n) {
+    const int dflt = (3 * n * n) / 2 + 8 * n + 16;
+    if (const char* v = std::getenv("SBG_QL_LOG_CAPACITY")) {
+        const int c = std::atoi(v);
+        if (c >= 16 && c < dflt) return c;
+    }
+    return dflt;
+}
+
 size_t workspace_bytes_per_pair(int n) {
     const size_t nn = static_cast<size_t>(n) * n;
-    return 16 * nn + 16 * n + 8 * n * 2;
+    const size_t cap = static_cast<size_t>((3 * n * n) / 2 + 8 * n + 16);    // the default (largest) capacity
+    return 16 * nn + 16 * n + 8 * n * 2 + 16 * cap + 4 * n + 4;
 }
 
 Workspace carve_workspace(void* base, int n, int capacity) {
@@ -376,6 +527,10 @@ Workspace carve_workspace(void* base, int n, int capacity) {
     w.tau = reinterpret_cast<double2*>(take(16 * n * cap));
     w.d = reinterpret_cast<double*>(take(8 * n * cap));
     w.e = reinterpret_cast<double*>(take(8 * n * cap));
+    w.log_cap = ql_log_capacity(n);
+    w.log = take(16 * static_cast<size_t>(w.log_cap) * cap);
+    w.perm = reinterpret_cast<int*>(take(4 * n * cap));
+    w.flag = reinterpret_cast<int*>(take(4 * cap));
     return w;
 }
 
@@ -425,19 +580,46 @@ cudaError_t launch_tridiag_ql(int n, int batch, const Workspace& ws, double* W, 
 
 size_t refine_smem_bytes(int n, int threads) { return RefineSmem(n, threads / 32).total; }
 
-cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
-                                 int refine_steps, int warps_per_cta, int refine_threads, cudaStream_t stream) {
+size_t ql_chain_smem_bytes(int n, int threads, bool single) {
+    return (single ? 4 : 8) * 2 * static_cast<size_t>(n) * threads;
+}
+size_t ql_apply_smem_bytes(int n, int warps_per_cta, bool single) {
+    return (single ? ql_apply_warp_bytes<float>(n) : ql_apply_warp_bytes<double>(n)) * warps_per_cta;
+}
+
+cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                             bool single, int chain_threads, int apply_warps, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
-    const size_t smem = tridiag_smem_bytes(n, warps_per_cta, true);
-    const size_t rsmem = refine_smem_bytes(n, refine_threads);
-    if (smem > static_cast<size_t>(max_smem_optin()) || rsmem > static_cast<size_t>(max_smem_optin()))
+    const size_t cs = ql_chain_smem_bytes(n, chain_threads, single);
+    const size_t as = ql_apply_smem_bytes(n, apply_warps, single);
+    if (cs > static_cast<size_t>(max_smem_optin()) || as > static_cast<size_t>(max_smem_optin()))
         return cudaErrorInvalidValue;
-    static std::once_flag f, f128, f256;
-    set_max_smem_once(k_tridiag<float>, f);
-    const int grid = (batch + warps_per_cta - 1) / warps_per_cta;
-    k_tridiag<float><<<grid, 32 * warps_per_cta, smem, stream>>>(n, batch, ws, W, X, info);
-    cudaError_t err = cudaGetLastError();
+    const int cgrid = (batch + chain_threads - 1) / chain_threads;
+    const int agrid = (batch + apply_warps - 1) / apply_warps;
+    static std::once_flag fcd, fcf, fad, faf;
+    if (single) {
+        set_max_smem_once(k_ql_chain<float>, fcf);
+        set_max_smem_once(k_ql_apply<float>, faf);
+        k_ql_chain<float><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info);
+        k_ql_apply<float><<<agrid, 32 * apply_warps, as, stream>>>(n, batch, ws, W, X, info);
+    } else {
+        set_max_smem_once(k_ql_chain<double>, fcd);
+        set_max_smem_once(k_ql_apply<double>, fad);
+        k_ql_chain<double><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info);
+        k_ql_apply<double><<<agrid, 32 * apply_warps, as, stream>>>(n, batch, ws, W, X, info);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                                 int refine_steps, int chain_threads, int apply_warps, int refine_threads,
+                                 cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    const size_t rsmem = refine_smem_bytes(n, refine_threads);
+    if (rsmem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+    cudaError_t err = launch_ql_logged(n, batch, ws, W, X, info, true, chain_threads, apply_warps, stream);
     if (err != cudaSuccess) return err;
+    static std::once_flag f128, f256;
     if (refine_threads == 128) {
         set_max_smem_once(k_refine<128>, f128);
         k_refine<128><<<batch, 128, rsmem, stream>>>(n, batch, ws, W, X, info, refine_steps);

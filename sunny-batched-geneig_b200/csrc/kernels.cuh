@@ -15,14 +15,27 @@ namespace sbg {
 //   d,e n   real      tridiagonal diagonal / subdiagonal
 // The tridiagonal eigenvectors Z (n*n real) are written into the caller's X buffer,
 // which the back-transform kernel then overwrites with X in place.
+//   log  cap entries (16 B)  the QL rotation log of the pair (ql_chain)
+//   perm n int               sort permutation of the QL eigenvalues
+//   flag 1 int               1 if the log overflowed (the apply kernel then runs the
+//                            warp-per-pair QL for that pair)
 struct Workspace {
     double2* LV = nullptr;
     double2* tau = nullptr;
     double* d = nullptr;
     double* e = nullptr;
+    void* log = nullptr;
+    int* perm = nullptr;
+    int* flag = nullptr;
+    int log_cap = 0;    // entries per pair
     int capacity = 0;   // pairs
     int n = 0;
 };
+
+// Rotation-log capacity per pair: ~1.1 n^2 rotations are typical (about two QL sweeps per
+// eigenvalue); pairs that need more fall back to the warp-per-pair QL.  The environment
+// variable SBG_QL_LOG_CAPACITY lowers it (a testing knob that forces the fallback).
+int ql_log_capacity(int n);
 
 size_t workspace_bytes_per_pair(int n);
 // Carves a Workspace for `capacity` pairs of size n out of `base` (256-byte aligned).
@@ -44,13 +57,20 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
                           const Workspace& ws, double2* out, int* info, int threads, cudaStream_t stream);
 cudaError_t launch_tridiag_ql(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
                               int warps_per_cta, cudaStream_t stream);
+// Two-kernel QL: thread-per-pair scalar chain logging rotations, then a warp-per-pair
+// application of the log to Z (single = FP32 chain and Z, the mixed form's first half).
+cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                             bool single, int chain_threads, int apply_warps, cudaStream_t stream);
 cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
-                                 int refine_steps, int warps_per_cta, int refine_threads, cudaStream_t stream);
+                                 int refine_steps, int chain_threads, int apply_warps, int refine_threads,
+                                 cudaStream_t stream);
 cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
                         int threads, cudaStream_t stream);
 
 size_t reduce_smem_bytes(int mode, int n);
 size_t tridiag_smem_bytes(int n, int warps_per_cta, bool single);
+size_t ql_chain_smem_bytes(int n, int threads, bool single);
+size_t ql_apply_smem_bytes(int n, int warps_per_cta, bool single);
 size_t back_smem_bytes(int n);
 size_t refine_smem_bytes(int n, int threads);
 int max_smem_optin();

@@ -41,12 +41,17 @@ __device__ int potrf_lower(cplx<R>* L, int ld, int n, R* invd) {
         if (tid == 0) invd[k] = inv;
         const int m = n - k - 1;
         const C* colk = L + k * ld;
-        for (int idx = tid; idx < m * m; idx += T) {
-            const int jj = idx / m, ii = idx - jj * m;
-            if (ii < jj) continue;
-            const int i = k + 1 + ii, j = k + 1 + jj;
+        // thread (row r, column chunk c) updates L(k+1+r, k+1+j) for j in its chunk, j <= r
+        const int chunks = max(1, T / max(m, 1));
+        const int cw = (m + chunks - 1) / chunks;
+        for (int t = tid; t < m * chunks; t += T) {
+            const int r = t % m, c = t / m;
+            const int i = k + 1 + r;
             const C lik = cscale(colk[i], invdd);
-            L[i + j * ld] = cfmsc(lik, colk[j], L[i + j * ld]);
+            const int j1 = min(r + 1, (c + 1) * cw);
+            C* Li = L + i + (k + 1) * ld;
+            for (int jj = c * cw; jj < j1; ++jj)
+                Li[jj * ld] = cfmsc(lik, colk[k + 1 + jj], Li[jj * ld]);
         }
         __syncthreads();
         pd = d; pinv = inv;
@@ -544,6 +549,98 @@ __device__ double oa_refine_step(int n, const double* dT, const double* eT, cons
     for (int w = 0; w < nw; ++w) em = fmax(em, red[4 * w + 3]);
     __syncthreads();
     return em;
+}
+
+// ============================================================================ QL, scalar chain only
+// The same implicit QL as tridiag_ql, run by ONE thread for one pair, with d and
+// e in shared memory interleaved over the CTA (element i of thread t at
+// [i * stride + t]).  Instead of rotating Z, every rotation (c, s) is appended
+// to a per-pair log in global memory: a sweep is a header entry
+// (top = m - 1, count) followed by `count` rotations acting on column pairs
+// (i, i+1), i = top, top-1, ..., top-count+1.  A header with count = 0 and
+// top = -1 ends the log.  The eigenvalues are sorted ascending and perm[k]
+// receives the pre-sort column index of eigenvalue k.
+// Returns the number of unconverged off-diagonals, or -1 if the log capacity
+// (cap entries) would be exceeded (the caller then falls back to tridiag_ql).
+template <typename R>
+__device__ int ql_chain(int n, R* d, R* e, int stride, cplx<R>* log, int cap, int* perm, double* W) {
+    using C = cplx<R>;
+    const R eps = sizeof(R) == 8 ? R(1.1102230246251565e-16) : R(5.9604645e-08);
+    const R eps2 = eps * eps;
+    const R safmin = sizeof(R) == 8 ? R(2.2250738585072014e-308) : R(1.17549435e-38);
+#define D(i) d[(i) * stride]
+#define E(i) e[(i) * stride]
+    R anorm = R(0);
+    for (int i = 0; i < n; ++i) anorm = fmax(anorm, fabs(D(i)));
+    for (int i = 0; i + 1 < n; ++i) anorm = fmax(anorm, fabs(E(i)));
+    if (!(anorm > R(0)) || !isfinite(anorm)) anorm = R(1);
+    const R sc = R(1) / anorm;
+    for (int i = 0; i < n; ++i) D(i) *= sc;
+    for (int i = 0; i + 1 < n; ++i) E(i) *= sc;
+    E(n - 1) = R(0);
+    int pos = 0, unconverged = 0;
+    const int maxit = 30;
+    for (int l = 0; l < n; ++l) {
+        int iter = 0;
+        for (;;) {
+            int m = l;
+            for (; m < n - 1; ++m) {
+                const R em = E(m);
+                if (em * em <= (eps2 * fabs(D(m))) * fabs(D(m + 1)) + safmin) break;
+            }
+            if (m == l) break;
+            if (iter == maxit) { ++unconverged; break; }
+            ++iter;
+            if (pos + (m - l) + 2 > cap) return -1;
+            const int hdr = pos++;
+            const R el = E(l), dl = D(l);
+            R g = (D(l + 1) - dl) / (R(2) * el);
+            R r = sqrt(fma(g, g, R(1)));
+            g = D(m) - dl + el / (g + copysign(r, g));
+            R s = R(1), c = R(1), p = R(0);
+            bool early = false;
+            int i = m - 1;
+            R ei = E(i), di = D(i);
+            for (; i >= l; --i) {
+                const R f = s * ei, b = c * ei;
+                const R rr = fma(f, f, g * g);
+                if (rr == R(0)) { D(i + 1) -= p; E(m) = R(0); early = true; break; }
+                const R di1 = D(i + 1);
+                const R ei_next = (i > l) ? E(i - 1) : R(0);     // prefetch: not written in this sweep
+                const R di_next = (i > l) ? D(i - 1) : R(0);
+                const R ri = rsqrt(rr);
+                E(i + 1) = rr * ri;
+                s = f * ri;
+                c = g * ri;
+                g = di1 - p;
+                r = fma(di - g, s, R(2) * c * b);
+                p = s * r;
+                D(i + 1) = g + p;
+                g = fma(c, r, -b);
+                log[pos++] = mk<R>(c, s);
+                ei = ei_next; di = di_next;
+            }
+            log[hdr] = mk<R>(R(m - 1), R(early ? (m - 1 - i) : (m - l)));
+            if (early) continue;
+            D(l) -= p; E(l) = g; E(m) = R(0);
+        }
+    }
+    log[pos] = mk<R>(R(-1), R(0));
+    // selection sort with the permutation recorded
+    for (int k = 0; k < n; ++k) perm[k] = k;
+    for (int k = 0; k + 1 < n; ++k) {
+        int j = k;
+        R pmin = D(k);
+        for (int t = k + 1; t < n; ++t) if (D(t) < pmin) { j = t; pmin = D(t); }
+        if (j != k) {
+            D(j) = D(k); D(k) = pmin;
+            const int tp = perm[k]; perm[k] = perm[j]; perm[j] = tp;
+        }
+    }
+    for (int k = 0; k < n; ++k) W[k] = static_cast<double>(D(k) * anorm);
+#undef D
+#undef E
+    return unconverged;
 }
 
 }  // namespace sbg

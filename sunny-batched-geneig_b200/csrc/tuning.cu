@@ -26,7 +26,7 @@ namespace sbg {
 namespace {
 
 constexpr const char* kTableMagic = "SBGTUNE";
-constexpr int kTableVersion = 1;
+constexpr int kTableVersion = 2;
 constexpr const char* kLibVersion = "sbg-geneig-0.1";
 
 std::mutex g_mu;
@@ -35,7 +35,9 @@ std::map<std::tuple<int, int, int>, Schedule> g_in_process;   // (device, n, pre
 bool fits(int n, int precision, const Schedule& s) {
     const size_t lim = static_cast<size_t>(max_smem_optin());
     if (reduce_smem_bytes(kReduceFull, n) > lim || back_smem_bytes(n) > lim) return false;
-    if (tridiag_smem_bytes(n, s.ql_warps, precision == SBG_PRECISION_MIXED) > lim) return false;
+    const bool single = precision == SBG_PRECISION_MIXED;
+    if (ql_chain_smem_bytes(n, s.chain_threads, single) > lim) return false;
+    if (ql_apply_smem_bytes(n, s.ql_warps, single) > lim) return false;
     if (precision == SBG_PRECISION_MIXED && refine_smem_bytes(n, s.refine_threads) > lim) return false;
     return true;
 }
@@ -89,7 +91,7 @@ bool load_table(const std::string& path, const std::string& key, std::vector<Tab
         std::string tag;
         TableEntry e{};
         es >> tag >> e.n >> e.precision >> e.s.reduce_threads >> e.s.back_threads >> e.s.ql_warps >>
-            e.s.refine_threads >> e.us;
+            e.s.chain_threads >> e.s.refine_threads >> e.us;
         if (tag != "entry" || !es) { out.clear(); return false; }
         out.push_back(e);
     }
@@ -117,7 +119,7 @@ void save_table(const std::string& path, const std::string& key, const std::vect
     body << "device " << key << "\n";
     for (const auto& e : entries)
         body << "entry " << e.n << " " << e.precision << " " << e.s.reduce_threads << " " << e.s.back_threads << " "
-             << e.s.ql_warps << " " << e.s.refine_threads << " " << e.us << "\n";
+             << e.s.ql_warps << " " << e.s.chain_threads << " " << e.s.refine_threads << " " << e.us << "\n";
     const std::string b = body.str();
     char buf[32];
     std::snprintf(buf, sizeof(buf), "%016llx", static_cast<unsigned long long>(fnv1a(b)));
@@ -204,9 +206,9 @@ struct Bench {
     int* inf() { return static_cast<int*>(info.p); }
     void eig(const Schedule& s) {
         if (precision == SBG_PRECISION_MIXED)
-            launch_tridiag_mixed(n, count, ws, w(), x(), inf(), 3, s.ql_warps, s.refine_threads, st);
+            launch_tridiag_mixed(n, count, ws, w(), x(), inf(), 3, s.chain_threads, s.ql_warps, s.refine_threads, st);
         else
-            launch_tridiag_ql(n, count, ws, w(), x(), inf(), s.ql_warps, st);
+            launch_ql_logged(n, count, ws, w(), x(), inf(), false, s.chain_threads, s.ql_warps, st);
     }
     void full(const Schedule& s) {
         launch_reduce(kReduceFull, a(), b(), n, count, ws, nullptr, inf(), s.reduce_threads, st);
@@ -260,15 +262,17 @@ bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double&
     {
         double bt = 1e30;
         std::vector<int> refine_opts = precision == SBG_PRECISION_MIXED ? std::vector<int>{128, 256} : std::vector<int>{256};
-        for (int w : warp_opts)
-            for (int rt : refine_opts) {
-                Schedule s = win;
-                s.ql_warps = w;
-                s.refine_threads = rt;
-                if (!fits(n, precision, s)) continue;
-                double ms = median_ms([&] { bench.eig(s); }, 3, bench.st);
-                if (ms < bt) { bt = ms; win.ql_warps = w; win.refine_threads = rt; }
-            }
+        for (int ct : {64, 128, 256})
+            for (int w : warp_opts)
+                for (int rt : refine_opts) {
+                    Schedule s = win;
+                    s.ql_warps = w;
+                    s.chain_threads = ct;
+                    s.refine_threads = rt;
+                    if (!fits(n, precision, s)) continue;
+                    double ms = median_ms([&] { bench.eig(s); }, 3, bench.st);
+                    if (ms < bt) { bt = ms; win.ql_warps = w; win.chain_threads = ct; win.refine_threads = rt; }
+                }
         t_total += bt;
     }
     // k_back (restores Z before every run: the kernel overwrites it with X)
@@ -317,8 +321,9 @@ bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double&
     }
     best = win;
     best_us = 1e3 * t_total / count;
-    std::fprintf(stderr, "[sbg autotune] n=%d precision=%d: reduce=%d back=%d ql_warps=%d refine=%d (%.3f us/pair)\n",
-                 n, precision, win.reduce_threads, win.back_threads, win.ql_warps, win.refine_threads, best_us);
+    std::fprintf(stderr, "[sbg autotune] n=%d precision=%d: reduce=%d back=%d ql_chain=%d ql_apply_warps=%d refine=%d "
+                 "(%.3f us/pair)\n", n, precision, win.reduce_threads, win.back_threads, win.chain_threads,
+                 win.ql_warps, win.refine_threads, best_us);
     return true;
 }
 
@@ -330,6 +335,8 @@ Schedule default_schedule(int n, int precision) {
     s.back_threads = n > 24 ? 256 : 128;
     s.refine_threads = n > 24 ? 256 : 128;
     s.ql_warps = n <= 32 ? 8 : (n <= 64 ? 4 : 2);
+    s.chain_threads = 128;
+    while (s.chain_threads > 32 && !fits(n, precision, s)) s.chain_threads /= 2;
     while (s.ql_warps > 1 && !fits(n, precision, s)) s.ql_warps /= 2;
     return s;
 }
