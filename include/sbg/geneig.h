@@ -170,6 +170,30 @@ int sbg_solver_precision(const sbg_solver* s);
 /* Largest n each form supports on this device (shared-memory bound). */
 int sbg_max_n(int precision);
 
+/* ------------------------------------------------------------------ allocation-free solve */
+/* This entry point has no counterpart in the reference.
+ *
+ * For callers that cannot let a library allocate device memory: frameworks that own every byte
+ * of device memory through their own pool allocator, applications running under a fixed memory
+ * budget they pre-allocated, and latency-sensitive loops that cannot absorb the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  It runs the same plain FP64 solve as
+ * sbg_solver_launch, but its scratch is one fixed array compiled into the library,
+ * SBG_NOALLOC_SCRATCH_BYTES long, which every GPU that loads the library keeps until process
+ * exit.  The caller still provides A, B, W, X and info.
+ *   - It allocates nothing (no cudaMalloc, cudaFree or allocating library call).
+ *   - Limit: batch * sbg_workspace_bytes_per_pair(n, SBG_PRECISION_FP64) + 1792 must fit in
+ *     SBG_NOALLOC_SCRATCH_BYTES (at n = 54 that is 533 pairs); larger batches are rejected with
+ *     SBG_ERR_INVALID_VALUE and a message in sbg_last_error() — split them into slices.
+ *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress)
+ *     and caches it; make that first call before any stream capture.
+ *   - All calls share the one array and it keeps the last call's contents (nothing in it needs
+ *     to start at zero).  Calls that overlap on the GPU race on it: order them on one stream.
+ * Returns an sbg_status. */
+#define SBG_NOALLOC_SCRATCH_BYTES (64u << 20)
+int sbg_geneig_full_noalloc_launch(int n, const cuDoubleComplex* d_A, const cuDoubleComplex* d_B,
+                                   double* d_W, cuDoubleComplex* d_X, int* d_info, int batch,
+                                   cudaStream_t stream);
+
 /* Autotune table (the analogue of the reference's on-disk cubin cache,
  * nvrtc_solver.cpp:403-431): path of this device's table file, written into buf.
  * Directory: $SUNNY_GENEIG_CACHE_DIR, else $XDG_CACHE_HOME/sunny_geneig_b200, else

@@ -67,6 +67,10 @@ int default_chunk_pairs(int n) {
 
 }  // namespace
 
+namespace sbg {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace sbg
+
 struct sbg_solver {
     int n = 0;
     int device = 0;

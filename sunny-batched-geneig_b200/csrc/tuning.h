@@ -51,5 +51,7 @@ TuneResult select_schedule(const TuneRequest& req);
 std::string tuning_cache_dir();
 std::string tuning_table_path(int device);
 void forget_in_process();
+// Message returned by sbg_last_error() on this host thread.
+void set_last_error(const std::string& msg);
 
 }  // namespace sbg

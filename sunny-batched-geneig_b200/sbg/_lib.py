@@ -62,6 +62,7 @@ SIGNATURES = {
     "sbg_max_n": (I, [I]),
     "sbg_tuning_table_path": (I, [I, ctypes.c_char_p, SZ]),
     "sbg_tuning_forget_in_process": (I, []),
+    "sbg_geneig_full_noalloc_launch": (I, [I, P, P, P, P, P, I, P]),
 }
 
 
