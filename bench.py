@@ -46,12 +46,13 @@ FRAC = 1e-3
 METRIC = "solves/s at n=54: FP32+refine vs plain FP64 on same B200, eig relerr <=1e-12"
 EIG_GATE = 1e-12
 # LAPACK flop counts per solve (real flops, complex multiply-add = 8):
-# potrf 4/3 n^3 + hegst 4 n^3 + hetrd 16/3 n^3 | steqr 12 n^3 | ungtr 16/3 n^3 + back-trsm 4 n^3
-STAGE_FLOPS = {"reduce": (4 / 3 + 4 + 16 / 3) * N ** 3, "eig": 12.0 * N ** 3, "back": (16 / 3 + 4) * N ** 3}
+# potrf 4/3 n^3 + hegst 4 n^3 | hetrd 16/3 n^3 | steqr 12 n^3 | ungtr 16/3 n^3 + back-trsm 4 n^3
+STAGE_FLOPS = {"reduce": (4 / 3 + 4) * N ** 3, "tridiag": 16 / 3 * N ** 3, "eig": 12.0 * N ** 3,
+               "back": (16 / 3 + 4) * N ** 3}
 FLOPS_PER_SOLVE = 32.0 * N ** 3
 # algorithmic bytes per solve: read A, B; write X, W, info
 BYTES_PER_SOLVE = 48 * N * N + 8 * N + 4
-STAGE_BYTES = {"reduce": 32 * N * N, "eig": 16 * N, "back": 16 * N * N + 8 * N + 4}
+STAGE_BYTES = {"reduce": 32 * N * N, "tridiag": 0, "eig": 16 * N, "back": 16 * N * N + 8 * N + 4}
 
 
 def env_int(name, default):

@@ -147,11 +147,12 @@ int sbg_solver_solve_host(sbg_solver* s, const cuDoubleComplex* h_A, const cuDou
 
 /* Per-stage timing: when enabled, every launch records CUDA events around each stage
  * kernel on the launch stream.  sbg_solver_read_stage_times synchronizes on them and
- * returns, per stage (0 = Cholesky + reduction + tridiagonalisation, 1 = tridiagonal
- * eigensolve (QL, or QL + refinement for the mixed form), 2 = back-transform), the summed
- * milliseconds and the number of kernel launches, then clears the record. */
+ * returns, per stage (0 = Cholesky + two-sided reduction, 1 = Householder
+ * tridiagonalisation, 2 = tridiagonal eigensolve (QL, or QL + refinement for the mixed
+ * form), 3 = back-transform), the summed milliseconds and the number of kernel launches,
+ * then clears the record. */
 int sbg_solver_enable_stage_timing(sbg_solver* s, int enable);
-int sbg_solver_read_stage_times(sbg_solver* s, double* ms_out3, int* launches_out3);
+int sbg_solver_read_stage_times(sbg_solver* s, double* ms_out4, int* launches_out4);
 
 /* Device bytes of workspace per pair for a given n and precision. */
 size_t sbg_workspace_bytes_per_pair(int n, int precision);

@@ -144,9 +144,12 @@ struct sbg_solver {
                    const sbg::Workspace& ws, cudaStream_t stream) {
         cudaEvent_t ev;
         stage_begin(stream, &ev);
-        check_cuda(sbg::launch_reduce(sbg::kReduceFull, A, B, n, cnt, ws, nullptr, info,
+        check_cuda(sbg::launch_reduce(sbg::kReduceFull, A, B, n, cnt, ws, X, info,
                                       sched.reduce_threads, stream), "reduce kernel");
         stage_end(stream, ev, 0, 1);
+        stage_begin(stream, &ev);
+        check_cuda(sbg::launch_hetrd(n, cnt, X, ws, info, sched.hetrd_threads, stream), "hetrd kernel");
+        stage_end(stream, ev, 1, 1);
         stage_begin(stream, &ev);
         if (precision == SBG_PRECISION_MIXED)
             check_cuda(sbg::launch_tridiag_mixed(n, cnt, ws, W, X, info, refine_steps, sched.chain_threads,
@@ -155,11 +158,11 @@ struct sbg_solver {
         else
             check_cuda(sbg::launch_ql_logged(n, cnt, ws, W, X, info, false, sched.chain_threads, sched.ql_warps,
                                              stream), "QL kernels");
-        stage_end(stream, ev, 1, precision == SBG_PRECISION_MIXED ? 3 : 2);
+        stage_end(stream, ev, 2, precision == SBG_PRECISION_MIXED ? 3 : 2);
         stage_begin(stream, &ev);
         check_cuda(sbg::launch_back(sbg::kBackFull, n, cnt, ws, X, info, sched.back_threads, stream),
                    "back-transform kernel");
-        stage_end(stream, ev, 2, 1);
+        stage_end(stream, ev, 3, 1);
     }
 
     void solve_host(const double2* hA, const double2* hB, double* hW, double2* hX, int* hinfo, int batch,
@@ -235,6 +238,7 @@ int supported_max_n(int precision) {
     int best = 0;
     for (int n = 1; n <= 256; ++n) {
         size_t need = std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, n), sbg::back_smem_bytes(n));
+        need = std::max(need, sbg::hetrd_smem_bytes(n));
         need = std::max(need, sbg::ql_apply_smem_bytes(n, 1, precision == SBG_PRECISION_MIXED));
         need = std::max(need, sbg::ql_chain_smem_bytes(n, 32, precision == SBG_PRECISION_MIXED));
         if (precision == SBG_PRECISION_MIXED) need = std::max(need, sbg::refine_smem_bytes(n, 128));
@@ -394,7 +398,7 @@ int sbg_solver_read_stage_times(sbg_solver* s, double* ms, int* launches) {
             std::lock_guard<std::mutex> lock(s->mu);
             evs.swap(s->stage_events);
         }
-        for (int k = 0; k < 3; ++k) { ms[k] = 0.0; launches[k] = 0; }
+        for (int k = 0; k < 4; ++k) { ms[k] = 0.0; launches[k] = 0; }
         for (auto& e : evs) {
             check_cuda(cudaEventSynchronize(e.b), "cudaEventSynchronize");
             float t = 0.f;
@@ -494,8 +498,9 @@ void geneig_reduce_eig_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComp
     report_void(guarded([&] {
         sbg_solver* s = default_n54_solver();
         sbg::Workspace ws = s->workspace(0, 1, stream);
-        check_cuda(sbg::launch_reduce(sbg::kReduceFull, c2(d_H), c2(d_S), 54, 1, ws, nullptr, d_info,
+        check_cuda(sbg::launch_reduce(sbg::kReduceFull, c2(d_H), c2(d_S), 54, 1, ws, c2(d_V), d_info,
                                       s->sched.reduce_threads, stream), "reduce kernel");
+        check_cuda(sbg::launch_hetrd(54, 1, c2(d_V), ws, d_info, s->sched.hetrd_threads, stream), "hetrd kernel");
         check_cuda(sbg::launch_ql_logged(54, 1, ws, d_W, c2(d_V), d_info, false, s->sched.chain_threads,
                                          s->sched.ql_warps, stream), "QL kernels");
         check_cuda(sbg::launch_back(sbg::kBackQOnly, 54, 1, ws, c2(d_V), d_info, s->sched.back_threads, stream),
@@ -529,8 +534,10 @@ void geneig_finish_n54_launch(const cuDoubleComplex* d_L, const cuDoubleComplex*
         sbg::Workspace ws = s->workspace(0, cap, stream);
         for (int off = 0; off < batch_size; off += ws.capacity) {
             const int cnt = std::min(ws.capacity, batch_size - off);
-            check_cuda(sbg::launch_reduce(sbg::kReduceFromLM, c2(d_M) + nn * off, c2(d_L) + nn * off, 54, cnt, ws,
+            check_cuda(sbg::launch_reduce(sbg::kReduceFromLM, nullptr, c2(d_L) + nn * off, 54, cnt, ws,
                                           nullptr, d_info + off, s->sched.reduce_threads, stream), "reduce kernel");
+            check_cuda(sbg::launch_hetrd(54, cnt, c2(d_M) + nn * off, ws, d_info + off, s->sched.hetrd_threads, stream),
+                       "hetrd kernel");
             check_cuda(sbg::launch_ql_logged(54, cnt, ws, d_W + 54 * off, c2(d_U) + nn * off, d_info + off, false,
                                              s->sched.chain_threads, s->sched.ql_warps, stream), "QL kernels");
             check_cuda(sbg::launch_back(sbg::kBackFull, 54, cnt, ws, c2(d_U) + nn * off, d_info + off,

@@ -74,8 +74,14 @@ template <typename R> __device__ __forceinline__ R group_sum(R v, int width) {
 }
 
 // Leading dimension for an n x n tile of 16- or 8-byte elements in shared memory:
-// odd, so a warp walking a row (stride ld) touches distinct banks.
-__host__ __device__ __forceinline__ int tile_ld(int n) { return n | 1; }
+// odd, so a warp walking a row (stride ld) touches distinct banks, and never 7 mod 8,
+// where a walk along a diagonal (stride ld + 1 complex = a multiple of 128 bytes)
+// would put every lane in the same bank.
+__host__ __device__ __forceinline__ int tile_ld(int n) {
+    int ld = n | 1;
+    if ((ld & 7) == 7) ld += 2;
+    return ld;
+}
 
 // ----------------------------------------------------------------------------- bulk copy
 

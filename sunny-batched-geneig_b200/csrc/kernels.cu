@@ -25,38 +25,18 @@ __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a -
 
 // Shared-memory carve-up of k_reduce.
 struct ReduceSmem {
-    size_t Ls, As, invd, vbuf, pbuf, wbuf, sh, d, e, tau, bar, total;
+    size_t Ls, As, invd, bar, total;
     __host__ __device__ ReduceSmem(int n) {
         const size_t ld = static_cast<size_t>(tile_ld(n));
         size_t o = 0;
         Ls = o;   o += 16 * ld * n;
         As = o;   o += 16 * ld * n;
         invd = o; o += align_up(8 * n, 16);
-        vbuf = o; o += 16 * n;
-        pbuf = o; o += 32 * n;
-        wbuf = o; o += 16 * n;
-        sh = o;   o += 32;
-        d = o;    o += align_up(8 * n, 16);
-        e = o;    o += align_up(8 * n, 16);
-        tau = o;  o += 16 * n;
         bar = o;  o += 16;
         total = o;
     }
 };
 
-struct BackSmem {
-    size_t LVs, Ys, invd, tau, bar, total;
-    __host__ __device__ BackSmem(int n) {
-        const size_t ld = static_cast<size_t>(tile_ld(n));
-        size_t o = 0;
-        LVs = o;  o += 16 * ld * n;
-        Ys = o;   o += 16 * ld * n;
-        invd = o; o += align_up(8 * n, 16);
-        tau = o;  o += 16 * n;
-        bar = o;  o += 16;
-        total = o;
-    }
-};
 
 template <typename R>
 __host__ __device__ inline size_t tridiag_warp_bytes(int n) {
@@ -79,8 +59,8 @@ __device__ inline bool wait_copies(uint64_t* bar, int* info_word) {
 }
 
 // ----------------------------------------------------------------------------- k_reduce
-template <int T>
-__global__ void __launch_bounds__(T) k_reduce(int mode, const double2* __restrict__ A,
+template <int T, int G, int RM>
+__global__ void __launch_bounds__(T, T == 256 ? 2 : 1) k_reduce(int mode, const double2* __restrict__ A,
                                               const double2* __restrict__ B, int n, int batch,
                                               Workspace ws, double2* __restrict__ out,
                                               int* __restrict__ info) {
@@ -92,20 +72,13 @@ __global__ void __launch_bounds__(T) k_reduce(int mode, const double2* __restric
     double2* Ls = reinterpret_cast<double2*>(smem + lay.Ls);
     double2* As = reinterpret_cast<double2*>(smem + lay.As);
     double* invd = reinterpret_cast<double*>(smem + lay.invd);
-    double2* vbuf = reinterpret_cast<double2*>(smem + lay.vbuf);
-    double2* pbuf = reinterpret_cast<double2*>(smem + lay.pbuf);
-    double2* wbuf = reinterpret_cast<double2*>(smem + lay.wbuf);
-    double2* sh = reinterpret_cast<double2*>(smem + lay.sh);
-    double* d_s = reinterpret_cast<double*>(smem + lay.d);
-    double* e_s = reinterpret_cast<double*>(smem + lay.e);
-    double2* tau_s = reinterpret_cast<double2*>(smem + lay.tau);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + lay.bar);
 
     const int tid = threadIdx.x;
     const size_t mat = static_cast<size_t>(n) * n;
-    const double2* Ab = A + mat * b;     // A, or M in kReduceFromLM
+    const double2* Ab = A + mat * b;     // A (unused in kReduceChol / kReduceFromLM)
     const double2* Bb = B + mat * b;     // B, or L in kReduceFromLM
-    const bool need_a = mode != kReduceChol;
+    const bool need_a = mode != kReduceChol && mode != kReduceFromLM;
 
     // ---- stage the pair into shared memory: B (lower part of each column) and A
     if (tid == 0) { mbar_init(bar, 1); fence_mbar_init(); }
@@ -124,7 +97,6 @@ __global__ void __launch_bounds__(T) k_reduce(int mode, const double2* __restric
     }
     wait_copies(bar, info + b);
 
-    const int G = pick_group(T, n);
     int st = 0;
     if (mode == kReduceFromLM) {
         for (int i = tid; i < n; i += T) invd[i] = 1.0 / Ls[i + i * ld].x;
@@ -145,37 +117,129 @@ __global__ void __launch_bounds__(T) k_reduce(int mode, const double2* __restric
         return;
     }
     if (mode != kReduceFromLM) {
-        trsm_left_lower(Ls, ld, invd, As, ld, n, G);
+        const int g = tid % G;
+        double2 y[RM];
+        {   // W = L^{-1} A: column j = tid / G, rows g + G r in registers
+            const int j = tid / G;
+            const bool valid = j < n;
+#pragma unroll
+            for (int r = 0; r < RM; ++r) {
+                const int i = g + G * r;
+                y[r] = (valid && i < n) ? As[i + j * ld] : make_double2(0.0, 0.0);
+            }
+            seg_trsm_lower<G, RM>(Ls, ld, invd, y, n, g);
+            if (valid) {
+#pragma unroll
+                for (int r = 0; r < RM; ++r) {
+                    const int i = g + G * r;
+                    if (i < n) As[i + j * ld] = y[r];
+                }
+            }
+        }
         __syncthreads();
-        trsm_right_lowerH(Ls, ld, invd, As, ld, n, G);
+        {   // C = W L^{-H} (lower part): row i = tid / G, columns g + G r in registers
+            const int i = tid / G;
+            const bool valid = i < n;
+            const int kmax = min(n - 1, (tid | 31) / G);
+#pragma unroll
+            for (int r = 0; r < RM; ++r) {
+                const int kk = g + G * r;
+                y[r] = (valid && kk < n) ? As[i + kk * ld] : make_double2(0.0, 0.0);
+            }
+            seg_trsm_right_lowerH<G, RM>(Ls, ld, invd, y, kmax, valid ? i : -1, g);
+            if (valid) {
+#pragma unroll
+                for (int r = 0; r < RM; ++r) {
+                    const int kk = g + G * r;
+                    if (kk <= i) As[i + kk * ld] = y[r];
+                }
+            }
+        }
         __syncthreads();
     }
-    if (mode == kReduceHegst) {
+    if (mode == kReduceHegst || mode == kReduceFull) {
+        double2* Mg = out + mat * b;
         for (size_t idx = tid; idx < mat; idx += T) {
             const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
             double2 v = make_double2(0.0, 0.0);
             if (i >= j) { v = As[i + j * ld]; if (i == j) v.y = 0.0; }
-            out[mat * b + idx] = v;
+            if (i >= j || mode == kReduceHegst) Mg[idx] = v;
         }
-        if (tid == 0) info[b] = 0;
-        return;
     }
-    // ---- tridiagonalise C, then store L (lower) and the reflectors (rows, upper) in one tile
+    if (mode == kReduceFull || mode == kReduceFromLM) {
+        // L into the lower triangle of the pair's LV tile (the reflectors fill the upper part later)
+        double2* LVg = ws.LV + mat * b;
+        for (size_t idx = tid; idx < mat; idx += T) {
+            const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
+            if (i >= j) LVg[idx] = Ls[i + j * ld];
+        }
+    }
+    if (tid == 0) info[b] = 0;
+}
+
+// ----------------------------------------------------------------------------- k_hetrd
+// One CTA per pair, one tile: C (lower triangle) staged by TMA bulk copies, reduced
+// to tridiagonal form; the reflectors go to the upper part of the pair's LV tile.
+struct HetrdSmem {
+    size_t As, vbuf, pbuf, wbuf, sh, d, e, tau, bar, total;
+    __host__ __device__ HetrdSmem(int n) {
+        const size_t ld = static_cast<size_t>(tile_ld(n));
+        size_t o = 0;
+        As = o;   o += 16 * ld * n;
+        vbuf = o; o += 16 * n;
+        pbuf = o; o += 32 * n;
+        wbuf = o; o += 16 * n;
+        sh = o;   o += 32;
+        d = o;    o += align_up(8 * n, 16);
+        e = o;    o += align_up(8 * n, 16);
+        tau = o;  o += 16 * n;
+        bar = o;  o += 16;
+        total = o;
+    }
+};
+
+template <int T>
+__global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __restrict__ C, Workspace ws,
+                                             const int* __restrict__ info) {
+    const int b = blockIdx.x;
+    if (b >= batch) return;
+    if (info[b] != 0) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const HetrdSmem lay(n);
+    const int ld = tile_ld(n);
+    double2* As = reinterpret_cast<double2*>(smem + lay.As);
+    double2* vbuf = reinterpret_cast<double2*>(smem + lay.vbuf);
+    double2* pbuf = reinterpret_cast<double2*>(smem + lay.pbuf);
+    double2* wbuf = reinterpret_cast<double2*>(smem + lay.wbuf);
+    double2* sh = reinterpret_cast<double2*>(smem + lay.sh);
+    double* d_s = reinterpret_cast<double*>(smem + lay.d);
+    double* e_s = reinterpret_cast<double*>(smem + lay.e);
+    double2* tau_s = reinterpret_cast<double2*>(smem + lay.tau);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + lay.bar);
+    const int tid = threadIdx.x;
+    const size_t mat = static_cast<size_t>(n) * n;
+    const double2* Cb = C + mat * b;
+    if (tid == 0) { mbar_init(bar, 1); fence_mbar_init(); }
+    __syncthreads();
+    if (tid < 32) {
+        if (tid == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(16 * (static_cast<size_t>(n) * (n + 1) / 2)));
+        __syncwarp();
+        for (int j = tid; j < n; j += 32)
+            bulk_g2s(As + j + static_cast<size_t>(j) * ld, Cb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
+    }
+    wait_copies(bar, nullptr);
     hetrd_lower(As, ld, n, d_s, e_s, tau_s, vbuf, pbuf, wbuf, sh);
+    // reflector k, component i >= k+2, sits at A(i, k); it goes to LV(k, i)
     double2* LVg = ws.LV + mat * b;
     for (size_t idx = tid; idx < mat; idx += T) {
-        const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
-        double2 v = make_double2(0.0, 0.0);
-        if (i >= j) v = Ls[i + j * ld];
-        else if (j >= i + 2) v = As[j + i * ld];       // LV(i, j) = v_i(j)
-        LVg[idx] = v;
+        const int i = static_cast<int>(idx / n), k = static_cast<int>(idx - static_cast<size_t>(i) * n);
+        if (i >= k + 2) LVg[k + static_cast<size_t>(i) * n] = As[i + k * ld];
     }
     for (int i = tid; i < n; i += T) {
         ws.d[static_cast<size_t>(n) * b + i] = d_s[i];
         ws.e[static_cast<size_t>(n) * b + i] = e_s[i];
         ws.tau[static_cast<size_t>(n) * b + i] = (i + 1 < n) ? tau_s[i] : make_double2(0.0, 0.0);
     }
-    if (tid == 0) info[b] = 0;
 }
 
 // ----------------------------------------------------------------------------- k_tridiag
@@ -437,8 +501,25 @@ __global__ void k_ql_apply(int n, int batch, Workspace ws, double* __restrict__ 
 }
 
 // ----------------------------------------------------------------------------- k_back
-template <int T>
-__global__ void __launch_bounds__(T) k_back(int mode, int n, int batch, Workspace ws,
+// One CTA per pair: X = L^{-H} Q Z.  Column j of Z is held in registers by a group
+// of G lanes (lane g owns rows g + G r), read straight from the X buffer; only the
+// LV tile (L below, reflectors above the superdiagonal) is staged in shared memory
+// by TMA bulk copies.  The result is written over Z.
+struct BackSmem {
+    size_t LVs, invd, tau, bar, total;
+    __host__ __device__ BackSmem(int n) {
+        const size_t ld = static_cast<size_t>(tile_ld(n));
+        size_t o = 0;
+        LVs = o;  o += 16 * ld * n;
+        invd = o; o += align_up(8 * n, 16);
+        tau = o;  o += 16 * n;
+        bar = o;  o += 16;
+        total = o;
+    }
+};
+
+template <int T, int G, int RM>
+__global__ void __launch_bounds__(T, T == 256 ? 2 : 1) k_back(int mode, int n, int batch, Workspace ws,
                                             double2* __restrict__ X, const int* __restrict__ info) {
     const int b = blockIdx.x;
     if (b >= batch) return;
@@ -454,7 +535,6 @@ __global__ void __launch_bounds__(T) k_back(int mode, int n, int batch, Workspac
     const BackSmem lay(n);
     const int ld = tile_ld(n);
     double2* LVs = reinterpret_cast<double2*>(smem + lay.LVs);
-    double2* Ys = reinterpret_cast<double2*>(smem + lay.Ys);
     double* invd = reinterpret_cast<double*>(smem + lay.invd);
     double2* tau_s = reinterpret_cast<double2*>(smem + lay.tau);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + lay.bar);
@@ -468,25 +548,27 @@ __global__ void __launch_bounds__(T) k_back(int mode, int n, int batch, Workspac
         for (int j = tid; j < n; j += 32)
             bulk_g2s(LVs + static_cast<size_t>(j) * ld, LVg + static_cast<size_t>(j) * n, 16u * n, bar);
     }
+    const int g = tid % G, j = tid / G;
+    const bool valid = j < n;
     const double* Zg = reinterpret_cast<const double*>(Xb);
-    for (size_t idx = tid; idx < mat; idx += T) {
-        const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
-        Ys[r + c * ld] = make_double2(Zg[idx], 0.0);
+    double2 y[RM];
+#pragma unroll
+    for (int r = 0; r < RM; ++r) {
+        const int i = g + G * r;
+        y[r] = make_double2((valid && i < n) ? Zg[i + static_cast<size_t>(j) * n] : 0.0, 0.0);
     }
     for (int i = tid; i < n; i += T) tau_s[i] = ws.tau[static_cast<size_t>(n) * b + i];
     wait_copies(bar, nullptr);
     for (int i = tid; i < n; i += T) invd[i] = 1.0 / LVs[i + i * ld].x;
-    __syncthreads();
-    const int G = pick_group(T, n);
-    apply_q_left<double>(LVs, ld, tau_s, Ys, ld, n, G);
-    __syncthreads();
-    if (mode == kBackFull) {
-        trsm_left_lowerH(LVs, ld, invd, Ys, ld, n, G);
-        __syncthreads();
-    }
-    for (size_t idx = tid; idx < mat; idx += T) {
-        const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
-        Xb[idx] = Ys[r + c * ld];
+    __syncthreads();              // also: every thread has read its Z before any X is written
+    seg_apply_q<G, RM>(LVs, ld, tau_s, y, n, g);
+    if (mode == kBackFull) seg_trsm_lowerH<G, RM>(LVs, ld, invd, y, n, g);
+    if (valid) {
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+            const int i = g + G * r;
+            if (i < n) Xb[i + static_cast<size_t>(j) * n] = y[r];
+        }
     }
 }
 
@@ -550,18 +632,55 @@ size_t tridiag_smem_bytes(int n, int warps_per_cta, bool single) {
     return (single ? tridiag_warp_bytes<float>(n) : tridiag_warp_bytes<double>(n)) * warps_per_cta;
 }
 
+// The register-segment kernels: (threads T, lanes per column G, rows per lane RM) by
+// size: n <= 32 -> (256, 8, 4), n <= 64 -> (256, 4, 16), else (512, 4, 22) (n <= 88).
+#define SBG_DISPATCH_BY_N(n, KERNEL, ...)                                              \
+    do {                                                                               \
+        if ((n) <= 32) { KERNEL<256, 8, 4>(__VA_ARGS__); }                             \
+        else if ((n) <= 64) { KERNEL<256, 4, 16>(__VA_ARGS__); }                       \
+        else { KERNEL<512, 4, 22>(__VA_ARGS__); }                                      \
+    } while (0)
+
+template <int T, int G, int RM>
+void run_reduce(int mode, const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* out,
+                int* info, size_t smem, cudaStream_t stream) {
+    static std::once_flag f;
+    set_max_smem_once(k_reduce<T, G, RM>, f);
+    k_reduce<T, G, RM><<<batch, T, smem, stream>>>(mode, A, B, n, batch, ws, out, info);
+}
+
+template <int T, int G, int RM>
+void run_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info, size_t smem,
+              cudaStream_t stream) {
+    static std::once_flag f;
+    set_max_smem_once(k_back<T, G, RM>, f);
+    k_back<T, G, RM><<<batch, T, smem, stream>>>(mode, n, batch, ws, X, info);
+}
+
 cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, int batch,
-                          const Workspace& ws, double2* out, int* info, int threads, cudaStream_t stream) {
+                          const Workspace& ws, double2* out, int* info, int /*threads*/, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
+    if (n > 84) return cudaErrorInvalidValue;
     const size_t smem = reduce_smem_bytes(mode, n);
+    if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+    SBG_DISPATCH_BY_N(n, run_reduce, mode, A, B, n, batch, ws, out, info, smem, stream);
+    return cudaGetLastError();
+}
+
+size_t hetrd_smem_bytes(int n) { return HetrdSmem(n).total; }
+
+cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, const int* info, int threads,
+                         cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    const size_t smem = hetrd_smem_bytes(n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     static std::once_flag f128, f256;
     if (threads == 128) {
-        set_max_smem_once(k_reduce<128>, f128);
-        k_reduce<128><<<batch, 128, smem, stream>>>(mode, A, B, n, batch, ws, out, info);
+        set_max_smem_once(k_hetrd<128>, f128);
+        k_hetrd<128><<<batch, 128, smem, stream>>>(n, batch, C, ws, info);
     } else {
-        set_max_smem_once(k_reduce<256>, f256);
-        k_reduce<256><<<batch, 256, smem, stream>>>(mode, A, B, n, batch, ws, out, info);
+        set_max_smem_once(k_hetrd<256>, f256);
+        k_hetrd<256><<<batch, 256, smem, stream>>>(n, batch, C, ws, info);
     }
     return cudaGetLastError();
 }
@@ -631,18 +750,12 @@ cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* 
 }
 
 cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
-                        int threads, cudaStream_t stream) {
+                        int /*threads*/, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
+    if (n > 84) return cudaErrorInvalidValue;
     const size_t smem = back_smem_bytes(n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
-    static std::once_flag f128, f256;
-    if (threads == 128) {
-        set_max_smem_once(k_back<128>, f128);
-        k_back<128><<<batch, 128, smem, stream>>>(mode, n, batch, ws, X, info);
-    } else {
-        set_max_smem_once(k_back<256>, f256);
-        k_back<256><<<batch, 256, smem, stream>>>(mode, n, batch, ws, X, info);
-    }
+    SBG_DISPATCH_BY_N(n, run_back, mode, n, batch, ws, X, info, smem, stream);
     return cudaGetLastError();
 }
 

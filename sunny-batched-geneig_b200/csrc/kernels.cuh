@@ -42,10 +42,10 @@ size_t workspace_bytes_per_pair(int n);
 Workspace carve_workspace(void* base, int n, int capacity);
 
 enum ReduceMode : int {
-    kReduceFull = 0,      // potrf + hegst + hetrd  -> ws.LV/tau/d/e
+    kReduceFull = 0,      // potrf + hegst          -> L into ws.LV (lower), C lower into out
     kReduceChol = 1,      // potrf only             -> out (L, strict upper zeroed)
     kReduceHegst = 2,     // potrf + hegst          -> out (M lower, strict upper zeroed)
-    kReduceFromLM = 3,    // hetrd of a given M     -> ws (L copied in)
+    kReduceFromLM = 3,    // given L                -> L copied into ws.LV (lower)
 };
 enum BackMode : int {
     kBackFull = 0,        // X = L^{-H} Q Z
@@ -57,6 +57,11 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
                           const Workspace& ws, double2* out, int* info, int threads, cudaStream_t stream);
 cudaError_t launch_tridiag_ql(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
                               int warps_per_cta, cudaStream_t stream);
+// Householder tridiagonalisation of C (lower triangle read, column-major, ld = n) ->
+// reflectors into ws.LV (rows above the superdiagonal), tau, d, e.  Pairs with info != 0 skip.
+cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, const int* info, int threads,
+                         cudaStream_t stream);
+size_t hetrd_smem_bytes(int n);
 // Two-kernel QL: thread-per-pair scalar chain logging rotations, then a warp-per-pair
 // application of the log to Z (single = FP32 chain and Z, the mixed form's first half).
 cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,

@@ -643,4 +643,110 @@ __device__ int ql_chain(int n, R* d, R* e, int stride, cplx<R>* log, int cap, in
     return unconverged;
 }
 
+// ============================================================================ register-segment solvers
+// Column (or row) work where the G lanes of a group share one column and lane g keeps
+// the entries of rows i = g + G r, r < RM, in registers for the whole stage; only L
+// or the reflectors are read from shared memory (the same address for every group:
+// a broadcast).  Requires n <= G * RM and n <= (threads / G) columns per pass.
+
+// Selects seg[r] for a runtime r (unrolled, so seg stays in registers).
+template <int RM, typename C>
+__device__ __forceinline__ C seg_get(const C (&seg)[RM], int r) {
+    C v = seg[0];
+#pragma unroll
+    for (int q = 1; q < RM; ++q) if (q == r) v = seg[q];
+    return v;
+}
+template <int RM, typename C>
+__device__ __forceinline__ void seg_set(C (&seg)[RM], int r, C v) {
+#pragma unroll
+    for (int q = 0; q < RM; ++q) if (q == r) seg[q] = v;
+}
+
+// y <- L^{-1} y (forward substitution) on the column segment; L column-major in smem.
+template <int G, int RM, typename C, typename R>
+__device__ __forceinline__ void seg_trsm_lower(const C* L, int ldl, const R* invd, C (&y)[RM], int n, int g) {
+    for (int k = 0; k < n; ++k) {
+        const int owner = k % G, rk = k / G;
+        C wk = seg_get(y, rk);
+        wk = cscale(wk, invd[k]);
+        if (g == owner) seg_set(y, rk, wk);
+        wk = cshfl(wk, owner, G);
+        const C* lk = L + k * ldl;
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+            const int i = g + G * r;
+            if (i > k && i < n) y[r] = cfms(lk[i], wk, y[r]);
+        }
+    }
+}
+
+// Row segment of W (columns kk = g + G r of row i) <- W L^{-H}, only kk <= i formed.
+template <int G, int RM, typename C, typename R>
+__device__ __forceinline__ void seg_trsm_right_lowerH(const C* L, int ldl, const R* invd, C (&y)[RM], int kmax,
+                                                      int i, int g) {
+    for (int k = 0; k <= kmax; ++k) {
+        const int owner = k % G, rk = k / G;
+        C ck = seg_get(y, rk);
+        ck = cscale(ck, invd[k]);
+        if (g == owner && k <= i) seg_set(y, rk, ck);
+        ck = cshfl(ck, owner, G);
+        const C* lk = L + k * ldl;
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+            const int kk = g + G * r;
+            if (kk > k && kk <= i) y[r] = cfmsc(ck, lk[kk], y[r]);
+        }
+    }
+}
+
+// y <- Q y with the reflectors along the rows of LV (see apply_q_left).
+template <int G, int RM, typename C>
+__device__ __forceinline__ void seg_apply_q(const C* LV, int ld, const C* tau, C (&y)[RM], int n, int g) {
+    using R = decltype(C().x);
+    for (int k = n - 2; k >= 0; --k) {
+        const C tk = tau[k];
+        if (tk.x == R(0) && tk.y == R(0)) continue;
+        const C* vrow = LV + k;                    // v_k(i) = LV(k, i) = vrow[i * ld], i >= k + 2
+        C s = mk<R>(R(0), R(0));
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+            const int i = g + G * r;
+            if (i > k && i < n) {
+                const C vi = (i == k + 1) ? mk<R>(R(1), R(0)) : vrow[i * ld];
+                s = cfmac(vi, y[r], s);
+            }
+        }
+        s.x = group_sum(s.x, G);
+        s.y = group_sum(s.y, G);
+        s = cmul(tk, s);
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+            const int i = g + G * r;
+            if (i > k && i < n) {
+                const C vi = (i == k + 1) ? mk<R>(R(1), R(0)) : vrow[i * ld];
+                y[r] = cfms(vi, s, y[r]);
+            }
+        }
+    }
+}
+
+// y <- L^{-H} y (backward substitution) on the column segment.
+template <int G, int RM, typename C, typename R>
+__device__ __forceinline__ void seg_trsm_lowerH(const C* L, int ldl, const R* invd, C (&y)[RM], int n, int g) {
+    for (int k = n - 1; k >= 0; --k) {
+        const int owner = k % G, rk = k / G;
+        C xk = seg_get(y, rk);
+        xk = cscale(xk, invd[k]);
+        if (g == owner) seg_set(y, rk, xk);
+        xk = cshfl(xk, owner, G);
+        const C* lrow = L + k;                     // L(k, i) = lrow[i * ldl], i < k
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+            const int i = g + G * r;
+            if (i < k) y[r] = cfms(cconj(lrow[i * ldl]), xk, y[r]);
+        }
+    }
+}
+
 }  // namespace sbg

@@ -26,7 +26,7 @@ namespace sbg {
 namespace {
 
 constexpr const char* kTableMagic = "SBGTUNE";
-constexpr int kTableVersion = 2;
+constexpr int kTableVersion = 3;
 constexpr const char* kLibVersion = "sbg-geneig-0.1";
 
 std::mutex g_mu;
@@ -34,7 +34,7 @@ std::map<std::tuple<int, int, int>, Schedule> g_in_process;   // (device, n, pre
 
 bool fits(int n, int precision, const Schedule& s) {
     const size_t lim = static_cast<size_t>(max_smem_optin());
-    if (reduce_smem_bytes(kReduceFull, n) > lim || back_smem_bytes(n) > lim) return false;
+    if (reduce_smem_bytes(kReduceFull, n) > lim || back_smem_bytes(n) > lim || hetrd_smem_bytes(n) > lim) return false;
     const bool single = precision == SBG_PRECISION_MIXED;
     if (ql_chain_smem_bytes(n, s.chain_threads, single) > lim) return false;
     if (ql_apply_smem_bytes(n, s.ql_warps, single) > lim) return false;
@@ -90,7 +90,7 @@ bool load_table(const std::string& path, const std::string& key, std::vector<Tab
         std::istringstream es(lines[i]);
         std::string tag;
         TableEntry e{};
-        es >> tag >> e.n >> e.precision >> e.s.reduce_threads >> e.s.back_threads >> e.s.ql_warps >>
+        es >> tag >> e.n >> e.precision >> e.s.reduce_threads >> e.s.hetrd_threads >> e.s.back_threads >> e.s.ql_warps >>
             e.s.chain_threads >> e.s.refine_threads >> e.us;
         if (tag != "entry" || !es) { out.clear(); return false; }
         out.push_back(e);
@@ -118,7 +118,8 @@ void save_table(const std::string& path, const std::string& key, const std::vect
     body << kTableMagic << " " << kTableVersion << "\n";
     body << "device " << key << "\n";
     for (const auto& e : entries)
-        body << "entry " << e.n << " " << e.precision << " " << e.s.reduce_threads << " " << e.s.back_threads << " "
+        body << "entry " << e.n << " " << e.precision << " " << e.s.reduce_threads << " " << e.s.hetrd_threads << " "
+             << e.s.back_threads << " "
              << e.s.ql_warps << " " << e.s.chain_threads << " " << e.s.refine_threads << " " << e.us << "\n";
     const std::string b = body.str();
     char buf[32];
@@ -211,7 +212,8 @@ struct Bench {
             launch_ql_logged(n, count, ws, w(), x(), inf(), false, s.chain_threads, s.ql_warps, st);
     }
     void full(const Schedule& s) {
-        launch_reduce(kReduceFull, a(), b(), n, count, ws, nullptr, inf(), s.reduce_threads, st);
+        launch_reduce(kReduceFull, a(), b(), n, count, ws, x(), inf(), s.reduce_threads, st);
+        launch_hetrd(n, count, x(), ws, inf(), s.hetrd_threads, st);
         eig(s);
         launch_back(kBackFull, n, count, ws, x(), inf(), s.back_threads, st);
     }
@@ -252,9 +254,19 @@ bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double&
     {
         double bt = 1e30;
         for (int t : thread_opts) {
-            double ms = median_ms([&] { launch_reduce(kReduceFull, bench.a(), bench.b(), n, count, bench.ws, nullptr,
+            double ms = median_ms([&] { launch_reduce(kReduceFull, bench.a(), bench.b(), n, count, bench.ws, bench.x(),
                                                       bench.inf(), t, bench.st); }, 3, bench.st);
             if (ms < bt) { bt = ms; win.reduce_threads = t; }
+        }
+        t_total += bt;
+    }
+    // k_hetrd (reads C from X, which k_reduce just wrote; idempotent)
+    {
+        double bt = 1e30;
+        for (int t : thread_opts) {
+            double ms = median_ms([&] { launch_hetrd(n, count, bench.x(), bench.ws, bench.inf(), t, bench.st); },
+                                  3, bench.st);
+            if (ms < bt) { bt = ms; win.hetrd_threads = t; }
         }
         t_total += bt;
     }
@@ -321,8 +333,9 @@ bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double&
     }
     best = win;
     best_us = 1e3 * t_total / count;
-    std::fprintf(stderr, "[sbg autotune] n=%d precision=%d: reduce=%d back=%d ql_chain=%d ql_apply_warps=%d refine=%d "
-                 "(%.3f us/pair)\n", n, precision, win.reduce_threads, win.back_threads, win.chain_threads,
+    std::fprintf(stderr, "[sbg autotune] n=%d precision=%d: reduce=%d hetrd=%d back=%d ql_chain=%d ql_apply_warps=%d "
+                 "refine=%d (%.3f us/pair)\n", n, precision, win.reduce_threads, win.hetrd_threads, win.back_threads,
+                 win.chain_threads,
                  win.ql_warps, win.refine_threads, best_us);
     return true;
 }
@@ -332,6 +345,7 @@ bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double&
 Schedule default_schedule(int n, int precision) {
     Schedule s;
     s.reduce_threads = n > 24 ? 256 : 128;
+    s.hetrd_threads = n > 24 ? 256 : 128;
     s.back_threads = n > 24 ? 256 : 128;
     s.refine_threads = n > 24 ? 256 : 128;
     s.ql_warps = n <= 32 ? 8 : (n <= 64 ? 4 : 2);
@@ -367,7 +381,8 @@ TuneResult select_schedule(const TuneRequest& req) {
     if (req.force_threads) {
         if (req.force_threads != 128 && req.force_threads != 256)
             throw std::runtime_error("force_block_dim_x must be 128 or 256");
-        r.sched.reduce_threads = r.sched.back_threads = r.sched.refine_threads = req.force_threads;
+        r.sched.reduce_threads = r.sched.hetrd_threads = r.sched.back_threads = r.sched.refine_threads =
+            req.force_threads;
     }
     if (req.force_ql_warps) {
         if (req.force_ql_warps < 1 || req.force_ql_warps > 16) throw std::runtime_error("batches_per_block must be 1..16");

@@ -17,12 +17,14 @@ namespace sbg {
 
 struct Schedule {
     int reduce_threads = 256;   // threads per CTA of k_reduce
+    int hetrd_threads = 256;    // threads per CTA of k_hetrd
     int back_threads = 256;     // threads per CTA of k_back
     int ql_warps = 4;           // pairs (warps) per CTA of the QL rotation-application kernel
     int chain_threads = 128;    // pairs (threads) per CTA of the QL scalar-chain kernel
     int refine_threads = 256;   // threads per CTA of k_refine (mixed form)
     bool operator==(const Schedule& o) const {
-        return reduce_threads == o.reduce_threads && back_threads == o.back_threads && ql_warps == o.ql_warps &&
+        return reduce_threads == o.reduce_threads && hetrd_threads == o.hetrd_threads &&
+               back_threads == o.back_threads && ql_warps == o.ql_warps &&
                chain_threads == o.chain_threads && refine_threads == o.refine_threads;
     }
 };

@@ -157,12 +157,16 @@ class Solver:
     def enable_stage_timing(self, enable: bool = True) -> None:
         _check(self._lib.sbg_solver_enable_stage_timing(self._h, int(enable)), "sbg_solver_enable_stage_timing")
 
+    STAGES = ("reduce", "tridiag", "eig", "back")
+
     def read_stage_times(self):
-        """{stage: (ms, kernel launches)} for stages reduce, eig, back since the last read."""
-        ms = (ctypes.c_double * 3)()
-        nl = (ctypes.c_int * 3)()
+        """{stage: (ms, kernel launches)} since the last read, for the stages
+        reduce (potrf + two-sided reduction), tridiag (Householder), eig (QL /
+        QL + refinement) and back (Q Z and L^{-H})."""
+        ms = (ctypes.c_double * 4)()
+        nl = (ctypes.c_int * 4)()
         _check(self._lib.sbg_solver_read_stage_times(self._h, ms, nl), "sbg_solver_read_stage_times")
-        return {k: (ms[i], nl[i]) for i, k in enumerate(("reduce", "eig", "back"))}
+        return {k: (ms[i], nl[i]) for i, k in enumerate(self.STAGES)}
 
     def reserve(self, pairs: int, stream_slots: int = 1) -> None:
         _check(self._lib.sbg_solver_reserve(self._h, pairs, stream_slots), "sbg_solver_reserve")
