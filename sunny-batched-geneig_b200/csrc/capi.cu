@@ -238,7 +238,7 @@ int supported_max_n(int precision) {
     int best = 0;
     for (int n = 1; n <= 256; ++n) {
         size_t need = std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, n), sbg::back_smem_bytes(n));
-        need = std::max(need, sbg::hetrd_smem_bytes(n));
+        need = std::max(need, sbg::hetrd_smem_bytes(n, 128));
         need = std::max(need, sbg::ql_apply_smem_bytes(n, 1, precision == SBG_PRECISION_MIXED));
         need = std::max(need, sbg::ql_chain_smem_bytes(n, 32, precision == SBG_PRECISION_MIXED));
         if (precision == SBG_PRECISION_MIXED) need = std::max(need, sbg::refine_smem_bytes(n, 128));

@@ -60,7 +60,7 @@ __device__ inline bool wait_copies(uint64_t* bar, int* info_word) {
 
 // ----------------------------------------------------------------------------- k_reduce
 template <int T, int G, int RM>
-__global__ void __launch_bounds__(T, T == 256 ? 2 : 1) k_reduce(int mode, const double2* __restrict__ A,
+__global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_reduce(int mode, const double2* __restrict__ A,
                                               const double2* __restrict__ B, int n, int batch,
                                               Workspace ws, double2* __restrict__ out,
                                               int* __restrict__ info) {
@@ -181,15 +181,15 @@ __global__ void __launch_bounds__(T, T == 256 ? 2 : 1) k_reduce(int mode, const 
 // One CTA per pair, one tile: C (lower triangle) staged by TMA bulk copies, reduced
 // to tridiagonal form; the reflectors go to the upper part of the pair's LV tile.
 struct HetrdSmem {
-    size_t As, vbuf, pbuf, wbuf, sh, d, e, tau, bar, total;
-    __host__ __device__ HetrdSmem(int n) {
+    size_t As, vw, pbuf, ww, d, e, tau, bar, total;
+    __host__ __device__ HetrdSmem(int n, int threads) {
         const size_t ld = static_cast<size_t>(tile_ld(n));
+        const size_t nw = static_cast<size_t>(threads / 32);
         size_t o = 0;
         As = o;   o += 16 * ld * n;
-        vbuf = o; o += 16 * n;
+        vw = o;   o += 16 * n * nw;
         pbuf = o; o += 32 * n;
-        wbuf = o; o += 16 * n;
-        sh = o;   o += 32;
+        ww = o;   o += 16 * n * nw;
         d = o;    o += align_up(8 * n, 16);
         e = o;    o += align_up(8 * n, 16);
         tau = o;  o += 16 * n;
@@ -197,7 +197,6 @@ struct HetrdSmem {
         total = o;
     }
 };
-
 template <int T>
 __global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __restrict__ C, Workspace ws,
                                              const int* __restrict__ info) {
@@ -205,13 +204,12 @@ __global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __
     if (b >= batch) return;
     if (info[b] != 0) return;
     extern __shared__ __align__(16) unsigned char smem[];
-    const HetrdSmem lay(n);
+    const HetrdSmem lay(n, T);
     const int ld = tile_ld(n);
     double2* As = reinterpret_cast<double2*>(smem + lay.As);
-    double2* vbuf = reinterpret_cast<double2*>(smem + lay.vbuf);
+    double2* vw = reinterpret_cast<double2*>(smem + lay.vw);
     double2* pbuf = reinterpret_cast<double2*>(smem + lay.pbuf);
-    double2* wbuf = reinterpret_cast<double2*>(smem + lay.wbuf);
-    double2* sh = reinterpret_cast<double2*>(smem + lay.sh);
+    double2* ww = reinterpret_cast<double2*>(smem + lay.ww);
     double* d_s = reinterpret_cast<double*>(smem + lay.d);
     double* e_s = reinterpret_cast<double*>(smem + lay.e);
     double2* tau_s = reinterpret_cast<double2*>(smem + lay.tau);
@@ -228,7 +226,7 @@ __global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __
             bulk_g2s(As + j + static_cast<size_t>(j) * ld, Cb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
     }
     wait_copies(bar, nullptr);
-    hetrd_lower(As, ld, n, d_s, e_s, tau_s, vbuf, pbuf, wbuf, sh);
+    hetrd_lower(As, ld, n, d_s, e_s, tau_s, vw, pbuf, ww);
     // reflector k, component i >= k+2, sits at A(i, k); it goes to LV(k, i)
     double2* LVg = ws.LV + mat * b;
     for (size_t idx = tid; idx < mat; idx += T) {
@@ -236,6 +234,53 @@ __global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __
         if (i >= k + 2) LVg[k + static_cast<size_t>(i) * n] = As[i + k * ld];
     }
     for (int i = tid; i < n; i += T) {
+        ws.d[static_cast<size_t>(n) * b + i] = d_s[i];
+        ws.e[static_cast<size_t>(n) * b + i] = e_s[i];
+        ws.tau[static_cast<size_t>(n) * b + i] = (i + 1 < n) ? tau_s[i] : make_double2(0.0, 0.0);
+    }
+}
+
+// ----------------------------------------------------------------------------- k_hetrd_warp
+// One WARP per pair (n <= 65): C's lower triangle is bulk-copied column by column into
+// a packed lower-triangular tile (n(n+1)/2 complex; 23.8 KB at n = 54, so eight pairs
+// fit an SM) and reduced by hetrd_warp_packed with warp-level synchronisation only.
+__host__ __device__ inline size_t hetrd_warp_bytes(int n) {
+    return align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16) + 16 * 2 * n + 2 * align_up(8 * n, 16) + 16 * n + 16;
+}
+constexpr int kHetrdWarpsPerCta = 2;
+constexpr int kHetrdWarpMaxN = 65;
+
+__global__ void __launch_bounds__(32 * kHetrdWarpsPerCta) k_hetrd_warp(int n, int batch, const double2* __restrict__ C,
+                                                                      Workspace ws, const int* __restrict__ info) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * kHetrdWarpsPerCta + warp;
+    if (b >= batch) return;
+    if (info[b] != 0) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned char* base = smem + hetrd_warp_bytes(n) * warp;
+    double2* P = reinterpret_cast<double2*>(base);
+    double2* vb = reinterpret_cast<double2*>(base + align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16));
+    double2* wb = vb + n;
+    double* d_s = reinterpret_cast<double*>(wb + n);
+    double* e_s = d_s + align_up(8 * n, 16) / 8;
+    double2* tau_s = reinterpret_cast<double2*>(e_s + align_up(8 * n, 16) / 8);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tau_s + n);
+    const size_t mat = static_cast<size_t>(n) * n;
+    const double2* Cb = C + mat * b;
+    if (lane == 0) { mbar_init(bar, 1); fence_mbar_init(); }
+    __syncwarp();
+    if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(16 * (static_cast<size_t>(n) * (n + 1) / 2)));
+    __syncwarp();
+    for (int j = lane; j < n; j += 32)
+        bulk_g2s(P + pk(j, n), Cb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
+    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) mbar_wait_bounded(bar, 0, kMaxPolls);
+    hetrd_warp_packed<double>(P, n, d_s, e_s, tau_s, vb, wb);
+    double2* LVg = ws.LV + mat * b;
+    for (int k = 0; k + 2 < n; ++k) {
+        const double2* col = P + pk(k, n) - k;           // col[i] = A(i, k), i >= k
+        for (int i = k + 2 + lane; i < n; i += 32) LVg[k + static_cast<size_t>(i) * n] = col[i];
+    }
+    for (int i = lane; i < n; i += 32) {
         ws.d[static_cast<size_t>(n) * b + i] = d_s[i];
         ws.e[static_cast<size_t>(n) * b + i] = e_s[i];
         ws.tau[static_cast<size_t>(n) * b + i] = (i + 1 < n) ? tau_s[i] : make_double2(0.0, 0.0);
@@ -390,41 +435,90 @@ __global__ void k_ql_chain(int n, int batch, Workspace ws, double* __restrict__ 
 }
 
 // ----------------------------------------------------------------------------- k_ql_apply
-// One warp per pair: Z = I, then every logged rotation applied to the rows the lane
-// owns (r = lane + 32 q), Z row-major in shared memory with an odd leading
-// dimension.  The log is read 32 entries at a time (one coalesced load, staged in
-// shared memory, read back by broadcast); within a sweep the rotation at column i
-// only needs z_i loaded, z_{i+1} being carried in a register.  Columns are written
-// out in the sorted order of the eigenvalues.  A pair whose log overflowed is
-// solved here by the warp-per-pair QL instead.
+// Applies each pair's rotation log to Z = I.  Rows of Z are independent, so a pair
+// gets ceil(n / 32) warps and every lane owns ONE row (Z row-major in shared memory,
+// odd leading dimension); the warps of a pair stream the log independently and never
+// synchronise with each other.  The log is read 32 entries at a time (one coalesced
+// load, staged in a per-warp shared buffer, read back by broadcast); within a sweep
+// the rotation at column i loads z_i and carries z_{i+1} in a register.  Columns are
+// written out in the sorted order of the eigenvalues.  A pair whose log overflowed is
+// solved by the warp-per-pair QL on warp 0 of that pair instead.
 template <typename R>
-__host__ __device__ inline size_t ql_apply_warp_bytes(int n) {
-    return align_up(sizeof(R) * static_cast<size_t>(n) * tile_ld(n), 16) + 2 * 32 * sizeof(cplx<R>) +
-           align_up(sizeof(R) * 2 * n, 16);
+__host__ __device__ inline size_t ql_apply_pair_bytes(int n) {
+    const int wpp = (n + 31) / 32;
+    return align_up(sizeof(R) * static_cast<size_t>(n) * tile_ld(n), 16) +
+           static_cast<size_t>(wpp) * 2 * 32 * sizeof(cplx<R>) + align_up(sizeof(R) * 2 * n, 16);
 }
 
 template <typename R>
 __global__ void k_ql_apply(int n, int batch, Workspace ws, double* __restrict__ W, double2* __restrict__ X,
                            int* __restrict__ info) {
     using C = cplx<R>;
-    constexpr int MAXQ = 3;
+    const int wpp = (n + 31) / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (b >= batch) return;
-    if (info[b] > n || info[b] < 0) return;
+    const int pair_in_cta = warp / wpp, wip = warp - pair_in_cta * wpp;
+    const int pairs_per_cta = (blockDim.x >> 5) / wpp;
+    const int b = blockIdx.x * pairs_per_cta + pair_in_cta;
     extern __shared__ __align__(16) unsigned char smem[];
     const int ldz = tile_ld(n);
-    unsigned char* base = smem + ql_apply_warp_bytes<R>(n) * warp;
+    unsigned char* base = smem + ql_apply_pair_bytes<R>(n) * pair_in_cta;
     R* Z = reinterpret_cast<R*>(base);
-    C* stage = reinterpret_cast<C*>(base + align_up(sizeof(R) * static_cast<size_t>(n) * ldz, 16));
-    R* dd = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(stage) + 2 * 32 * sizeof(C));
+    C* stage = reinterpret_cast<C*>(base + align_up(sizeof(R) * static_cast<size_t>(n) * ldz, 16)) + wip * 64;
+    R* dd = reinterpret_cast<R*>(base + align_up(sizeof(R) * static_cast<size_t>(n) * ldz, 16) +
+                                 static_cast<size_t>(wpp) * 2 * 32 * sizeof(C));
     R* ee = dd + n;
-    const size_t mat = static_cast<size_t>(n) * n;
-    for (int r = lane; r < n; r += 32)
-        for (int c = 0; c < n; ++c) Z[r * ldz + c] = (r == c) ? R(1) : R(0);
-    const int* perm = ws.perm + static_cast<size_t>(n) * b;
-    bool identity_perm = false;
-    if (ws.flag[b]) {
+    const bool live = b < batch && !(info[min(b, batch - 1)] > n || info[min(b, batch - 1)] < 0);
+    const int row = wip * 32 + lane;
+    const bool own = live && row < n;
+    R* zrow = Z + row * ldz;
+    if (own)
+        for (int c = 0; c < n; ++c) zrow[c] = (row == c) ? R(1) : R(0);
+    __syncthreads();      // every row is initialised before a fallback warp rotates all of them
+    const bool fallback = live && ws.flag[b] != 0;
+    if (live && !fallback) {
+        const C* log = reinterpret_cast<const C*>(ws.log) + static_cast<size_t>(ws.log_cap) * b;
+        const int cap = ws.log_cap;
+        int loaded = 0, buf = 0, remaining = 0, col = 0;
+        C pre = log[lane];
+        R carry = R(0);
+        bool done = false;
+        while (!done) {
+            stage[buf * 32 + lane] = pre;
+            __syncwarp();
+            loaded += 32;
+            if (loaded < cap) pre = log[min(loaded + lane, cap - 1)];
+            const C* st = stage + buf * 32;
+            int k = 0;
+            while (k < 32) {
+                if (remaining == 0) {
+                    const C h = st[k++];
+                    const int top = static_cast<int>(h.x);
+                    if (top < 0) { done = true; break; }
+                    remaining = static_cast<int>(h.y);
+                    col = top;
+                    if (own && remaining > 0) carry = zrow[col + 1];
+                    continue;
+                }
+                const int take = min(remaining, 32 - k);
+                if (own) {
+                    for (int t = 0; t < take; ++t) {
+                        const C cs = st[k + t];
+                        const R zi = zrow[col - t];
+                        zrow[col - t + 1] = fma(cs.y, zi, cs.x * carry);
+                        carry = fma(cs.x, zi, -cs.y * carry);
+                    }
+                }
+                k += take;
+                col -= take;
+                remaining -= take;
+                if (remaining == 0 && own) zrow[col + 1] = carry;
+            }
+            __syncwarp();
+            buf ^= 1;
+            if (!done && loaded >= cap) done = true;      // malformed log guard (never reached)
+        }
+    }
+    if (fallback && wip == 0) {
         for (int i = lane; i < n; i += 32) {
             dd[i] = static_cast<R>(ws.d[static_cast<size_t>(n) * b + i]);
             ee[i] = static_cast<R>(ws.e[static_cast<size_t>(n) * b + i]);
@@ -433,70 +527,13 @@ __global__ void k_ql_apply(int n, int batch, Workspace ws, double* __restrict__ 
         const int unconv = tridiag_ql<R>(n, dd, ee, Z, ldz);
         for (int i = lane; i < n; i += 32) W[static_cast<size_t>(n) * b + i] = static_cast<double>(dd[i]);
         if (lane == 0 && unconv) info[b] = unconv;
-        identity_perm = true;
-    } else {
-        __syncwarp();
-        const C* log = reinterpret_cast<const C*>(ws.log) + static_cast<size_t>(ws.log_cap) * b;
-        int p = 0;                         // next entry to consume
-        int loaded = 0;                    // entries [loaded - 32, loaded) are staged in buf
-        int buf = 0;
-        C pre = log[lane];                 // prefetched batch
-        int remaining = 0, col = 0;
-        R carry[MAXQ];
-        bool done = false;
-        while (!done) {
-            // stage the prefetched batch, prefetch the next one
-            stage[buf * 32 + lane] = pre;
-            __syncwarp();
-            const int batch_base = loaded;
-            loaded += 32;
-            if (loaded < ws.log_cap) pre = log[min(loaded + lane, ws.log_cap - 1)];
-            for (int k = 0; k < 32 && !done; ++k, ++p) {
-                const C ent = stage[buf * 32 + k];
-                if (remaining == 0) {
-                    const int top = static_cast<int>(ent.x);
-                    if (top < 0) { done = true; break; }
-                    remaining = static_cast<int>(ent.y);
-                    col = top;
-#pragma unroll
-                    for (int q = 0; q < MAXQ; ++q) {
-                        const int r = lane + 32 * q;
-                        if (r < n) carry[q] = Z[r * ldz + col + 1];
-                    }
-                    continue;
-                }
-                const R c = ent.x, s = ent.y;
-#pragma unroll
-                for (int q = 0; q < MAXQ; ++q) {
-                    const int r = lane + 32 * q;
-                    if (r < n) {
-                        R* zr = Z + r * ldz;
-                        const R zi = zr[col], zi1 = carry[q];
-                        zr[col + 1] = fma(s, zi, c * zi1);
-                        carry[q] = fma(c, zi, -s * zi1);
-                    }
-                }
-                --col;
-                if (--remaining == 0) {
-#pragma unroll
-                    for (int q = 0; q < MAXQ; ++q) {
-                        const int r = lane + 32 * q;
-                        if (r < n) Z[r * ldz + col + 1] = carry[q];
-                    }
-                }
-            }
-            (void)batch_base;
-            __syncwarp();
-            buf ^= 1;
-            if (loaded >= ws.log_cap && !done) done = true;   // malformed log guard (never reached)
-        }
-        __syncwarp();
     }
-    R* Zg = reinterpret_cast<R*>(X + mat * b);
-    for (size_t idx = lane; idx < mat; idx += 32) {
-        const int k = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(k) * n);
-        const int src = identity_perm ? k : perm[k];
-        Zg[idx] = Z[r * ldz + src];
+    __syncthreads();      // the fallback's warp wrote every row; all rows are final
+    if (own) {
+        const size_t mat = static_cast<size_t>(n) * n;
+        R* Zg = reinterpret_cast<R*>(X + mat * b);
+        const int* perm = ws.perm + static_cast<size_t>(n) * b;
+        for (int k = 0; k < n; ++k) Zg[row + static_cast<size_t>(k) * n] = zrow[fallback ? k : perm[k]];
     }
 }
 
@@ -519,7 +556,7 @@ struct BackSmem {
 };
 
 template <int T, int G, int RM>
-__global__ void __launch_bounds__(T, T == 256 ? 2 : 1) k_back(int mode, int n, int batch, Workspace ws,
+__global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_back(int mode, int n, int batch, Workspace ws,
                                             double2* __restrict__ X, const int* __restrict__ info) {
     const int b = blockIdx.x;
     if (b >= batch) return;
@@ -633,11 +670,11 @@ size_t tridiag_smem_bytes(int n, int warps_per_cta, bool single) {
 }
 
 // The register-segment kernels: (threads T, lanes per column G, rows per lane RM) by
-// size: n <= 32 -> (256, 8, 4), n <= 64 -> (256, 4, 16), else (512, 4, 22) (n <= 88).
+// size: n <= 32 -> (256, 8, 4), n <= 64 -> (512, 8, 8), else (512, 4, 22) (n <= 88).
 #define SBG_DISPATCH_BY_N(n, KERNEL, ...)                                              \
     do {                                                                               \
         if ((n) <= 32) { KERNEL<256, 8, 4>(__VA_ARGS__); }                             \
-        else if ((n) <= 64) { KERNEL<256, 4, 16>(__VA_ARGS__); }                       \
+        else if ((n) <= 64) { KERNEL<512, 8, 8>(__VA_ARGS__); }                        \
         else { KERNEL<512, 4, 22>(__VA_ARGS__); }                                      \
     } while (0)
 
@@ -667,12 +704,20 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
     return cudaGetLastError();
 }
 
-size_t hetrd_smem_bytes(int n) { return HetrdSmem(n).total; }
+size_t hetrd_smem_bytes(int n, int threads) { return HetrdSmem(n, threads).total; }
 
 cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, const int* info, int threads,
                          cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
-    const size_t smem = hetrd_smem_bytes(n);
+    if (n <= kHetrdWarpMaxN) {
+        const size_t smem = hetrd_warp_bytes(n) * kHetrdWarpsPerCta;
+        static std::once_flag fw;
+        set_max_smem_once(k_hetrd_warp, fw);
+        const int grid = (batch + kHetrdWarpsPerCta - 1) / kHetrdWarpsPerCta;
+        k_hetrd_warp<<<grid, 32 * kHetrdWarpsPerCta, smem, stream>>>(n, batch, C, ws, info);
+        return cudaGetLastError();
+    }
+    const size_t smem = hetrd_smem_bytes(n, threads == 128 ? 128 : 256);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     static std::once_flag f128, f256;
     if (threads == 128) {
@@ -702,8 +747,9 @@ size_t refine_smem_bytes(int n, int threads) { return RefineSmem(n, threads / 32
 size_t ql_chain_smem_bytes(int n, int threads, bool single) {
     return (single ? 4 : 8) * 2 * static_cast<size_t>(n) * threads;
 }
-size_t ql_apply_smem_bytes(int n, int warps_per_cta, bool single) {
-    return (single ? ql_apply_warp_bytes<float>(n) : ql_apply_warp_bytes<double>(n)) * warps_per_cta;
+// pairs_per_cta pairs of ceil(n / 32) warps each share a CTA.
+size_t ql_apply_smem_bytes(int n, int pairs_per_cta, bool single) {
+    return (single ? ql_apply_pair_bytes<float>(n) : ql_apply_pair_bytes<double>(n)) * pairs_per_cta;
 }
 
 cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
@@ -714,18 +760,19 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
     if (cs > static_cast<size_t>(max_smem_optin()) || as > static_cast<size_t>(max_smem_optin()))
         return cudaErrorInvalidValue;
     const int cgrid = (batch + chain_threads - 1) / chain_threads;
-    const int agrid = (batch + apply_warps - 1) / apply_warps;
+    const int agrid = (batch + apply_warps - 1) / apply_warps;     // apply_warps = pairs per CTA
+    const int athreads = 32 * ((n + 31) / 32) * apply_warps;
     static std::once_flag fcd, fcf, fad, faf;
     if (single) {
         set_max_smem_once(k_ql_chain<float>, fcf);
         set_max_smem_once(k_ql_apply<float>, faf);
         k_ql_chain<float><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info);
-        k_ql_apply<float><<<agrid, 32 * apply_warps, as, stream>>>(n, batch, ws, W, X, info);
+        k_ql_apply<float><<<agrid, athreads, as, stream>>>(n, batch, ws, W, X, info);
     } else {
         set_max_smem_once(k_ql_chain<double>, fcd);
         set_max_smem_once(k_ql_apply<double>, fad);
         k_ql_chain<double><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info);
-        k_ql_apply<double><<<agrid, 32 * apply_warps, as, stream>>>(n, batch, ws, W, X, info);
+        k_ql_apply<double><<<agrid, athreads, as, stream>>>(n, batch, ws, W, X, info);
     }
     return cudaGetLastError();
 }

@@ -61,7 +61,7 @@ cudaError_t launch_tridiag_ql(int n, int batch, const Workspace& ws, double* W, 
 // reflectors into ws.LV (rows above the superdiagonal), tau, d, e.  Pairs with info != 0 skip.
 cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, const int* info, int threads,
                          cudaStream_t stream);
-size_t hetrd_smem_bytes(int n);
+size_t hetrd_smem_bytes(int n, int threads);
 // Two-kernel QL: thread-per-pair scalar chain logging rotations, then a warp-per-pair
 // application of the log to Z (single = FP32 chain and Z, the mixed form's first half).
 cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,

@@ -126,108 +126,98 @@ __device__ void trsm_right_lowerH(const cplx<R>* L, int ldl, const R* invd, cplx
 // H_k = I - tau_k v_k v_k^H with v_k = (0_{k+1}, 1, A(k+2:n, k)) stored in place.
 // Outputs d[0:n], e[0:n-1] (real), tau[0:n-1].  The steps are LAPACK zhetd2's
 // (reflector as zlarfg, p = tau A22 v, w = p - tau/2 (p^H v) v,
-// A22 -= v w^H + w v^H); the team splits the Hermitian matvec into a row walk
-// over the lower part and a column walk over the mirrored upper part.
-// Scratch: vbuf, wbuf (n complex), pbuf (2n complex), sh (2 complex).
+// A22 -= v w^H + w v^H).  Two CTA barriers per step: every warp computes the
+// reflector and w itself (into its own slices of vw / ww, n complex per warp), so no
+// warp waits on another for those; the barriers only separate the Hermitian matvec
+// (a row walk over the lower part and a column walk over the mirrored upper part,
+// partial sums in pbuf, 2n complex) from the rank-2 update, and the update from the
+// next step.
 template <typename R>
 __device__ void hetrd_lower(cplx<R>* A, int lda, int n, R* d, R* e, cplx<R>* tau,
-                            cplx<R>* vbuf, cplx<R>* pbuf, cplx<R>* wbuf, cplx<R>* sh) {
+                            cplx<R>* vw_all, cplx<R>* pbuf, cplx<R>* ww_all) {
     using C = cplx<R>;
     const int tid = threadIdx.x, T = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5;
+    C* vw = vw_all + warp * n;
+    C* ww = ww_all + warp * n;
     for (int k = 0; k + 1 < n; ++k) {
         const int m = n - k - 1;
         C* x = A + (k + 1) + k * lda;                    // x[0..m) = A(k+1:n, k)
-        if (warp == 0) {
-            R s2 = R(0);
-            for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
-            s2 = warp_sum(s2);
-            const C alpha = x[0];
-            C tk, scale;
-            R beta;
-            if (s2 == R(0) && alpha.y == R(0)) {
-                tk = mk<R>(R(0), R(0)); beta = alpha.x; scale = mk<R>(R(0), R(0));
-            } else {
-                const R nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
-                beta = alpha.x >= R(0) ? -nrm : nrm;
-                tk = mk<R>((beta - alpha.x) / beta, -alpha.y / beta);
-                const R ar = alpha.x - beta, ai = alpha.y;   // scale = 1 / (alpha - beta)
-                const R den = ar * ar + ai * ai;
-                scale = mk<R>(ar / den, -ai / den);
-            }
-            if (tk.x != R(0) || tk.y != R(0)) {
-                for (int i = 1 + lane; i < m; i += 32) {
-                    const C vi = cmul(x[i], scale);
-                    x[i] = vi; vbuf[i] = vi;
-                }
-            }
-            if (lane == 0) {
-                vbuf[0] = mk<R>(R(1), R(0));
-                sh[0] = tk;
-                e[k] = beta;
-                tau[k] = tk;
-            }
+        // ---- reflector (every warp)
+        R s2 = R(0);
+        for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
+        s2 = warp_sum(s2);
+        const C alpha = x[0];
+        C tk, scale;
+        R beta;
+        if (s2 == R(0) && alpha.y == R(0)) {
+            tk = mk<R>(R(0), R(0)); beta = alpha.x; scale = mk<R>(R(0), R(0));
+        } else {
+            const R nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
+            beta = alpha.x >= R(0) ? -nrm : nrm;
+            tk = mk<R>((beta - alpha.x) / beta, -alpha.y / beta);
+            const R ar = alpha.x - beta, ai = alpha.y;   // scale = 1 / (alpha - beta)
+            const R den = ar * ar + ai * ai;
+            scale = mk<R>(ar / den, -ai / den);
         }
-        __syncthreads();
-        const C tk = sh[0];
-        if (tk.x == R(0) && tk.y == R(0)) {               // H_k = I; keep the diagonal real
-            if (tid == 0) A[(k + 1) + (k + 1) * lda].y = R(0);
-            __syncthreads();
-            continue;
-        }
+        if (tid == 0) { e[k] = beta; tau[k] = tk; }
+        if (tk.x == R(0) && tk.y == R(0)) continue;      // H_k = I (uniform: same value in every warp)
+        for (int i = lane; i < m; i += 32) vw[i] = (i == 0) ? mk<R>(R(1), R(0)) : cmul(x[i], scale);
+        __syncwarp();
+        // ---- p partial sums: part 0 = sum_{j<=r} A22(r,j) v_j, part 1 = sum_{j>r} conj(A22(j,r)) v_j
         C* A22 = A + (k + 1) + (k + 1) * lda;
-        // p partial sums: part 0 = sum_{j<=r} A22(r,j) v_j, part 1 = sum_{j>r} conj(A22(j,r)) v_j
         for (int t = tid; t < 2 * m; t += T) {
             const int part = t >= m, r = t - part * m;
             C acc0 = mk<R>(R(0), R(0)), acc1 = mk<R>(R(0), R(0));
             if (part == 0) {
                 int j = 0;
                 for (; j + 1 < r; j += 2) {
-                    acc0 = cfma(A22[r + j * lda], vbuf[j], acc0);
-                    acc1 = cfma(A22[r + (j + 1) * lda], vbuf[j + 1], acc1);
+                    acc0 = cfma(A22[r + j * lda], vw[j], acc0);
+                    acc1 = cfma(A22[r + (j + 1) * lda], vw[j + 1], acc1);
                 }
-                for (; j < r; ++j) acc0 = cfma(A22[r + j * lda], vbuf[j], acc0);
+                for (; j < r; ++j) acc0 = cfma(A22[r + j * lda], vw[j], acc0);
                 const R drr = A22[r + r * lda].x;
-                acc0.x = fma(drr, vbuf[r].x, acc0.x);
-                acc0.y = fma(drr, vbuf[r].y, acc0.y);
+                acc0.x = fma(drr, vw[r].x, acc0.x);
+                acc0.y = fma(drr, vw[r].y, acc0.y);
             } else {
                 const C* col = A22 + r * lda;
                 int j = r + 1;
                 for (; j + 1 < m; j += 2) {
-                    acc0 = cfmac(col[j], vbuf[j], acc0);
-                    acc1 = cfmac(col[j + 1], vbuf[j + 1], acc1);
+                    acc0 = cfmac(col[j], vw[j], acc0);
+                    acc1 = cfmac(col[j + 1], vw[j + 1], acc1);
                 }
-                for (; j < m; ++j) acc0 = cfmac(col[j], vbuf[j], acc0);
+                for (; j < m; ++j) acc0 = cfmac(col[j], vw[j], acc0);
             }
             pbuf[t] = cadd(acc0, acc1);
         }
         __syncthreads();
-        if (warp == 0) {
-            // p = tau (part0 + part1); alpha2 = -tau/2 (p^H v); w = p + alpha2 v
-            C dot = mk<R>(R(0), R(0));
-            for (int r = lane; r < m; r += 32) {
-                const C p = cmul(tk, cadd(pbuf[r], pbuf[m + r]));
-                wbuf[r] = p;
-                dot = cfmac(p, vbuf[r], dot);
-            }
-            dot.x = warp_sum(dot.x);
-            dot.y = warp_sum(dot.y);
-            const C a2 = cscale(cmul(tk, dot), R(-0.5));
-            for (int r = lane; r < m; r += 32) wbuf[r] = cfma(a2, vbuf[r], wbuf[r]);
+        // the scaled reflector replaces x (nobody reads column k after the barrier above)
+        if (warp == 0)
+            for (int i = 1 + lane; i < m; i += 32) x[i] = vw[i];
+        // ---- p = tau (part0 + part1); alpha2 = -tau/2 (p^H v); w = p + alpha2 v (every warp)
+        C dot = mk<R>(R(0), R(0));
+        for (int r = lane; r < m; r += 32) {
+            const C p = cmul(tk, cadd(pbuf[r], pbuf[m + r]));
+            ww[r] = p;
+            dot = cfmac(p, vw[r], dot);
         }
-        __syncthreads();
-        // A22 -= v w^H + w v^H on the lower triangle; thread (row r, column chunk c)
+        dot.x = warp_sum(dot.x);
+        dot.y = warp_sum(dot.y);
+        const C a2 = cscale(cmul(tk, dot), R(-0.5));
+        for (int r = lane; r < m; r += 32) ww[r] = cfma(a2, vw[r], ww[r]);
+        __syncwarp();
+        // ---- A22 -= v w^H + w v^H on the lower triangle; thread (row r, column chunk c)
         {
             const int chunks = max(1, T / m);
             const int cw = (m + chunks - 1) / chunks;
             for (int t = tid; t < m * chunks; t += T) {
                 const int r = t % m, c = t / m;
-                const C vr = vbuf[r], wr = wbuf[r];
+                const C vr = vw[r], wr = ww[r];
                 const int j0 = c * cw, j1 = min(r + 1, (c + 1) * cw);
                 for (int j = j0; j < j1; ++j) {
                     C a = A22[r + j * lda];
-                    a = cfmsc(vr, wbuf[j], a);
-                    a = cfmsc(wr, vbuf[j], a);
+                    a = cfmsc(vr, ww[j], a);
+                    a = cfmsc(wr, vw[j], a);
                     if (j == r) a.y = R(0);
                     A22[r + j * lda] = a;
                 }
@@ -674,9 +664,10 @@ __device__ __forceinline__ void seg_trsm_lower(const C* L, int ldl, const R* inv
         wk = cshfl(wk, owner, G);
         const C* lk = L + k * ldl;
 #pragma unroll
-        for (int r = 0; r < RM; ++r) {
+        for (int r = RM - 1; r >= 0; --r) {          // active rows i > k form a suffix of r
             const int i = g + G * r;
-            if (i > k && i < n) y[r] = cfms(lk[i], wk, y[r]);
+            if (i <= k) break;
+            if (i < n) y[r] = cfms(lk[i], wk, y[r]);
         }
     }
 }
@@ -693,9 +684,10 @@ __device__ __forceinline__ void seg_trsm_right_lowerH(const C* L, int ldl, const
         ck = cshfl(ck, owner, G);
         const C* lk = L + k * ldl;
 #pragma unroll
-        for (int r = 0; r < RM; ++r) {
+        for (int r = RM - 1; r >= 0; --r) {          // active columns k < kk <= i
             const int kk = g + G * r;
-            if (kk > k && kk <= i) y[r] = cfmsc(ck, lk[kk], y[r]);
+            if (kk <= k) break;
+            if (kk <= i) y[r] = cfmsc(ck, lk[kk], y[r]);
         }
     }
 }
@@ -710,9 +702,10 @@ __device__ __forceinline__ void seg_apply_q(const C* LV, int ld, const C* tau, C
         const C* vrow = LV + k;                    // v_k(i) = LV(k, i) = vrow[i * ld], i >= k + 2
         C s = mk<R>(R(0), R(0));
 #pragma unroll
-        for (int r = 0; r < RM; ++r) {
+        for (int r = RM - 1; r >= 0; --r) {          // active rows i > k form a suffix of r
             const int i = g + G * r;
-            if (i > k && i < n) {
+            if (i <= k) break;
+            if (i < n) {
                 const C vi = (i == k + 1) ? mk<R>(R(1), R(0)) : vrow[i * ld];
                 s = cfmac(vi, y[r], s);
             }
@@ -721,9 +714,10 @@ __device__ __forceinline__ void seg_apply_q(const C* LV, int ld, const C* tau, C
         s.y = group_sum(s.y, G);
         s = cmul(tk, s);
 #pragma unroll
-        for (int r = 0; r < RM; ++r) {
+        for (int r = RM - 1; r >= 0; --r) {
             const int i = g + G * r;
-            if (i > k && i < n) {
+            if (i <= k) break;
+            if (i < n) {
                 const C vi = (i == k + 1) ? mk<R>(R(1), R(0)) : vrow[i * ld];
                 y[r] = cfms(vi, s, y[r]);
             }
@@ -742,11 +736,117 @@ __device__ __forceinline__ void seg_trsm_lowerH(const C* L, int ldl, const R* in
         xk = cshfl(xk, owner, G);
         const C* lrow = L + k;                     // L(k, i) = lrow[i * ldl], i < k
 #pragma unroll
-        for (int r = 0; r < RM; ++r) {
+        for (int r = 0; r < RM; ++r) {               // active rows i < k form a prefix of r
             const int i = g + G * r;
-            if (i < k) y[r] = cfms(cconj(lrow[i * ldl]), xk, y[r]);
+            if (i >= k) break;
+            y[r] = cfms(cconj(lrow[i * ldl]), xk, y[r]);
         }
     }
+}
+
+// ============================================================================ hetrd, one warp, packed
+// Column-major packed lower triangle: A(i, j), i >= j, at P[pk(j, n) + i - j].
+__host__ __device__ __forceinline__ int pk(int j, int n) { return j * n - (j * (j - 1)) / 2; }
+
+// The Householder tridiagonalisation of hetrd_lower (LAPACK zhetd2's steps) run by ONE
+// warp on a packed lower triangle, for n <= 65: at step k lane L owns trailing rows
+// L and m-1-L (m = n-k-1), which balances both the Hermitian matvec (m terms per row)
+// and the rank-2 update (r+1 terms for row r).  Only __syncwarp is needed.  The
+// scaled reflector replaces A(k+2:n, k).  vb, wb: m complex of scratch each.
+template <typename R>
+__device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, cplx<R>* vb, cplx<R>* wb) {
+    using C = cplx<R>;
+    const int lane = threadIdx.x & 31;
+    for (int k = 0; k + 1 < n; ++k) {
+        const int m = n - k - 1;
+        C* x = P + pk(k, n) + 1;                        // x[i] = A(k+1+i, k)
+        R s2 = R(0);
+        for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
+        s2 = warp_sum(s2);
+        const C alpha = x[0];
+        C tk, scale;
+        R beta;
+        if (s2 == R(0) && alpha.y == R(0)) {
+            tk = mk<R>(R(0), R(0)); beta = alpha.x; scale = mk<R>(R(0), R(0));
+        } else {
+            const R nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
+            beta = alpha.x >= R(0) ? -nrm : nrm;
+            tk = mk<R>((beta - alpha.x) / beta, -alpha.y / beta);
+            const R ar = alpha.x - beta, ai = alpha.y;
+            const R den = ar * ar + ai * ai;
+            scale = mk<R>(ar / den, -ai / den);
+        }
+        if (lane == 0) { e[k] = beta; tau[k] = tk; }
+        if (tk.x == R(0) && tk.y == R(0)) continue;
+        for (int i = lane; i < m; i += 32) {
+            const C v = (i == 0) ? mk<R>(R(1), R(0)) : cmul(x[i], scale);
+            vb[i] = v;
+            if (i > 0) x[i] = v;
+        }
+        __syncwarp();
+        // trailing matrix A22(r, j) = A(k+1+r, k+1+j): column j starts at P + pk(k+1+j, n)
+        const int base = k + 1;
+        const int h = (m + 1) >> 1;
+        const int r1 = lane, r2 = m - 1 - lane;
+        const bool own1 = lane < h;
+        const bool own2 = lane < h && r2 != r1;
+        // ---- p = tau A22 v for the owned rows
+        C p1 = mk<R>(R(0), R(0)), p2 = mk<R>(R(0), R(0));
+        if (own1) {
+            C a0 = mk<R>(R(0), R(0)), a1 = mk<R>(R(0), R(0));
+            for (int j = 0; j < r1; ++j) a0 = cfma(P[pk(base + j, n) + r1 - j], vb[j], a0);      // lower, row walk
+            const C* col = P + pk(base + r1, n);                                                  // column r1
+            a1.x = fma(col[0].x, vb[r1].x, a1.x);
+            a1.y = fma(col[0].x, vb[r1].y, a1.y);
+            for (int j = r1 + 1; j < m; ++j) a1 = cfmac(col[j - r1], vb[j], a1);                // mirrored upper
+            p1 = cmul(tk, cadd(a0, a1));
+        }
+        if (own2) {
+            C a0 = mk<R>(R(0), R(0)), a1 = mk<R>(R(0), R(0));
+            for (int j = 0; j < r2; ++j) a0 = cfma(P[pk(base + j, n) + r2 - j], vb[j], a0);
+            const C* col = P + pk(base + r2, n);
+            a1.x = fma(col[0].x, vb[r2].x, a1.x);
+            a1.y = fma(col[0].x, vb[r2].y, a1.y);
+            for (int j = r2 + 1; j < m; ++j) a1 = cfmac(col[j - r2], vb[j], a1);
+            p2 = cmul(tk, cadd(a0, a1));
+        }
+        // ---- w = p - tau/2 (p^H v) v
+        C dot = mk<R>(R(0), R(0));
+        if (own1) dot = cfmac(p1, vb[r1], dot);
+        if (own2) dot = cfmac(p2, vb[r2], dot);
+        dot.x = warp_sum(dot.x);
+        dot.y = warp_sum(dot.y);
+        const C a2 = cscale(cmul(tk, dot), R(-0.5));
+        C w1 = mk<R>(R(0), R(0)), w2 = mk<R>(R(0), R(0));
+        if (own1) { w1 = cfma(a2, vb[r1], p1); wb[r1] = w1; }
+        if (own2) { w2 = cfma(a2, vb[r2], p2); wb[r2] = w2; }
+        __syncwarp();
+        // ---- A22 -= v w^H + w v^H on the lower triangle of the owned rows
+        if (own1) {
+            const C v1 = vb[r1];
+            for (int j = 0; j <= r1; ++j) {
+                C* a = P + pk(base + j, n) + r1 - j;
+                C t = cfmsc(v1, wb[j], *a);
+                t = cfmsc(w1, vb[j], t);
+                if (j == r1) t.y = R(0);
+                *a = t;
+            }
+        }
+        if (own2) {
+            const C v2 = vb[r2];
+            for (int j = 0; j <= r2; ++j) {
+                C* a = P + pk(base + j, n) + r2 - j;
+                C t = cfmsc(v2, wb[j], *a);
+                t = cfmsc(w2, vb[j], t);
+                if (j == r2) t.y = R(0);
+                *a = t;
+            }
+        }
+        __syncwarp();
+    }
+    for (int i = lane; i < n; i += 32) d[i] = P[pk(i, n)].x;
+    if (lane == 0 && n >= 1) e[n - 1] = R(0);
+    __syncwarp();
 }
 
 }  // namespace sbg

@@ -34,7 +34,7 @@ std::map<std::tuple<int, int, int>, Schedule> g_in_process;   // (device, n, pre
 
 bool fits(int n, int precision, const Schedule& s) {
     const size_t lim = static_cast<size_t>(max_smem_optin());
-    if (reduce_smem_bytes(kReduceFull, n) > lim || back_smem_bytes(n) > lim || hetrd_smem_bytes(n) > lim) return false;
+    if (reduce_smem_bytes(kReduceFull, n) > lim || back_smem_bytes(n) > lim || hetrd_smem_bytes(n, s.hetrd_threads) > lim) return false;
     const bool single = precision == SBG_PRECISION_MIXED;
     if (ql_chain_smem_bytes(n, s.chain_threads, single) > lim) return false;
     if (ql_apply_smem_bytes(n, s.ql_warps, single) > lim) return false;

@@ -235,5 +235,7 @@ def test_near_goldstone_both_forms(oracle_mod):
         W, X, info = run(54, A, B, prec)
         assert (info == 0).all()
         s = Mx.summarize(A, B, W, X, Wr, Xr, 54)
-        assert (np.abs(W - Wr) / scale).max() < 1e-12, (prec, s)
+        err = np.abs(W - Wr) / scale
+        at = np.unravel_index(int(err.argmax()), err.shape)
+        assert err.max() < 1e-12, (prec, float(err.max()), at, float(W[at]), float(Wr[at]), float(cond[at]), s)
         assert s["residual"] < 1e-12 and s["orth"] < 1e-9, (prec, s)
