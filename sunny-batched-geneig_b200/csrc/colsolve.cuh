@@ -1,0 +1,155 @@
+// Column-per-thread stage functions for n <= NMAX (NMAX = 32 or 64).
+//
+// One thread owns a whole column (or row) of the n x n operand in registers,
+// y[0..NMAX).  Every sweep over the rows is a switch fall-through chain: it enters
+// at the first active row (n - 1 or k - 1, the same for every thread of the warp),
+// each case handles one row with a compile-time register index, and a `break` out
+// of the switch ends the sweep at the active range's edge.  The pivot a
+// substitution needs next is carried out of the sweep in a register, so no dynamic
+// register index is ever formed, and each value that becomes final is stored
+// straight to its destination.  L and the Householder reflectors are read from
+// shared memory; all threads of the CTA read the same address at the same time
+// (a broadcast).
+//
+// Packed lower-triangular tiles use column-major packing: A(i, j), i >= j, at
+// P[pk(j, n) + i - j] (pk in stages.cuh).
+#pragma once
+
+#include "stages.cuh"
+
+// Row-slot sequences, descending: SBG_DESC64(C) expands to C(63) C(62) ... C(0).
+#define SBG_DESC64(C) C(63) C(62) C(61) C(60) C(59) C(58) C(57) C(56) C(55) C(54) C(53) C(52) C(51) C(50) C(49) C(48) C(47) C(46) C(45) C(44) C(43) C(42) C(41) C(40) C(39) C(38) C(37) C(36) C(35) C(34) C(33) C(32) C(31) C(30) C(29) C(28) C(27) C(26) C(25) C(24) C(23) C(22) C(21) C(20) C(19) C(18) C(17) C(16) C(15) C(14) C(13) C(12) C(11) C(10) C(9) C(8) C(7) C(6) C(5) C(4) C(3) C(2) C(1) C(0)
+#define SBG_DESC32(C) C(31) C(30) C(29) C(28) C(27) C(26) C(25) C(24) C(23) C(22) C(21) C(20) C(19) C(18) C(17) C(16) C(15) C(14) C(13) C(12) C(11) C(10) C(9) C(8) C(7) C(6) C(5) C(4) C(3) C(2) C(1) C(0)
+// Cases I >= NMAX are never entered (the entry row is < n <= NMAX); their bodies are
+// discarded at compile time.
+#define SBG_SWEEP(NMAX, C) SBG_DESC64(C)
+
+namespace sbg {
+
+// ---------------------------------------------------------------- potrf, one warp, packed
+// Right-looking lower Cholesky of the packed tile P by one warp (n <= 65): at column k
+// lane L scales row k+1+L (and k+1+m-1-L) of column k, then updates the trailing rows it
+// owns (balanced pairs, as in hetrd_warp_packed).  invd[k] = 1 / L_kk.  Returns 0 or the
+// order of the first non-positive (or NaN) leading minor, the zpotrf convention.
+template <typename R>
+__device__ int potrf_warp_packed(cplx<R>* P, int n, R* invd) {
+    using C = cplx<R>;
+    const int lane = threadIdx.x & 31;
+    for (int k = 0; k < n; ++k) {
+        C* colk = P + pk(k, n);                   // colk[i - k] = A(i, k), i >= k
+        const R dkk = colk[0].x;
+        if (!(dkk > R(0))) return k + 1;          // uniform: every lane reads the same word
+        const R dsq = sqrt(dkk);
+        const R inv = R(1) / dsq;
+        const int m = n - k - 1;
+        __syncwarp();
+        if (lane == 0) { colk[0] = mk<R>(dsq, R(0)); invd[k] = inv; }
+        for (int i = 1 + lane; i <= m; i += 32) colk[i] = cscale(colk[i], inv);
+        __syncwarp();
+        // trailing A22(r, j) -= l_r conj(l_j), l = colk[1..m], j <= r
+        const int base = k + 1;
+        const int h = (m + 1) >> 1;
+        const int r1 = lane, r2 = m - 1 - lane;
+        if (lane < h) {
+            const C l1 = colk[1 + r1];
+            for (int j = 0; j <= r1; ++j) {
+                C* a = P + pk(base + j, n) + r1 - j;
+                *a = cfmsc(l1, colk[1 + j], *a);
+            }
+            if (r2 != r1) {
+                const C l2 = colk[1 + r2];
+                for (int j = 0; j <= r2; ++j) {
+                    C* a = P + pk(base + j, n) + r2 - j;
+                    *a = cfmsc(l2, colk[1 + j], *a);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------- forward substitution
+// y <- L^{-1} y for the thread's column; L packed (Lp) in shared memory.  Each solved
+// entry w_k is stored through out(k, w_k) as soon as it is final.
+template <int NMAX, typename R, typename Out>
+__device__ __forceinline__ void col_trsm_lower(const cplx<R>* Lp, const R* invd, cplx<R> (&y)[NMAX], int n,
+                                               Out&& out) {
+    using C = cplx<R>;
+    C piv = y[0];
+    for (int k = 0; k < n; ++k) {
+        const C wk = cscale(piv, invd[k]);
+        out(k, wk);
+        const C* lk = Lp + pk(k, n) - k;          // lk[i] = L(i, k)
+        // rows n-1 .. k+1; the last one updated (k + 1) is the next pivot
+#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { if ((I) <= k) break; y[I] = cfms(lk[I], wk, y[I]); piv = y[I]; }
+        switch (n - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
+#undef SBG_SLOT
+    }
+}
+
+// Row i of C = W L^{-H}, columns kk <= i (the rest is not needed: C is Hermitian).
+// y holds W(i, 0..i); the solved C(i, k) go through out(k, c).
+template <int NMAX, typename R, typename Out>
+__device__ __forceinline__ void row_trsm_right_lowerH(const cplx<R>* Lp, const R* invd, cplx<R> (&y)[NMAX], int n,
+                                                      int i, Out&& out) {
+    using C = cplx<R>;
+    C piv = y[0];
+    for (int k = 0; k <= i; ++k) {
+        const C ck = cscale(piv, invd[k]);
+        out(k, ck);
+        const C* lk = Lp + pk(k, n) - k;          // lk[kk] = L(kk, k)
+        // columns n-1 .. k+1, only kk <= i change; the last one (k + 1) is the next pivot
+#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { if ((I) <= k) break; \
+                                     if ((I) <= i) { y[I] = cfmsc(ck, lk[I], y[I]); piv = y[I]; } }
+        switch (n - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
+#undef SBG_SLOT
+    }
+}
+
+// y <- Q y, Q = H_0 ... H_{n-2}, reflectors along the rows of the LV tile (ld); the
+// superdiagonal entry LV(k, k+1) holds v_k(k+1) = 1.
+template <int NMAX, typename R>
+__device__ __forceinline__ void col_apply_q(const cplx<R>* LV, int ld, const cplx<R>* tau, cplx<R> (&y)[NMAX], int n) {
+    using C = cplx<R>;
+    for (int k = n - 2; k >= 0; --k) {
+        const C tk = tau[k];
+        if (tk.x == R(0) && tk.y == R(0)) continue;
+        const C* vtop = LV + k + (n - 1) * ld;   // v_k(i) at LV + k + i * ld, i >= k + 1; walked downwards
+        C s0 = mk<R>(R(0), R(0)), s1 = mk<R>(R(0), R(0));
+        const C* pv = vtop;
+#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { if ((I) <= k) break; \
+        if ((I) & 1) s1 = cfmac(*pv, y[I], s1); else s0 = cfmac(*pv, y[I], s0); pv -= ld; }
+        switch (n - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
+#undef SBG_SLOT
+        const C s = cmul(tk, cadd(s0, s1));
+        pv = vtop;
+#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { if ((I) <= k) break; y[I] = cfms(*pv, s, y[I]); pv -= ld; }
+        switch (n - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
+#undef SBG_SLOT
+    }
+}
+
+// x = L^{-H} y (backward substitution), L full lower in the LV tile (ld); each x_k
+// goes through out(k, x_k) as soon as it is final.
+template <int NMAX, typename R, typename Out>
+__device__ __forceinline__ void col_trsm_lowerH(const cplx<R>* LV, int ld, const R* invd, cplx<R> (&y)[NMAX], int n,
+                                                Out&& out) {
+    using C = cplx<R>;
+    C piv = y[0];
+#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { piv = y[I]; } break;
+    switch (n - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
+#undef SBG_SLOT
+    for (int k = n - 1; k >= 0; --k) {
+        const C xk = cscale(piv, invd[k]);
+        out(k, xk);
+        const C* pl = LV + k + (k - 1) * ld;     // L(k, i) at LV + k + i * ld, i < k; walked downwards
+        // rows k-1 .. 0; the first one updated (k - 1) is the next pivot
+#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { y[I] = cfms(cconj(*pl), xk, y[I]); pl -= ld; \
+                                                        if ((I) == k - 1) piv = y[I]; }
+        switch (k - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
+#undef SBG_SLOT
+    }
+}
+
+}  // namespace sbg

@@ -13,6 +13,7 @@
 // resident), while the BLAS2/BLAS3-shaped stages run a CTA per pair.
 #include "kernels.cuh"
 #include "stages.cuh"
+#include "colsolve.cuh"
 
 #include <cstdlib>
 #include <mutex>
@@ -177,6 +178,176 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_reduce(int mode, const d
     if (tid == 0) info[b] = 0;
 }
 
+struct BackSmem {
+    size_t LVs, invd, tau, bar, total;
+    __host__ __device__ BackSmem(int n) {
+        const size_t ld = static_cast<size_t>(tile_ld(n));
+        size_t o = 0;
+        LVs = o;  o += 16 * ld * n;
+        invd = o; o += align_up(8 * n, 16);
+        tau = o;  o += 16 * n;
+        bar = o;  o += 16;
+        total = o;
+    }
+};
+
+// ----------------------------------------------------------------------------- k_potrf_warp
+// One WARP per pair (n <= 64): B's lower triangle bulk-copied into a packed tile,
+// Cholesky by potrf_warp_packed; L goes to `out` (strict upper zeroed, the staged
+// Cholesky) or to the lower triangle of the pair's LV tile (the full solve).
+__host__ __device__ inline size_t potrf_warp_bytes(int n) {
+    return align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16) + align_up(8 * n, 16) + 16;
+}
+constexpr int kPotrfWarpsPerCta = 2;
+constexpr int kColMaxN = 56;      // column-per-thread kernels: y[NMAX] in registers, NMAX in {32, 48, 56}
+
+__global__ void __launch_bounds__(32 * kPotrfWarpsPerCta) k_potrf_warp(int mode, const double2* __restrict__ B, int n,
+                                                                      int batch, Workspace ws, double2* __restrict__ out,
+                                                                      int* __restrict__ info) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * kPotrfWarpsPerCta + warp;
+    if (b >= batch) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned char* base = smem + potrf_warp_bytes(n) * warp;
+    double2* P = reinterpret_cast<double2*>(base);
+    double* invd = reinterpret_cast<double*>(base + align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(invd) + align_up(8 * n, 16));
+    const size_t mat = static_cast<size_t>(n) * n;
+    const double2* Bb = B + mat * b;
+    if (lane == 0) { mbar_init(bar, 1); fence_mbar_init(); }
+    __syncwarp();
+    if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(16 * (static_cast<size_t>(n) * (n + 1) / 2)));
+    __syncwarp();
+    for (int j = lane; j < n; j += 32)
+        bulk_g2s(P + pk(j, n), Bb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
+    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) mbar_wait_bounded(bar, 0, kMaxPolls);
+    const int st = potrf_warp_packed<double>(P, n, invd);
+    if (st != 0) {
+        if (lane == 0) info[b] = (mode == kReduceFull) ? n + st : st;
+        return;
+    }
+    __syncwarp();
+    double2* dst = (mode == kReduceChol) ? out + mat * b : ws.LV + mat * b;
+    for (int j = 0; j < n; ++j) {
+        const double2* col = P + pk(j, n) - j;     // col[i] = L(i, j), i >= j
+        for (int i = lane; i < n; i += 32) {
+            if (i >= j) dst[i + static_cast<size_t>(j) * n] = col[i];
+            else if (mode == kReduceChol) dst[i + static_cast<size_t>(j) * n] = make_double2(0.0, 0.0);
+        }
+    }
+    if (lane == 0) info[b] = 0;
+}
+
+// ----------------------------------------------------------------------------- k_hegst_col
+// One CTA of NMAX threads per pair (n <= NMAX): C = L^{-1} A L^{-H}.  Thread j solves
+// column j of W = L^{-1} A in registers and stores it to the pair's X slice (in L2);
+// after the barrier thread i reads row i of W back and solves row i of C = W L^{-H},
+// columns k <= i, writing C's lower triangle over its own row.  Only the packed L
+// lives in shared memory.  kReduceHegst also zeroes the strict upper triangle.
+__host__ __device__ inline size_t hegst_col_bytes(int n) {
+    return align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16) + align_up(8 * n, 16) + 16;
+}
+
+template <int NMAX>
+__global__ void __launch_bounds__(NMAX, 4) k_hegst_col(int mode, const double2* __restrict__ A, const Workspace ws,
+                                                    double2* __restrict__ out, int n, int batch,
+                                                    const int* __restrict__ info) {
+    const int b = blockIdx.x;
+    if (b >= batch) return;
+    if (info[b] != 0) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double2* Lp = reinterpret_cast<double2*>(smem);
+    double* invd = reinterpret_cast<double*>(smem + align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(reinterpret_cast<unsigned char*>(invd) + align_up(8 * n, 16));
+    const int tid = threadIdx.x;
+    const size_t mat = static_cast<size_t>(n) * n;
+    const double2* Lg = ws.LV + mat * b;
+    const double2* Ab = A + mat * b;
+    double2* Ob = out + mat * b;
+    if (tid == 0) { mbar_init(bar, 1); fence_mbar_init(); }
+    __syncthreads();
+    if (tid < 32) {
+        if (tid == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(16 * (static_cast<size_t>(n) * (n + 1) / 2)));
+        __syncwarp();
+        for (int j = tid; j < n; j += 32)
+            bulk_g2s(Lp + pk(j, n), Lg + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
+    }
+    const bool own = tid < n;
+    double2 y[NMAX];
+#pragma unroll
+    for (int i = 0; i < NMAX; ++i)
+        y[i] = (own && i < n) ? Ab[i + static_cast<size_t>(tid) * n] : make_double2(0.0, 0.0);
+    wait_copies(bar, nullptr);
+    for (int i = tid; i < n; i += NMAX) invd[i] = 1.0 / Lp[pk(i, n)].x;
+    __syncthreads();
+    if (own) col_trsm_lower<NMAX>(Lp, invd, y, n, [&](int k, double2 w) { Ob[k + static_cast<size_t>(tid) * n] = w; });
+    __syncthreads();
+    if (own) {
+        const int i = tid;
+#pragma unroll
+        for (int kk = 0; kk < NMAX; ++kk) y[kk] = (kk <= i) ? Ob[i + static_cast<size_t>(kk) * n] : make_double2(0.0, 0.0);
+        row_trsm_right_lowerH<NMAX>(Lp, invd, y, n, i, [&](int k, double2 c) {
+            if (k == i) c.y = 0.0;
+            Ob[i + static_cast<size_t>(k) * n] = c;
+        });
+        if (mode == kReduceHegst)
+            for (int k = i + 1; k < n; ++k) Ob[i + static_cast<size_t>(k) * n] = make_double2(0.0, 0.0);
+    }
+}
+
+// ----------------------------------------------------------------------------- k_back_col
+// One CTA of NMAX threads per pair (n <= NMAX): thread j holds column j of Z in
+// registers, applies Q and L^{-H}, and stores X(:, j) (kBackQOnly: Q Z).
+template <int NMAX>
+__global__ void __launch_bounds__(NMAX, 4) k_back_col(int mode, int n, int batch, Workspace ws,
+                                                   double2* __restrict__ X, const int* __restrict__ info) {
+    const int b = blockIdx.x;
+    if (b >= batch) return;
+    const size_t mat = static_cast<size_t>(n) * n;
+    double2* Xb = X + mat * b;
+    const int tid = threadIdx.x;
+    if (info[b] > n || info[b] < 0) {
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        for (size_t idx = tid; idx < mat; idx += NMAX) Xb[idx] = make_double2(nan, nan);
+        return;
+    }
+    extern __shared__ __align__(16) unsigned char smem[];
+    const BackSmem lay(n);
+    const int ld = tile_ld(n);
+    double2* LVs = reinterpret_cast<double2*>(smem + lay.LVs);
+    double* invd = reinterpret_cast<double*>(smem + lay.invd);
+    double2* tau_s = reinterpret_cast<double2*>(smem + lay.tau);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + lay.bar);
+    const double2* LVg = ws.LV + mat * b;
+    if (tid == 0) { mbar_init(bar, 1); fence_mbar_init(); }
+    __syncthreads();
+    if (tid < 32) {
+        if (tid == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(16 * mat));
+        __syncwarp();
+        for (int j = tid; j < n; j += 32)
+            bulk_g2s(LVs + static_cast<size_t>(j) * ld, LVg + static_cast<size_t>(j) * n, 16u * n, bar);
+    }
+    const bool own = tid < n;
+    const double* Zg = reinterpret_cast<const double*>(Xb);
+    double2 y[NMAX];
+#pragma unroll
+    for (int i = 0; i < NMAX; ++i)
+        y[i] = make_double2((own && i < n) ? Zg[i + static_cast<size_t>(tid) * n] : 0.0, 0.0);
+    for (int i = tid; i < n; i += NMAX) tau_s[i] = ws.tau[static_cast<size_t>(n) * b + i];
+    wait_copies(bar, nullptr);
+    for (int i = tid; i < n; i += NMAX) invd[i] = 1.0 / LVs[i + i * ld].x;
+    __syncthreads();               // all of Z is in registers before any X is stored over it
+    if (!own) return;
+    col_apply_q<NMAX, double>(LVs, ld, tau_s, y, n);
+    double2* xcol = Xb + static_cast<size_t>(tid) * n;
+    if (mode == kBackFull) {
+        col_trsm_lowerH<NMAX>(LVs, ld, invd, y, n, [&](int k, double2 x) { xcol[k] = x; });
+    } else {
+#pragma unroll
+        for (int i = 0; i < NMAX; ++i) if (i < n) xcol[i] = y[i];
+    }
+}
+
 // ----------------------------------------------------------------------------- k_hetrd
 // One CTA per pair, one tile: C (lower triangle) staged by TMA bulk copies, reduced
 // to tridiagonal form; the reflectors go to the upper part of the pair's LV tile.
@@ -232,6 +403,7 @@ __global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __
     for (size_t idx = tid; idx < mat; idx += T) {
         const int i = static_cast<int>(idx / n), k = static_cast<int>(idx - static_cast<size_t>(i) * n);
         if (i >= k + 2) LVg[k + static_cast<size_t>(i) * n] = As[i + k * ld];
+        else if (i == k + 1) LVg[k + static_cast<size_t>(i) * n] = make_double2(1.0, 0.0);
     }
     for (int i = tid; i < n; i += T) {
         ws.d[static_cast<size_t>(n) * b + i] = d_s[i];
@@ -276,9 +448,10 @@ __global__ void __launch_bounds__(32 * kHetrdWarpsPerCta) k_hetrd_warp(int n, in
     if (!mbar_wait_bounded(bar, 0, kMaxPolls)) mbar_wait_bounded(bar, 0, kMaxPolls);
     hetrd_warp_packed<double>(P, n, d_s, e_s, tau_s, vb, wb);
     double2* LVg = ws.LV + mat * b;
-    for (int k = 0; k + 2 < n; ++k) {
+    for (int k = 0; k + 1 < n; ++k) {                    // LV(k, k+1) = v_k(k+1) = 1
         const double2* col = P + pk(k, n) - k;           // col[i] = A(i, k), i >= k
-        for (int i = k + 2 + lane; i < n; i += 32) LVg[k + static_cast<size_t>(i) * n] = col[i];
+        for (int i = k + 1 + lane; i < n; i += 32)
+            LVg[k + static_cast<size_t>(i) * n] = (i == k + 1) ? make_double2(1.0, 0.0) : col[i];
     }
     for (int i = lane; i < n; i += 32) {
         ws.d[static_cast<size_t>(n) * b + i] = d_s[i];
@@ -381,12 +554,58 @@ __global__ void __launch_bounds__(T) k_refine(int n, int batch, Workspace ws, do
         double* t = Za; Za = Zb; Zb = t;
         if (em < 1e-15) break;                       // uniform: em is the same on every thread
     }
+    // Acceptance: every refined pair must satisfy ||T z - lam z|| <= 256 eps ||T||_F ||z||.  When the
+    // FP32 start was too coarse for the refinement to separate eigenvalues (e.g. small eigenvalues
+    // of a T with a wide spectrum: FP32 resolves them only to ~6e-8 ||T||), the pair is solved by
+    // the FP64 QL here instead.
+    double worst = 0.0, tn = 0.0;
+    for (int i = tid; i < n; i += T) tn = fma(dT[i], dT[i], (i + 1 < n) ? fma(2.0 * eT[i], eT[i], tn) : tn);
+    for (int c = tid; c < n; c += T) {
+        const double* z = Za + c * ld;
+        double r2 = 0.0, z2 = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double v = (dT[i] - lam[c]) * z[i];
+            if (i > 0) v = fma(eT[i - 1], z[i - 1], v);
+            if (i + 1 < n) v = fma(eT[i], z[i + 1], v);
+            r2 = fma(v, v, r2);
+            z2 = fma(z[i], z[i], z2);
+        }
+        worst = fmax(worst, sqrt(r2 / fmax(z2, 1e-300)));
+    }
+    tn = warp_sum(tn);
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) worst = fmax(worst, shfl_xor(worst, m));
+    if ((tid & 31) == 0) { red[4 * (tid >> 5)] = tn; red[4 * (tid >> 5) + 1] = worst; }
+    __syncthreads();
+    double tnorm = 0.0, rmax = 0.0;
+    for (int w = 0; w < T / 32; ++w) { tnorm += red[4 * w]; rmax = fmax(rmax, red[4 * w + 1]); }
+    __syncthreads();
+    const bool fallback = !(rmax <= 256.0 * 1.1102230246251565e-16 * sqrt(tnorm));
+    if (fallback) {
+        // FP64 QL on (d, e) with Za read as a row-major tile (Za[r * ld + c] = Z(r, c))
+        for (int idx = tid; idx < n * ld; idx += T) Za[idx] = 0.0;
+        __syncthreads();
+        for (int i = tid; i < n; i += T) Za[i * ld + i] = 1.0;
+        __syncthreads();
+        if (tid < 32) {
+            const int unconv = tridiag_ql<double>(n, dT, eT, Za, ld);
+            if (tid == 0 && unconv) info[b] = unconv;
+        }
+        __syncthreads();
+        const size_t mat2 = static_cast<size_t>(n) * n;
+        double* Zg2 = reinterpret_cast<double*>(X + mat2 * b);
+        for (size_t idx = tid; idx < mat2; idx += T) {
+            const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
+            Zg2[idx] = Za[r * ld + c];
+        }
+        for (int i = tid; i < n; i += T) W[static_cast<size_t>(n) * b + i] = dT[i];
+        return;
+    }
     // ascending order (the FP32 order can differ for near-equal eigenvalues)
     if (tid == 0) {
         for (int i = 0; i + 1 < n; ++i) {
             int k = i;
             for (int j = i + 1; j < n; ++j) if (lam[j] < lam[k]) k = j;
-            red[0] = 0.0;
             if (k != i) { const double t = lam[i]; lam[i] = lam[k]; lam[k] = t; }
             reinterpret_cast<int*>(TZ)[i] = k;       // swap record
         }
@@ -542,18 +761,6 @@ __global__ void k_ql_apply(int n, int batch, Workspace ws, double* __restrict__ 
 // of G lanes (lane g owns rows g + G r), read straight from the X buffer; only the
 // LV tile (L below, reflectors above the superdiagonal) is staged in shared memory
 // by TMA bulk copies.  The result is written over Z.
-struct BackSmem {
-    size_t LVs, invd, tau, bar, total;
-    __host__ __device__ BackSmem(int n) {
-        const size_t ld = static_cast<size_t>(tile_ld(n));
-        size_t o = 0;
-        LVs = o;  o += 16 * ld * n;
-        invd = o; o += align_up(8 * n, 16);
-        tau = o;  o += 16 * n;
-        bar = o;  o += 16;
-        total = o;
-    }
-};
 
 template <int T, int G, int RM>
 __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_back(int mode, int n, int batch, Workspace ws,
@@ -694,10 +901,36 @@ void run_back(int mode, int n, int batch, const Workspace& ws, double2* X, const
     k_back<T, G, RM><<<batch, T, smem, stream>>>(mode, n, batch, ws, X, info);
 }
 
+template <int NMAX>
+void run_hegst_col(int mode, const double2* A, const Workspace& ws, double2* out, int n, int batch, const int* info,
+                   cudaStream_t stream) {
+    static std::once_flag f;
+    set_max_smem_once(k_hegst_col<NMAX>, f);
+    k_hegst_col<NMAX><<<batch, NMAX, hegst_col_bytes(n), stream>>>(mode, A, ws, out, n, batch, info);
+}
+
 cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, int batch,
                           const Workspace& ws, double2* out, int* info, int /*threads*/, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
+    if (!B || !info) return cudaErrorInvalidValue;
+    if ((mode == kReduceChol || mode == kReduceHegst || mode == kReduceFull) && !out) return cudaErrorInvalidValue;
+    if ((mode == kReduceHegst || mode == kReduceFull) && !A) return cudaErrorInvalidValue;
+    if ((mode == kReduceFull || mode == kReduceFromLM) && !ws.LV) return cudaErrorInvalidValue;
     if (n > 84) return cudaErrorInvalidValue;
+    // The two-kernel path hands L from k_potrf_warp to k_hegst_col through ws.LV, so it
+    // needs a workspace (the staged Cholesky alone does not).
+    if (n <= kColMaxN && mode != kReduceFromLM && (mode == kReduceChol || ws.LV != nullptr)) {
+        static std::once_flag fp;
+        set_max_smem_once(k_potrf_warp, fp);
+        const int grid = (batch + kPotrfWarpsPerCta - 1) / kPotrfWarpsPerCta;
+        k_potrf_warp<<<grid, 32 * kPotrfWarpsPerCta, potrf_warp_bytes(n) * kPotrfWarpsPerCta, stream>>>(
+            mode, B, n, batch, ws, out, info);
+        if (mode == kReduceChol) return cudaGetLastError();
+        if (n <= 32) run_hegst_col<32>(mode, A, ws, out, n, batch, info, stream);
+        else if (n <= 48) run_hegst_col<48>(mode, A, ws, out, n, batch, info, stream);
+        else run_hegst_col<56>(mode, A, ws, out, n, batch, info, stream);
+        return cudaGetLastError();
+    }
     const size_t smem = reduce_smem_bytes(mode, n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     SBG_DISPATCH_BY_N(n, run_reduce, mode, A, B, n, batch, ws, out, info, smem, stream);
@@ -709,6 +942,7 @@ size_t hetrd_smem_bytes(int n, int threads) { return HetrdSmem(n, threads).total
 cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, const int* info, int threads,
                          cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
+    if (!C || !info || !ws.LV || !ws.d || !ws.e || !ws.tau) return cudaErrorInvalidValue;
     if (n <= kHetrdWarpMaxN) {
         const size_t smem = hetrd_warp_bytes(n) * kHetrdWarpsPerCta;
         static std::once_flag fw;
@@ -755,6 +989,7 @@ size_t ql_apply_smem_bytes(int n, int pairs_per_cta, bool single) {
 cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
                              bool single, int chain_threads, int apply_warps, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
+    if (!W || !X || !info || !ws.d || !ws.e || !ws.log || !ws.perm || !ws.flag) return cudaErrorInvalidValue;
     const size_t cs = ql_chain_smem_bytes(n, chain_threads, single);
     const size_t as = ql_apply_smem_bytes(n, apply_warps, single);
     if (cs > static_cast<size_t>(max_smem_optin()) || as > static_cast<size_t>(max_smem_optin()))
@@ -796,12 +1031,27 @@ cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* 
     return cudaGetLastError();
 }
 
+template <int NMAX>
+void run_back_col(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info, size_t smem,
+                  cudaStream_t stream) {
+    static std::once_flag f;
+    set_max_smem_once(k_back_col<NMAX>, f);
+    k_back_col<NMAX><<<batch, NMAX, smem, stream>>>(mode, n, batch, ws, X, info);
+}
+
 cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
                         int /*threads*/, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
+    if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
     if (n > 84) return cudaErrorInvalidValue;
     const size_t smem = back_smem_bytes(n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+    if (n <= kColMaxN) {
+        if (n <= 32) run_back_col<32>(mode, n, batch, ws, X, info, smem, stream);
+        else if (n <= 48) run_back_col<48>(mode, n, batch, ws, X, info, smem, stream);
+        else run_back_col<56>(mode, n, batch, ws, X, info, smem, stream);
+        return cudaGetLastError();
+    }
     SBG_DISPATCH_BY_N(n, run_back, mode, n, batch, ws, X, info, smem, stream);
     return cudaGetLastError();
 }
