@@ -1,0 +1,683 @@
+// Stage kernels for pairs beyond one SM's shared memory (84 < n <= 256).
+//
+//   k_reduce_big     one CLUSTER of CS CTAs per pair.  Column j of every n x n operand
+//                    lives in CTA j % CS of the cluster (cyclic, so the work of the
+//                    triangular stages is spread evenly), in that CTA's shared memory:
+//                    the lower triangle of B / L packed by columns, and A / W / C as full
+//                    columns.  It runs
+//                      potrf  B = L L^H, right-looking; the pivot column is read by every
+//                             CTA from its owner over DSMEM; one cluster barrier per column;
+//                      hegst  W = L^{-1} A and C = L^{-1} W^H (C is Hermitian, so
+//                             C = (W L^{-H})^H): warp-per-column register solves with L staged
+//                             a panel of columns at a time from the owners over DSMEM; W^H is
+//                             formed through the pair's X buffer (L2-resident);
+//                      hetrd  the owner of column k forms reflector k; every CTA reads it over
+//                             DSMEM, forms its share of the Hermitian matvec from its own
+//                             columns, the shares are summed over DSMEM, and each CTA applies
+//                             the rank-2 update to its own columns (two cluster barriers per
+//                             column);
+//                    and writes L, the reflectors, d, e, tau and info.
+//   k_ql_apply_rows  the QL rotation log applied to one 32-row block of Z per CTA (a pair's
+//                    n x n Z does not fit one SM here); a pair whose log overflowed is solved
+//                    by the warp QL of its first block with Z in the X buffer's second half.
+//   k_back_big       one cluster per pair, each CTA a contiguous block of columns:
+//                    X = L^{-H} Q Z with warp-per-column register solves, the reflectors
+//                    and L staged a panel at a time from ws.LV.  The cluster barrier only
+//                    orders every CTA's read of Z before any write of X (they alias).
+//
+// Workspace use (big n): ws.LV holds L in its lower triangle (diagonal included) and
+// reflector v_k packed along column n-1-k of the strict upper triangle:
+// v_k(k+1+s) = LV(s, n-1-k), s = 0 .. n-2-k (v_k(k+1) = 1 stored explicitly).
+#include "kernels.cuh"
+#include "stages.cuh"
+
+#include <cooperative_groups.h>
+#include <mutex>
+
+namespace cg = cooperative_groups;
+
+namespace sbg {
+
+namespace {
+
+__host__ __device__ inline size_t big_align(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+constexpr int kBigThreads = 256;
+constexpr int kBigWarps = kBigThreads / 32;
+constexpr int kBigPanel = 4;        // L columns / reflectors staged per panel of the register solves
+
+// Own columns of cluster rank r: global j = t * CS + r, t = 0 .. own_cols - 1.
+__host__ __device__ inline int own_cols(int n, int cs, int r) { return n > r ? (n - r + cs - 1) / cs : 0; }
+// Packed offset of own column t (rows j .. n-1 of global column j = t * cs + r).
+__host__ __device__ inline int own_off(int t, int n, int cs, int r) { return t * (n - r) - cs * t * (t - 1) / 2; }
+
+template <typename T>
+__device__ __forceinline__ T* peer(T* p, int rank) {
+    return cg::this_cluster().map_shared_rank(p, static_cast<unsigned>(rank));
+}
+template <int CS>
+__device__ __forceinline__ void cluster_barrier() {
+    if constexpr (CS == 1) __syncthreads();
+    else cg::this_cluster().sync();
+}
+
+// Visits the packed-lower elements (i >= j) of own columns t0 .. nc-1, spread over the
+// CTA's threads: f(t, j, i).
+template <class F>
+__device__ __forceinline__ void for_own_lower(int n, int cs, int r, int t0, int nc, F&& f) {
+    if (t0 >= nc) return;
+    const int base = own_off(t0, n, cs, r);
+    const int total = own_off(nc, n, cs, r) - base;
+    int t = t0, tbeg = 0, tend = n - (t0 * cs + r);          // flat range of column t
+    for (int p = threadIdx.x; p < total; p += blockDim.x) {
+        while (p >= tend) { ++t; tbeg = tend; tend += n - (t * cs + r); }
+        const int j = t * cs + r;
+        f(t, j, j + (p - tbeg));
+    }
+}
+
+__device__ __forceinline__ double2 block_sum2(double2 v, double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v.x = warp_sum(v.x);
+    v.y = warp_sum(v.y);
+    __syncthreads();                     // red is free (its previous readers are done)
+    if (lane == 0) { red[2 * warp] = v.x; red[2 * warp + 1] = v.y; }
+    __syncthreads();
+    double2 s = make_double2(0.0, 0.0);
+    for (int w = 0; w < kBigWarps; ++w) { s.x += red[2 * w]; s.y += red[2 * w + 1]; }
+    return s;
+}
+
+// ----------------------------------------------------------------------------- k_reduce_big
+struct BigReduceSmem {
+    size_t Lp, Cc, panel, invd, sdot, red, misc, bar, total;
+    __host__ __device__ BigReduceSmem(int n, int cs) {
+        const int nc0 = (n + cs - 1) / cs;
+        size_t o = 0;
+        Lp = o;    o += big_align(16 * static_cast<size_t>(own_off(nc0, n, cs, 0)), 16);
+        Cc = o;    o += 16 * static_cast<size_t>(nc0) * n;
+        panel = o; o += 16 * static_cast<size_t>(kBigPanel) * n;      // >= 3 n: v, w, p of hetrd
+        invd = o;  o += big_align(8 * static_cast<size_t>(n), 16);
+        sdot = o;  o += 16 * static_cast<size_t>(nc0);
+        red = o;   o += 16 * kBigWarps;
+        misc = o;  o += 48;                                           // fail flag; tau by step parity
+        bar = o;   o += 16;
+        total = o;
+    }
+};
+
+// y <- L^{-1} y for the warp's columns y[c], c < ncw (rows lane + 32 q in registers),
+// L distributed over the cluster (packed own columns Lp); columns of L are staged a
+// panel at a time into `panel` by the whole CTA.  Every thread of the CTA must call it.
+template <int CS, int RM, int NCW>
+__device__ __forceinline__ void big_lower_solve(double2 (&y)[NCW][RM], int ncw, int n, double2* Lp, double2* panel,
+                                                const double* invd) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int k0 = 0; k0 < n; k0 += kBigPanel) {
+        __syncthreads();                                  // the previous panel is consumed
+        for (int q = 0; q < kBigPanel && k0 + q < n; ++q) {
+            const int k = k0 + q, o = k % CS;
+            const double2* src = peer(Lp, o) + own_off(k / CS, n, CS, o) - k;   // src[i] = L(i, k)
+            for (int i = k + 1 + tid; i < n; i += kBigThreads) panel[q * n + i] = src[i];
+        }
+        __syncthreads();
+        for (int q = 0; q < kBigPanel; ++q) {
+            const int k = k0 + q;
+            if (k >= n) break;
+            const double ik = invd[k];
+            double2 lv[RM];
+#pragma unroll
+            for (int r = 0; r < RM; ++r) {
+                const int i = lane + 32 * r;
+                lv[r] = (i > k && i < n) ? panel[q * n + i] : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int c = 0; c < NCW; ++c) {
+                if (c < ncw) {
+                    double2 piv = cshfl(seg_get(y[c], k >> 5), k & 31);
+                    piv = cscale(piv, ik);
+                    if (lane == (k & 31)) seg_set(y[c], k >> 5, piv);
+#pragma unroll
+                    for (int r = 0; r < RM; ++r)
+                        if (lane + 32 * r > k) y[c][r] = cfms(lv[r], piv, y[c][r]);
+                }
+            }
+        }
+    }
+}
+
+template <int CS, int RM>
+__global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __restrict__ A,
+                                                            const double2* __restrict__ B, int n, int batch,
+                                                            Workspace ws, double2* __restrict__ X,
+                                                            int* __restrict__ info) {
+    constexpr int NCW = ((32 * RM + CS - 1) / CS + kBigWarps - 1) / kBigWarps;   // own columns per warp (max)
+    const int r = CS == 1 ? 0 : static_cast<int>(cg::this_cluster().block_rank());
+    const int b = blockIdx.x / CS;                     // grid = batch * CS: b < batch
+    extern __shared__ __align__(16) unsigned char smem[];
+    const BigReduceSmem lay(n, CS);
+    double2* Lp = reinterpret_cast<double2*>(smem + lay.Lp);
+    double2* Cc = reinterpret_cast<double2*>(smem + lay.Cc);
+    double2* panel = reinterpret_cast<double2*>(smem + lay.panel);
+    double* invd = reinterpret_cast<double*>(smem + lay.invd);
+    double2* sdot = reinterpret_cast<double2*>(smem + lay.sdot);
+    double* red = reinterpret_cast<double*>(smem + lay.red);
+    int* s_fail = reinterpret_cast<int*>(smem + lay.misc);
+    double2* s_tau = reinterpret_cast<double2*>(smem + lay.misc + 16);    // [2]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + lay.bar);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nc = own_cols(n, CS, r);
+    const size_t mat = static_cast<size_t>(n) * n;
+    const double2* Ab = A + mat * b;
+    const double2* Bb = B + mat * b;
+    double2* Xb = X + mat * b;
+    double2* LVb = ws.LV + mat * b;
+    double* db = ws.d + static_cast<size_t>(n) * b;
+    double* eb = ws.e + static_cast<size_t>(n) * b;
+    double2* taub = ws.tau + static_cast<size_t>(n) * b;
+
+    // ---- stage own columns: lower part of B (packed) and all of A
+    if (tid == 0) { *s_fail = 0; mbar_init(bar, 1); fence_mbar_init(); }
+    __syncthreads();
+    if (warp == 0) {
+        if (lane == 0) mbar_arrive_expect_tx(bar, 16u * static_cast<uint32_t>(own_off(nc, n, CS, r) + n * nc));
+        __syncwarp();
+        for (int t = lane; t < nc; t += 32) {
+            const int j = t * CS + r;
+            bulk_g2s(Lp + own_off(t, n, CS, r), Bb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
+            bulk_g2s(Cc + static_cast<size_t>(t) * n, Ab + static_cast<size_t>(j) * n, 16u * n, bar);
+        }
+    }
+    int status = 0;
+    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+        status = kInfoCopyTimeout;
+        mbar_wait_bounded(bar, 0, kMaxPolls);
+    }
+    cluster_barrier<CS>();                             // every CTA of the cluster is running
+
+    // ---- potrf (right-looking, cyclic columns)
+    int fail = 0;
+    for (int k = 0; k < n; ++k) {
+        const int o = k % CS;
+        if (r == o) {
+            double2* col = Lp + own_off(k / CS, n, CS, r);             // col[i - k] = B(i, k)
+            const double dkk = col[0].x;
+            __syncthreads();                                            // dkk read before it is replaced
+            if (!(dkk > 0.0)) {
+                if (tid == 0) *s_fail = k + 1;
+            } else {
+                const double dsq = sqrt(dkk), inv = 1.0 / dsq;
+                for (int i = 1 + tid; i < n - k; i += kBigThreads) col[i] = cscale(col[i], inv);
+                if (tid == 0) col[0] = make_double2(dsq, 0.0);
+            }
+        }
+        cluster_barrier<CS>();
+        fail = *peer(s_fail, o);
+        if (fail) break;                                                // uniform over the cluster
+        const int m = n - k - 1;
+        if (m == 0) break;
+        const double2* lk = peer(Lp, o) + own_off(k / CS, n, CS, o) + 1;   // lk[i'] = L(k+1+i', k)
+        for (int i = tid; i < m; i += kBigThreads) panel[i] = lk[i];
+        __syncthreads();
+        const int t0 = k + 1 > r ? (k + 1 - r + CS - 1) / CS : 0;
+        for_own_lower(n, CS, r, t0, nc, [&](int t, int j, int i) {
+            double2* a = Lp + own_off(t, n, CS, r) + (i - j);
+            *a = cfmsc(panel[i - k - 1], panel[j - k - 1], *a);
+        });
+        __syncthreads();
+    }
+
+    if (!fail) {
+        for (int k = tid; k < n; k += kBigThreads) {
+            const int o = k % CS;
+            invd[k] = 1.0 / peer(Lp, o)[own_off(k / CS, n, CS, o)].x;
+        }
+        // ---- W = L^{-1} A on own columns (warp w: own columns t = w + 8 c)
+        const int ncw = nc > warp ? (nc - warp + kBigWarps - 1) / kBigWarps : 0;
+        double2 y[NCW][RM];
+#pragma unroll
+        for (int c = 0; c < NCW; ++c)
+#pragma unroll
+            for (int q = 0; q < RM; ++q) {
+                const int i = lane + 32 * q, t = warp + kBigWarps * c;
+                y[c][q] = (c < ncw && i < n) ? Cc[static_cast<size_t>(t) * n + i] : make_double2(0.0, 0.0);
+            }
+        big_lower_solve<CS, RM, NCW>(y, ncw, n, Lp, panel, invd);
+#pragma unroll
+        for (int c = 0; c < NCW; ++c)
+#pragma unroll
+            for (int q = 0; q < RM; ++q) {
+                const int i = lane + 32 * q, j = (warp + kBigWarps * c) * CS + r;
+                if (c < ncw && i < n) Xb[i + static_cast<size_t>(j) * n] = y[c][q];
+            }
+        __threadfence();
+        cluster_barrier<CS>();                          // all of W is in X
+        // ---- C = L^{-1} W^H: column j of W^H is conj(row j of W)
+#pragma unroll
+        for (int c = 0; c < NCW; ++c)
+#pragma unroll
+            for (int q = 0; q < RM; ++q) {
+                const int i = lane + 32 * q, j = (warp + kBigWarps * c) * CS + r;
+                y[c][q] = (c < ncw && i < n) ? cconj(Xb[j + static_cast<size_t>(i) * n]) : make_double2(0.0, 0.0);
+            }
+        big_lower_solve<CS, RM, NCW>(y, ncw, n, Lp, panel, invd);
+#pragma unroll
+        for (int c = 0; c < NCW; ++c)
+#pragma unroll
+            for (int q = 0; q < RM; ++q) {
+                const int i = lane + 32 * q, t = warp + kBigWarps * c, j = t * CS + r;
+                double2 v = y[c][q];
+                if (i == j) v.y = 0.0;
+                if (c < ncw && i < n) Cc[static_cast<size_t>(t) * n + i] = v;
+            }
+        __syncthreads();
+
+        // ---- hetrd (LAPACK zhetd2's steps, lower)
+        double2* vl = panel;                 // v_k(k+1+i'), i' < m
+        double2* wl = panel + n;             // w(k+1+i')
+        double2* pb = panel + 2 * n;         // this CTA's share of A22 v
+        for (int k = 0; k + 1 < n; ++k) {
+            const int m = n - k - 1, o = k % CS, tk_loc = k / CS;
+            if (r == o && warp == 0) {
+                double2* x = Cc + static_cast<size_t>(tk_loc) * n + (k + 1);   // x[i'] = C(k+1+i', k)
+                double s2 = 0.0;
+                for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
+                s2 = warp_sum(s2);
+                const double2 alpha = x[0];
+                double2 tk, scale;
+                double beta;
+                if (s2 == 0.0 && alpha.y == 0.0) {
+                    tk = make_double2(0.0, 0.0); beta = alpha.x; scale = make_double2(0.0, 0.0);
+                } else {
+                    const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
+                    beta = alpha.x >= 0.0 ? -nrm : nrm;
+                    tk = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+                    const double ar = alpha.x - beta, ai = alpha.y, den = ar * ar + ai * ai;
+                    scale = make_double2(ar / den, -ai / den);
+                }
+                __syncwarp();                                               // alpha read by every lane
+                if (tk.x != 0.0 || tk.y != 0.0) {
+                    for (int i = 1 + lane; i < m; i += 32) x[i] = cmul(x[i], scale);
+                    if (lane == 0) x[0] = make_double2(1.0, 0.0);
+                }
+                if (lane == 0) {
+                    s_tau[k & 1] = tk;
+                    db[k] = Cc[static_cast<size_t>(tk_loc) * n + k].x;
+                    eb[k] = beta;
+                    taub[k] = tk;
+                }
+            }
+            cluster_barrier<CS>();
+            const double2 tk = peer(s_tau, o)[k & 1];
+            if (tk.x == 0.0 && tk.y == 0.0) continue;                       // H_k = I (uniform)
+            const double2* vsrc = peer(Cc, o) + static_cast<size_t>(tk_loc) * n + (k + 1);
+            for (int i = tid; i < m; i += kBigThreads) vl[i] = vsrc[i];
+            __syncthreads();
+            const int t0 = k + 1 > r ? (k + 1 - r + CS - 1) / CS : 0;
+            // own column j > k: sdot[t] = sum_{i > j} conj(C(i, j)) v_i   (the mirrored upper part)
+            for (int t = t0 + warp; t < nc; t += kBigWarps) {
+                const int j = t * CS + r;
+                const double2* col = Cc + static_cast<size_t>(t) * n;
+                double2 acc = make_double2(0.0, 0.0);
+                for (int i = j + 1 + lane; i < n; i += 32) acc = cfmac(col[i], vl[i - k - 1], acc);
+                acc.x = warp_sum(acc.x);
+                acc.y = warp_sum(acc.y);
+                if (lane == 0) sdot[t] = acc;
+            }
+            __syncthreads();
+            // row i = k+1+i': sum over own columns k < j <= i of C(i, j) v_j, plus sdot for i's own column
+            for (int ii = tid; ii < m; ii += kBigThreads) {
+                const int i = k + 1 + ii;
+                double2 acc = make_double2(0.0, 0.0);
+                for (int t = t0; t < nc; ++t) {
+                    const int j = t * CS + r;
+                    if (j > i) break;
+                    const double2 c = Cc[static_cast<size_t>(t) * n + i];
+                    const double2 vj = vl[j - k - 1];
+                    if (j == i) { acc.x = fma(c.x, vj.x, acc.x); acc.y = fma(c.x, vj.y, acc.y); }
+                    else acc = cfma(c, vj, acc);
+                }
+                if (i >= r && (i - r) % CS == 0) acc = cadd(acc, sdot[(i - r) / CS]);
+                pb[ii] = acc;
+            }
+            cluster_barrier<CS>();
+            // p = tau * (sum of the shares); alpha2 = -tau/2 (p^H v); w = p + alpha2 v
+            double2 dl = make_double2(0.0, 0.0);
+            for (int ii = tid; ii < m; ii += kBigThreads) {
+                double2 s = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < CS; ++q) s = cadd(s, peer(pb, q)[ii]);
+                const double2 p = cmul(tk, s);
+                wl[ii] = p;
+                dl = cfmac(p, vl[ii], dl);
+            }
+            const double2 dot = block_sum2(dl, red);
+            const double2 a2 = cscale(cmul(tk, dot), -0.5);
+            for (int ii = tid; ii < m; ii += kBigThreads) wl[ii] = cfma(a2, vl[ii], wl[ii]);
+            __syncthreads();
+            // own trailing columns: C(i, j) -= v_i conj(w_j) + w_i conj(v_j), i >= j
+            for_own_lower(n, CS, r, t0, nc, [&](int t, int j, int i) {
+                double2* a = Cc + static_cast<size_t>(t) * n + i;
+                const int ii = i - k - 1, jj = j - k - 1;
+                double2 v = cfmsc(vl[ii], wl[jj], *a);
+                v = cfmsc(wl[ii], vl[jj], v);
+                if (i == j) v.y = 0.0;
+                *a = v;
+            });
+            __syncthreads();
+        }
+        if (r == (n - 1) % CS && tid == 0) {
+            db[n - 1] = Cc[static_cast<size_t>((n - 1) / CS) * n + (n - 1)].x;
+            eb[n - 1] = 0.0;
+            taub[n - 1] = make_double2(0.0, 0.0);
+        }
+        // ---- L -> LV lower; reflector k -> LV(s, n-1-k), s = i - k - 1
+        for_own_lower(n, CS, r, 0, nc, [&](int t, int j, int i) {
+            LVb[i + static_cast<size_t>(j) * n] = Lp[own_off(t, n, CS, r) + (i - j)];
+            if (i > j) LVb[(i - j - 1) + static_cast<size_t>(n - 1 - j) * n] = Cc[static_cast<size_t>(t) * n + i];
+        });
+    }
+    if (r == 0 && tid == 0) info[b] = (fail ? n + fail : 0) | status;
+    cluster_barrier<CS>();                              // no CTA leaves while a peer may read its memory
+}
+
+// ----------------------------------------------------------------------------- k_ql_apply_rows
+template <typename R>
+__host__ __device__ inline size_t ql_rows_bytes(int n) {
+    return big_align(sizeof(R) * 32 * static_cast<size_t>(tile_ld(n)), 16) + 64 * sizeof(cplx<R>) +
+           big_align(sizeof(R) * 2 * static_cast<size_t>(n), 16);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(32) k_ql_apply_rows(int n, int batch, Workspace ws, double* __restrict__ W,
+                                                      double2* __restrict__ X, int* __restrict__ info) {
+    using C = cplx<R>;
+    const int nrb = (n + 31) / 32;                     // row blocks per pair
+    const int b = blockIdx.x / nrb, rb = blockIdx.x - b * nrb, lane = threadIdx.x;
+    if (b >= batch) return;
+    if (info[b] > n || info[b] < 0) return;            // B not positive definite: the back stage writes NaN
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int ldz = tile_ld(n);
+    R* Z = reinterpret_cast<R*>(smem);
+    C* stage = reinterpret_cast<C*>(smem + big_align(sizeof(R) * 32 * static_cast<size_t>(ldz), 16));
+    R* dd = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(stage) + 64 * sizeof(C));
+    R* ee = dd + n;
+    const size_t mat = static_cast<size_t>(n) * n;
+    R* Zg = reinterpret_cast<R*>(X + mat * b);
+    if (ws.flag[b] != 0) {                             // log overflow: warp QL on block 0
+        if (rb != 0) return;
+        R* Zs = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(X + mat * b) + 8 * mat);   // row-major, ld n
+        for (size_t idx = lane; idx < mat; idx += 32) Zs[idx] = (idx / n == idx % n) ? R(1) : R(0);
+        for (int i = lane; i < n; i += 32) {
+            dd[i] = static_cast<R>(ws.d[static_cast<size_t>(n) * b + i]);
+            ee[i] = static_cast<R>(ws.e[static_cast<size_t>(n) * b + i]);
+        }
+        __syncwarp();
+        const int unconv = tridiag_ql<R>(n, dd, ee, Zs, n);
+        for (int i = lane; i < n; i += 32) W[static_cast<size_t>(n) * b + i] = static_cast<double>(dd[i]);
+        if (lane == 0 && unconv) info[b] = unconv;
+        __syncwarp();
+        for (int row = lane; row < n; row += 32)
+            for (int k = 0; k < n; ++k) Zg[row + static_cast<size_t>(k) * n] = Zs[static_cast<size_t>(row) * n + k];
+        return;
+    }
+    const int row = rb * 32 + lane;
+    const bool own = row < n;
+    R* zrow = Z + lane * ldz;
+    if (own)
+        for (int c = 0; c < n; ++c) zrow[c] = (row == c) ? R(1) : R(0);
+    __syncwarp();
+    ql_log_apply_row<R>(reinterpret_cast<const C*>(ws.log) + static_cast<size_t>(ws.log_cap) * b, ws.log_cap, stage,
+                        zrow, own);
+    if (own) {
+        const int* perm = ws.perm + static_cast<size_t>(n) * b;
+        for (int k = 0; k < n; ++k) Zg[row + static_cast<size_t>(k) * n] = zrow[perm[k]];
+    }
+}
+
+// ----------------------------------------------------------------------------- k_back_big
+struct BigBackSmem {
+    size_t panel, tau, invd, total;
+    __host__ __device__ explicit BigBackSmem(int n) {
+        size_t o = 0;
+        panel = o; o += 16 * static_cast<size_t>(kBigPanel) * n;
+        tau = o;   o += 16 * static_cast<size_t>(n);
+        invd = o;  o += big_align(8 * static_cast<size_t>(n), 16);
+        total = o;
+    }
+};
+
+template <int CS, int RM>
+__global__ void __launch_bounds__(kBigThreads) k_back_big(int mode, int n, int batch, Workspace ws,
+                                                          double2* __restrict__ X, const int* __restrict__ info) {
+    constexpr int NCW = ((32 * RM + CS - 1) / CS + kBigWarps - 1) / kBigWarps;
+    const int r = CS == 1 ? 0 : static_cast<int>(cg::this_cluster().block_rank());
+    const int b = blockIdx.x / CS;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const BigBackSmem lay(n);
+    double2* panel = reinterpret_cast<double2*>(smem + lay.panel);
+    double2* taus = reinterpret_cast<double2*>(smem + lay.tau);
+    double* invd = reinterpret_cast<double*>(smem + lay.invd);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const size_t mat = static_cast<size_t>(n) * n;
+    double2* Xb = X + mat * b;
+    const double2* LVb = ws.LV + mat * b;
+    const int nb = (n + CS - 1) / CS, c0 = r * nb, nc = max(0, min(n, c0 + nb) - c0);
+    const int ncw = nc > warp ? (nc - warp + kBigWarps - 1) / kBigWarps : 0;
+    const bool bad = info[b] > n || info[b] < 0;
+    double2 y[NCW][RM];
+    const double* Zg = reinterpret_cast<const double*>(Xb);
+#pragma unroll
+    for (int c = 0; c < NCW; ++c)
+#pragma unroll
+        for (int q = 0; q < RM; ++q) {
+            const int i = lane + 32 * q, j = c0 + warp + kBigWarps * c;
+            y[c][q] = make_double2((!bad && c < ncw && i < n) ? Zg[i + static_cast<size_t>(j) * n] : 0.0, 0.0);
+        }
+    if (!bad) {
+        for (int k = tid; k < n; k += kBigThreads) {
+            taus[k] = ws.tau[static_cast<size_t>(n) * b + k];
+            invd[k] = 1.0 / LVb[k + static_cast<size_t>(k) * n].x;
+        }
+    }
+    cluster_barrier<CS>();                              // every CTA has read its Z before X is written
+    if (bad) {
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        for (int idx = tid; idx < n * nc; idx += kBigThreads)
+            Xb[static_cast<size_t>(c0) * n + idx] = make_double2(nan, nan);
+        return;
+    }
+    // ---- Y = Q Z: H_k for k = n-2 .. 0
+    for (int k0 = n - 2; k0 >= 0; k0 -= kBigPanel) {
+        __syncthreads();
+        for (int q = 0; q < kBigPanel && k0 - q >= 0; ++q) {
+            const int k = k0 - q;
+            const double2* src = LVb + static_cast<size_t>(n - 1 - k) * n - (k + 1);    // src[i] = v_k(i)
+            for (int i = k + 1 + tid; i < n; i += kBigThreads) panel[q * n + i] = src[i];
+        }
+        __syncthreads();
+        for (int q = 0; q < kBigPanel; ++q) {
+            const int k = k0 - q;
+            if (k < 0) break;
+            const double2 tk = taus[k];
+            if (tk.x == 0.0 && tk.y == 0.0) continue;
+            double2 lv[RM];
+#pragma unroll
+            for (int s = 0; s < RM; ++s) {
+                const int i = lane + 32 * s;
+                lv[s] = (i > k && i < n) ? panel[q * n + i] : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int c = 0; c < NCW; ++c) {
+                if (c < ncw) {
+                    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int s = 0; s < RM; ++s) acc = cfmac(lv[s], y[c][s], acc);
+                    acc.x = warp_sum(acc.x);
+                    acc.y = warp_sum(acc.y);
+                    const double2 sc = cmul(tk, acc);
+#pragma unroll
+                    for (int s = 0; s < RM; ++s) y[c][s] = cfms(lv[s], sc, y[c][s]);
+                }
+            }
+        }
+    }
+    // ---- X = L^{-H} Y: x_k = (y_k - sum_{i > k} conj(L(i, k)) x_i) / L(k, k), k = n-1 .. 0
+    if (mode == kBackFull) {
+        for (int k0 = n - 1; k0 >= 0; k0 -= kBigPanel) {
+            __syncthreads();
+            for (int q = 0; q < kBigPanel && k0 - q >= 0; ++q) {
+                const int k = k0 - q;
+                const double2* src = LVb + static_cast<size_t>(k) * n;           // src[i] = L(i, k)
+                for (int i = k + 1 + tid; i < n; i += kBigThreads) panel[q * n + i] = src[i];
+            }
+            __syncthreads();
+            for (int q = 0; q < kBigPanel; ++q) {
+                const int k = k0 - q;
+                if (k < 0) break;
+                const double ik = invd[k];
+                double2 lv[RM];
+#pragma unroll
+                for (int s = 0; s < RM; ++s) {
+                    const int i = lane + 32 * s;
+                    lv[s] = (i > k && i < n) ? panel[q * n + i] : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int c = 0; c < NCW; ++c) {
+                    if (c < ncw) {
+                        double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+                        for (int s = 0; s < RM; ++s) acc = cfmac(lv[s], y[c][s], acc);
+                        acc.x = warp_sum(acc.x);
+                        acc.y = warp_sum(acc.y);
+                        double2 xk = cshfl(seg_get(y[c], k >> 5), k & 31);
+                        xk = cscale(csub(xk, acc), ik);
+                        if (lane == (k & 31)) seg_set(y[c], k >> 5, xk);
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < NCW; ++c)
+#pragma unroll
+        for (int q = 0; q < RM; ++q) {
+            const int i = lane + 32 * q, j = c0 + warp + kBigWarps * c;
+            if (c < ncw && i < n) Xb[i + static_cast<size_t>(j) * n] = y[c][q];
+        }
+}
+
+template <class K>
+void set_big_smem_once(K kernel, std::once_flag& flag, size_t bytes) {
+    std::call_once(flag, [&]() {
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    });
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_clustered(void (*kernel)(KArgs...), int cs, int grid, int threads, size_t smem,
+                             cudaStream_t stream, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(static_cast<unsigned>(threads));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = static_cast<unsigned>(cs);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
+// (cluster size, rows per lane) by n: n <= 96 -> (4, 3), <= 128 -> (4, 4), <= 160 -> (8, 5),
+// <= 192 -> (8, 6), <= 256 -> (8, 8).
+#define SBG_BIG_DISPATCH(n, FN, ...)                                              \
+    do {                                                                          \
+        if ((n) <= 96) FN<4, 3>(__VA_ARGS__);                                     \
+        else if ((n) <= 128) FN<4, 4>(__VA_ARGS__);                               \
+        else if ((n) <= 160) FN<8, 5>(__VA_ARGS__);                               \
+        else if ((n) <= 192) FN<8, 6>(__VA_ARGS__);                               \
+        else FN<8, 8>(__VA_ARGS__);                                               \
+    } while (0)
+
+template <int CS, int RM>
+void run_reduce_big(cudaError_t* err, const double2* A, const double2* B, int n, int batch, const Workspace& ws,
+                    double2* X, int* info, cudaStream_t stream) {
+    const size_t smem = BigReduceSmem(n, CS).total;
+    static std::once_flag f;
+    set_big_smem_once(k_reduce_big<CS, RM>, f, static_cast<size_t>(max_smem_optin()));
+    *err = launch_clustered(k_reduce_big<CS, RM>, CS, batch * CS, kBigThreads, smem, stream, A, B, n, batch, ws, X,
+                            info);
+}
+
+template <int CS, int RM>
+void run_back_big(cudaError_t* err, int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
+                  cudaStream_t stream) {
+    const size_t smem = BigBackSmem(n).total;
+    static std::once_flag f;
+    set_big_smem_once(k_back_big<CS, RM>, f, static_cast<size_t>(max_smem_optin()));
+    *err = launch_clustered(k_back_big<CS, RM>, CS, batch * CS, kBigThreads, smem, stream, mode, n, batch, ws, X,
+                            info);
+}
+
+template <int CS, int RM>
+void big_smem_of(size_t* out, int n) { *out = BigReduceSmem(n, CS).total; }
+
+}  // namespace
+
+bool big_path(int n) { return n > kSmallMaxN && n <= kBigMaxN; }
+
+size_t big_reduce_smem_bytes(int n) {
+    size_t s = 0;
+    SBG_BIG_DISPATCH(n, big_smem_of, &s, n);
+    return s;
+}
+
+cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
+                              int* info, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    if (!A || !B || !X || !info || !ws.LV || !ws.d || !ws.e || !ws.tau) return cudaErrorInvalidValue;
+    if (!big_path(n)) return cudaErrorInvalidValue;
+    cudaError_t err = cudaSuccess;
+    SBG_BIG_DISPATCH(n, run_reduce_big, &err, A, B, n, batch, ws, X, info, stream);
+    return err != cudaSuccess ? err : cudaGetLastError();
+}
+
+size_t ql_rows_smem_bytes(int n, bool single) { return single ? ql_rows_bytes<float>(n) : ql_rows_bytes<double>(n); }
+
+cudaError_t launch_ql_rows(int n, int batch, const Workspace& ws, double* W, double2* X, int* info, bool single,
+                           int chain_threads, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    if (!W || !X || !info || !ws.d || !ws.e || !ws.log || !ws.perm || !ws.flag) return cudaErrorInvalidValue;
+    const size_t cs = ql_chain_smem_bytes(n, chain_threads, single);
+    const size_t as = ql_rows_smem_bytes(n, single);
+    if (cs > static_cast<size_t>(max_smem_optin()) || as > static_cast<size_t>(max_smem_optin()))
+        return cudaErrorInvalidValue;
+    cudaError_t err = launch_ql_chain(n, batch, ws, W, info, single, chain_threads, stream);
+    if (err != cudaSuccess) return err;
+    const int grid = ((n + 31) / 32) * batch;
+    static std::once_flag fd, ff;
+    if (single) {
+        set_big_smem_once(k_ql_apply_rows<float>, ff, static_cast<size_t>(max_smem_optin()));
+        k_ql_apply_rows<float><<<grid, 32, as, stream>>>(n, batch, ws, W, X, info);
+    } else {
+        set_big_smem_once(k_ql_apply_rows<double>, fd, static_cast<size_t>(max_smem_optin()));
+        k_ql_apply_rows<double><<<grid, 32, as, stream>>>(n, batch, ws, W, X, info);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_back_big(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
+                            cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
+    if (!big_path(n)) return cudaErrorInvalidValue;
+    cudaError_t err = cudaSuccess;
+    SBG_BIG_DISPATCH(n, run_back_big, &err, mode, n, batch, ws, X, info, stream);
+    return err != cudaSuccess ? err : cudaGetLastError();
+}
+
+}  // namespace sbg

@@ -236,7 +236,15 @@ struct DeviceGuard {
 int supported_max_n(int precision) {
     const size_t lim = static_cast<size_t>(sbg::max_smem_optin());
     int best = 0;
-    for (int n = 1; n <= 256; ++n) {
+    const bool single = precision == SBG_PRECISION_MIXED;
+    for (int n = 1; n <= sbg::kBigMaxN; ++n) {
+        if (n > sbg::kSmallMaxN) {          // cluster kernels
+            if (single) break;              // the refinement kernel holds five n x n tiles: small n only
+            size_t need = std::max(sbg::big_reduce_smem_bytes(n), sbg::ql_rows_smem_bytes(n, false));
+            need = std::max(need, sbg::ql_chain_smem_bytes(n, 32, false));
+            if (sbg::big_path(n) && need <= lim) best = n;
+            continue;
+        }
         size_t need = std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, n), sbg::back_smem_bytes(n));
         need = std::max(need, sbg::hetrd_smem_bytes(n, 128));
         need = std::max(need, sbg::ql_apply_smem_bytes(n, 1, precision == SBG_PRECISION_MIXED));
@@ -261,7 +269,7 @@ void create_solver(int n, int device, const sbg_solver_options* o, sbg_solver** 
     if (device < 0 || device >= ndev) throw Error(SBG_ERR_INVALID_VALUE, "device_id out of range");
     DeviceGuard g(device);
     if (n > supported_max_n(opts.precision))
-        throw Error(SBG_ERR_UNSUPPORTED, "n = " + std::to_string(n) + " exceeds the single-CTA limit (" +
+        throw Error(SBG_ERR_UNSUPPORTED, "n = " + std::to_string(n) + " exceeds the supported maximum (" +
                                              std::to_string(supported_max_n(opts.precision)) + ")");
     std::unique_ptr<sbg_solver> s(new sbg_solver);
     s->n = n;

@@ -17,12 +17,14 @@
 
 #include "stages.cuh"
 
-// Row-slot sequences, descending: SBG_DESC64(C) expands to C(63) C(62) ... C(0).
+// Row-slot sequences.  SBG_DESC64(C) expands to C(63) C(62) ... C(0) (a one-jump
+// select, e.g. of a pivot); SBG_BLOCKS(K) expands to K(7) ... K(0), one `case` per block
+// of 8 rows, so that the rows of a block are straight-line code the scheduler can
+// interleave, and SBG_ROWS8(S, B) expands to S(8B+7) ... S(8B) inside a block.
 #define SBG_DESC64(C) C(63) C(62) C(61) C(60) C(59) C(58) C(57) C(56) C(55) C(54) C(53) C(52) C(51) C(50) C(49) C(48) C(47) C(46) C(45) C(44) C(43) C(42) C(41) C(40) C(39) C(38) C(37) C(36) C(35) C(34) C(33) C(32) C(31) C(30) C(29) C(28) C(27) C(26) C(25) C(24) C(23) C(22) C(21) C(20) C(19) C(18) C(17) C(16) C(15) C(14) C(13) C(12) C(11) C(10) C(9) C(8) C(7) C(6) C(5) C(4) C(3) C(2) C(1) C(0)
-#define SBG_DESC32(C) C(31) C(30) C(29) C(28) C(27) C(26) C(25) C(24) C(23) C(22) C(21) C(20) C(19) C(18) C(17) C(16) C(15) C(14) C(13) C(12) C(11) C(10) C(9) C(8) C(7) C(6) C(5) C(4) C(3) C(2) C(1) C(0)
-// Cases I >= NMAX are never entered (the entry row is < n <= NMAX); their bodies are
-// discarded at compile time.
-#define SBG_SWEEP(NMAX, C) SBG_DESC64(C)
+#define SBG_BLOCKS(K) K(7) K(6) K(5) K(4) K(3) K(2) K(1) K(0)
+#define SBG_ROWS8(S, B) S((B) * 8 + 7) S((B) * 8 + 6) S((B) * 8 + 5) S((B) * 8 + 4) \
+                        S((B) * 8 + 3) S((B) * 8 + 2) S((B) * 8 + 1) S((B) * 8 + 0)
 
 namespace sbg {
 
@@ -50,18 +52,15 @@ __device__ int potrf_warp_packed(cplx<R>* P, int n, R* invd) {
         const int base = k + 1;
         const int h = (m + 1) >> 1;
         const int r1 = lane, r2 = m - 1 - lane;
+        // A22(r, j) at P + pk(base) + r - j + sum_{t<j} (m - t): advances by m - j - 1 per column
         if (lane < h) {
             const C l1 = colk[1 + r1];
-            for (int j = 0; j <= r1; ++j) {
-                C* a = P + pk(base + j, n) + r1 - j;
-                *a = cfmsc(l1, colk[1 + j], *a);
-            }
+            C* a = P + pk(base, n) + r1;
+            for (int j = 0; j <= r1; ++j) { *a = cfmsc(l1, colk[1 + j], *a); a += m - j - 1; }
             if (r2 != r1) {
                 const C l2 = colk[1 + r2];
-                for (int j = 0; j <= r2; ++j) {
-                    C* a = P + pk(base + j, n) + r2 - j;
-                    *a = cfmsc(l2, colk[1 + j], *a);
-                }
+                a = P + pk(base, n) + r2;
+                for (int j = 0; j <= r2; ++j) { *a = cfmsc(l2, colk[1 + j], *a); a += m - j - 1; }
             }
         }
         __syncwarp();
@@ -76,15 +75,20 @@ template <int NMAX, typename R, typename Out>
 __device__ __forceinline__ void col_trsm_lower(const cplx<R>* Lp, const R* invd, cplx<R> (&y)[NMAX], int n,
                                                Out&& out) {
     using C = cplx<R>;
-    C piv = y[0];
     for (int k = 0; k < n; ++k) {
+        C piv = y[0];
+#define SBG_SEL(I) case I: if constexpr ((I) < NMAX) piv = y[I]; break;
+        switch (k) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
         const C wk = cscale(piv, invd[k]);
         out(k, wk);
         const C* lk = Lp + pk(k, n) - k;          // lk[i] = L(i, k)
-        // rows n-1 .. k+1; the last one updated (k + 1) is the next pivot
-#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { if ((I) <= k) break; y[I] = cfms(lk[I], wk, y[I]); piv = y[I]; }
-        switch (n - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
-#undef SBG_SLOT
+        // rows n-1 .. k+1, by blocks of 8 from the block of n-1 down to the block of k+1
+#define SBG_S(I) if constexpr ((I) < NMAX) { if ((I) > k && (I) < n) y[I] = cfms(lk[I], wk, y[I]); }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= k) break; SBG_ROWS8(SBG_S, B)
+        switch ((n - 1) >> 3) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
     }
 }
 
@@ -92,18 +96,21 @@ __device__ __forceinline__ void col_trsm_lower(const cplx<R>* Lp, const R* invd,
 // y holds W(i, 0..i); the solved C(i, k) go through out(k, c).
 template <int NMAX, typename R, typename Out>
 __device__ __forceinline__ void row_trsm_right_lowerH(const cplx<R>* Lp, const R* invd, cplx<R> (&y)[NMAX], int n,
-                                                      int i, Out&& out) {
+                                                      int i, int kmax, Out&& out) {
     using C = cplx<R>;
-    C piv = y[0];
-    for (int k = 0; k <= i; ++k) {
+    for (int k = 0; k <= kmax; ++k) {            // kmax: the largest row of the warp (uniform loop)
+        C piv = y[0];
+#define SBG_SEL(I) case I: if constexpr ((I) < NMAX) piv = y[I]; break;
+        switch (k) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
         const C ck = cscale(piv, invd[k]);
-        out(k, ck);
+        if (k <= i) out(k, ck);
         const C* lk = Lp + pk(k, n) - k;          // lk[kk] = L(kk, k)
-        // columns n-1 .. k+1, only kk <= i change; the last one (k + 1) is the next pivot
-#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { if ((I) <= k) break; \
-                                     if ((I) <= i) { y[I] = cfmsc(ck, lk[I], y[I]); piv = y[I]; } }
-        switch (n - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
-#undef SBG_SLOT
+#define SBG_S(I) if constexpr ((I) < NMAX) { if ((I) > k && (I) <= i) y[I] = cfmsc(ck, lk[I], y[I]); }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= k) break; SBG_ROWS8(SBG_S, B)
+        switch (kmax >> 3) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
     }
 }
 
@@ -115,18 +122,20 @@ __device__ __forceinline__ void col_apply_q(const cplx<R>* LV, int ld, const cpl
     for (int k = n - 2; k >= 0; --k) {
         const C tk = tau[k];
         if (tk.x == R(0) && tk.y == R(0)) continue;
-        const C* vtop = LV + k + (n - 1) * ld;   // v_k(i) at LV + k + i * ld, i >= k + 1; walked downwards
-        C s0 = mk<R>(R(0), R(0)), s1 = mk<R>(R(0), R(0));
-        const C* pv = vtop;
-#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { if ((I) <= k) break; \
-        if ((I) & 1) s1 = cfmac(*pv, y[I], s1); else s0 = cfmac(*pv, y[I], s0); pv -= ld; }
-        switch (n - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
-#undef SBG_SLOT
+        const C* vrow = LV + k;                   // v_k(i) = vrow[i * ld], i >= k + 1
+        C s0 = mk<R>(R(0), R(0)), s1 = s0;
+#define SBG_S(I) if constexpr ((I) < NMAX) { if ((I) > k && (I) < n) { \
+        if ((I) & 1) s1 = cfmac(vrow[(I) * ld], y[I], s1); else s0 = cfmac(vrow[(I) * ld], y[I], s0); } }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= k) break; SBG_ROWS8(SBG_S, B)
+        switch ((n - 1) >> 3) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
         const C s = cmul(tk, cadd(s0, s1));
-        pv = vtop;
-#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { if ((I) <= k) break; y[I] = cfms(*pv, s, y[I]); pv -= ld; }
-        switch (n - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
-#undef SBG_SLOT
+#define SBG_S(I) if constexpr ((I) < NMAX) { if ((I) > k && (I) < n) y[I] = cfms(vrow[(I) * ld], s, y[I]); }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= k) break; SBG_ROWS8(SBG_S, B)
+        switch ((n - 1) >> 3) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
     }
 }
 
@@ -136,19 +145,21 @@ template <int NMAX, typename R, typename Out>
 __device__ __forceinline__ void col_trsm_lowerH(const cplx<R>* LV, int ld, const R* invd, cplx<R> (&y)[NMAX], int n,
                                                 Out&& out) {
     using C = cplx<R>;
-    C piv = y[0];
-#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { piv = y[I]; } break;
-    switch (n - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
-#undef SBG_SLOT
     for (int k = n - 1; k >= 0; --k) {
+        C piv = y[0];
+#define SBG_SEL(I) case I: if constexpr ((I) < NMAX) piv = y[I]; break;
+        switch (k) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
         const C xk = cscale(piv, invd[k]);
         out(k, xk);
-        const C* pl = LV + k + (k - 1) * ld;     // L(k, i) at LV + k + i * ld, i < k; walked downwards
-        // rows k-1 .. 0; the first one updated (k - 1) is the next pivot
-#define SBG_SLOT(I) case I: if constexpr ((I) < NMAX) { y[I] = cfms(cconj(*pl), xk, y[I]); pl -= ld; \
-                                                        if ((I) == k - 1) piv = y[I]; }
-        switch (k - 1) { SBG_SWEEP(NMAX, SBG_SLOT); default: break; }
-#undef SBG_SLOT
+        if (k == 0) break;
+        const C* lrow = LV + k;                   // L(k, i) = lrow[i * ld], i < k
+        // rows k-1 .. 0, by blocks of 8 from the block of k-1 down to block 0
+#define SBG_S(I) if constexpr ((I) < NMAX) { if ((I) < k) y[I] = cfms(cconj(lrow[(I) * ld]), xk, y[I]); }
+#define SBG_K(B) case B: SBG_ROWS8(SBG_S, B)
+        switch ((k - 1) >> 3) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
     }
 }
 

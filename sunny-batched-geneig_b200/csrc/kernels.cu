@@ -286,7 +286,8 @@ __global__ void __launch_bounds__(NMAX, 4) k_hegst_col(int mode, const double2* 
         const int i = tid;
 #pragma unroll
         for (int kk = 0; kk < NMAX; ++kk) y[kk] = (kk <= i) ? Ob[i + static_cast<size_t>(kk) * n] : make_double2(0.0, 0.0);
-        row_trsm_right_lowerH<NMAX>(Lp, invd, y, n, i, [&](int k, double2 c) {
+        const int kmax = min(n - 1, (tid | 31));            // the warp's largest row: uniform loop bound
+        row_trsm_right_lowerH<NMAX>(Lp, invd, y, n, i, kmax, [&](int k, double2 c) {
             if (k == i) c.y = 0.0;
             Ob[i + static_cast<size_t>(k) * n] = c;
         });
@@ -694,49 +695,9 @@ __global__ void k_ql_apply(int n, int batch, Workspace ws, double* __restrict__ 
         for (int c = 0; c < n; ++c) zrow[c] = (row == c) ? R(1) : R(0);
     __syncthreads();      // every row is initialised before a fallback warp rotates all of them
     const bool fallback = live && ws.flag[b] != 0;
-    if (live && !fallback) {
-        const C* log = reinterpret_cast<const C*>(ws.log) + static_cast<size_t>(ws.log_cap) * b;
-        const int cap = ws.log_cap;
-        int loaded = 0, buf = 0, remaining = 0, col = 0;
-        C pre = log[lane];
-        R carry = R(0);
-        bool done = false;
-        while (!done) {
-            stage[buf * 32 + lane] = pre;
-            __syncwarp();
-            loaded += 32;
-            if (loaded < cap) pre = log[min(loaded + lane, cap - 1)];
-            const C* st = stage + buf * 32;
-            int k = 0;
-            while (k < 32) {
-                if (remaining == 0) {
-                    const C h = st[k++];
-                    const int top = static_cast<int>(h.x);
-                    if (top < 0) { done = true; break; }
-                    remaining = static_cast<int>(h.y);
-                    col = top;
-                    if (own && remaining > 0) carry = zrow[col + 1];
-                    continue;
-                }
-                const int take = min(remaining, 32 - k);
-                if (own) {
-                    for (int t = 0; t < take; ++t) {
-                        const C cs = st[k + t];
-                        const R zi = zrow[col - t];
-                        zrow[col - t + 1] = fma(cs.y, zi, cs.x * carry);
-                        carry = fma(cs.x, zi, -cs.y * carry);
-                    }
-                }
-                k += take;
-                col -= take;
-                remaining -= take;
-                if (remaining == 0 && own) zrow[col + 1] = carry;
-            }
-            __syncwarp();
-            buf ^= 1;
-            if (!done && loaded >= cap) done = true;      // malformed log guard (never reached)
-        }
-    }
+    if (live && !fallback)
+        ql_log_apply_row<R>(reinterpret_cast<const C*>(ws.log) + static_cast<size_t>(ws.log_cap) * b, ws.log_cap,
+                            stage, zrow, own);
     if (fallback && wip == 0) {
         for (int i = lane; i < n; i += 32) {
             dd[i] = static_cast<R>(ws.d[static_cast<size_t>(n) * b + i]);
@@ -916,7 +877,10 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
     if ((mode == kReduceChol || mode == kReduceHegst || mode == kReduceFull) && !out) return cudaErrorInvalidValue;
     if ((mode == kReduceHegst || mode == kReduceFull) && !A) return cudaErrorInvalidValue;
     if ((mode == kReduceFull || mode == kReduceFromLM) && !ws.LV) return cudaErrorInvalidValue;
-    if (n > 84) return cudaErrorInvalidValue;
+    if (n > kSmallMaxN) {
+        if (mode != kReduceFull) return cudaErrorInvalidValue;
+        return launch_reduce_big(A, B, n, batch, ws, out, info, stream);
+    }
     // The two-kernel path hands L from k_potrf_warp to k_hegst_col through ws.LV, so it
     // needs a workspace (the staged Cholesky alone does not).
     if (n <= kColMaxN && mode != kReduceFromLM && (mode == kReduceChol || ws.LV != nullptr)) {
@@ -943,6 +907,7 @@ cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws
                          cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!C || !info || !ws.LV || !ws.d || !ws.e || !ws.tau) return cudaErrorInvalidValue;
+    if (n > kSmallMaxN) return big_path(n) ? cudaSuccess : cudaErrorInvalidValue;   // done by the reduce kernel
     if (n <= kHetrdWarpMaxN) {
         const size_t smem = hetrd_warp_bytes(n) * kHetrdWarpsPerCta;
         static std::once_flag fw;
@@ -986,10 +951,29 @@ size_t ql_apply_smem_bytes(int n, int pairs_per_cta, bool single) {
     return (single ? ql_apply_pair_bytes<float>(n) : ql_apply_pair_bytes<double>(n)) * pairs_per_cta;
 }
 
+cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, int* info, bool single,
+                            int chain_threads, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    if (!W || !info || !ws.d || !ws.e || !ws.log || !ws.perm || !ws.flag) return cudaErrorInvalidValue;
+    const size_t cs = ql_chain_smem_bytes(n, chain_threads, single);
+    if (cs > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+    const int cgrid = (batch + chain_threads - 1) / chain_threads;
+    static std::once_flag fcd, fcf;
+    if (single) {
+        set_max_smem_once(k_ql_chain<float>, fcf);
+        k_ql_chain<float><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info);
+    } else {
+        set_max_smem_once(k_ql_chain<double>, fcd);
+        k_ql_chain<double><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
                              bool single, int chain_threads, int apply_warps, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!W || !X || !info || !ws.d || !ws.e || !ws.log || !ws.perm || !ws.flag) return cudaErrorInvalidValue;
+    if (n > kSmallMaxN) return launch_ql_rows(n, batch, ws, W, X, info, single, chain_threads, stream);
     const size_t cs = ql_chain_smem_bytes(n, chain_threads, single);
     const size_t as = ql_apply_smem_bytes(n, apply_warps, single);
     if (cs > static_cast<size_t>(max_smem_optin()) || as > static_cast<size_t>(max_smem_optin()))
@@ -1016,6 +1000,7 @@ cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* 
                                  int refine_steps, int chain_threads, int apply_warps, int refine_threads,
                                  cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
+    if (n > kSmallMaxN) return cudaErrorInvalidValue;
     const size_t rsmem = refine_smem_bytes(n, refine_threads);
     if (rsmem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     cudaError_t err = launch_ql_logged(n, batch, ws, W, X, info, true, chain_threads, apply_warps, stream);
@@ -1043,7 +1028,7 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
                         int /*threads*/, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
-    if (n > 84) return cudaErrorInvalidValue;
+    if (n > kSmallMaxN) return launch_back_big(mode, n, batch, ws, X, info, stream);
     const size_t smem = back_smem_bytes(n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     if (n <= kColMaxN) {

@@ -72,6 +72,26 @@ cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* 
 cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
                         int threads, cudaStream_t stream);
 
+// Pairs with n <= kSmallMaxN are solved by CTA-per-pair (or warp-per-pair) stage kernels;
+// kSmallMaxN < n <= kBigMaxN by the cluster kernels of bigsolve.cu.  For those the reduce
+// launch (kReduceFull only) also tridiagonalises, so launch_hetrd has nothing left to do,
+// and the reflectors are stored along the columns of LV's strict upper triangle
+// (v_k(k+1+s) = LV(s, n-1-k)) instead of its rows.
+constexpr int kSmallMaxN = 84;
+constexpr int kBigMaxN = 256;
+bool big_path(int n);
+size_t big_reduce_smem_bytes(int n);
+size_t ql_rows_smem_bytes(int n, bool single);
+cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
+                              int* info, cudaStream_t stream);
+cudaError_t launch_ql_rows(int n, int batch, const Workspace& ws, double* W, double2* X, int* info, bool single,
+                           int chain_threads, cudaStream_t stream);
+cudaError_t launch_back_big(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
+                            cudaStream_t stream);
+// The QL scalar chain alone (thread per pair): W, the rotation log, perm, flag.
+cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, int* info, bool single,
+                            int chain_threads, cudaStream_t stream);
+
 size_t reduce_smem_bytes(int mode, int n);
 size_t tridiag_smem_bytes(int n, int warps_per_cta, bool single);
 size_t ql_chain_smem_bytes(int n, int threads, bool single);

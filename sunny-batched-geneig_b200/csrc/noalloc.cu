@@ -72,7 +72,7 @@ extern "C" int sbg_geneig_full_noalloc_launch(int n, const cuDoubleComplex* d_A,
     if (batch == 0) return SBG_OK;
     if (!d_A || !d_B || !d_W || !d_X || !d_info) return fail(SBG_ERR_INVALID_VALUE, "null device pointer");
     if (n > sbg_max_n(SBG_PRECISION_FP64))
-        return fail(SBG_ERR_UNSUPPORTED, "n = " + std::to_string(n) + " exceeds the single-CTA limit");
+        return fail(SBG_ERR_UNSUPPORTED, "n = " + std::to_string(n) + " exceeds the supported maximum");
     const size_t need = scratch_needed(n, batch);
     if (need > static_cast<size_t>(SBG_NOALLOC_SCRATCH_BYTES)) {
         const size_t per = sbg::workspace_bytes_per_pair(n);

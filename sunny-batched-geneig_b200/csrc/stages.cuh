@@ -744,6 +744,58 @@ __device__ __forceinline__ void seg_trsm_lowerH(const C* L, int ldl, const R* in
     }
 }
 
+// ============================================================================ QL log application
+// Applies one pair's rotation log (ql_chain's format: a header (top, count), then count
+// rotations (c, s) for columns top, top-1, ...; a header with top < 0 ends the log) to
+// the row zrow of Z owned by this lane (own = false: the lane only helps stream the
+// log).  The log is read 32 entries at a time with one coalesced load into the warp's
+// stage buffer (64 entries, double-buffered) and read back by broadcast; within a sweep
+// the rotation at column i loads z_i and carries z_{i+1} in a register.
+template <typename R>
+__device__ __forceinline__ void ql_log_apply_row(const cplx<R>* log, int cap, cplx<R>* stage, R* zrow, bool own) {
+    using C = cplx<R>;
+    const int lane = threadIdx.x & 31;
+    int loaded = 0, buf = 0, remaining = 0, col = 0;
+    C pre = log[lane];
+    R carry = R(0);
+    bool done = false;
+    while (!done) {
+        stage[buf * 32 + lane] = pre;
+        __syncwarp();
+        loaded += 32;
+        if (loaded < cap) pre = log[min(loaded + lane, cap - 1)];
+        const C* st = stage + buf * 32;
+        int k = 0;
+        while (k < 32) {
+            if (remaining == 0) {
+                const C h = st[k++];
+                const int top = static_cast<int>(h.x);
+                if (top < 0) { done = true; break; }
+                remaining = static_cast<int>(h.y);
+                col = top;
+                if (own && remaining > 0) carry = zrow[col + 1];
+                continue;
+            }
+            const int take = min(remaining, 32 - k);
+            if (own) {
+                for (int t = 0; t < take; ++t) {
+                    const C cs = st[k + t];
+                    const R zi = zrow[col - t];
+                    zrow[col - t + 1] = fma(cs.y, zi, cs.x * carry);
+                    carry = fma(cs.x, zi, -cs.y * carry);
+                }
+            }
+            k += take;
+            col -= take;
+            remaining -= take;
+            if (remaining == 0 && own) zrow[col + 1] = carry;
+        }
+        __syncwarp();
+        buf ^= 1;
+        if (!done && loaded >= cap) done = true;      // malformed log guard (never reached)
+    }
+}
+
 // ============================================================================ hetrd, one warp, packed
 // Column-major packed lower triangle: A(i, j), i >= j, at P[pk(j, n) + i - j].
 __host__ __device__ __forceinline__ int pk(int j, int n) { return j * n - (j * (j - 1)) / 2; }
@@ -791,24 +843,39 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
         const bool own1 = lane < h;
         const bool own2 = lane < h && r2 != r1;
         // ---- p = tau A22 v for the owned rows
+        // Row walk of the packed lower part: A22(r, j) sits at P + c0 + r - j + sum_{t<j} (n - base - t),
+        // so the address advances by (m - j - 1) from column j to j + 1 (incremental, no pk() per term).
+        const C* c0 = P + pk(base, n);
         C p1 = mk<R>(R(0), R(0)), p2 = mk<R>(R(0), R(0));
         if (own1) {
-            C a0 = mk<R>(R(0), R(0)), a1 = mk<R>(R(0), R(0));
-            for (int j = 0; j < r1; ++j) a0 = cfma(P[pk(base + j, n) + r1 - j], vb[j], a0);      // lower, row walk
-            const C* col = P + pk(base + r1, n);                                                  // column r1
+            C a0 = mk<R>(R(0), R(0)), a1 = mk<R>(R(0), R(0)), a2 = mk<R>(R(0), R(0));
+            const C* pa = c0 + r1;
+            int j = 0;
+            for (; j + 1 < r1; j += 2) {
+                a0 = cfma(*pa, vb[j], a0); pa += m - j - 1;
+                a2 = cfma(*pa, vb[j + 1], a2); pa += m - j - 2;
+            }
+            for (; j < r1; ++j) { a0 = cfma(*pa, vb[j], a0); pa += m - j - 1; }
+            const C* col = pa;                                                   // = A22(r1, r1), column r1
             a1.x = fma(col[0].x, vb[r1].x, a1.x);
             a1.y = fma(col[0].x, vb[r1].y, a1.y);
-            for (int j = r1 + 1; j < m; ++j) a1 = cfmac(col[j - r1], vb[j], a1);                // mirrored upper
-            p1 = cmul(tk, cadd(a0, a1));
+            for (int t = 1; t + r1 < m; ++t) a1 = cfmac(col[t], vb[r1 + t], a1);   // mirrored upper
+            p1 = cmul(tk, cadd(cadd(a0, a2), a1));
         }
         if (own2) {
-            C a0 = mk<R>(R(0), R(0)), a1 = mk<R>(R(0), R(0));
-            for (int j = 0; j < r2; ++j) a0 = cfma(P[pk(base + j, n) + r2 - j], vb[j], a0);
-            const C* col = P + pk(base + r2, n);
+            C a0 = mk<R>(R(0), R(0)), a1 = mk<R>(R(0), R(0)), a2 = mk<R>(R(0), R(0));
+            const C* pa = c0 + r2;
+            int j = 0;
+            for (; j + 1 < r2; j += 2) {
+                a0 = cfma(*pa, vb[j], a0); pa += m - j - 1;
+                a2 = cfma(*pa, vb[j + 1], a2); pa += m - j - 2;
+            }
+            for (; j < r2; ++j) { a0 = cfma(*pa, vb[j], a0); pa += m - j - 1; }
+            const C* col = pa;
             a1.x = fma(col[0].x, vb[r2].x, a1.x);
             a1.y = fma(col[0].x, vb[r2].y, a1.y);
-            for (int j = r2 + 1; j < m; ++j) a1 = cfmac(col[j - r2], vb[j], a1);
-            p2 = cmul(tk, cadd(a0, a1));
+            for (int t = 1; t + r2 < m; ++t) a1 = cfmac(col[t], vb[r2 + t], a1);
+            p2 = cmul(tk, cadd(cadd(a0, a2), a1));
         }
         // ---- w = p - tau/2 (p^H v) v
         C dot = mk<R>(R(0), R(0));
@@ -824,23 +891,29 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
         // ---- A22 -= v w^H + w v^H on the lower triangle of the owned rows
         if (own1) {
             const C v1 = vb[r1];
-            for (int j = 0; j <= r1; ++j) {
-                C* a = P + pk(base + j, n) + r1 - j;
+            C* a = P + pk(base, n) + r1;
+            for (int j = 0; j < r1; ++j) {
                 C t = cfmsc(v1, wb[j], *a);
-                t = cfmsc(w1, vb[j], t);
-                if (j == r1) t.y = R(0);
-                *a = t;
+                *a = cfmsc(w1, vb[j], t);
+                a += m - j - 1;
             }
+            C t = cfmsc(v1, wb[r1], *a);
+            t = cfmsc(w1, vb[r1], t);
+            t.y = R(0);
+            *a = t;
         }
         if (own2) {
             const C v2 = vb[r2];
-            for (int j = 0; j <= r2; ++j) {
-                C* a = P + pk(base + j, n) + r2 - j;
+            C* a = P + pk(base, n) + r2;
+            for (int j = 0; j < r2; ++j) {
                 C t = cfmsc(v2, wb[j], *a);
-                t = cfmsc(w2, vb[j], t);
-                if (j == r2) t.y = R(0);
-                *a = t;
+                *a = cfmsc(w2, vb[j], t);
+                a += m - j - 1;
             }
+            C t = cfmsc(v2, wb[r2], *a);
+            t = cfmsc(w2, vb[r2], t);
+            t.y = R(0);
+            *a = t;
         }
         __syncwarp();
     }

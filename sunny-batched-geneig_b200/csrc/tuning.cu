@@ -34,6 +34,11 @@ std::map<std::tuple<int, int, int>, Schedule> g_in_process;   // (device, n, pre
 
 bool fits(int n, int precision, const Schedule& s) {
     const size_t lim = static_cast<size_t>(max_smem_optin());
+    if (n > kSmallMaxN) {                 // cluster kernels (FP64 only)
+        if (precision == SBG_PRECISION_MIXED || !big_path(n)) return false;
+        return big_reduce_smem_bytes(n) <= lim && ql_rows_smem_bytes(n, false) <= lim &&
+               ql_chain_smem_bytes(n, s.chain_threads, false) <= lim;
+    }
     if (reduce_smem_bytes(kReduceFull, n) > lim || back_smem_bytes(n) > lim || hetrd_smem_bytes(n, s.hetrd_threads) > lim) return false;
     const bool single = precision == SBG_PRECISION_MIXED;
     if (ql_chain_smem_bytes(n, s.chain_threads, single) > lim) return false;
