@@ -311,7 +311,9 @@ def main():
 
     # choose the headline form: fastest that meets the gate on the sample
     def ok(r):
-        return r["acc"] is None or (r["acc"]["eig_rel"] <= EIG_GATE and r["info_nonzero"] == 0)
+        a = r["acc"]
+        return a is None or (a["eig_rel"] <= EIG_GATE and a["residual"] <= EIG_GATE and a["orth"] <= EIG_GATE
+                             and r["info_nonzero"] == 0)
     eligible = [f for f in forms if ok(results[f])] or forms
     best = max(eligible, key=lambda f: results[f]["value"])
     R = results[best]

@@ -418,10 +418,16 @@ __device__ int tridiag_ql(int n, R* d, R* e, R* Z, int ldz) {
 // Every product runs in FP64.  TZ, Rm, Sm are n x n scratch tiles (same ld);
 // Znew receives Z'.  red is 4 doubles of scratch per warp.  Returns
 // max_{i != j} |E_ij| (the size of the correction), identical on every thread.
+// floor_rel > 0 raises delta to at least floor_rel ||T||_F: pairs closer than that are
+// then only orthogonalised (E_ij = R_ij / 2).  The formula's division by the gap turns
+// the O(eps ||T||) rounding of S_ij into an O(eps ||T|| / gap) error of E_ij, which
+// breaks the orthogonality of nearly degenerate pairs; their directions are already
+// accurate to that level, so a final step with the floor restores Z^T Z = I to O(R^2)
+// and keeps the residual at O(eps ||T||).
 template <int TB>
 __device__ double oa_refine_step(int n, const double* dT, const double* eT, const double* Z, int ld,
                                  double* TZ, double* Rm, double* Sm, double* Znew, double* lam,
-                                 double* red) {
+                                 double* red, double floor_rel) {
     const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = T >> 5;
     // TZ = T Z
     for (int idx = tid; idx < n * n; idx += T) {
@@ -489,7 +495,7 @@ __device__ double oa_refine_step(int n, const double* dT, const double* eT, cons
     __syncthreads();
     double S2 = 0.0, R2 = 0.0, T2 = 0.0;
     for (int w = 0; w < nw; ++w) { S2 += red[4 * w]; R2 += red[4 * w + 1]; T2 += red[4 * w + 2]; }
-    const double delta = 2.0 * (sqrt(S2) + sqrt(T2) * sqrt(R2));
+    const double delta = fmax(2.0 * (sqrt(S2) + sqrt(T2) * sqrt(R2)), floor_rel * sqrt(T2));
     // E (over Sm)
     double emax = 0.0;
     for (int idx = tid; idx < n * n; idx += T) {
