@@ -168,8 +168,40 @@ int sbg_solver_autotune_sweep_ran(const sbg_solver* s);
 const char* sbg_solver_cache_layer_used(const sbg_solver* s);
 int sbg_solver_precision(const sbg_solver* s);
 
-/* Largest n each form supports on this device (shared-memory bound). */
+/* Largest n each form supports on this device (shared-memory bound).  FP64: 256 (n <= 84
+ * one CTA or warp per pair, 84 < n <= 256 one thread-block cluster per pair); mixed: the
+ * refinement kernel's limit (n <= 75 or so). */
 int sbg_max_n(int precision);
+
+/* ------------------------------------------------------------------ uneven-n queue */
+/* No counterpart in the reference, whose runtime-n solver (nvrtc_solver.hpp:99-145) serves one n
+ * per instance; this replaces "one NvrtcGeneigSolver + one launch per n" for a mixed batch.
+ * A queue is planned once for the orders n[0..count) of a batch and launched any number of times:
+ *   - Packed layout: pair p's A, B and X are n[p] x n[p] column-major starting at element
+ *     sum_{q<p} n[q]^2 of d_A / d_B / d_X; its eigenvalues at element sum_{q<p} n[q] of d_W; its
+ *     info at d_info[p].  A and B are read as in sbg_solver_launch (A full, B lower).
+ *   - Every n gets its own solver with the per-n schedule (opts->tuning_mode as in
+ *     sbg_solver_create: the table, or the autotuner); opts->precision = MIXED applies to the
+ *     n that the mixed form supports (sbg_max_n) and the others run FP64 (sbg_queue_bucket reports
+ *     which); opts->workspace_pairs > 0 caps the pairs per internal chunk.
+ *   - sbg_launch_queue is asynchronous on `stream`: it replays one CUDA graph in which all n run
+ *     concurrently (captured on the first launch, and again when the buffers change).
+ * All calls return an sbg_status. */
+typedef struct sbg_queue sbg_queue;
+int sbg_queue_create(const int* n, int count, int device_id, const sbg_solver_options* opts, sbg_queue** out);
+int sbg_queue_destroy(sbg_queue* q);
+int sbg_launch_queue(sbg_queue* q, const cuDoubleComplex* d_A, const cuDoubleComplex* d_B, double* d_W,
+                     cuDoubleComplex* d_X, int* d_info, cudaStream_t stream);
+int sbg_queue_size(const sbg_queue* q);
+/* Complex elements of the packed A (= B, X) and doubles of the packed W. */
+long long sbg_queue_matrix_elements(const sbg_queue* q);
+long long sbg_queue_vector_elements(const sbg_queue* q);
+/* Distinct n (buckets, largest n first) and, per bucket, its n, pair count, pairs per chunk,
+ * precision and whether its schedule came from the autotuner. */
+int sbg_queue_buckets(const sbg_queue* q);
+int sbg_queue_bucket(const sbg_queue* q, int i, int* n, int* count, int* chunk, int* precision, int* was_autotuned);
+/* How many times the launch graph was captured (1 while the buffers stay the same). */
+int sbg_queue_graph_builds(const sbg_queue* q);
 
 /* ------------------------------------------------------------------ allocation-free solve */
 /* This entry point has no counterpart in the reference.

@@ -1,0 +1,228 @@
+// Internal: the solver handle behind the C ABI (capi.cu) and the uneven-n queue
+// (queue.cu), with the error plumbing both use.  Not part of the public header.
+#pragma once
+
+#include "sbg/geneig.h"
+#include "kernels.cuh"
+#include "tuning.h"
+
+#include <algorithm>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace sbgi {
+
+extern thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+inline void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw Error(e == cudaErrorMemoryAllocation ? SBG_ERR_NO_MEMORY : SBG_ERR_CUDA,
+                    std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return SBG_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.status;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return SBG_ERR_INTERNAL;
+    } catch (...) {
+        g_last_error = "unknown exception";
+        return SBG_ERR_INTERNAL;
+    }
+}
+
+// Device workspace of one stream slot; grows on demand, never during capture.
+struct Slot {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int capacity = 0;
+};
+
+inline int default_chunk_pairs(int n) {
+    const size_t per = sbg::workspace_bytes_per_pair(n);
+    const size_t target = size_t(1) << 30;     // about 1 GiB of scratch per stream slot
+    size_t pairs = target / std::max<size_t>(per, 1);
+    pairs = std::min<size_t>(std::max<size_t>(pairs, 1024), 65536);
+    return static_cast<int>(pairs);
+}
+
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) check_cuda(cudaSetDevice(dev), "cudaSetDevice");
+    }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+// Creates a solver for order n (throws Error).
+void create_solver(int n, int device, const sbg_solver_options* o, sbg_solver** out);
+
+}  // namespace sbgi
+
+using namespace sbgi;
+
+struct sbg_solver {
+    int n = 0;
+    int device = 0;
+    int precision = SBG_PRECISION_FP64;
+    int refine_steps = 2;
+    int chunk_pairs = 0;
+    sbg::Schedule sched;
+    bool autotuned = false;
+    bool sweep_ran = false;
+    const char* layer = "compile";
+    std::mutex mu;
+    std::vector<Slot> slots;
+    // staging buffers of the host-buffer path, one per internal stream
+    struct Staging { void* A = nullptr; void* B = nullptr; void* X = nullptr; void* W = nullptr; void* info = nullptr;
+                     int capacity = 0; cudaStream_t stream = nullptr; };
+    std::vector<Staging> staging;
+    // per-stage event timing
+    bool timing = false;
+    struct StageEvents { int stage; int kernels; cudaEvent_t a, b; };
+    std::vector<StageEvents> stage_events;
+
+    ~sbg_solver() {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(device);
+        for (auto& s : slots) if (s.ptr) cudaFree(s.ptr);
+        for (auto& st : staging) {
+            if (st.stream) cudaStreamDestroy(st.stream);
+            for (void* p : {st.A, st.B, st.X, st.W, st.info}) if (p) cudaFree(p);
+        }
+        for (auto& e : stage_events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+        cudaSetDevice(prev);
+    }
+
+    void stage_begin(cudaStream_t stream, cudaEvent_t* a) {
+        *a = nullptr;
+        if (!timing) return;
+        check_cuda(cudaEventCreate(a), "cudaEventCreate");
+        check_cuda(cudaEventRecord(*a, stream), "cudaEventRecord");
+    }
+    void stage_end(cudaStream_t stream, cudaEvent_t a, int stage, int kernels) {
+        if (!timing || !a) return;
+        cudaEvent_t b;
+        check_cuda(cudaEventCreate(&b), "cudaEventCreate");
+        check_cuda(cudaEventRecord(b, stream), "cudaEventRecord");
+        std::lock_guard<std::mutex> lock(mu);
+        stage_events.push_back({stage, kernels, a, b});
+    }
+
+    sbg::Workspace workspace(int slot_idx, int pairs, cudaStream_t stream) {
+        std::lock_guard<std::mutex> lock(mu);
+        if (static_cast<int>(slots.size()) <= slot_idx) slots.resize(slot_idx + 1);
+        Slot& s = slots[slot_idx];
+        if (s.capacity < pairs) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            if (stream) check_cuda(cudaStreamIsCapturing(stream, &cs), "cudaStreamIsCapturing");
+            if (cs != cudaStreamCaptureStatusNone)
+                throw Error(SBG_ERR_CAPTURING, "workspace must grow while the stream is capturing; "
+                                               "call sbg_solver_reserve before capture");
+            if (s.ptr) { check_cuda(cudaFree(s.ptr), "cudaFree"); s.ptr = nullptr; s.capacity = 0; }
+            const size_t bytes = sbg::workspace_bytes_per_pair(n) * static_cast<size_t>(pairs) + 5 * 256;
+            check_cuda(cudaMalloc(&s.ptr, bytes), "cudaMalloc(workspace)");
+            s.bytes = bytes;
+            s.capacity = pairs;
+        }
+        return sbg::carve_workspace(s.ptr, n, s.capacity);
+    }
+
+    // One chunk of at most chunk_pairs pairs through the three stages.
+    void run_chunk(const double2* A, const double2* B, double* W, double2* X, int* info, int cnt,
+                   const sbg::Workspace& ws, cudaStream_t stream) {
+        cudaEvent_t ev;
+        stage_begin(stream, &ev);
+        check_cuda(sbg::launch_reduce(sbg::kReduceFull, A, B, n, cnt, ws, X, info,
+                                      sched.reduce_threads, stream), "reduce kernel");
+        stage_end(stream, ev, 0, 1);
+        stage_begin(stream, &ev);
+        check_cuda(sbg::launch_hetrd(n, cnt, X, ws, info, sched.hetrd_threads, stream), "hetrd kernel");
+        stage_end(stream, ev, 1, 1);
+        stage_begin(stream, &ev);
+        if (precision == SBG_PRECISION_MIXED)
+            check_cuda(sbg::launch_tridiag_mixed(n, cnt, ws, W, X, info, refine_steps, sched.chain_threads,
+                                                 sched.ql_warps, sched.refine_threads, stream),
+                       "mixed eigensolve kernels");
+        else
+            check_cuda(sbg::launch_ql_logged(n, cnt, ws, W, X, info, false, sched.chain_threads, sched.ql_warps,
+                                             stream), "QL kernels");
+        stage_end(stream, ev, 2, precision == SBG_PRECISION_MIXED ? 3 : 2);
+        stage_begin(stream, &ev);
+        check_cuda(sbg::launch_back(sbg::kBackFull, n, cnt, ws, X, info, sched.back_threads, stream),
+                   "back-transform kernel");
+        stage_end(stream, ev, 3, 1);
+    }
+
+    void solve_host(const double2* hA, const double2* hB, double* hW, double2* hX, int* hinfo, int batch,
+                    int chunk, int nstreams) {
+        if (batch < 0 || chunk <= 0 || nstreams <= 0) throw Error(SBG_ERR_INVALID_VALUE, "bad solve_host arguments");
+        if (batch == 0) return;
+        if (!hA || !hB || !hW || !hX || !hinfo) throw Error(SBG_ERR_INVALID_VALUE, "null host pointer");
+        chunk = std::min(chunk, batch);
+        const size_t nn = static_cast<size_t>(n) * n;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            if (static_cast<int>(staging.size()) < nstreams) staging.resize(nstreams);
+            for (int i = 0; i < nstreams; ++i) {
+                Staging& st = staging[i];
+                if (!st.stream) check_cuda(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+                if (st.capacity < chunk) {
+                    for (void** p : {&st.A, &st.B, &st.X, &st.W, &st.info}) if (*p) { cudaFree(*p); *p = nullptr; }
+                    check_cuda(cudaMalloc(&st.A, 16 * nn * chunk), "cudaMalloc(staging)");
+                    check_cuda(cudaMalloc(&st.B, 16 * nn * chunk), "cudaMalloc(staging)");
+                    check_cuda(cudaMalloc(&st.X, 16 * nn * chunk), "cudaMalloc(staging)");
+                    check_cuda(cudaMalloc(&st.W, 8 * static_cast<size_t>(n) * chunk), "cudaMalloc(staging)");
+                    check_cuda(cudaMalloc(&st.info, 4 * static_cast<size_t>(chunk)), "cudaMalloc(staging)");
+                    st.capacity = chunk;
+                }
+            }
+        }
+        int idx = 0;
+        for (int off = 0; off < batch; off += chunk, ++idx) {
+            const int cnt = std::min(chunk, batch - off);
+            Staging& st = staging[idx % nstreams];
+            check_cuda(cudaMemcpyAsync(st.A, hA + nn * off, 16 * nn * cnt, cudaMemcpyHostToDevice, st.stream), "H2D A");
+            check_cuda(cudaMemcpyAsync(st.B, hB + nn * off, 16 * nn * cnt, cudaMemcpyHostToDevice, st.stream), "H2D B");
+            launch(static_cast<double2*>(st.A), static_cast<double2*>(st.B), static_cast<double*>(st.W),
+                   static_cast<double2*>(st.X), static_cast<int*>(st.info), cnt, st.stream, idx % nstreams);
+            check_cuda(cudaMemcpyAsync(hX + nn * off, st.X, 16 * nn * cnt, cudaMemcpyDeviceToHost, st.stream), "D2H X");
+            check_cuda(cudaMemcpyAsync(hW + static_cast<size_t>(n) * off, st.W, 8 * static_cast<size_t>(n) * cnt,
+                                       cudaMemcpyDeviceToHost, st.stream), "D2H W");
+            check_cuda(cudaMemcpyAsync(hinfo + off, st.info, 4 * static_cast<size_t>(cnt), cudaMemcpyDeviceToHost,
+                                       st.stream), "D2H info");
+        }
+        for (int i = 0; i < nstreams; ++i) check_cuda(cudaStreamSynchronize(staging[i].stream), "cudaStreamSynchronize");
+    }
+
+    void launch(const double2* A, const double2* B, double* W, double2* X, int* info, int batch,
+                cudaStream_t stream, int slot_idx = 0) {
+        if (batch < 0) throw Error(SBG_ERR_INVALID_VALUE, "batch < 0");
+        if (batch == 0) return;
+        if (!A || !B || !W || !X || !info) throw Error(SBG_ERR_INVALID_VALUE, "null device pointer");
+        const size_t nn = static_cast<size_t>(n) * n;
+        const int cap = std::min(batch, chunk_pairs);
+        sbg::Workspace ws = workspace(slot_idx, cap, stream);
+        for (int off = 0; off < batch; off += ws.capacity) {
+            const int cnt = std::min(ws.capacity, batch - off);
+            run_chunk(A + nn * off, B + nn * off, W + static_cast<size_t>(n) * off, X + nn * off, info + off,
+                      cnt, ws, stream);
+        }
+    }
+};

@@ -22,7 +22,7 @@ from . import _lib
 from ._lib import SolverOptions, load
 
 __all__ = [
-    "Solver", "SolverError", "solve", "to_colmajor", "from_colmajor", "max_n",
+    "Solver", "SolverError", "Queue", "pack_pairs", "unpack", "solve", "to_colmajor", "from_colmajor", "max_n",
     "geneig_full_n54_batched", "chol_n54", "reduce_n54", "reduce_eig_n54", "full_n54", "finish_n54",
     "PRECISIONS", "fixed_n54_introspection", "tuning_table_path", "tuning_forget_in_process",
 ]
@@ -194,6 +194,108 @@ class Solver:
     @property
     def cache_layer_used(self) -> str:
         return self._lib.sbg_solver_cache_layer_used(self._h).decode()
+
+
+class Queue:
+    """A planned batch of pairs of uneven order (sbg_queue_create / sbg_launch_queue).
+
+    ns: the order of every pair, in batch order.  Buffers are packed: pair p's A, B and X
+    are n[p] x n[p] column-major back to back (``offsets()`` gives where each starts), W
+    holds n[p] eigenvalues per pair back to back, info one int per pair.  ``pack_pairs`` /
+    ``unpack`` convert from / to lists of flat (n*n,) matrices.  One ``launch`` replays one
+    CUDA graph with every n running concurrently.
+    """
+
+    def __init__(self, ns, device: int = 0, *, precision: str = "fp64", tuning: str = "suggested",
+                 cache: str = "auto", refine_steps: int = 0, chunk_pairs: int = 0):
+        lib = load()
+        opts = SolverOptions()
+        lib.sbg_solver_options_init(ctypes.byref(opts))
+        opts.tuning_mode = _TUNING[tuning]
+        opts.cache_mode = _CACHE[cache]
+        opts.precision = PRECISIONS[precision]
+        opts.refine_steps = refine_steps
+        opts.workspace_pairs = chunk_pairs
+        ns = [int(v) for v in ns]
+        arr = (ctypes.c_int * max(1, len(ns)))(*ns)
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(device):
+            _check(lib.sbg_queue_create(arr, len(ns), device, ctypes.byref(opts), ctypes.byref(handle)),
+                   "sbg_queue_create")
+        self._h = handle
+        self._lib = lib
+        self.ns = ns
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.sbg_queue_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self) -> int:
+        return int(self._lib.sbg_queue_size(self._h))
+
+    @property
+    def matrix_elements(self) -> int:
+        return int(self._lib.sbg_queue_matrix_elements(self._h))
+
+    @property
+    def vector_elements(self) -> int:
+        return int(self._lib.sbg_queue_vector_elements(self._h))
+
+    @property
+    def graph_builds(self) -> int:
+        return int(self._lib.sbg_queue_graph_builds(self._h))
+
+    def buckets(self):
+        """[{n, count, chunk, precision, autotuned}] per distinct n, largest n first."""
+        out = []
+        for i in range(int(self._lib.sbg_queue_buckets(self._h))):
+            v = [ctypes.c_int() for _ in range(5)]
+            _check(self._lib.sbg_queue_bucket(self._h, i, *[ctypes.byref(x) for x in v]), "sbg_queue_bucket")
+            out.append({"n": v[0].value, "count": v[1].value, "chunk": v[2].value,
+                        "precision": "mixed" if v[3].value == 1 else "fp64", "autotuned": bool(v[4].value)})
+        return out
+
+    def offsets(self):
+        """(matrix element offset, vector element offset) of every pair."""
+        mo, vo, m, v = [], [], 0, 0
+        for n in self.ns:
+            mo.append(m); vo.append(v)
+            m += n * n; v += n
+        return mo, vo
+
+    def launch(self, A, B, W, X, info, stream=None) -> None:
+        for name, t, dt, size in (("A", A, torch.complex128, self.matrix_elements),
+                                  ("B", B, torch.complex128, self.matrix_elements),
+                                  ("W", W, torch.float64, self.vector_elements),
+                                  ("X", X, torch.complex128, self.matrix_elements),
+                                  ("info", info, torch.int32, len(self))):
+            if not t.is_cuda or t.dtype != dt or not t.is_contiguous() or t.numel() != size:
+                raise ValueError(f"{name} must be a contiguous CUDA {dt} tensor of {size} elements")
+        _check(self._lib.sbg_launch_queue(self._h, _ptr(A), _ptr(B), _ptr(W), _ptr(X), _ptr(info), _stream(stream)),
+               "sbg_launch_queue")
+
+
+def pack_pairs(mats):
+    """List of flat (n*n,) column-major matrices -> one packed 1-D tensor."""
+    return torch.cat([m.reshape(-1) for m in mats])
+
+
+def unpack(packed, ns, square: bool = True):
+    """Packed 1-D tensor -> list of per-pair flat tensors (n*n each, or n each if not square)."""
+    out, o = [], 0
+    for n in ns:
+        k = n * n if square else n
+        out.append(packed[o:o + k])
+        o += k
+    return out
 
 
 def solve(A, B, *, precision: str = "fp64", device: int = 0, solver: Solver | None = None, stream=None):

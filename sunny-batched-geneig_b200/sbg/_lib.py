@@ -14,6 +14,7 @@ P = ctypes.c_void_p
 I = ctypes.c_int
 U = ctypes.c_uint
 SZ = ctypes.c_size_t
+LL = ctypes.c_longlong
 
 # Every exported symbol with (restype, argtypes); the CPU tests check this list
 # against include/sbg/geneig.h.
@@ -63,6 +64,15 @@ SIGNATURES = {
     "sbg_tuning_table_path": (I, [I, ctypes.c_char_p, SZ]),
     "sbg_tuning_forget_in_process": (I, []),
     "sbg_geneig_full_noalloc_launch": (I, [I, P, P, P, P, P, I, P]),
+    "sbg_queue_create": (I, [P, I, I, P, P]),
+    "sbg_queue_destroy": (I, [P]),
+    "sbg_launch_queue": (I, [P, P, P, P, P, P, P]),
+    "sbg_queue_size": (I, [P]),
+    "sbg_queue_matrix_elements": (LL, [P]),
+    "sbg_queue_vector_elements": (LL, [P]),
+    "sbg_queue_buckets": (I, [P]),
+    "sbg_queue_bucket": (I, [P, I, P, P, P, P, P]),
+    "sbg_queue_graph_builds": (I, [P]),
 }
 
 

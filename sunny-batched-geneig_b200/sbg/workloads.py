@@ -161,3 +161,22 @@ def uneven_sizes(total: int, seed: int = 3, sizes=UNEVEN_SIZES, weights=UNEVEN_W
     rng = np.random.default_rng(seed)
     rng.shuffle(ns)
     return ns
+
+
+def uneven(total: int, seed: int = 3, frac: float = 1e-3, sizes=UNEVEN_SIZES, weights=UNEVEN_WEIGHTS,
+           device="cpu", eigvalsh=None):
+    """The uneven batch: `total` Bogoliubov pairs (A = diag(I, -I), B shifted to
+    lambda_min = frac ||B||) with n drawn from `sizes` in proportions `weights`, shuffled
+    with `seed`.  Returns (ns, A_packed, B_packed) in the queue's packed layout: the pairs
+    of each n are generated together (seed + n) and scattered to their batch positions."""
+    ns = uneven_sizes(total, seed, sizes, weights)
+    mo = np.concatenate([[0], np.cumsum(ns.astype(np.int64) ** 2)])
+    A = torch.empty(int(mo[-1]), dtype=torch.complex128, device=device)
+    B = torch.empty_like(A)
+    for n in sorted(set(int(v) for v in ns)):
+        pos = np.nonzero(ns == n)[0]
+        An, Bn = bogoliubov(n // 2, len(pos), seed=seed + n, frac=frac, device=device, eigvalsh=eigvalsh)
+        idx = torch.as_tensor((mo[pos][:, None] + np.arange(n * n)[None, :]).reshape(-1), device=device)
+        A[idx] = An.reshape(-1).to(device)
+        B[idx] = Bn.reshape(-1).to(device)
+    return ns, A, B
