@@ -54,6 +54,27 @@ FLOPS_PER_SOLVE = 32.0 * N ** 3
 BYTES_PER_SOLVE = 48 * N * N + 8 * N + 4
 STAGE_BYTES = {"reduce": 32 * N * N, "tridiag": 0, "eig": 16 * N, "back": 16 * N * N + 8 * N + 4}
 
+# The other configurations (bench.py --workload NAME): fixed-n Bogoliubov / q-sweep batches and the
+# uneven-n batch through the queue.  Each prints one JSON line of the same shape as the headline.
+OTHER_WORKLOADS = {
+    "bogoliubov54": dict(kind="bogoliubov", N=27, pairs=4096, frac=1e-2, goldstone=None,
+                         desc="Bogoliubov pairs n=54 (N=27), lambda_min(B)=1e-2||B||, A=diag(I,-I), seed 0"),
+    "qsweep32": dict(kind="qsweep", N=16, pairs=GRID ** 3, frac=1e-3, goldstone=None,
+                     desc="q-sweep n=32 (N=16 sites, 4 bonds/site, 64^3 grid), lambda_min(B)=1e-3||B||"),
+    "goldstone96": dict(kind="bogoliubov", N=48, pairs=100000, frac=1e-3, goldstone=1e-8,
+                        desc="near-Goldstone Bogoliubov pairs n=96, kappa(B)~1e8 (null mode 1e-8||B|| injected)"),
+    "goldstone192": dict(kind="bogoliubov", N=96, pairs=10000, frac=1e-3, goldstone=1e-8,
+                         desc="near-Goldstone Bogoliubov pairs n=192, kappa(B)~1e8 (cluster/DSMEM path)"),
+    "uneven": dict(kind="uneven", pairs=500000, frac=1e-3,
+                   desc="uneven batch: n in {12,24,32,54,96,128} at 10/20/20/30/15/5 %, shuffled (seed 3), "
+                        "Bogoliubov B lambda_min=1e-3||B||, one queue launch (CUDA graph)"),
+}
+
+
+def stage_flops(n):
+    return {"reduce": (4 / 3 + 4) * n ** 3, "tridiag": 16 / 3 * n ** 3, "eig": 12.0 * n ** 3,
+            "back": (16 / 3 + 4) * n ** 3}
+
 
 def env_int(name, default):
     try:
@@ -74,6 +95,8 @@ def parse():
     ap.add_argument("--e2e-pairs", type=int, default=0, help="0 = the full workload if host memory allows")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="qsweep54", choices=["qsweep54"] + sorted(OTHER_WORKLOADS),
+                    help="qsweep54 is the headline line; the others measure the remaining configurations")
     return ap.parse_args()
 
 
@@ -131,23 +154,24 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ workload
 
-def make_workload(torch, sbg, pairs: int, seed: int, device):
+def make_workload(torch, sbg, pairs: int, seed: int, device, n_sites: int = N_SITES):
     """q-sweep pairs on the device; the shift uses the eigenvalues of B0, computed by
     the FP64 solver itself with B = I (a standard Hermitian eigenproblem)."""
     from sbg import workloads as wl
-    nn = N * N
-    A = wl.metric_A(N_SITES, pairs, device)
+    n = 2 * n_sites
+    nn = n * n
+    A = wl.metric_A(n_sites, pairs, device)
     B = torch.empty((pairs, nn), dtype=torch.complex128, device=device)
-    eye = torch.eye(N, dtype=torch.complex128, device=device).reshape(1, nn)
-    solver = sbg.Solver(N, precision="fp64", workspace_pairs=16384)
+    eye = torch.eye(n, dtype=torch.complex128, device=device).reshape(1, nn)
+    solver = sbg.Solver(n, torch.cuda.current_device(), precision="fp64", workspace_pairs=16384)
     chunk = 16384
     for off in range(0, pairs, chunk):
         cnt = min(chunk, pairs - off)
         q = wl.qsweep_points(GRID, off % GRID ** 3, cnt, device)
-        B0 = wl.qsweep_B0(N_SITES, q, seed)
+        B0 = wl.qsweep_B0(n_sites, q, seed)
         Bc = wl._colmajor(B0)
         I = eye.expand(cnt, nn).contiguous()
-        W = torch.empty((cnt, N), dtype=torch.float64, device=device)
+        W = torch.empty((cnt, n), dtype=torch.float64, device=device)
         X = torch.empty_like(Bc)
         info = torch.empty(cnt, dtype=torch.int32, device=device)
         solver.launch(Bc, I, W, X, info)
@@ -220,6 +244,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "qsweep54":
+        return run_other(args)
     import torch
     import torch.distributed as dist
     import sbg
@@ -391,6 +417,264 @@ def main():
         print(json.dumps(line), flush=True)
     for s in solvers.values():
         s.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def solver_eigvalsh(torch, sbg, device, chunk=16384):
+    """Eigenvalues of Hermitian (batch, n, n) tensors by this library's FP64 solver with B = I
+    (used only to shift the synthetic B to its target lambda_min)."""
+    from sbg import workloads as wl
+
+    def f(M):
+        b, n, _ = M.shape
+        s = sbg.Solver(n, device.index or 0, precision="fp64", workspace_pairs=min(chunk, b))
+        out = torch.empty((b, n), dtype=torch.float64, device=device)
+        eye = torch.eye(n, dtype=torch.complex128, device=device).reshape(1, n * n)
+        for off in range(0, b, chunk):
+            cnt = min(chunk, b - off)
+            Bc = wl._colmajor(M[off:off + cnt].to(device))
+            X = torch.empty_like(Bc)
+            info = torch.empty(cnt, dtype=torch.int32, device=device)
+            s.launch(Bc, eye.expand(cnt, n * n).contiguous(), out[off:off + cnt], X, info)
+        torch.cuda.synchronize()
+        s.close()
+        return out
+    return f
+
+
+def cond_scaled_eig_err(n, B, W, Wr, Xr):
+    """max |dl_i| / (|l_i| kappa_i + max|l|), kappa_i = ||B|| ||x_i||^2: the eigenvalue error against
+    each eigenvalue's own perturbation scale (what an FP64 method can promise when B is ill-conditioned)."""
+    from oracle import metrics as Mx
+    normB = np.linalg.norm(Mx.as_mats(B, n), ord=2, axis=(1, 2))
+    cond = normB[:, None] * np.linalg.norm(Mx.as_mats(Xr, n), axis=1) ** 2
+    scale = np.abs(Wr) * cond + np.abs(Wr).max(axis=1, keepdims=True)
+    return float((np.abs(W - Wr) / scale).max())
+
+
+def run_other(args):
+    import torch
+    import torch.distributed as dist
+    import sbg
+    from sbg import workloads as wl
+    from oracle import metrics as Mx
+
+    cfg = OTHER_WORKLOADS[args.workload]
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    eigh = solver_eigvalsh(torch, sbg, device)
+    pairs = cfg["pairs"]
+    threads = None
+    peak = fp64_peak_tflops(torch)
+    result = {}
+    if cfg["kind"] == "uneven":
+        ns, A, B = wl.uneven(pairs, seed=3 + 1000 * rank, frac=cfg["frac"], device=device, eigvalsh=eigh)
+        q = sbg.Queue(ns, local)
+        W = torch.empty(q.vector_elements, dtype=torch.float64, device=device)
+        X = torch.empty_like(A)
+        info = torch.empty(pairs, dtype=torch.int32, device=device)
+        stream = torch.cuda.current_stream()
+        q.launch(A, B, W, X, info, stream)
+        torch.cuda.synchronize()
+        for _ in range(args.warmup):
+            q.launch(A, B, W, X, info, stream)
+        barrier()
+        clock = ClockSampler(local)
+        clock.start()
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            q.launch(A, B, W, X, info, stream)
+        e1.record(stream)
+        barrier()
+        clocks = clock.stop()
+        ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        value = world * pairs / (ms / 1e3)
+        flops = float(np.sum(32.0 * ns.astype(np.float64) ** 3))
+        result.update(value=value, ms=ms, clocks=clocks, n_mix={int(n): int((ns == n).sum()) for n in set(ns.tolist())},
+                      buckets=q.buckets(), info_nonzero=int((info != 0).sum().item()),
+                      roofline={"bound": "fp64", "kernel": "whole queue (all stage kernels)",
+                                "achieved": flops / (ms / 1e3) / 1e12, "peak": peak["tflops"], "unit": "TFLOP/s",
+                                "frac": flops / (ms / 1e3) / 1e12 / peak["tflops"], "traffic": None,
+                                "peak_source": peak["source"]})
+        if rank == 0 and not args.no_cpu:
+            from oracle import oracle as O
+            threads = O.host_threads()
+            Al = sbg.unpack(A, ns); Bl = sbg.unpack(B, ns)
+            Wl = sbg.unpack(W, ns, square=False); Xl = sbg.unpack(X, ns)
+            acc, t_mix = {}, 0.0
+            for n in sorted(set(ns.tolist())):
+                pos = np.nonzero(ns == n)[0][:64]
+                a = torch.stack([Al[p] for p in pos]).cpu().numpy(); b = torch.stack([Bl[p] for p in pos]).cpu().numpy()
+                t0 = time.perf_counter()
+                Wr, Xr, _ = O.hegv(a, b, n, nthreads=threads)
+                t_mix += (time.perf_counter() - t0) / len(pos) * int((ns == n).sum())
+                Wq = torch.stack([Wl[p] for p in pos]).cpu().numpy(); Xq = torch.stack([Xl[p] for p in pos]).cpu().numpy()
+                sm = Mx.summarize(a, b, Wq, Xq, Wr, Xr, n)
+                acc[int(n)] = {k: sm[k] for k in ("eig_rel", "residual", "orth", "cluster_sin")}
+            result["accuracy"] = acc
+            result["cpu"] = {"value": pairs / t_mix, "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": f"64 pairs per n, LAPACKE_zhegv per pair over {threads} host threads, "
+                                       "per-n time weighted by the batch's n mix"}
+        if not args.no_e2e:
+            hA = torch.empty(A.numel(), dtype=A.dtype, pin_memory=True); hA.copy_(A)
+            hB = torch.empty_like(hA, pin_memory=True); hB.copy_(B)
+            hX = torch.empty_like(hA, pin_memory=True)
+            hW = torch.empty(W.numel(), dtype=W.dtype, pin_memory=True)
+            hI = torch.empty(pairs, dtype=torch.int32, pin_memory=True)
+            times = []
+            for _ in range(max(1, min(args.steps, 3))):
+                barrier()
+                t0 = time.perf_counter()
+                A.copy_(hA, non_blocking=True); B.copy_(hB, non_blocking=True)
+                q.launch(A, B, W, X, info, stream)
+                hX.copy_(X, non_blocking=True); hW.copy_(W, non_blocking=True); hI.copy_(info, non_blocking=True)
+                torch.cuda.synchronize()
+                times.append(time.perf_counter() - t0)
+            t = max_over_ranks(statistics.median(times))
+            result["e2e"] = {"value": world * pairs / t, "unit": "solves/s", "h2d_bytes_per_step": 2 * 16 * A.numel(),
+                             "d2h_bytes_per_step": 16 * A.numel() + 8 * W.numel() + 4 * pairs}
+        q.close()
+        n_label = "uneven"
+    else:
+        N_ = cfg["N"]; n = 2 * N_
+        if cfg["kind"] == "qsweep":
+            A, B = make_workload(torch, sbg, pairs, seed=rank, device=device, n_sites=N_)
+        else:
+            A, B = wl.bogoliubov(N_, pairs, seed=rank, frac=cfg["frac"], goldstone=cfg["goldstone"], device=device,
+                                 eigvalsh=eigh)
+            A = A.to(device); B = B.to(device)
+        W = torch.empty((pairs, n), dtype=torch.float64, device=device)
+        X = torch.empty_like(B)
+        info = torch.empty(pairs, dtype=torch.int32, device=device)
+        forms = [f for f in args.forms.split(",") if f and (f == "fp64" or n <= sbg.max_n("mixed"))]
+        chunk = 65536
+        stream = torch.cuda.current_stream()
+        cap = 2048 if n <= 64 else (512 if n <= 128 else 128)
+        rng = np.random.default_rng(1234)
+        sample_idx = np.sort(rng.choice(pairs, size=min(args.sample, pairs, cap), replace=False))
+        ref = None
+        if rank == 0 and not args.no_cpu:
+            from oracle import oracle as O
+            threads = O.host_threads()
+            a = A[torch.as_tensor(sample_idx, device=device)].cpu().numpy()
+            b = B[torch.as_tensor(sample_idx, device=device)].cpu().numpy()
+            t0 = time.perf_counter()
+            Wr, Xr, _ = O.hegv(a, b, n, nthreads=threads)
+            ref = (a, b, Wr, Xr, time.perf_counter() - t0)
+        forms_out = {}
+        for f in forms:
+            s = sbg.Solver(n, local, precision=f, workspace_pairs=chunk)
+            s.launch(A, B, W, X, info, stream)
+            torch.cuda.synchronize()
+            acc = None
+            if ref is not None:
+                idx = torch.as_tensor(sample_idx, device=device)
+                Wq = W[idx].cpu().numpy(); Xq = X[idx].cpu().numpy()
+                sm = Mx.summarize(ref[0], ref[1], Wq, Xq, ref[2], ref[3], n)
+                acc = {k: sm[k] for k in ("eig_rel", "eig_rel_norm", "residual", "orth", "cluster_sin", "phase_err")}
+                acc["eig_err_cond_scaled"] = cond_scaled_eig_err(n, ref[1], Wq, ref[2], ref[3])
+                acc["lapack_residual"] = float(Mx.residual(ref[0], ref[1], ref[3], ref[2], n).max())
+                acc["lapack_orth"] = float(Mx.orth(ref[1], ref[3], n).max())
+            for _ in range(args.warmup):
+                s.launch(A, B, W, X, info, stream)
+            barrier()
+            clock = ClockSampler(local)
+            clock.start()
+            e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                s.launch(A, B, W, X, info, stream)
+            e1.record(stream)
+            barrier()
+            clocks = clock.stop()
+            ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+            s.enable_stage_timing(True)
+            for _ in range(2):
+                s.launch(A, B, W, X, info, stream)
+            torch.cuda.synchronize()
+            st = {k: (v[0] / 2, v[1] / 2) for k, v in s.read_stage_times().items()}
+            s.enable_stage_timing(False)
+            forms_out[f] = dict(value=world * pairs / (ms / 1e3), ms=ms, accuracy=acc, clocks=clocks, stages=st,
+                                info_nonzero=int((info != 0).sum().item()), solver=s)
+        best = max(forms_out, key=lambda f: forms_out[f]["value"])
+        R = forms_out[best]
+        fl = stage_flops(n)
+        st = R["stages"]
+        if st["tridiag"][1] == 0:                  # the cluster path tridiagonalises inside its reduce kernel
+            fl["reduce"] += fl["tridiag"]
+        top = max(st, key=lambda k: st[k][0])
+        ms_top = st[top][0] / max(1, st[top][1])
+        units = pairs / max(1, st[top][1])
+        achieved = fl[top] * units / (ms_top / 1e3) / 1e12
+        result.update(value=R["value"], ms=R["ms"], clocks=R["clocks"], info_nonzero=R["info_nonzero"],
+                      roofline={"bound": "fp64", "kernel": top, "achieved": achieved, "peak": peak["tflops"],
+                                "unit": "TFLOP/s", "frac": achieved / peak["tflops"], "traffic": None,
+                                "peak_source": peak["source"],
+                                "whole_solve": {"achieved_tflops": 32.0 * n ** 3 * R["value"] / world / 1e12,
+                                                "frac": 32.0 * n ** 3 * R["value"] / world / 1e12 / peak["tflops"]}},
+                      forms={f: {"value": r["value"], "ms_per_step": r["ms"], "accuracy": r["accuracy"],
+                                 "stage_ms_per_step": {k: v[0] for k, v in r["stages"].items()}}
+                             for f, r in forms_out.items()}, form=best)
+        if ref is not None:
+            result["cpu"] = {"value": len(sample_idx) / ref[4], "unit": "solves/s", "cores": threads, "kind": "port",
+                             "sample": f"{len(sample_idx)} pairs of the workload, LAPACKE_zhegv per pair over "
+                                       f"{threads} host threads"}
+        if not args.no_e2e:
+            ep = max(1, min(pairs, 65536, int(4e9 // (16 * n * n))))      # about 4 GB of pinned A
+            hA = torch.empty((ep, n * n), dtype=torch.complex128, pin_memory=True); hA.copy_(A[:ep])
+            hB = torch.empty_like(hA, pin_memory=True); hB.copy_(B[:ep])
+            hX = torch.empty_like(hA, pin_memory=True)
+            hW = torch.empty((ep, n), dtype=torch.float64, pin_memory=True)
+            hI = torch.empty(ep, dtype=torch.int32, pin_memory=True)
+            s = R["solver"]
+            s.solve_host(hA, hB, hW, hX, hI, chunk_size=min(16384, ep), num_streams=3)
+            times = []
+            for _ in range(max(1, min(args.steps, 3))):
+                barrier()
+                t0 = time.perf_counter()
+                s.solve_host(hA, hB, hW, hX, hI, chunk_size=min(16384, ep), num_streams=3)
+                times.append(time.perf_counter() - t0)
+            t = max_over_ranks(statistics.median(times))
+            result["e2e"] = {"value": world * ep / t, "unit": "solves/s", "h2d_bytes_per_step": 2 * 16 * n * n * ep,
+                             "d2h_bytes_per_step": (16 * n * n + 8 * n + 4) * ep, "pairs_per_step": ep}
+        for r in forms_out.values():
+            r["solver"].close()
+        n_label = str(n)
+    if rank == 0:
+        line = {
+            "metric": f"solves/s ({args.workload})", "value": result["value"], "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": result["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": cfg["desc"], "n": n_label, "pairs_per_gpu": pairs,
+                       "l2": "inputs larger than L2; no flush" if pairs * 32 * 54 * 54 > 126e6 else "inputs in L2"},
+            "roofline": result["roofline"], "cpu_baseline": result.get("cpu"), "e2e": result.get("e2e"),
+            "clocks": result["clocks"], "info_nonzero": result["info_nonzero"],
+        }
+        for k in ("forms", "form", "accuracy", "n_mix", "buckets"):
+            if k in result:
+                line[k] = result[k]
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
