@@ -54,6 +54,11 @@ FLOPS_PER_SOLVE = 32.0 * N ** 3
 BYTES_PER_SOLVE = 48 * N * N + 8 * N + 4
 STAGE_BYTES = {"reduce": 32 * N * N, "tridiag": 0, "eig": 16 * N, "back": 16 * N * N + 8 * N + 4}
 
+# DRAM bytes (read + write) per pair of each FP64 stage at n = 54, from one ncu capture of a
+# 16,384-pair solve (profiles/ncu_stage_kernels_qsweep_n54_16384pairs.md); DRAM traffic grows in
+# proportion to the pairs a launch processes, so traffic per launch = this x pairs per launch.
+TRAFFIC_PER_PAIR_N54 = {"reduce": 51.4e3 + 120.0e3, "tridiag": 52.2e3, "eig": 52.8e3 + 76.2e3, "back": 114.0e3}
+
 # The other configurations (bench.py --workload NAME): fixed-n Bogoliubov / q-sweep batches and the
 # uneven-n batch through the queue.  Each prints one JSON line of the same shape as the headline.
 OTHER_WORKLOADS = {
@@ -391,7 +396,10 @@ def main():
         achieved = STAGE_FLOPS[top] * units / (ms_top / 1e3) / 1e12
         hbm_achieved = BYTES_PER_SOLVE * R["value"] / world / 1e9
         roofline = {"bound": "fp64", "kernel": top, "achieved": achieved, "peak": fp64_peak["tflops"],
-                    "unit": "TFLOP/s", "frac": achieved / fp64_peak["tflops"], "traffic": None,
+                    "unit": "TFLOP/s", "frac": achieved / fp64_peak["tflops"],
+                    "traffic": TRAFFIC_PER_PAIR_N54[top] * units if best == "fp64" else None,
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per pair, 16,384-pair "
+                                      "capture, scaled to the launch's pairs",
                     "peak_source": fp64_peak["source"],
                     "algorithmic_flops_per_pair": STAGE_FLOPS[top], "pairs_per_launch": units,
                     "avg_launch_ms": ms_top,
