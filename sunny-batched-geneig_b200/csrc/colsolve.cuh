@@ -163,4 +163,68 @@ __device__ __forceinline__ void col_trsm_lowerH(const cplx<R>* LV, int ld, const
     }
 }
 
+// ---------------------------------------------------------------- G lanes per column
+// The same sweeps with a column's rows spread over G adjacent lanes (G = 1 or 2): lane g of
+// the group holds rows i = G r + g in y[r], r < RM.  Control flow is uniform over the group
+// (the sweep's block range is taken for the whole group, rows are predicated), so the
+// group's partial dot products combine with one shuffle; every lane of the warp must call.
+
+// y <- Q y (see col_apply_q).
+template <int G, int RM, typename R>
+__device__ __forceinline__ void grp_apply_q(const cplx<R>* LV, int ld, const cplx<R>* tau, cplx<R> (&y)[RM], int n,
+                                            int g) {
+    using C = cplx<R>;
+    const int nb = ((n - 1) / G) >> 3;               // block of the highest slot any lane holds
+    for (int k = n - 2; k >= 0; --k) {
+        const C tk = tau[k];
+        if (tk.x == R(0) && tk.y == R(0)) continue;
+        const C* vrow = LV + k;                      // v_k(i) = vrow[i * ld], i >= k + 1
+        const int kb = (k + 1) / G - 1;              // slots <= kb are inactive on every lane
+        C s0 = mk<R>(R(0), R(0)), s1 = s0;
+#define SBG_S(I) if constexpr ((I) < RM) { const int i = G * (I) + g; if (i > k && i < n) { \
+        if ((I) & 1) s1 = cfmac(vrow[i * ld], y[I], s1); else s0 = cfmac(vrow[i * ld], y[I], s0); } }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= kb) break; SBG_ROWS8(SBG_S, B)
+        switch (nb) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+        C s = cadd(s0, s1);
+        if constexpr (G > 1) {
+#pragma unroll
+            for (int m = 1; m < G; m <<= 1) { s.x += shfl_xor(s.x, m); s.y += shfl_xor(s.y, m); }
+        }
+        s = cmul(tk, s);
+        asm volatile("" ::: "memory");               // reload v_k below rather than hold it in registers
+#define SBG_S(I) if constexpr ((I) < RM) { const int i = G * (I) + g; if (i > k && i < n) y[I] = cfms(vrow[i * ld], s, y[I]); }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= kb) break; SBG_ROWS8(SBG_S, B)
+        switch (nb) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+    }
+}
+
+// x = L^{-H} y (see col_trsm_lowerH); out(k, x_k) is called on the lane that holds row k.
+template <int G, int RM, typename R, typename Out>
+__device__ __forceinline__ void grp_trsm_lowerH(const cplx<R>* LV, int ld, const R* invd, cplx<R> (&y)[RM], int n,
+                                                int g, Out&& out) {
+    using C = cplx<R>;
+    const int lane = threadIdx.x & 31;
+    for (int k = n - 1; k >= 0; --k) {
+        const int rk = k / G, gk = k - rk * G;       // row k: slot rk of lane gk
+        C piv = y[0];
+#define SBG_SEL(I) case I: if constexpr ((I) < RM) piv = y[I]; break;
+        switch (rk) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
+        if constexpr (G > 1) piv = cshfl(piv, (lane & ~(G - 1)) | gk);
+        const C xk = cscale(piv, invd[k]);
+        if (g == gk) out(k, xk);
+        if (k == 0) break;
+        const C* lrow = LV + k;                      // L(k, i) = lrow[i * ld], i < k
+#define SBG_S(I) if constexpr ((I) < RM) { const int i = G * (I) + g; if (i < k) y[I] = cfms(cconj(lrow[i * ld]), xk, y[I]); }
+#define SBG_K(B) case B: SBG_ROWS8(SBG_S, B)
+        switch (((k - 1) / G) >> 3) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+    }
+}
+
 }  // namespace sbg

@@ -180,8 +180,8 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_reduce(int mode, const d
 
 struct BackSmem {
     size_t LVs, invd, tau, bar, total;
-    __host__ __device__ BackSmem(int n) {
-        const size_t ld = static_cast<size_t>(tile_ld(n));
+    __host__ __device__ BackSmem(int n, int tile_ld_override = 0) {
+        const size_t ld = static_cast<size_t>(tile_ld_override > 0 ? tile_ld_override : tile_ld(n));
         size_t o = 0;
         LVs = o;  o += 16 * ld * n;
         invd = o; o += align_up(8 * n, 16);
@@ -297,11 +297,21 @@ __global__ void __launch_bounds__(NMAX, 4) k_hegst_col(int mode, const double2* 
 }
 
 // ----------------------------------------------------------------------------- k_back_col
-// One CTA of NMAX threads per pair (n <= NMAX): thread j holds column j of Z in
-// registers, applies Q and L^{-H}, and stores X(:, j) (kBackQOnly: Q Z).
-template <int NMAX>
-__global__ void __launch_bounds__(NMAX, 4) k_back_col(int mode, int n, int batch, Workspace ws,
-                                                   double2* __restrict__ X, const int* __restrict__ info) {
+// One CTA per pair (n <= NMAX): the G adjacent lanes of group j hold column j of Z in
+// registers (rows G r + g), apply Q and L^{-H}, and store X(:, j) (kBackQOnly: Q Z).  The
+// CTA is rounded up to whole warps; lanes of columns j >= n run the sweeps on zeros (the
+// group shuffles need the full warp) and store nothing.
+template <int NMAX, int G>
+__host__ __device__ constexpr int back_col_threads() { return (NMAX * G + 31) / 32 * 32; }
+
+template <int NMAX, int G>
+__global__ void __launch_bounds__(back_col_threads<NMAX, G>(), G == 1 ? 4 : 3) k_back_col(int mode, int n, int batch, Workspace ws,
+                                                                            double2* __restrict__ X,
+                                                                            const int* __restrict__ info) {
+    constexpr int T = back_col_threads<NMAX, G>();
+    constexpr int RM = (NMAX + G - 1) / G;
+    // tile_ld(NMAX) as a compile-time stride: every row slot's offset is an immediate
+    constexpr int LDC = (((NMAX | 1) & 7) == 7) ? (NMAX | 1) + 2 : (NMAX | 1);
     const int b = blockIdx.x;
     if (b >= batch) return;
     const size_t mat = static_cast<size_t>(n) * n;
@@ -309,12 +319,12 @@ __global__ void __launch_bounds__(NMAX, 4) k_back_col(int mode, int n, int batch
     const int tid = threadIdx.x;
     if (info[b] > n || info[b] < 0) {
         const double nan = __longlong_as_double(0x7ff8000000000000ll);
-        for (size_t idx = tid; idx < mat; idx += NMAX) Xb[idx] = make_double2(nan, nan);
+        for (size_t idx = tid; idx < mat; idx += T) Xb[idx] = make_double2(nan, nan);
         return;
     }
     extern __shared__ __align__(16) unsigned char smem[];
-    const BackSmem lay(n);
-    const int ld = tile_ld(n);
+    const BackSmem lay(n, LDC);
+    constexpr int ld = LDC;
     double2* LVs = reinterpret_cast<double2*>(smem + lay.LVs);
     double* invd = reinterpret_cast<double*>(smem + lay.invd);
     double2* tau_s = reinterpret_cast<double2*>(smem + lay.tau);
@@ -328,24 +338,29 @@ __global__ void __launch_bounds__(NMAX, 4) k_back_col(int mode, int n, int batch
         for (int j = tid; j < n; j += 32)
             bulk_g2s(LVs + static_cast<size_t>(j) * ld, LVg + static_cast<size_t>(j) * n, 16u * n, bar);
     }
-    const bool own = tid < n;
+    const int col = tid / G, g = tid - col * G;
+    const bool own = col < n;
     const double* Zg = reinterpret_cast<const double*>(Xb);
-    double2 y[NMAX];
+    double2 y[RM];
 #pragma unroll
-    for (int i = 0; i < NMAX; ++i)
-        y[i] = make_double2((own && i < n) ? Zg[i + static_cast<size_t>(tid) * n] : 0.0, 0.0);
-    for (int i = tid; i < n; i += NMAX) tau_s[i] = ws.tau[static_cast<size_t>(n) * b + i];
+    for (int r = 0; r < RM; ++r) {
+        const int i = G * r + g;
+        y[r] = make_double2((own && i < n) ? Zg[i + static_cast<size_t>(col) * n] : 0.0, 0.0);
+    }
+    for (int i = tid; i < n; i += T) tau_s[i] = ws.tau[static_cast<size_t>(n) * b + i];
     wait_copies(bar, nullptr);
-    for (int i = tid; i < n; i += NMAX) invd[i] = 1.0 / LVs[i + i * ld].x;
+    for (int i = tid; i < n; i += T) invd[i] = 1.0 / LVs[i + i * ld].x;
     __syncthreads();               // all of Z is in registers before any X is stored over it
-    if (!own) return;
-    col_apply_q<NMAX, double>(LVs, ld, tau_s, y, n);
-    double2* xcol = Xb + static_cast<size_t>(tid) * n;
+    grp_apply_q<G, RM, double>(LVs, ld, tau_s, y, n, g);
+    double2* xcol = Xb + static_cast<size_t>(col) * n;
     if (mode == kBackFull) {
-        col_trsm_lowerH<NMAX>(LVs, ld, invd, y, n, [&](int k, double2 x) { xcol[k] = x; });
-    } else {
+        grp_trsm_lowerH<G, RM>(LVs, ld, invd, y, n, g, [&](int k, double2 x) { if (own) xcol[k] = x; });
+    } else if (own) {
 #pragma unroll
-        for (int i = 0; i < NMAX; ++i) if (i < n) xcol[i] = y[i];
+        for (int r = 0; r < RM; ++r) {
+            const int i = G * r + g;
+            if (i < n) xcol[i] = y[r];
+        }
     }
 }
 
@@ -1018,12 +1033,22 @@ cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* 
     return cudaGetLastError();
 }
 
+template <int NMAX, int G>
+void run_back_col_g(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info, size_t smem,
+                    cudaStream_t stream) {
+    static std::once_flag f;
+    set_max_smem_once(k_back_col<NMAX, G>, f);
+    smem = BackSmem(n, (((NMAX | 1) & 7) == 7) ? (NMAX | 1) + 2 : (NMAX | 1)).total;
+    k_back_col<NMAX, G><<<batch, back_col_threads<NMAX, G>(), smem, stream>>>(mode, n, batch, ws, X, info);
+}
+
+// One lane per column: measured at n = 54, splitting a column over 2 lanes (G = 2, 3 CTAs
+// per SM) gives the same time as G = 1 (4 CTAs per SM); the per-lane chain halves but the
+// shuffles and the lower occupancy eat the gain.
 template <int NMAX>
 void run_back_col(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info, size_t smem,
                   cudaStream_t stream) {
-    static std::once_flag f;
-    set_max_smem_once(k_back_col<NMAX>, f);
-    k_back_col<NMAX><<<batch, NMAX, smem, stream>>>(mode, n, batch, ws, X, info);
+    run_back_col_g<NMAX, 1>(mode, n, batch, ws, X, info, smem, stream);
 }
 
 cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
