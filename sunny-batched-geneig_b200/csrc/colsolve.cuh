@@ -53,14 +53,17 @@ __device__ int potrf_warp_packed(cplx<R>* P, int n, R* invd) {
         const int h = (m + 1) >> 1;
         const int r1 = lane, r2 = m - 1 - lane;
         // A22(r, j) at P + pk(base) + r - j + sum_{t<j} (m - t): advances by m - j - 1 per column
+        // rows r1 (r1 + 1 terms) then r2 (r2 + 1 terms) in one loop of uniform length m + 1
         if (lane < h) {
-            const C l1 = colk[1 + r1];
+            const int tot = (r2 != r1) ? r1 + r2 + 2 : r1 + 1;
             C* a = P + pk(base, n) + r1;
-            for (int j = 0; j <= r1; ++j) { *a = cfmsc(l1, colk[1 + j], *a); a += m - j - 1; }
-            if (r2 != r1) {
-                const C l2 = colk[1 + r2];
-                a = P + pk(base, n) + r2;
-                for (int j = 0; j <= r2; ++j) { *a = cfmsc(l2, colk[1 + j], *a); a += m - j - 1; }
+            C l = colk[1 + r1];
+            int jj = 0;
+            for (int t = 0; t < tot; ++t) {
+                if (t == r1 + 1) { a = P + pk(base, n) + r2; l = colk[1 + r2]; jj = 0; }
+                *a = cfmsc(l, colk[1 + jj], *a);
+                a += m - jj - 1;
+                ++jj;
             }
         }
         __syncwarp();

@@ -848,40 +848,59 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
         const int r1 = lane, r2 = m - 1 - lane;
         const bool own1 = lane < h;
         const bool own2 = lane < h && r2 != r1;
-        // ---- p = tau A22 v for the owned rows
+        // ---- p = tau A22 v for the owned rows.  Each lane walks its two rows in ONE loop of
+        // uniform length (row r1's terms, then row r2's), so no lane waits for the others' longer
+        // row: the pair (r1, r2 = m-1-r1) has m-1 terms in the lower row walk, m-1 in the
+        // mirrored column walk and m+1 in the rank-2 update.
         // Row walk of the packed lower part: A22(r, j) sits at P + c0 + r - j + sum_{t<j} (n - base - t),
         // so the address advances by (m - j - 1) from column j to j + 1 (incremental, no pk() per term).
-        const C* c0 = P + pk(base, n);
+        C* c0 = P + pk(base, n);
         C p1 = mk<R>(R(0), R(0)), p2 = mk<R>(R(0), R(0));
         if (own1) {
-            C a0 = mk<R>(R(0), R(0)), a1 = mk<R>(R(0), R(0)), a2 = mk<R>(R(0), R(0));
+            const C zero = mk<R>(R(0), R(0));
+            // lower row walk: r1 terms of row r1, then r2 terms of row r2
+            C acc0 = zero, acc1 = zero, low1 = zero;
             const C* pa = c0 + r1;
-            int j = 0;
-            for (; j + 1 < r1; j += 2) {
-                a0 = cfma(*pa, vb[j], a0); pa += m - j - 1;
-                a2 = cfma(*pa, vb[j + 1], a2); pa += m - j - 2;
+            const C* diag1 = nullptr;
+            const int tot = own2 ? r1 + r2 : r1;
+            int jj = 0;
+            for (int t = 0; t < tot; ++t) {
+                if (t == r1) { diag1 = pa; low1 = cadd(acc0, acc1); acc0 = zero; acc1 = zero; pa = c0 + r2; jj = 0; }
+                if (t & 1) acc1 = cfma(*pa, vb[jj], acc1); else acc0 = cfma(*pa, vb[jj], acc0);
+                pa += m - jj - 1;
+                ++jj;
             }
-            for (; j < r1; ++j) { a0 = cfma(*pa, vb[j], a0); pa += m - j - 1; }
-            const C* col = pa;                                                   // = A22(r1, r1), column r1
-            a1.x = fma(col[0].x, vb[r1].x, a1.x);
-            a1.y = fma(col[0].x, vb[r1].y, a1.y);
-            for (int t = 1; t + r1 < m; ++t) a1 = cfmac(col[t], vb[r1 + t], a1);   // mirrored upper
-            p1 = cmul(tk, cadd(cadd(a0, a2), a1));
-        }
-        if (own2) {
-            C a0 = mk<R>(R(0), R(0)), a1 = mk<R>(R(0), R(0)), a2 = mk<R>(R(0), R(0));
-            const C* pa = c0 + r2;
-            int j = 0;
-            for (; j + 1 < r2; j += 2) {
-                a0 = cfma(*pa, vb[j], a0); pa += m - j - 1;
-                a2 = cfma(*pa, vb[j + 1], a2); pa += m - j - 2;
+            // own2: the switch ran (r2 >= 1), acc holds row r2 and pa points at A22(r2, r2);
+            // otherwise acc holds row r1 and pa points at A22(r1, r1)
+            C low2 = zero;
+            const C* diag2 = nullptr;
+            if (own2) { low2 = cadd(acc0, acc1); diag2 = pa; }
+            else { low1 = cadd(acc0, acc1); diag1 = pa; }
+            // mirrored upper column walk: m-1-r1 terms of column r1, then r1 terms of column r2
+            const int sw = m - 1 - r1;
+            const int tot2 = own2 ? m - 1 : sw;
+            C u0 = zero, u1 = zero, up1 = zero;
+            const C* cp = diag1;
+            int vbase = r1, tt = 1;
+            bool switched = false;
+            for (int t = 0; t < tot2; ++t) {
+                if (t == sw) { up1 = cadd(u0, u1); u0 = zero; u1 = zero; cp = diag2; vbase = r2; tt = 1; switched = true; }
+                if (t & 1) u1 = cfmac(cp[tt], vb[vbase + tt], u1); else u0 = cfmac(cp[tt], vb[vbase + tt], u0);
+                ++tt;
             }
-            for (; j < r2; ++j) { a0 = cfma(*pa, vb[j], a0); pa += m - j - 1; }
-            const C* col = pa;
-            a1.x = fma(col[0].x, vb[r2].x, a1.x);
-            a1.y = fma(col[0].x, vb[r2].y, a1.y);
-            for (int t = 1; t + r2 < m; ++t) a1 = cfmac(col[t], vb[r2 + t], a1);
-            p2 = cmul(tk, cadd(cadd(a0, a2), a1));
+            C up2 = zero;
+            if (switched) up2 = cadd(u0, u1);
+            else up1 = cadd(u0, u1);
+            C a1 = up1;
+            a1.x = fma(diag1[0].x, vb[r1].x, a1.x);
+            a1.y = fma(diag1[0].x, vb[r1].y, a1.y);
+            p1 = cmul(tk, cadd(low1, a1));
+            if (own2) {
+                C a2v = up2;
+                a2v.x = fma(diag2[0].x, vb[r2].x, a2v.x);
+                a2v.y = fma(diag2[0].x, vb[r2].y, a2v.y);
+                p2 = cmul(tk, cadd(low2, a2v));
+            }
         }
         // ---- w = p - tau/2 (p^H v) v
         C dot = mk<R>(R(0), R(0));
@@ -894,32 +913,22 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
         if (own1) { w1 = cfma(a2, vb[r1], p1); wb[r1] = w1; }
         if (own2) { w2 = cfma(a2, vb[r2], p2); wb[r2] = w2; }
         __syncwarp();
-        // ---- A22 -= v w^H + w v^H on the lower triangle of the owned rows
+        // ---- A22 -= v w^H + w v^H on the lower triangle of the owned rows: r1 + 1 terms of
+        // row r1 (diagonal last), then r2 + 1 terms of row r2, in one loop
         if (own1) {
-            const C v1 = vb[r1];
-            C* a = P + pk(base, n) + r1;
-            for (int j = 0; j < r1; ++j) {
-                C t = cfmsc(v1, wb[j], *a);
-                *a = cfmsc(w1, vb[j], t);
-                a += m - j - 1;
+            const int tot = own2 ? r1 + r2 + 2 : r1 + 1;
+            C* a = c0 + r1;
+            C vr = vb[r1], wr = w1;
+            int row = r1, jj = 0;
+            for (int t = 0; t < tot; ++t) {
+                if (t == r1 + 1) { a = c0 + r2; vr = vb[r2]; wr = w2; row = r2; jj = 0; }
+                C tv = cfmsc(vr, wb[jj], *a);
+                tv = cfmsc(wr, vb[jj], tv);
+                if (jj == row) tv.y = R(0);
+                *a = tv;
+                a += m - jj - 1;
+                ++jj;
             }
-            C t = cfmsc(v1, wb[r1], *a);
-            t = cfmsc(w1, vb[r1], t);
-            t.y = R(0);
-            *a = t;
-        }
-        if (own2) {
-            const C v2 = vb[r2];
-            C* a = P + pk(base, n) + r2;
-            for (int j = 0; j < r2; ++j) {
-                C t = cfmsc(v2, wb[j], *a);
-                *a = cfmsc(w2, vb[j], t);
-                a += m - j - 1;
-            }
-            C t = cfmsc(v2, wb[r2], *a);
-            t = cfmsc(w2, vb[r2], t);
-            t.y = R(0);
-            *a = t;
         }
         __syncwarp();
     }
