@@ -1,6 +1,8 @@
-// Stage kernels for pairs beyond one SM's shared memory (84 < n <= 256).
+// Stage kernels for pairs beyond one CTA-per-pair tile of the small path (84 < n <= 256).
 //
-//   k_reduce_big     one CLUSTER of CS CTAs per pair.  Column j of every n x n operand
+//   k_reduce_mid     84 < n <= 160: one CTA per pair on the packed lower triangle (potrf,
+//                    hegst, hetrd; see below).
+//   k_reduce_big     160 < n <= 256: one CLUSTER of CS CTAs per pair.  Column j of every n x n operand
 //                    lives in CTA j % CS of the cluster (cyclic, so the work of the
 //                    triangular stages is spread evenly), in that CTA's shared memory:
 //                    the lower triangle of B / L packed by columns, and A / W / C as full
@@ -381,6 +383,324 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
     cluster_barrier<CS>();                              // no CTA leaves while a peer may read its memory
 }
 
+// ----------------------------------------------------------------------------- k_reduce_mid
+// One CTA per pair for 84 < n <= kMidMaxN, where the packed lower triangle (n(n+1)/2 complex,
+// 206 KB at n = 160) fits one SM's shared memory, so no cluster barrier is needed:
+//   potrf   B's lower triangle (TMA bulk copies, packed) factored in place, right-looking;
+//   hegst   W = L^{-1} A, then C = L^{-1} W^H with kMidLanes lanes per column (rows g + 8 r in
+//           registers), L read from the packed tile; W is parked in the pair's LV slot and C's
+//           lower triangle in its X slot (both L2-resident), L then goes to LV's lower triangle;
+//   hetrd   C's lower triangle is loaded into the tile and tridiagonalised (zhetd2's steps);
+//           reflector k goes to LV's column n-1-k (the big path's convention).
+// The Cholesky and rank-2 updates walk the balanced row pairs (q, m-1-q) of the trailing
+// matrix, each pair's fused walk split over kMidGroup threads; the Hermitian matvec splits the
+// pair's row walk and mirrored column walk the same way and combines by shuffles.
+constexpr int kMidThreads = 256;
+constexpr int kMidGroup = 4;            // threads per row pair
+constexpr int kMidLanes = 8;            // lanes per column in the triangular solves
+
+// A22(r, j) of the trailing matrix starting at c0 (packed by columns, order m) is at
+// c0 + mid_off(j, m) + r; the address advances by m - j - 1 from column j to j + 1.
+__device__ __forceinline__ int mid_off(int j, int m) { return j * m - j * (j - 1) / 2 - j; }
+
+struct MidSmem {
+    size_t P, vb, wb, pb, invd, red, misc, bar, total;
+    __host__ __device__ explicit MidSmem(int n) {
+        size_t o = 0;
+        P = o;    o += big_align(16 * static_cast<size_t>(n) * (n + 1) / 2, 16);
+        vb = o;   o += 16 * static_cast<size_t>(n);
+        wb = o;   o += 16 * static_cast<size_t>(n);
+        pb = o;   o += 16 * static_cast<size_t>(n);
+        invd = o; o += big_align(8 * static_cast<size_t>(n), 16);
+        red = o;  o += 16 * kBigWarps;
+        misc = o; o += 80;                // fail flag; tau and 1/(alpha - beta) by step parity
+        bar = o;  o += 16;
+        total = o;
+    }
+};
+
+// f(a, row, j) on the packed-lower elements A22(row, j), j <= row, of the row pairs
+// (q, m-1-q): each pair's walk (row q's q+1 terms, then row m-1-q's) split into kMidGroup chunks.
+template <class F>
+__device__ __forceinline__ void mid_pair_walk(double2* c0, int m, F&& f) {
+    const int h = (m + 1) >> 1;
+    const int grp = threadIdx.x / kMidGroup, sub = threadIdx.x % kMidGroup;
+    for (int q = grp; q < h; q += kMidThreads / kMidGroup) {
+        const int r1 = q, r2 = m - 1 - q;
+        const int tot = (r2 != r1) ? m + 1 : r1 + 1;
+        const int t0 = sub * tot / kMidGroup, t1 = (sub + 1) * tot / kMidGroup;
+        int row = t0 <= r1 ? r1 : r2;
+        int jj = t0 <= r1 ? t0 : t0 - r1 - 1;
+        double2* a = c0 + mid_off(jj, m) + row;
+        for (int t = t0; t < t1; ++t) {
+            if (t == r1 + 1) { row = r2; jj = 0; a = c0 + r2; }
+            f(a, row, jj);
+            a += m - jj - 1;
+            ++jj;
+        }
+    }
+}
+
+// y <- L^{-1} y for the group's column (rows g + kMidLanes r), L packed in shared memory.
+template <int RM>
+__device__ __forceinline__ void mid_lower_solve(double2 (&y)[RM], const double2* P, const double* invd, int n, int g) {
+    const int lane = threadIdx.x & 31;
+    for (int k = 0; k < n; ++k) {
+        const int rk = k / kMidLanes, gk = k - rk * kMidLanes;
+        double2 piv = cshfl(seg_get(y, rk), (lane & ~(kMidLanes - 1)) | gk);
+        piv = cscale(piv, invd[k]);
+        if (g == gk) seg_set(y, rk, piv);
+        const double2* lk = P + pk(k, n) - k;                 // lk[i] = L(i, k)
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+            const int i = g + kMidLanes * r;
+            if (i > k && i < n) y[r] = cfms(lk[i], piv, y[r]);
+        }
+    }
+}
+
+template <int RM>
+__global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __restrict__ A,
+                                                            const double2* __restrict__ B, int n, int batch,
+                                                            Workspace ws, double2* __restrict__ X,
+                                                            int* __restrict__ info) {
+    const int b = blockIdx.x;
+    if (b >= batch) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const MidSmem lay(n);
+    double2* P = reinterpret_cast<double2*>(smem + lay.P);
+    double2* vb = reinterpret_cast<double2*>(smem + lay.vb);
+    double2* wb = reinterpret_cast<double2*>(smem + lay.wb);
+    double2* pb = reinterpret_cast<double2*>(smem + lay.pb);
+    double* invd = reinterpret_cast<double*>(smem + lay.invd);
+    double* red = reinterpret_cast<double*>(smem + lay.red);
+    int* s_fail = reinterpret_cast<int*>(smem + lay.misc);
+    double2* s_tk = reinterpret_cast<double2*>(smem + lay.misc + 16);      // [2]
+    double2* s_sc = reinterpret_cast<double2*>(smem + lay.misc + 48);      // [2]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + lay.bar);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const size_t mat = static_cast<size_t>(n) * n;
+    const double2* Ab = A + mat * b;
+    const double2* Bb = B + mat * b;
+    double2* Xb = X + mat * b;
+    double2* LVb = ws.LV + mat * b;
+    double* db = ws.d + static_cast<size_t>(n) * b;
+    double* eb = ws.e + static_cast<size_t>(n) * b;
+    double2* taub = ws.tau + static_cast<size_t>(n) * b;
+
+    if (tid == 0) { *s_fail = 0; mbar_init(bar, 1); fence_mbar_init(); }
+    __syncthreads();
+    if (warp == 0) {
+        if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(16 * (static_cast<size_t>(n) * (n + 1) / 2)));
+        __syncwarp();
+        for (int j = lane; j < n; j += 32)
+            bulk_g2s(P + pk(j, n), Bb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
+    }
+    int status = 0;
+    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+        status = kInfoCopyTimeout;
+        mbar_wait_bounded(bar, 0, kMaxPolls);
+    }
+
+    // ---- potrf
+    for (int k = 0; k < n; ++k) {
+        double2* col = P + pk(k, n);                              // col[i - k] = A(i, k)
+        const double dkk = col[0].x;
+        __syncthreads();                                          // every thread has read dkk
+        if (!(dkk > 0.0)) { if (tid == 0) *s_fail = k + 1; break; }     // uniform
+        const double dsq = sqrt(dkk), inv = 1.0 / dsq;
+        const int m = n - k - 1;
+        for (int i = 1 + tid; i <= m; i += kMidThreads) col[i] = cscale(col[i], inv);
+        if (tid == 0) { col[0] = make_double2(dsq, 0.0); invd[k] = inv; }
+        __syncthreads();
+        if (m == 0) break;
+        const double2* l = col + 1;                               // l[r] = L(k+1+r, k)
+        mid_pair_walk(P + pk(k + 1, n), m, [&](double2* a, int row, int j) { *a = cfmsc(l[row], l[j], *a); });
+        __syncthreads();
+    }
+    __syncthreads();
+    const int fail = *s_fail;
+    if (fail) {
+        if (tid == 0) info[b] = (n + fail) | status;
+        return;
+    }
+
+    // ---- hegst: 8 lanes per column, 32 columns per pass
+    {
+        const int g = tid % kMidLanes;
+        const int cpp = kMidThreads / kMidLanes;
+        for (int c0 = 0; c0 < n; c0 += cpp) {                     // W = L^{-1} A -> LV slot
+            const int j = c0 + tid / kMidLanes;
+            const bool own = j < n;
+            double2 y[RM];
+#pragma unroll
+            for (int r = 0; r < RM; ++r) {
+                const int i = g + kMidLanes * r;
+                y[r] = (own && i < n) ? Ab[i + static_cast<size_t>(j) * n] : make_double2(0.0, 0.0);
+            }
+            mid_lower_solve<RM>(y, P, invd, n, g);
+#pragma unroll
+            for (int r = 0; r < RM; ++r) {
+                const int i = g + kMidLanes * r;
+                if (own && i < n) LVb[i + static_cast<size_t>(j) * n] = y[r];
+            }
+        }
+        __syncthreads();
+        for (int c0 = 0; c0 < n; c0 += cpp) {                     // C = L^{-1} W^H -> X slot (lower)
+            const int j = c0 + tid / kMidLanes;
+            const bool own = j < n;
+            double2 y[RM];
+#pragma unroll
+            for (int r = 0; r < RM; ++r) {
+                const int i = g + kMidLanes * r;
+                y[r] = (own && i < n) ? cconj(LVb[j + static_cast<size_t>(i) * n]) : make_double2(0.0, 0.0);
+            }
+            mid_lower_solve<RM>(y, P, invd, n, g);
+#pragma unroll
+            for (int r = 0; r < RM; ++r) {
+                const int i = g + kMidLanes * r;
+                double2 v = y[r];
+                if (i == j) v.y = 0.0;
+                if (own && i < n && i >= j) Xb[i + static_cast<size_t>(j) * n] = v;
+            }
+        }
+        __syncthreads();
+    }
+    // L -> LV lower (W is no longer needed), then C's lower triangle -> the tile
+    for (size_t idx = tid; idx < mat; idx += kMidThreads) {
+        const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
+        if (i >= j) LVb[idx] = P[pk(j, n) + i - j];
+    }
+    __syncthreads();
+    for (size_t idx = tid; idx < mat; idx += kMidThreads) {
+        const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
+        if (i >= j) P[pk(j, n) + i - j] = Xb[idx];
+    }
+    __syncthreads();
+
+    // ---- hetrd
+    const int grp = tid / kMidGroup, sub = tid % kMidGroup;
+    for (int k = 0; k + 1 < n; ++k) {
+        const int m = n - k - 1;
+        double2* x = P + pk(k, n) + 1;                            // x[i] = A(k+1+i, k)
+        if (warp == 0) {
+            double s2 = 0.0;
+            for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
+            s2 = warp_sum(s2);
+            const double2 alpha = x[0];
+            double2 tk, scale;
+            double beta;
+            if (s2 == 0.0 && alpha.y == 0.0) {
+                tk = make_double2(0.0, 0.0); beta = alpha.x; scale = make_double2(0.0, 0.0);
+            } else {
+                const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
+                beta = alpha.x >= 0.0 ? -nrm : nrm;
+                tk = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+                const double ar = alpha.x - beta, ai = alpha.y, den = ar * ar + ai * ai;
+                scale = make_double2(ar / den, -ai / den);
+            }
+            if (lane == 0) {
+                s_tk[k & 1] = tk;
+                s_sc[k & 1] = scale;
+                db[k] = P[pk(k, n)].x;
+                eb[k] = beta;
+                taub[k] = tk;
+            }
+        }
+        __syncthreads();
+        const double2 tk = s_tk[k & 1];
+        if (tk.x == 0.0 && tk.y == 0.0) continue;                 // H_k = I (uniform)
+        const double2 scale = s_sc[k & 1];
+        for (int i = tid; i < m; i += kMidThreads) {
+            const double2 v = (i == 0) ? make_double2(1.0, 0.0) : cmul(x[i], scale);
+            vb[i] = v;
+            x[i] = v;
+        }
+        __syncthreads();
+        // p = tau A22 v over the row pairs; warp-uniform loop (the group shuffles need whole warps)
+        double2* c0 = P + pk(k + 1, n);
+        const int h = (m + 1) >> 1;
+        for (int qb = 0; qb < h; qb += kMidThreads / kMidGroup) {
+            const int q = qb + grp;
+            const bool act = q < h;
+            const int r1 = q, r2 = m - 1 - q;
+            const bool two = act && r2 != r1;
+            double2 lo1 = make_double2(0.0, 0.0), lo2 = lo1, up1 = lo1, up2 = lo1;
+            if (act) {
+                // lower row walk: row r1's r1 terms, then row r2's r2 terms
+                const int tot = two ? r1 + r2 : r1;
+                const int t0 = sub * tot / kMidGroup, t1 = (sub + 1) * tot / kMidGroup;
+                int jj = t0 < r1 ? t0 : t0 - r1;
+                const double2* a = c0 + mid_off(jj, m) + (t0 < r1 ? r1 : r2);
+                for (int t = t0; t < t1; ++t) {
+                    if (t == r1) { jj = 0; a = c0 + r2; }
+                    if (t < r1) lo1 = cfma(*a, vb[jj], lo1); else lo2 = cfma(*a, vb[jj], lo2);
+                    a += m - jj - 1;
+                    ++jj;
+                }
+                // mirrored column walk: column r1 below the diagonal (m-1-r1 terms), then column r2's
+                const int sw = m - 1 - r1;
+                const int tot2 = two ? m - 1 : sw;
+                const int u0 = sub * tot2 / kMidGroup, u1 = (sub + 1) * tot2 / kMidGroup;
+                const double2* d1 = c0 + mid_off(r1, m) + r1;
+                const double2* d2 = c0 + mid_off(r2, m) + r2;
+                for (int t = u0; t < u1; ++t) {
+                    if (t < sw) up1 = cfmac(d1[t + 1], vb[r1 + t + 1], up1);
+                    else up2 = cfmac(d2[t - sw + 1], vb[r2 + t - sw + 1], up2);
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < kMidGroup; o <<= 1) {
+                lo1.x += shfl_xor(lo1.x, o); lo1.y += shfl_xor(lo1.y, o);
+                lo2.x += shfl_xor(lo2.x, o); lo2.y += shfl_xor(lo2.y, o);
+                up1.x += shfl_xor(up1.x, o); up1.y += shfl_xor(up1.y, o);
+                up2.x += shfl_xor(up2.x, o); up2.y += shfl_xor(up2.y, o);
+            }
+            if (act && sub == 0) {
+                const double2* d1 = c0 + mid_off(r1, m) + r1;
+                double2 s = cadd(lo1, up1);
+                s.x = fma(d1[0].x, vb[r1].x, s.x);
+                s.y = fma(d1[0].x, vb[r1].y, s.y);
+                pb[r1] = cmul(tk, s);
+                if (two) {
+                    const double2* d2 = c0 + mid_off(r2, m) + r2;
+                    double2 s2v = cadd(lo2, up2);
+                    s2v.x = fma(d2[0].x, vb[r2].x, s2v.x);
+                    s2v.y = fma(d2[0].x, vb[r2].y, s2v.y);
+                    pb[r2] = cmul(tk, s2v);
+                }
+            }
+        }
+        __syncthreads();
+        // w = p - tau/2 (p^H v) v
+        double2 dl = make_double2(0.0, 0.0);
+        for (int i = tid; i < m; i += kMidThreads) dl = cfmac(pb[i], vb[i], dl);
+        const double2 dot = block_sum2(dl, red);
+        const double2 a2 = cscale(cmul(tk, dot), -0.5);
+        for (int i = tid; i < m; i += kMidThreads) wb[i] = cfma(a2, vb[i], pb[i]);
+        __syncthreads();
+        // A22 -= v w^H + w v^H (lower)
+        mid_pair_walk(c0, m, [&](double2* a, int row, int j) {
+            double2 v = cfmsc(vb[row], wb[j], *a);
+            v = cfmsc(wb[row], vb[j], v);
+            if (row == j) v.y = 0.0;
+            *a = v;
+        });
+        __syncthreads();
+    }
+    if (tid == 0) {
+        db[n - 1] = P[pk(n - 1, n)].x;
+        eb[n - 1] = 0.0;
+        taub[n - 1] = make_double2(0.0, 0.0);
+    }
+    // reflector k (rows k+1 .. n-1 of column k) -> LV(s, n-1-k), s = i - k - 1
+    for (size_t idx = tid; idx < mat; idx += kMidThreads) {
+        const int k = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(k) * n);
+        if (i > k) LVb[(i - k - 1) + static_cast<size_t>(n - 1 - k) * n] = P[pk(k, n) + i - k];
+    }
+    if (tid == 0) info[b] = status;
+}
+
 // ----------------------------------------------------------------------------- k_ql_apply_rows
 template <typename R>
 __host__ __device__ inline size_t ql_rows_bytes(int n) {
@@ -626,11 +946,22 @@ void run_back_big(cudaError_t* err, int mode, int n, int batch, const Workspace&
 template <int CS, int RM>
 void big_smem_of(size_t* out, int n) { *out = BigReduceSmem(n, CS).total; }
 
+constexpr int kMidMaxN = 160;             // the packed tile + buffers fit 227 KB up to here
+
+template <int RM>
+void run_reduce_mid(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X, int* info,
+                    cudaStream_t stream) {
+    static std::once_flag f;
+    set_big_smem_once(k_reduce_mid<RM>, f, static_cast<size_t>(max_smem_optin()));
+    k_reduce_mid<RM><<<batch, kMidThreads, MidSmem(n).total, stream>>>(A, B, n, batch, ws, X, info);
+}
+
 }  // namespace
 
 bool big_path(int n) { return n > kSmallMaxN && n <= kBigMaxN; }
 
 size_t big_reduce_smem_bytes(int n) {
+    if (n <= kMidMaxN) return MidSmem(n).total;
     size_t s = 0;
     SBG_BIG_DISPATCH(n, big_smem_of, &s, n);
     return s;
@@ -641,6 +972,12 @@ cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int bat
     if (batch <= 0) return cudaSuccess;
     if (!A || !B || !X || !info || !ws.LV || !ws.d || !ws.e || !ws.tau) return cudaErrorInvalidValue;
     if (!big_path(n)) return cudaErrorInvalidValue;
+    if (n <= kMidMaxN) {                     // one CTA per pair: no cluster barriers
+        if (n <= 96) run_reduce_mid<12>(A, B, n, batch, ws, X, info, stream);
+        else if (n <= 128) run_reduce_mid<16>(A, B, n, batch, ws, X, info, stream);
+        else run_reduce_mid<20>(A, B, n, batch, ws, X, info, stream);
+        return cudaGetLastError();
+    }
     cudaError_t err = cudaSuccess;
     SBG_BIG_DISPATCH(n, run_reduce_big, &err, A, B, n, batch, ws, X, info, stream);
     return err != cudaSuccess ? err : cudaGetLastError();
