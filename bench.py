@@ -100,6 +100,8 @@ def parse():
     ap.add_argument("--e2e-pairs", type=int, default=0, help="0 = the full workload if host memory allows")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload-pairs", type=int, default=0,
+                    help="pairs for --workload other than qsweep54 (0 = the configuration's own count)")
     ap.add_argument("--workload", default="qsweep54", choices=["qsweep54"] + sorted(OTHER_WORKLOADS),
                     help="qsweep54 is the headline line; the others measure the remaining configurations")
     return ap.parse_args()
@@ -491,7 +493,7 @@ def run_other(args):
         return float(t.item())
 
     eigh = solver_eigvalsh(torch, sbg, device)
-    pairs = cfg["pairs"]
+    pairs = args.workload_pairs or cfg["pairs"]
     threads = None
     peak = fp64_peak_tflops(torch)
     result = {}
