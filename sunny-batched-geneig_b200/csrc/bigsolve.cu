@@ -22,10 +22,11 @@
 //   k_ql_apply_rows  the QL rotation log applied to one 32-row block of Z per CTA (a pair's
 //                    n x n Z does not fit one SM here); a pair whose log overflowed is solved
 //                    by the warp QL of its first block with Z in the X buffer's second half.
-//   k_back_big       one cluster per pair, each CTA a contiguous block of columns:
-//                    X = L^{-H} Q Z with warp-per-column register solves, the reflectors
-//                    and L staged a panel at a time from ws.LV.  The cluster barrier only
-//                    orders every CTA's read of Z before any write of X (they alias).
+//   k_back_big       a cluster of ceil(n / 32) CTAs per pair, each CTA a contiguous block of
+//                    32 columns: X = L^{-H} Q Z with 8 (n <= 160) or 16 lanes per column
+//                    (a column's rows in registers across its lane group), the
+//                    reflectors and L staged a panel at a time from ws.LV.  The (cluster)
+//                    barrier only orders every CTA's read of Z before any write of X (they alias).
 //
 // Workspace use (big n): ws.LV holds L in its lower triangle (diagonal included) and
 // reflector v_k packed along column n-1-k of the strict upper triangle:
@@ -767,10 +768,14 @@ struct BigBackSmem {
     }
 };
 
-template <int CS, int RM>
+// Group grp (G consecutive lanes) of the CTA holds local columns grp + (256 / G) w, w < NCW,
+// rows g + G q in y[w][q]; every dot product combines over the group with log2 G shuffles.
+// The k loops are uniform over the CTA and inactive columns run on zeros (the group shuffles
+// need whole warps).
+template <int CS, int G, int RM, int NCW>
 __global__ void __launch_bounds__(kBigThreads) k_back_big(int mode, int n, int batch, Workspace ws,
                                                           double2* __restrict__ X, const int* __restrict__ info) {
-    constexpr int NCW = ((32 * RM + CS - 1) / CS + kBigWarps - 1) / kBigWarps;
+    constexpr int GROUPS = kBigThreads / G;
     const int r = CS == 1 ? 0 : static_cast<int>(cg::this_cluster().block_rank());
     const int b = blockIdx.x / CS;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -778,21 +783,21 @@ __global__ void __launch_bounds__(kBigThreads) k_back_big(int mode, int n, int b
     double2* panel = reinterpret_cast<double2*>(smem + lay.panel);
     double2* taus = reinterpret_cast<double2*>(smem + lay.tau);
     double* invd = reinterpret_cast<double*>(smem + lay.invd);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int grp = tid / G, g = tid - grp * G;
     const size_t mat = static_cast<size_t>(n) * n;
     double2* Xb = X + mat * b;
     const double2* LVb = ws.LV + mat * b;
     const int nb = (n + CS - 1) / CS, c0 = r * nb, nc = max(0, min(n, c0 + nb) - c0);
-    const int ncw = nc > warp ? (nc - warp + kBigWarps - 1) / kBigWarps : 0;
     const bool bad = info[b] > n || info[b] < 0;
     double2 y[NCW][RM];
     const double* Zg = reinterpret_cast<const double*>(Xb);
 #pragma unroll
-    for (int c = 0; c < NCW; ++c)
+    for (int w = 0; w < NCW; ++w)
 #pragma unroll
         for (int q = 0; q < RM; ++q) {
-            const int i = lane + 32 * q, j = c0 + warp + kBigWarps * c;
-            y[c][q] = make_double2((!bad && c < ncw && i < n) ? Zg[i + static_cast<size_t>(j) * n] : 0.0, 0.0);
+            const int i = g + G * q, lc = grp + GROUPS * w;
+            y[w][q] = make_double2((!bad && lc < nc && i < n) ? Zg[i + static_cast<size_t>(c0 + lc) * n] : 0.0, 0.0);
         }
     if (!bad) {
         for (int k = tid; k < n; k += kBigThreads) {
@@ -810,35 +815,37 @@ __global__ void __launch_bounds__(kBigThreads) k_back_big(int mode, int n, int b
     // ---- Y = Q Z: H_k for k = n-2 .. 0
     for (int k0 = n - 2; k0 >= 0; k0 -= kBigPanel) {
         __syncthreads();
-        for (int q = 0; q < kBigPanel && k0 - q >= 0; ++q) {
-            const int k = k0 - q;
+        for (int p = 0; p < kBigPanel && k0 - p >= 0; ++p) {
+            const int k = k0 - p;
             const double2* src = LVb + static_cast<size_t>(n - 1 - k) * n - (k + 1);    // src[i] = v_k(i)
-            for (int i = k + 1 + tid; i < n; i += kBigThreads) panel[q * n + i] = src[i];
+            for (int i = k + 1 + tid; i < n; i += kBigThreads) panel[p * n + i] = src[i];
         }
         __syncthreads();
-        for (int q = 0; q < kBigPanel; ++q) {
-            const int k = k0 - q;
+#pragma unroll 1
+        for (int p = 0; p < kBigPanel; ++p) {
+            const int k = k0 - p;
             if (k < 0) break;
             const double2 tk = taus[k];
             if (tk.x == 0.0 && tk.y == 0.0) continue;
             double2 lv[RM];
 #pragma unroll
-            for (int s = 0; s < RM; ++s) {
-                const int i = lane + 32 * s;
-                lv[s] = (i > k && i < n) ? panel[q * n + i] : make_double2(0.0, 0.0);
+            for (int q = 0; q < RM; ++q) {
+                const int i = g + G * q;
+                lv[q] = (i > k && i < n) ? panel[p * n + i] : make_double2(0.0, 0.0);
             }
 #pragma unroll
-            for (int c = 0; c < NCW; ++c) {
-                if (c < ncw) {
-                    double2 acc = make_double2(0.0, 0.0);
+            for (int w = 0; w < NCW; ++w) {
+                double2 a0 = make_double2(0.0, 0.0), a1 = a0;
 #pragma unroll
-                    for (int s = 0; s < RM; ++s) acc = cfmac(lv[s], y[c][s], acc);
-                    acc.x = warp_sum(acc.x);
-                    acc.y = warp_sum(acc.y);
-                    const double2 sc = cmul(tk, acc);
-#pragma unroll
-                    for (int s = 0; s < RM; ++s) y[c][s] = cfms(lv[s], sc, y[c][s]);
+                for (int q = 0; q < RM; ++q) {
+                    if (q & 1) a1 = cfmac(lv[q], y[w][q], a1); else a0 = cfmac(lv[q], y[w][q], a0);
                 }
+                double2 acc = cadd(a0, a1);
+#pragma unroll
+                for (int o = 1; o < G; o <<= 1) { acc.x += shfl_xor(acc.x, o); acc.y += shfl_xor(acc.y, o); }
+                const double2 sc = cmul(tk, acc);
+#pragma unroll
+                for (int q = 0; q < RM; ++q) y[w][q] = cfms(lv[q], sc, y[w][q]);
             }
         }
     }
@@ -846,44 +853,47 @@ __global__ void __launch_bounds__(kBigThreads) k_back_big(int mode, int n, int b
     if (mode == kBackFull) {
         for (int k0 = n - 1; k0 >= 0; k0 -= kBigPanel) {
             __syncthreads();
-            for (int q = 0; q < kBigPanel && k0 - q >= 0; ++q) {
-                const int k = k0 - q;
+            for (int p = 0; p < kBigPanel && k0 - p >= 0; ++p) {
+                const int k = k0 - p;
                 const double2* src = LVb + static_cast<size_t>(k) * n;           // src[i] = L(i, k)
-                for (int i = k + 1 + tid; i < n; i += kBigThreads) panel[q * n + i] = src[i];
+                for (int i = k + 1 + tid; i < n; i += kBigThreads) panel[p * n + i] = src[i];
             }
             __syncthreads();
-            for (int q = 0; q < kBigPanel; ++q) {
-                const int k = k0 - q;
+#pragma unroll 1
+            for (int p = 0; p < kBigPanel; ++p) {
+                const int k = k0 - p;
                 if (k < 0) break;
                 const double ik = invd[k];
+                const int rk = k / G, gk = k - rk * G;
                 double2 lv[RM];
 #pragma unroll
-                for (int s = 0; s < RM; ++s) {
-                    const int i = lane + 32 * s;
-                    lv[s] = (i > k && i < n) ? panel[q * n + i] : make_double2(0.0, 0.0);
+                for (int q = 0; q < RM; ++q) {
+                    const int i = g + G * q;
+                    lv[q] = (i > k && i < n) ? panel[p * n + i] : make_double2(0.0, 0.0);
                 }
 #pragma unroll
-                for (int c = 0; c < NCW; ++c) {
-                    if (c < ncw) {
-                        double2 acc = make_double2(0.0, 0.0);
+                for (int w = 0; w < NCW; ++w) {
+                    double2 a0 = make_double2(0.0, 0.0), a1 = a0;
 #pragma unroll
-                        for (int s = 0; s < RM; ++s) acc = cfmac(lv[s], y[c][s], acc);
-                        acc.x = warp_sum(acc.x);
-                        acc.y = warp_sum(acc.y);
-                        double2 xk = cshfl(seg_get(y[c], k >> 5), k & 31);
-                        xk = cscale(csub(xk, acc), ik);
-                        if (lane == (k & 31)) seg_set(y[c], k >> 5, xk);
+                    for (int q = 0; q < RM; ++q) {
+                        if (q & 1) a1 = cfmac(lv[q], y[w][q], a1); else a0 = cfmac(lv[q], y[w][q], a0);
                     }
+                    double2 acc = cadd(a0, a1);
+#pragma unroll
+                    for (int o = 1; o < G; o <<= 1) { acc.x += shfl_xor(acc.x, o); acc.y += shfl_xor(acc.y, o); }
+                    double2 xk = cshfl(seg_get(y[w], rk), (lane & ~(G - 1)) | gk);
+                    xk = cscale(csub(xk, acc), ik);
+                    if (g == gk) seg_set(y[w], rk, xk);
                 }
             }
         }
     }
 #pragma unroll
-    for (int c = 0; c < NCW; ++c)
+    for (int w = 0; w < NCW; ++w)
 #pragma unroll
         for (int q = 0; q < RM; ++q) {
-            const int i = lane + 32 * q, j = c0 + warp + kBigWarps * c;
-            if (c < ncw && i < n) Xb[i + static_cast<size_t>(j) * n] = y[c][q];
+            const int i = g + G * q, lc = grp + GROUPS * w;
+            if (lc < nc && i < n) Xb[i + static_cast<size_t>(c0 + lc) * n] = y[w][q];
         }
 }
 
@@ -933,14 +943,14 @@ void run_reduce_big(cudaError_t* err, const double2* A, const double2* B, int n,
                             info);
 }
 
-template <int CS, int RM>
+template <int CS, int G, int RM, int NCW>
 void run_back_big(cudaError_t* err, int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
                   cudaStream_t stream) {
     const size_t smem = BigBackSmem(n).total;
     static std::once_flag f;
-    set_big_smem_once(k_back_big<CS, RM>, f, static_cast<size_t>(max_smem_optin()));
-    *err = launch_clustered(k_back_big<CS, RM>, CS, batch * CS, kBigThreads, smem, stream, mode, n, batch, ws, X,
-                            info);
+    set_big_smem_once(k_back_big<CS, G, RM, NCW>, f, static_cast<size_t>(max_smem_optin()));
+    *err = launch_clustered(k_back_big<CS, G, RM, NCW>, CS, batch * CS, kBigThreads, smem, stream, mode, n, batch,
+                            ws, X, info);
 }
 
 template <int CS, int RM>
@@ -1013,7 +1023,13 @@ cudaError_t launch_back_big(int mode, int n, int batch, const Workspace& ws, dou
     if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
     if (!big_path(n)) return cudaErrorInvalidValue;
     cudaError_t err = cudaSuccess;
-    SBG_BIG_DISPATCH(n, run_back_big, &err, mode, n, batch, ws, X, info, stream);
+    // (CTAs per pair, rows per lane, columns per lane group): 8 lanes per column, rows 8 q + g
+    // (CTAs per pair, lanes per column, rows per lane, columns per lane group): one column
+    // per 8-lane group (32 columns per CTA) up to n = 160, two per 16-lane group above
+    if (n <= 96) run_back_big<3, 8, 12, 1>(&err, mode, n, batch, ws, X, info, stream);
+    else if (n <= 128) run_back_big<4, 8, 16, 1>(&err, mode, n, batch, ws, X, info, stream);
+    else if (n <= 160) run_back_big<5, 8, 20, 1>(&err, mode, n, batch, ws, X, info, stream);
+    else run_back_big<8, 16, 16, 2>(&err, mode, n, batch, ws, X, info, stream);
     return err != cudaSuccess ? err : cudaGetLastError();
 }
 

@@ -205,6 +205,37 @@ __device__ __forceinline__ void grp_apply_q(const cplx<R>* LV, int ld, const cpl
     }
 }
 
+// y <- L^{-1} y (see col_trsm_lower) with L packed by columns (Lp, order n): lane g of the
+// group holds rows G r + g.  Each solved w_k stays in its slot of the owning lane.
+template <int G, int RM, typename R>
+__device__ __forceinline__ void grp_trsm_lower_packed(const cplx<R>* Lp, const R* invd, cplx<R> (&y)[RM], int n,
+                                                      int g) {
+    using C = cplx<R>;
+    const int lane = threadIdx.x & 31;
+    const int nb = ((n - 1) / G) >> 3;
+    for (int k = 0; k < n; ++k) {
+        const int rk = k / G, gk = k - rk * G;
+        C piv = y[0];
+#define SBG_SEL(I) case I: if constexpr ((I) < RM) piv = y[I]; break;
+        switch (rk) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
+        if constexpr (G > 1) piv = cshfl(piv, (lane & ~(G - 1)) | gk);
+        const C wk = cscale(piv, invd[k]);
+        if (g == gk) {
+#define SBG_SET(I) case I: if constexpr ((I) < RM) y[I] = wk; break;
+            switch (rk) { SBG_DESC64(SBG_SET) default: break; }
+#undef SBG_SET
+        }
+        const C* lk = Lp + pk(k, n) - k;             // lk[i] = L(i, k)
+        const int kb = (k + 1) / G - 1;              // slots <= kb are inactive on every lane
+#define SBG_S(I) if constexpr ((I) < RM) { const int i = G * (I) + g; if (i > k && i < n) y[I] = cfms(lk[i], wk, y[I]); }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= kb) break; SBG_ROWS8(SBG_S, B)
+        switch (nb) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+    }
+}
+
 // x = L^{-H} y (see col_trsm_lowerH); out(k, x_k) is called on the lane that holds row k.
 template <int G, int RM, typename R, typename Out>
 __device__ __forceinline__ void grp_trsm_lowerH(const cplx<R>* LV, int ld, const R* invd, cplx<R> (&y)[RM], int n,
