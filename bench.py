@@ -378,6 +378,7 @@ def main():
         t = max_over_ranks(statistics.median(times))
         e2e = {"value": world * ep / t, "unit": "solves/s", "h2d_bytes_per_step": 2 * 16 * nn * ep,
                "d2h_bytes_per_step": (16 * nn + 8 * N + 4) * ep, "pairs_per_step": ep,
+               "h2d_gbs": 2 * 16 * nn * ep / t / 1e9, "d2h_gbs": (16 * nn + 8 * N + 4) * ep / t / 1e9,
                "host_info_nonzero": int((hI != 0).sum().item())}
         del hA, hB, hX
 
