@@ -183,14 +183,17 @@ __device__ __forceinline__ void grp_apply_q(const cplx<R>* LV, int ld, const cpl
         if (tk.x == R(0) && tk.y == R(0)) continue;
         const C* vrow = LV + k;                      // v_k(i) = vrow[i * ld], i >= k + 1
         const int kb = (k + 1) / G - 1;              // slots <= kb are inactive on every lane
-        C s0 = mk<R>(R(0), R(0)), s1 = s0;
+        C s0 = mk<R>(R(0), R(0)), s1 = s0, s2 = s0, s3 = s0;    // four chains: the dot's FMAs overlap
 #define SBG_S(I) if constexpr ((I) < RM) { const int i = G * (I) + g; if (i > k && i < n) { \
-        if ((I) & 1) s1 = cfmac(vrow[i * ld], y[I], s1); else s0 = cfmac(vrow[i * ld], y[I], s0); } }
+        if (((I) & 3) == 0) s0 = cfmac(vrow[i * ld], y[I], s0); \
+        else if (((I) & 3) == 1) s1 = cfmac(vrow[i * ld], y[I], s1); \
+        else if (((I) & 3) == 2) s2 = cfmac(vrow[i * ld], y[I], s2); \
+        else s3 = cfmac(vrow[i * ld], y[I], s3); } }
 #define SBG_K(B) case B: if ((B) * 8 + 7 <= kb) break; SBG_ROWS8(SBG_S, B)
         switch (nb) { SBG_BLOCKS(SBG_K) default: break; }
 #undef SBG_K
 #undef SBG_S
-        C s = cadd(s0, s1);
+        C s = cadd(cadd(s0, s1), cadd(s2, s3));
         if constexpr (G > 1) {
 #pragma unroll
             for (int m = 1; m < G; m <<= 1) { s.x += shfl_xor(s.x, m); s.y += shfl_xor(s.y, m); }
