@@ -248,10 +248,13 @@ __host__ __device__ inline size_t hegst_col_bytes(int n) {
     return align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16) + align_up(8 * n, 16) + 16;
 }
 
-template <int NMAX>
+// EXACT: n == NMAX is a compile-time constant (the common sizes get their own
+// instantiation, so every row-bound test folds away).
+template <int NMAX, bool EXACT>
 __global__ void __launch_bounds__(NMAX, 4) k_hegst_col(int mode, const double2* __restrict__ A, const Workspace ws,
-                                                    double2* __restrict__ out, int n, int batch,
+                                                    double2* __restrict__ out, int n_arg, int batch,
                                                     const int* __restrict__ info) {
+    const int n = EXACT ? NMAX : n_arg;
     const int b = blockIdx.x;
     if (b >= batch) return;
     if (info[b] != 0) return;
@@ -304,10 +307,11 @@ __global__ void __launch_bounds__(NMAX, 4) k_hegst_col(int mode, const double2* 
 template <int NMAX, int G>
 __host__ __device__ constexpr int back_col_threads() { return (NMAX * G + 31) / 32 * 32; }
 
-template <int NMAX, int G>
-__global__ void __launch_bounds__(back_col_threads<NMAX, G>(), G == 1 ? 4 : 3) k_back_col(int mode, int n, int batch, Workspace ws,
-                                                                            double2* __restrict__ X,
+template <int NMAX, int G, bool EXACT>
+__global__ void __launch_bounds__(back_col_threads<NMAX, G>(), G == 1 ? 4 : 3) k_back_col(int mode, int n_arg, int batch,
+                                                                            Workspace ws, double2* __restrict__ X,
                                                                             const int* __restrict__ info) {
+    const int n = EXACT ? NMAX : n_arg;              // EXACT: n is a compile-time constant
     constexpr int T = back_col_threads<NMAX, G>();
     constexpr int RM = (NMAX + G - 1) / G;
     // tile_ld(NMAX) as a compile-time stride: every row slot's offset is an immediate
@@ -879,12 +883,12 @@ void run_back(int mode, int n, int batch, const Workspace& ws, double2* X, const
     k_back<T, G, RM><<<batch, T, smem, stream>>>(mode, n, batch, ws, X, info);
 }
 
-template <int NMAX>
+template <int NMAX, bool EXACT = false>
 void run_hegst_col(int mode, const double2* A, const Workspace& ws, double2* out, int n, int batch, const int* info,
                    cudaStream_t stream) {
     static std::once_flag f;
-    set_max_smem_once(k_hegst_col<NMAX>, f);
-    k_hegst_col<NMAX><<<batch, NMAX, hegst_col_bytes(n), stream>>>(mode, A, ws, out, n, batch, info);
+    set_max_smem_once(k_hegst_col<NMAX, EXACT>, f);
+    k_hegst_col<NMAX, EXACT><<<batch, NMAX, hegst_col_bytes(n), stream>>>(mode, A, ws, out, n, batch, info);
 }
 
 cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, int batch,
@@ -907,7 +911,9 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
         k_potrf_warp<<<grid, 32 * kPotrfWarpsPerCta, potrf_warp_bytes(n) * kPotrfWarpsPerCta, stream>>>(
             mode, B, n, batch, ws, out, info);
         if (mode == kReduceChol) return cudaGetLastError();
-        if (n <= 32) run_hegst_col<32>(mode, A, ws, out, n, batch, info, stream);
+        if (n == 32) run_hegst_col<32, true>(mode, A, ws, out, n, batch, info, stream);
+        else if (n == 54) run_hegst_col<54, true>(mode, A, ws, out, n, batch, info, stream);
+        else if (n <= 32) run_hegst_col<32>(mode, A, ws, out, n, batch, info, stream);
         else if (n <= 48) run_hegst_col<48>(mode, A, ws, out, n, batch, info, stream);
         else run_hegst_col<56>(mode, A, ws, out, n, batch, info, stream);
         return cudaGetLastError();
@@ -1033,13 +1039,13 @@ cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* 
     return cudaGetLastError();
 }
 
-template <int NMAX, int G>
+template <int NMAX, int G, bool EXACT = false>
 void run_back_col_g(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info, size_t smem,
                     cudaStream_t stream) {
     static std::once_flag f;
-    set_max_smem_once(k_back_col<NMAX, G>, f);
+    set_max_smem_once(k_back_col<NMAX, G, EXACT>, f);
     smem = BackSmem(n, (((NMAX | 1) & 7) == 7) ? (NMAX | 1) + 2 : (NMAX | 1)).total;
-    k_back_col<NMAX, G><<<batch, back_col_threads<NMAX, G>(), smem, stream>>>(mode, n, batch, ws, X, info);
+    k_back_col<NMAX, G, EXACT><<<batch, back_col_threads<NMAX, G>(), smem, stream>>>(mode, n, batch, ws, X, info);
 }
 
 // One lane per column: measured at n = 54, splitting a column over 2 lanes (G = 2, 3 CTAs
@@ -1059,7 +1065,9 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
     const size_t smem = back_smem_bytes(n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     if (n <= kColMaxN) {
-        if (n <= 32) run_back_col<32>(mode, n, batch, ws, X, info, smem, stream);
+        if (n == 32) run_back_col_g<32, 1, true>(mode, n, batch, ws, X, info, smem, stream);
+        else if (n == 54) run_back_col_g<54, 1, true>(mode, n, batch, ws, X, info, smem, stream);
+        else if (n <= 32) run_back_col<32>(mode, n, batch, ws, X, info, smem, stream);
         else if (n <= 48) run_back_col<48>(mode, n, batch, ws, X, info, smem, stream);
         else run_back_col<56>(mode, n, batch, ws, X, info, smem, stream);
         return cudaGetLastError();
