@@ -738,6 +738,116 @@ __global__ void k_ql_apply(int n, int batch, Workspace ws, double* __restrict__ 
     }
 }
 
+// ----------------------------------------------------------------------------- k_ql_apply_reg
+// The rotation log applied with each lane's row of Z in REGISTERS (n <= NMAX = 32): a sweep
+// of rotations at columns col, col-1, ... enters an unrolled descending chain at case col
+// (every register index static) and updates (z_i, z_{i+1}) in place; the stage buffer
+// streaming is ql_log_apply_row's.  The columns are stored through the inverse sort
+// permutation (z[c] -> column pinv[c]), so no register is ever indexed at run time.  A pair
+// whose log overflowed is solved by the warp QL on its first warp with Z in the second half
+// of the pair's X slice (no shared-memory Z tile is kept for it).
+template <typename R>
+__host__ __device__ inline size_t ql_apply_reg_pair_bytes(int n) {
+    const int wpp = (n + 31) / 32;
+    return static_cast<size_t>(wpp) * 2 * 32 * sizeof(cplx<R>) + align_up(4 * static_cast<size_t>(n), 16) +
+           align_up(sizeof(R) * 2 * static_cast<size_t>(n), 16);
+}
+
+template <int NMAX, typename R>
+__global__ void k_ql_apply_reg(int n, int batch, Workspace ws, double* __restrict__ W, double2* __restrict__ X,
+                               int* __restrict__ info) {
+    using C = cplx<R>;
+    const int wpp = (n + 31) / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pair_in_cta = warp / wpp, wip = warp - pair_in_cta * wpp;
+    const int pairs_per_cta = (blockDim.x >> 5) / wpp;
+    const int b = blockIdx.x * pairs_per_cta + pair_in_cta;
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned char* base = smem + ql_apply_reg_pair_bytes<R>(n) * pair_in_cta;
+    C* stage = reinterpret_cast<C*>(base) + wip * 64;
+    int* pinv = reinterpret_cast<int*>(base + static_cast<size_t>(wpp) * 2 * 32 * sizeof(C));
+    R* dd = reinterpret_cast<R*>(base + static_cast<size_t>(wpp) * 2 * 32 * sizeof(C) + align_up(4 * static_cast<size_t>(n), 16));
+    R* ee = dd + n;
+    const bool live = b < batch && !(info[min(b, batch - 1)] > n || info[min(b, batch - 1)] < 0);
+    const bool fallback = live && ws.flag[b] != 0;
+    const int row = wip * 32 + lane;
+    const bool own = live && row < n;
+    R z[NMAX];
+#pragma unroll
+    for (int c = 0; c < NMAX; ++c) z[c] = (row == c) ? R(1) : R(0);
+    if (live && !fallback) {
+        const C* log = reinterpret_cast<const C*>(ws.log) + static_cast<size_t>(ws.log_cap) * b;
+        const int cap = ws.log_cap;
+        int loaded = 0, buf = 0, remaining = 0, col = 0;
+        C pre = log[lane];
+        bool done = false;
+        while (!done) {
+            stage[buf * 32 + lane] = pre;
+            __syncwarp();
+            loaded += 32;
+            if (loaded < cap) pre = log[min(loaded + lane, cap - 1)];
+            const C* st = stage + buf * 32;
+            int k = 0;
+            while (k < 32) {
+                if (remaining == 0) {
+                    const C h = st[k++];
+                    const int top = static_cast<int>(h.x);
+                    if (top < 0) { done = true; break; }
+                    remaining = static_cast<int>(h.y);
+                    col = top;
+                    continue;
+                }
+                const int take = min(remaining, 32 - k);
+                const C* e = st + k;
+                int rem = take;
+                // rotation at column I: (z_I, z_{I+1}) <- (c z_I - s z_{I+1}, s z_I + c z_{I+1})
+#define SBG_ROT(I) case I: if constexpr ((I) + 1 < NMAX) { if (rem == 0) break; const C cs = *e++; \
+                const R zi = z[I], zj = z[(I) + 1]; z[(I) + 1] = fma(cs.y, zi, cs.x * zj); \
+                z[I] = fma(cs.x, zi, -cs.y * zj); --rem; }
+                switch (col) { SBG_DESC64(SBG_ROT) default: break; }
+#undef SBG_ROT
+                k += take;
+                col -= take;
+                remaining -= take;
+            }
+            __syncwarp();
+            buf ^= 1;
+            if (!done && loaded >= cap) done = true;      // malformed log guard (never reached)
+        }
+    }
+    // inverse sort permutation, by the pair's threads
+    if (live && !fallback) {
+        const int* perm = ws.perm + static_cast<size_t>(n) * b;
+        for (int i = wip * 32 + lane; i < n; i += wpp * 32) pinv[perm[i]] = i;
+    }
+    __syncthreads();
+    const size_t mat = static_cast<size_t>(n) * n;
+    if (fallback) {
+        if (wip != 0) return;
+        R* Zs = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(X + mat * b) + 8 * mat);   // row-major, ld n
+        for (size_t idx = lane; idx < mat; idx += 32) Zs[idx] = (idx / n == idx % n) ? R(1) : R(0);
+        for (int i = lane; i < n; i += 32) {
+            dd[i] = static_cast<R>(ws.d[static_cast<size_t>(n) * b + i]);
+            ee[i] = static_cast<R>(ws.e[static_cast<size_t>(n) * b + i]);
+        }
+        __syncwarp();
+        const int unconv = tridiag_ql<R>(n, dd, ee, Zs, n);
+        for (int i = lane; i < n; i += 32) W[static_cast<size_t>(n) * b + i] = static_cast<double>(dd[i]);
+        if (lane == 0 && unconv) info[b] = unconv;
+        __syncwarp();
+        R* Zg = reinterpret_cast<R*>(X + mat * b);
+        for (int r = lane; r < n; r += 32)
+            for (int k = 0; k < n; ++k) Zg[r + static_cast<size_t>(k) * n] = Zs[static_cast<size_t>(r) * n + k];
+        return;
+    }
+    if (own) {
+        R* Zg = reinterpret_cast<R*>(X + mat * b);
+#pragma unroll
+        for (int c = 0; c < NMAX; ++c)
+            if (c < n) Zg[row + static_cast<size_t>(pinv[c]) * n] = z[c];
+    }
+}
+
 // ----------------------------------------------------------------------------- k_back
 // One CTA per pair: X = L^{-H} Q Z.  Column j of Z is held in registers by a group
 // of G lanes (lane g owns rows g + G r), read straight from the X buffer; only the
@@ -1004,6 +1114,23 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
     const int cgrid = (batch + chain_threads - 1) / chain_threads;
     const int agrid = (batch + apply_warps - 1) / apply_warps;     // apply_warps = pairs per CTA
     const int athreads = 32 * ((n + 31) / 32) * apply_warps;
+    if (n <= 32) {                                                  // Z rows in registers
+        // (measured: at n = 32 this beats the shared-memory Z tile by ~4 %; at n = 54 it is 30 %
+        // slower: 148 registers a lane and the per-chunk jump into the rotation chain cost more)
+        cudaError_t err = launch_ql_chain(n, batch, ws, W, info, single, chain_threads, stream);
+        if (err != cudaSuccess) return err;
+        // one pair per CTA: ~150 registers a lane, so small CTAs pack the SM best
+        const size_t rs = single ? ql_apply_reg_pair_bytes<float>(n) : ql_apply_reg_pair_bytes<double>(n);
+        const int rgrid = batch, rthreads = 32 * ((n + 31) / 32);
+        static std::once_flag r32d, r32f;
+#define SBG_RUN_REG(NM, R, FLAG)                                                                 \
+        { set_max_smem_once(k_ql_apply_reg<NM, R>, FLAG);                                          \
+          k_ql_apply_reg<NM, R><<<rgrid, rthreads, rs, stream>>>(n, batch, ws, W, X, info); }
+        if (single) SBG_RUN_REG(32, float, r32f)
+        else SBG_RUN_REG(32, double, r32d)
+#undef SBG_RUN_REG
+        return cudaGetLastError();
+    }
     static std::once_flag fcd, fcf, fad, faf;
     if (single) {
         set_max_smem_once(k_ql_chain<float>, fcf);
