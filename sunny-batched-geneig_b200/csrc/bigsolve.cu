@@ -414,7 +414,7 @@ struct MidSmem {
         pb = o;   o += 16 * static_cast<size_t>(n);
         invd = o; o += big_align(8 * static_cast<size_t>(n), 16);
         red = o;  o += 16 * kBigWarps;
-        misc = o; o += 80;                // fail flag; tau and 1/(alpha - beta) by step parity
+        misc = o; o += 48;                // fail flag; tau by step parity
         bar = o;  o += 16;
         total = o;
     }
@@ -477,7 +477,6 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
     double* red = reinterpret_cast<double*>(smem + lay.red);
     int* s_fail = reinterpret_cast<int*>(smem + lay.misc);
     double2* s_tk = reinterpret_cast<double2*>(smem + lay.misc + 16);      // [2]
-    double2* s_sc = reinterpret_cast<double2*>(smem + lay.misc + 48);      // [2]
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + lay.bar);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const size_t mat = static_cast<size_t>(n) * n;
@@ -579,7 +578,8 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
     }
     __syncthreads();
 
-    // ---- hetrd
+    // ---- hetrd: four CTA barriers per step (reflector and v by warp 0 | matvec with the dot
+    // product's per-warp partials | w | rank-2 update)
     const int grp = tid / kMidGroup, sub = tid % kMidGroup;
     for (int k = 0; k + 1 < n; ++k) {
         const int m = n - k - 1;
@@ -600,9 +600,16 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
                 const double ar = alpha.x - beta, ai = alpha.y, den = ar * ar + ai * ai;
                 scale = make_double2(ar / den, -ai / den);
             }
+            if (tk.x != 0.0 || tk.y != 0.0) {
+                __syncwarp();                                     // every lane has read alpha
+                for (int i = lane; i < m; i += 32) {
+                    const double2 v = (i == 0) ? make_double2(1.0, 0.0) : cmul(x[i], scale);
+                    vb[i] = v;
+                    x[i] = v;
+                }
+            }
             if (lane == 0) {
                 s_tk[k & 1] = tk;
-                s_sc[k & 1] = scale;
                 db[k] = P[pk(k, n)].x;
                 eb[k] = beta;
                 taub[k] = tk;
@@ -611,16 +618,10 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
         __syncthreads();
         const double2 tk = s_tk[k & 1];
         if (tk.x == 0.0 && tk.y == 0.0) continue;                 // H_k = I (uniform)
-        const double2 scale = s_sc[k & 1];
-        for (int i = tid; i < m; i += kMidThreads) {
-            const double2 v = (i == 0) ? make_double2(1.0, 0.0) : cmul(x[i], scale);
-            vb[i] = v;
-            x[i] = v;
-        }
-        __syncthreads();
         // p = tau A22 v over the row pairs; warp-uniform loop (the group shuffles need whole warps)
         double2* c0 = P + pk(k + 1, n);
         const int h = (m + 1) >> 1;
+        double2 dpart = make_double2(0.0, 0.0);                   // this lane's share of p^H v
         for (int qb = 0; qb < h; qb += kMidThreads / kMidGroup) {
             const int q = qb + grp;
             const bool act = q < h;
@@ -662,21 +663,28 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
                 double2 s = cadd(lo1, up1);
                 s.x = fma(d1[0].x, vb[r1].x, s.x);
                 s.y = fma(d1[0].x, vb[r1].y, s.y);
-                pb[r1] = cmul(tk, s);
+                const double2 p1 = cmul(tk, s);
+                pb[r1] = p1;
+                dpart = cfmac(p1, vb[r1], dpart);
                 if (two) {
                     const double2* d2 = c0 + mid_off(r2, m) + r2;
                     double2 s2v = cadd(lo2, up2);
                     s2v.x = fma(d2[0].x, vb[r2].x, s2v.x);
                     s2v.y = fma(d2[0].x, vb[r2].y, s2v.y);
-                    pb[r2] = cmul(tk, s2v);
+                    const double2 p2 = cmul(tk, s2v);
+                    pb[r2] = p2;
+                    dpart = cfmac(p2, vb[r2], dpart);
                 }
             }
         }
+        dpart.x = warp_sum(dpart.x);
+        dpart.y = warp_sum(dpart.y);
+        if (lane == 0) { red[2 * warp] = dpart.x; red[2 * warp + 1] = dpart.y; }
         __syncthreads();
         // w = p - tau/2 (p^H v) v
-        double2 dl = make_double2(0.0, 0.0);
-        for (int i = tid; i < m; i += kMidThreads) dl = cfmac(pb[i], vb[i], dl);
-        const double2 dot = block_sum2(dl, red);
+        double2 dot = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int w8 = 0; w8 < kBigWarps; ++w8) { dot.x += red[2 * w8]; dot.y += red[2 * w8 + 1]; }
         const double2 a2 = cscale(cmul(tk, dot), -0.5);
         for (int i = tid; i < m; i += kMidThreads) wb[i] = cfma(a2, vb[i], pb[i]);
         __syncthreads();

@@ -44,12 +44,6 @@ __host__ __device__ inline size_t tridiag_warp_bytes(int n) {
     return align_up(sizeof(R) * (static_cast<size_t>(n) * tile_ld(n) + 2 * n), 16);
 }
 
-__host__ __device__ inline int pick_group(int threads, int n) {
-    int g = 1;
-    while (g < 32 && threads / (2 * g) >= n) g *= 2;
-    return g;
-}
-
 // Waits for the bulk copies of this CTA; on the (never expected) timeout it flags
 // the pair and waits once more, bounded, so no copy lands after the CTA exits.
 __device__ inline bool wait_copies(uint64_t* bar, int* info_word) {
