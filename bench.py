@@ -357,7 +357,9 @@ def main():
         import psutil
         nn = N * N
         per_pair_host = 16 * nn * 3 + 8 * N + 4
-        limit = int(0.35 * psutil.virtual_memory().available / per_pair_host)
+        # every rank on this node pins its own buffers: share 35 % of the free host memory
+        local_world = max(1, env_int("LOCAL_WORLD_SIZE", world))
+        limit = int(0.35 * psutil.virtual_memory().available / (per_pair_host * local_world))
         ep = args.e2e_pairs or pairs
         ep = max(1024, min(ep, pairs, limit))
         hA = torch.empty((ep, nn), dtype=torch.complex128, pin_memory=True)
@@ -652,7 +654,8 @@ def run_other(args):
                              "sample": f"{len(sample_idx)} pairs of the workload, LAPACKE_zhegv per pair over "
                                        f"{threads} host threads"}
         if not args.no_e2e:
-            ep = max(1, min(pairs, 65536, int(4e9 // (16 * n * n))))      # about 4 GB of pinned A
+            local_world = max(1, env_int("LOCAL_WORLD_SIZE", world))
+            ep = max(1, min(pairs, 65536, int(4e9 // (16 * n * n * local_world))))   # ~4 GB of pinned A per node
             hA = torch.empty((ep, n * n), dtype=torch.complex128, pin_memory=True); hA.copy_(A[:ep])
             hB = torch.empty_like(hA, pin_memory=True); hB.copy_(B[:ep])
             hX = torch.empty_like(hA, pin_memory=True)
