@@ -33,6 +33,7 @@
 // v_k(k+1+s) = LV(s, n-1-k), s = 0 .. n-2-k (v_k(k+1) = 1 stored explicitly).
 #include "kernels.cuh"
 #include "stages.cuh"
+#include "colsolve.cuh"
 
 #include <cooperative_groups.h>
 #include <mutex>
@@ -442,24 +443,6 @@ __device__ __forceinline__ void mid_pair_walk(double2* c0, int m, F&& f) {
     }
 }
 
-// y <- L^{-1} y for the group's column (rows g + kMidLanes r), L packed in shared memory.
-template <int RM>
-__device__ __forceinline__ void mid_lower_solve(double2 (&y)[RM], const double2* P, const double* invd, int n, int g) {
-    const int lane = threadIdx.x & 31;
-    for (int k = 0; k < n; ++k) {
-        const int rk = k / kMidLanes, gk = k - rk * kMidLanes;
-        double2 piv = cshfl(seg_get(y, rk), (lane & ~(kMidLanes - 1)) | gk);
-        piv = cscale(piv, invd[k]);
-        if (g == gk) seg_set(y, rk, piv);
-        const double2* lk = P + pk(k, n) - k;                 // lk[i] = L(i, k)
-#pragma unroll
-        for (int r = 0; r < RM; ++r) {
-            const int i = g + kMidLanes * r;
-            if (i > k && i < n) y[r] = cfms(lk[i], piv, y[r]);
-        }
-    }
-}
-
 template <int RM>
 __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __restrict__ A,
                                                             const double2* __restrict__ B, int n, int batch,
@@ -538,7 +521,7 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
                 const int i = g + kMidLanes * r;
                 y[r] = (own && i < n) ? Ab[i + static_cast<size_t>(j) * n] : make_double2(0.0, 0.0);
             }
-            mid_lower_solve<RM>(y, P, invd, n, g);
+            grp_trsm_lower_packed<kMidLanes, RM, double>(P, invd, y, n, g);
 #pragma unroll
             for (int r = 0; r < RM; ++r) {
                 const int i = g + kMidLanes * r;
@@ -555,7 +538,7 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
                 const int i = g + kMidLanes * r;
                 y[r] = (own && i < n) ? cconj(LVb[j + static_cast<size_t>(i) * n]) : make_double2(0.0, 0.0);
             }
-            mid_lower_solve<RM>(y, P, invd, n, g);
+            grp_trsm_lower_packed<kMidLanes, RM, double>(P, invd, y, n, g);
 #pragma unroll
             for (int r = 0; r < RM; ++r) {
                 const int i = g + kMidLanes * r;
