@@ -205,15 +205,18 @@ def test_nan_input_terminates_with_info(oracle_mod):
     assert info[2] == 0
 
 
-def test_ql_log_overflow_falls_back(monkeypatch, oracle_mod):
-    """A rotation log too small for the QL: every pair takes the in-kernel warp QL."""
+@pytest.mark.parametrize("N", [12, 16, 27])
+def test_ql_log_overflow_falls_back(N, monkeypatch, oracle_mod):
+    """A rotation log too small for the QL: every pair takes the in-kernel warp QL (n <= 32:
+    the register-row apply kernel's fallback, Z in the X buffer; n = 54: the shared-memory one)."""
     monkeypatch.setenv("SBG_QL_LOG_CAPACITY", "40")
-    A, B = wl.bogoliubov(27, 64, seed=3)
+    n = 2 * N
+    A, B = wl.bogoliubov(N, 64, seed=3)
     A, B = A.numpy(), B.numpy()
-    Wr, Xr, _ = oracle_mod.hegv(A, B, 54, nthreads=8)
+    Wr, Xr, _ = oracle_mod.hegv(A, B, n, nthreads=8)
     for prec in ("fp64", "mixed"):
-        W, X, info = run(54, A, B, prec)
-        check(A, B, W, X, info, Wr, Xr, 54, relative=True)
+        W, X, info = run(n, A, B, prec)
+        check(A, B, W, X, info, Wr, Xr, n, relative=True)
 
 
 def test_near_goldstone_both_forms(oracle_mod):
