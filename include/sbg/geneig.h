@@ -112,7 +112,7 @@ typedef struct {
     int tuning_mode;          /* SBG_TUNING_*  (hpp:101) */
     int cache_mode;           /* SBG_CACHE_*   (hpp:102) */
     int precision;            /* SBG_PRECISION_FP64 (plain drop-in) or SBG_PRECISION_MIXED */
-    int refine_steps;         /* mixed form: Ogita-Aishima steps, 0 = default (2) */
+    int refine_steps;         /* mixed form: Ogita-Aishima steps, 0 = default (3; the last only orthogonalises near-degenerate pairs) */
     int workspace_pairs;      /* pairs per internal chunk; 0 = default */
 } sbg_solver_options;
 
@@ -121,7 +121,10 @@ void sbg_solver_options_init(sbg_solver_options* opts);
 int sbg_solver_create(int n, int device_id, const sbg_solver_options* opts, sbg_solver** out);
 int sbg_solver_destroy(sbg_solver* s);
 /* NvrtcGeneigSolver::launch (nvrtc_solver.cpp:1063-1076).  Any batch >= 0; no multiple-of-
- * pairs-per-CTA restriction (the reference's partial last block was unchecked). */
+ * pairs-per-CTA restriction (the reference's partial last block was unchecked).  The solver's
+ * device scratch is kept per stream (one workspace slot for each distinct stream it is launched
+ * on, the first stream taking slot 0), so launches on different streams may overlap, as the
+ * reference's may; launches on the same stream are ordered by it. */
 int sbg_solver_launch(sbg_solver* s, const cuDoubleComplex* d_A, const cuDoubleComplex* d_B,
                       double* d_W, cuDoubleComplex* d_X, int* d_info, int batch,
                       cudaStream_t stream);
@@ -131,8 +134,9 @@ int sbg_solver_launch_chunked(sbg_solver* s, const cuDoubleComplex* d_A,
                               const cuDoubleComplex* d_B, double* d_W, cuDoubleComplex* d_X,
                               int* d_info, int total, int chunk_size, int num_streams,
                               const cudaStream_t* streams);
-/* Pre-sizes the internal workspace (pairs per chunk, number of stream slots) so later
- * launches never allocate (required before capturing a launch into a CUDA graph). */
+/* Pre-sizes the internal workspace (pairs per chunk, number of stream slots: the first
+ * stream_slots distinct streams the solver is launched on) so later launches never allocate
+ * (required before capturing a launch into a CUDA graph). */
 int sbg_solver_reserve(sbg_solver* s, int pairs, int stream_slots);
 /* End-to-end solve of HOST-resident pairs: chunks of chunk_size pairs are copied to the
  * device, solved and copied back, round-robin over num_streams internal streams so the

@@ -173,9 +173,9 @@ int sbg_solver_launch_chunked(sbg_solver* s, const cuDoubleComplex* d_A, const c
         int idx = 0;
         for (int off = 0; off < total; off += chunk_size, ++idx) {
             const int cnt = std::min(chunk_size, total - off);
-            const int slot = idx % num_streams;     // one workspace per stream: chunks in flight never share
+            const int k = idx % num_streams;        // one workspace per stream: chunks in flight never share
             s->launch(c2(d_A) + nn * off, c2(d_B) + nn * off, d_W + static_cast<size_t>(s->n) * off,
-                      c2(d_X) + nn * off, d_info + off, cnt, streams[slot], slot);
+                      c2(d_X) + nn * off, d_info + off, cnt, streams[k]);
         }
     });
 }

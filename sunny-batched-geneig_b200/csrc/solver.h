@@ -88,6 +88,10 @@ struct sbg_solver {
     const char* layer = "compile";
     std::mutex mu;
     std::vector<Slot> slots;
+    // Workspace slot i serves stream slot_streams[i]: launches on different streams never share
+    // scratch (the reference's launches keep everything in shared memory, so they are independent
+    // across streams, and so are these).  The first stream a solver sees gets slot 0.
+    std::vector<cudaStream_t> slot_streams;
     // staging buffers of the host-buffer path, one per internal stream
     struct Staging { void* A = nullptr; void* B = nullptr; void* X = nullptr; void* W = nullptr; void* info = nullptr;
                      int capacity = 0; cudaStream_t stream = nullptr; };
@@ -123,6 +127,14 @@ struct sbg_solver {
         check_cuda(cudaEventRecord(b, stream), "cudaEventRecord");
         std::lock_guard<std::mutex> lock(mu);
         stage_events.push_back({stage, kernels, a, b});
+    }
+
+    int slot_for(cudaStream_t st) {
+        std::lock_guard<std::mutex> lock(mu);
+        for (size_t i = 0; i < slot_streams.size(); ++i)
+            if (slot_streams[i] == st) return static_cast<int>(i);
+        slot_streams.push_back(st);
+        return static_cast<int>(slot_streams.size()) - 1;
     }
 
     sbg::Workspace workspace(int slot_idx, int pairs, cudaStream_t stream) {
@@ -201,7 +213,7 @@ struct sbg_solver {
             check_cuda(cudaMemcpyAsync(st.A, hA + nn * off, 16 * nn * cnt, cudaMemcpyHostToDevice, st.stream), "H2D A");
             check_cuda(cudaMemcpyAsync(st.B, hB + nn * off, 16 * nn * cnt, cudaMemcpyHostToDevice, st.stream), "H2D B");
             launch(static_cast<double2*>(st.A), static_cast<double2*>(st.B), static_cast<double*>(st.W),
-                   static_cast<double2*>(st.X), static_cast<int*>(st.info), cnt, st.stream, idx % nstreams);
+                   static_cast<double2*>(st.X), static_cast<int*>(st.info), cnt, st.stream);
             check_cuda(cudaMemcpyAsync(hX + nn * off, st.X, 16 * nn * cnt, cudaMemcpyDeviceToHost, st.stream), "D2H X");
             check_cuda(cudaMemcpyAsync(hW + static_cast<size_t>(n) * off, st.W, 8 * static_cast<size_t>(n) * cnt,
                                        cudaMemcpyDeviceToHost, st.stream), "D2H W");
@@ -212,12 +224,13 @@ struct sbg_solver {
     }
 
     void launch(const double2* A, const double2* B, double* W, double2* X, int* info, int batch,
-                cudaStream_t stream, int slot_idx = 0) {
+                cudaStream_t stream, int slot_idx = -1) {
         if (batch < 0) throw Error(SBG_ERR_INVALID_VALUE, "batch < 0");
         if (batch == 0) return;
         if (!A || !B || !W || !X || !info) throw Error(SBG_ERR_INVALID_VALUE, "null device pointer");
         const size_t nn = static_cast<size_t>(n) * n;
         const int cap = std::min(batch, chunk_pairs);
+        if (slot_idx < 0) slot_idx = slot_for(stream);
         sbg::Workspace ws = workspace(slot_idx, cap, stream);
         for (int off = 0; off < batch; off += ws.capacity) {
             const int cnt = std::min(ws.capacity, batch - off);
