@@ -866,7 +866,7 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
             int jj = 0;
             for (int t = 0; t < tot; ++t) {
                 if (t == r1) { diag1 = pa; low1 = cadd(acc0, acc1); acc0 = zero; acc1 = zero; pa = c0 + r2; jj = 0; }
-                if (t & 1) acc1 = cfma(*pa, vb[jj], acc1); else acc0 = cfma(*pa, vb[jj], acc0);
+                acc0 = cfma(*pa, vb[jj], acc0);
                 pa += m - jj - 1;
                 ++jj;
             }
@@ -885,7 +885,7 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
             bool switched = false;
             for (int t = 0; t < tot2; ++t) {
                 if (t == sw) { up1 = cadd(u0, u1); u0 = zero; u1 = zero; cp = diag2; vbase = r2; tt = 1; switched = true; }
-                if (t & 1) u1 = cfmac(cp[tt], vb[vbase + tt], u1); else u0 = cfmac(cp[tt], vb[vbase + tt], u0);
+                u0 = cfmac(cp[tt], vb[vbase + tt], u0);
                 ++tt;
             }
             C up2 = zero;
@@ -920,15 +920,19 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
             C* a = c0 + r1;
             C vr = vb[r1], wr = w1;
             int row = r1, jj = 0;
+            C* dg1 = nullptr;
             for (int t = 0; t < tot; ++t) {
-                if (t == r1 + 1) { a = c0 + r2; vr = vb[r2]; wr = w2; row = r2; jj = 0; }
+                if (t == r1 + 1) { dg1 = a - (m - jj); a = c0 + r2; vr = vb[r2]; wr = w2; row = r2; jj = 0; }
                 C tv = cfmsc(vr, wb[jj], *a);
                 tv = cfmsc(wr, vb[jj], tv);
-                if (jj == row) tv.y = R(0);
                 *a = tv;
                 a += m - jj - 1;
                 ++jj;
             }
+            // the diagonal entries (each row's last term) stay real
+            if (dg1 == nullptr) dg1 = a - (m - jj);
+            else a[-(m - jj)].y = R(0);
+            dg1->y = R(0);
         }
         __syncwarp();
     }
