@@ -858,39 +858,48 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
         C p1 = mk<R>(R(0), R(0)), p2 = mk<R>(R(0), R(0));
         if (own1) {
             const C zero = mk<R>(R(0), R(0));
-            // lower row walk: r1 terms of row r1, then r2 terms of row r2
-            C acc0 = zero, acc1 = zero, low1 = zero;
+            // One loop runs both walks (each m-1 terms per lane for a full pair): the lower row
+            // walk (row r1's r1 terms, then row r2's r2) and the mirrored column walk (column r1's
+            // m-1-r1 terms below the diagonal, then column r2's r1) -- shared loop overhead, two
+            // independent FMA chains.
+            const int tot = own2 ? r1 + r2 : r1;              // lower walk length
+            const int sw = m - 1 - r1;
+            const int tot2 = own2 ? m - 1 : sw;               // column walk length (== tot when own2)
+            const C* diag1 = c0 + (r1 * m - r1 * (r1 - 1) / 2);          // A22(r1, r1)
+            const C* diag2 = c0 + (r2 * m - r2 * (r2 - 1) / 2);          // A22(r2, r2)
+            C acc = zero, low1 = zero, u = zero, up1 = zero;
             const C* pa = c0 + r1;
-            const C* diag1 = nullptr;
-            const int tot = own2 ? r1 + r2 : r1;
             int jj = 0;
-            for (int t = 0; t < tot; ++t) {
-                if (t == r1) { diag1 = pa; low1 = cadd(acc0, acc1); acc0 = zero; acc1 = zero; pa = c0 + r2; jj = 0; }
-                acc0 = cfma(*pa, vb[jj], acc0);
+            const C* cp = diag1 + 1;                          // next column-walk element
+            const C* vp = vb + r1 + 1;                        // its partner in v
+            bool lsw = false, usw = false;
+            const int both = tot < tot2 ? tot : tot2;
+            int t = 0;
+            for (; t < both; ++t) {
+                if (t == r1) { low1 = acc; acc = zero; pa = c0 + r2; jj = 0; lsw = true; }
+                if (t == sw) { up1 = u; u = zero; cp = diag2 + 1; vp = vb + r2 + 1; usw = true; }
+                acc = cfma(*pa, vb[jj], acc);
+                u = cfmac(*cp, *vp, u);
+                pa += m - jj - 1;
+                ++jj;
+                ++cp;
+                ++vp;
+            }
+            for (; t < tot; ++t) {                            // (only when the lengths differ)
+                if (t == r1) { low1 = acc; acc = zero; pa = c0 + r2; jj = 0; lsw = true; }
+                acc = cfma(*pa, vb[jj], acc);
                 pa += m - jj - 1;
                 ++jj;
             }
-            // own2: the switch ran (r2 >= 1), acc holds row r2 and pa points at A22(r2, r2);
-            // otherwise acc holds row r1 and pa points at A22(r1, r1)
-            C low2 = zero;
-            const C* diag2 = nullptr;
-            if (own2) { low2 = cadd(acc0, acc1); diag2 = pa; }
-            else { low1 = cadd(acc0, acc1); diag1 = pa; }
-            // mirrored upper column walk: m-1-r1 terms of column r1, then r1 terms of column r2
-            const int sw = m - 1 - r1;
-            const int tot2 = own2 ? m - 1 : sw;
-            C u0 = zero, u1 = zero, up1 = zero;
-            const C* cp = diag1;
-            int vbase = r1, tt = 1;
-            bool switched = false;
-            for (int t = 0; t < tot2; ++t) {
-                if (t == sw) { up1 = cadd(u0, u1); u0 = zero; u1 = zero; cp = diag2; vbase = r2; tt = 1; switched = true; }
-                u0 = cfmac(cp[tt], vb[vbase + tt], u0);
-                ++tt;
+            for (; t < tot2; ++t) {
+                if (t == sw) { up1 = u; u = zero; cp = diag2 + 1; vp = vb + r2 + 1; usw = true; }
+                u = cfmac(*cp, *vp, u);
+                ++cp;
+                ++vp;
             }
-            C up2 = zero;
-            if (switched) up2 = cadd(u0, u1);
-            else up1 = cadd(u0, u1);
+            C low2 = zero, up2 = zero;
+            if (lsw) low2 = acc; else low1 = acc;
+            if (usw) up2 = u; else up1 = u;
             C a1 = up1;
             a1.x = fma(diag1[0].x, vb[r1].x, a1.x);
             a1.y = fma(diag1[0].x, vb[r1].y, a1.y);
