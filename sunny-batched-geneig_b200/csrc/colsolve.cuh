@@ -42,7 +42,7 @@ __device__ int potrf_warp_packed(cplx<R>* P, int n, R* invd) {
         const R dkk = colk[0].x;
         if (!(dkk > R(0))) return k + 1;          // uniform: every lane reads the same word
         const R dsq = sqrt(dkk);
-        const R inv = R(1) / dsq;
+        const R inv = rsqrt(dkk);                 // in parallel with the square root, not after it
         const int m = n - k - 1;
         __syncwarp();
         if (lane == 0) { colk[0] = mk<R>(dsq, R(0)); invd[k] = inv; }

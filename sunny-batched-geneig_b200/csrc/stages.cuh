@@ -829,10 +829,11 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
         } else {
             const R nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
             beta = alpha.x >= R(0) ? -nrm : nrm;
-            tk = mk<R>((beta - alpha.x) / beta, -alpha.y / beta);
+            const R ib = R(1) / beta;                    // two reciprocals instead of four divisions
+            tk = mk<R>((beta - alpha.x) * ib, -alpha.y * ib);
             const R ar = alpha.x - beta, ai = alpha.y;
-            const R den = ar * ar + ai * ai;
-            scale = mk<R>(ar / den, -ai / den);
+            const R id = R(1) / (ar * ar + ai * ai);
+            scale = mk<R>(ar * id, -ai * id);
         }
         if (lane == 0) { e[k] = beta; tau[k] = tk; }
         if (tk.x == R(0) && tk.y == R(0)) continue;
