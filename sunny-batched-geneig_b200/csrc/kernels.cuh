@@ -92,6 +92,10 @@ cudaError_t launch_back_big(int mode, int n, int batch, const Workspace& ws, dou
 cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, int* info, bool single,
                             int chain_threads, cudaStream_t stream);
 
+// Kernels one full reduce launch (kReduceFull) issues for order n: the warp Cholesky and the
+// column hegst kernel for n <= 56, one kernel otherwise.
+inline int reduce_kernel_count(int n) { return n <= 56 ? 2 : 1; }
+
 size_t reduce_smem_bytes(int mode, int n);
 size_t tridiag_smem_bytes(int n, int warps_per_cta, bool single);
 size_t ql_chain_smem_bytes(int n, int threads, bool single);

@@ -163,10 +163,10 @@ struct sbg_solver {
         stage_begin(stream, &ev);
         check_cuda(sbg::launch_reduce(sbg::kReduceFull, A, B, n, cnt, ws, X, info,
                                       sched.reduce_threads, stream), "reduce kernel");
-        stage_end(stream, ev, 0, 1);
+        stage_end(stream, ev, 0, sbg::reduce_kernel_count(n));
         stage_begin(stream, &ev);
         check_cuda(sbg::launch_hetrd(n, cnt, X, ws, info, sched.hetrd_threads, stream), "hetrd kernel");
-        stage_end(stream, ev, 1, 1);
+        stage_end(stream, ev, 1, n > sbg::kSmallMaxN ? 0 : 1);       // large n: inside the reduce kernel
         stage_begin(stream, &ev);
         if (precision == SBG_PRECISION_MIXED)
             check_cuda(sbg::launch_tridiag_mixed(n, cnt, ws, W, X, info, refine_steps, sched.chain_threads,
