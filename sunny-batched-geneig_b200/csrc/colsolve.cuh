@@ -117,62 +117,14 @@ __device__ __forceinline__ void row_trsm_right_lowerH(const cplx<R>* Lp, const R
     }
 }
 
-// y <- Q y, Q = H_0 ... H_{n-2}, reflectors along the rows of the LV tile (ld); the
-// superdiagonal entry LV(k, k+1) holds v_k(k+1) = 1.
-template <int NMAX, typename R>
-__device__ __forceinline__ void col_apply_q(const cplx<R>* LV, int ld, const cplx<R>* tau, cplx<R> (&y)[NMAX], int n) {
-    using C = cplx<R>;
-    for (int k = n - 2; k >= 0; --k) {
-        const C tk = tau[k];
-        if (tk.x == R(0) && tk.y == R(0)) continue;
-        const C* vrow = LV + k;                   // v_k(i) = vrow[i * ld], i >= k + 1
-        C s0 = mk<R>(R(0), R(0)), s1 = s0;
-#define SBG_S(I) if constexpr ((I) < NMAX) { if ((I) > k && (I) < n) { \
-        if ((I) & 1) s1 = cfmac(vrow[(I) * ld], y[I], s1); else s0 = cfmac(vrow[(I) * ld], y[I], s0); } }
-#define SBG_K(B) case B: if ((B) * 8 + 7 <= k) break; SBG_ROWS8(SBG_S, B)
-        switch ((n - 1) >> 3) { SBG_BLOCKS(SBG_K) default: break; }
-#undef SBG_K
-#undef SBG_S
-        const C s = cmul(tk, cadd(s0, s1));
-#define SBG_S(I) if constexpr ((I) < NMAX) { if ((I) > k && (I) < n) y[I] = cfms(vrow[(I) * ld], s, y[I]); }
-#define SBG_K(B) case B: if ((B) * 8 + 7 <= k) break; SBG_ROWS8(SBG_S, B)
-        switch ((n - 1) >> 3) { SBG_BLOCKS(SBG_K) default: break; }
-#undef SBG_K
-#undef SBG_S
-    }
-}
-
-// x = L^{-H} y (backward substitution), L full lower in the LV tile (ld); each x_k
-// goes through out(k, x_k) as soon as it is final.
-template <int NMAX, typename R, typename Out>
-__device__ __forceinline__ void col_trsm_lowerH(const cplx<R>* LV, int ld, const R* invd, cplx<R> (&y)[NMAX], int n,
-                                                Out&& out) {
-    using C = cplx<R>;
-    for (int k = n - 1; k >= 0; --k) {
-        C piv = y[0];
-#define SBG_SEL(I) case I: if constexpr ((I) < NMAX) piv = y[I]; break;
-        switch (k) { SBG_DESC64(SBG_SEL) default: break; }
-#undef SBG_SEL
-        const C xk = cscale(piv, invd[k]);
-        out(k, xk);
-        if (k == 0) break;
-        const C* lrow = LV + k;                   // L(k, i) = lrow[i * ld], i < k
-        // rows k-1 .. 0, by blocks of 8 from the block of k-1 down to block 0
-#define SBG_S(I) if constexpr ((I) < NMAX) { if ((I) < k) y[I] = cfms(cconj(lrow[(I) * ld]), xk, y[I]); }
-#define SBG_K(B) case B: SBG_ROWS8(SBG_S, B)
-        switch ((k - 1) >> 3) { SBG_BLOCKS(SBG_K) default: break; }
-#undef SBG_K
-#undef SBG_S
-    }
-}
-
 // ---------------------------------------------------------------- G lanes per column
-// The same sweeps with a column's rows spread over G adjacent lanes (G = 1 or 2): lane g of
+// The sweeps with a column's rows spread over G adjacent lanes (G a power of two): lane g of
 // the group holds rows i = G r + g in y[r], r < RM.  Control flow is uniform over the group
 // (the sweep's block range is taken for the whole group, rows are predicated), so the
 // group's partial dot products combine with one shuffle; every lane of the warp must call.
 
-// y <- Q y (see col_apply_q).
+// y <- Q y, Q = H_0 ... H_{n-2}, reflectors along the rows of the LV tile (ld): v_k(i) = LV(k, i)
+// for i >= k + 1, the superdiagonal entry LV(k, k+1) holding v_k(k+1) = 1.
 template <int G, int RM, typename R>
 __device__ __forceinline__ void grp_apply_q(const cplx<R>* LV, int ld, const cplx<R>* tau, cplx<R> (&y)[RM], int n,
                                             int g) {
@@ -208,7 +160,7 @@ __device__ __forceinline__ void grp_apply_q(const cplx<R>* LV, int ld, const cpl
     }
 }
 
-// y <- L^{-1} y (see col_trsm_lower) with L packed by columns (Lp, order n): lane g of the
+// y <- L^{-1} y (forward substitution) with L packed by columns (Lp, order n): lane g of the
 // group holds rows G r + g.  Each solved w_k stays in its slot of the owning lane.
 template <int G, int RM, typename R>
 __device__ __forceinline__ void grp_trsm_lower_packed(const cplx<R>* Lp, const R* invd, cplx<R> (&y)[RM], int n,
@@ -239,7 +191,8 @@ __device__ __forceinline__ void grp_trsm_lower_packed(const cplx<R>* Lp, const R
     }
 }
 
-// x = L^{-H} y (see col_trsm_lowerH); out(k, x_k) is called on the lane that holds row k.
+// x = L^{-H} y (backward substitution), L full lower in the LV tile (ld); each x_k goes through
+// out(k, x_k), on the lane that holds row k, as soon as it is final.
 template <int G, int RM, typename R, typename Out>
 __device__ __forceinline__ void grp_trsm_lowerH(const cplx<R>* LV, int ld, const R* invd, cplx<R> (&y)[RM], int n,
                                                 int g, Out&& out) {

@@ -1,16 +1,18 @@
-// Stage kernels of the batched generalized eigensolve and their launchers.
+// Stage kernels of the batched generalized eigensolve for n <= 84, and the launchers
+// that route larger n to the cluster kernels of bigsolve.cu.
 //
-//   k_reduce   one CTA per pair: TMA bulk-copy A and the lower triangle of B into
-//              shared memory, potrf, C = L^{-1} A L^{-H}, Householder
-//              tridiagonalisation; writes L, the reflectors and (d, e, tau).
-//   k_tridiag  one warp per pair: implicit QL on (d, e) with the rotations
-//              accumulated into Z (shared memory), eigenvalues ascending -> W,
-//              Z -> the caller's X buffer.
-//   k_back     one CTA per pair: X = L^{-H} Q Z in shared memory, written over Z.
+//   reduce   k_potrf_warp + k_hegst_col (n <= 56) or k_reduce (57..84): B = L L^H and
+//            C = L^{-1} A L^{-H}; L into the workspace, C into the caller's X buffer.
+//   hetrd    k_hetrd_warp (n <= 65) or k_hetrd: Householder tridiagonalisation of C,
+//            reflectors and (d, e, tau) into the workspace.
+//   eig      k_ql_chain: the implicit-QL recurrence, one thread per pair, logging its
+//            rotations; k_ql_apply / k_ql_apply_reg replay the log onto Z (W ascending).
+//            The mixed form runs the recurrence in FP32 and refines with k_refine.
+//   back     k_back_col (n <= 56) or k_back: X = L^{-H} Q Z, written over Z.
 //
 // The split follows where the work is latency bound: the QL recurrence is a
-// dependent scalar chain per pair, so it runs with many pairs per SM (only Z is
-// resident), while the BLAS2/BLAS3-shaped stages run a CTA per pair.
+// dependent scalar chain per pair, so it runs with many pairs per SM, while the
+// BLAS2-shaped stages run a warp or a CTA per pair.
 #include "kernels.cuh"
 #include "stages.cuh"
 #include "colsolve.cuh"
@@ -38,11 +40,6 @@ struct ReduceSmem {
     }
 };
 
-
-template <typename R>
-__host__ __device__ inline size_t tridiag_warp_bytes(int n) {
-    return align_up(sizeof(R) * (static_cast<size_t>(n) * tile_ld(n) + 2 * n), 16);
-}
 
 // Waits for the bulk copies of this CTA; on the (never expected) timeout it flags
 // the pair and waits once more, bounded, so no copy lands after the CTA exits.
@@ -472,43 +469,6 @@ __global__ void __launch_bounds__(32 * kHetrdWarpsPerCta) k_hetrd_warp(int n, in
         ws.e[static_cast<size_t>(n) * b + i] = e_s[i];
         ws.tau[static_cast<size_t>(n) * b + i] = (i + 1 < n) ? tau_s[i] : make_double2(0.0, 0.0);
     }
-}
-
-// ----------------------------------------------------------------------------- k_tridiag
-// R = double: the plain path, Z (double) -> X region, W final.
-// R = float : the mixed path's first half, Z (float) -> X region, W provisional.
-template <typename R>
-__global__ void k_tridiag(int n, int batch, Workspace ws, double* __restrict__ W,
-                          double2* __restrict__ X, int* __restrict__ info) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (b >= batch) return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int ldz = tile_ld(n);
-    R* Z = reinterpret_cast<R*>(smem + tridiag_warp_bytes<R>(n) * warp);
-    R* d = Z + static_cast<size_t>(n) * ldz;
-    R* e = d + n;
-    const size_t mat = static_cast<size_t>(n) * n;
-    R* Zg = reinterpret_cast<R*>(X + mat * b);
-    double* Wb = W + static_cast<size_t>(n) * b;
-    if (info[b] != 0) {
-        for (int i = lane; i < n; i += 32) Wb[i] = __longlong_as_double(0x7ff8000000000000ll);
-        return;
-    }
-    for (int i = lane; i < n; i += 32) {
-        d[i] = static_cast<R>(ws.d[static_cast<size_t>(n) * b + i]);
-        e[i] = static_cast<R>(ws.e[static_cast<size_t>(n) * b + i]);
-    }
-    for (int r = lane; r < n; r += 32)
-        for (int c = 0; c < n; ++c) Z[r * ldz + c] = (r == c) ? R(1) : R(0);
-    __syncwarp();
-    const int unconv = tridiag_ql<R>(n, d, e, Z, ldz);
-    for (int i = lane; i < n; i += 32) Wb[i] = static_cast<double>(d[i]);
-    for (size_t idx = lane; idx < mat; idx += 32) {
-        const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
-        Zg[idx] = Z[r * ldz + c];
-    }
-    if (lane == 0 && unconv) info[b] = unconv;
 }
 
 // ----------------------------------------------------------------------------- k_refine
@@ -958,9 +918,6 @@ int max_smem_optin() {
 
 size_t reduce_smem_bytes(int, int n) { return ReduceSmem(n).total; }
 size_t back_smem_bytes(int n) { return BackSmem(n).total; }
-size_t tridiag_smem_bytes(int n, int warps_per_cta, bool single) {
-    return (single ? tridiag_warp_bytes<float>(n) : tridiag_warp_bytes<double>(n)) * warps_per_cta;
-}
 
 // The register-segment kernels: (threads T, lanes per column G, rows per lane RM) by
 // size: n <= 32 -> (256, 8, 4), n <= 64 -> (512, 8, 8), else (512, 4, 22) (n <= 88).
@@ -1053,18 +1010,6 @@ cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws
         set_max_smem_once(k_hetrd<256>, f256);
         k_hetrd<256><<<batch, 256, smem, stream>>>(n, batch, C, ws, info);
     }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_tridiag_ql(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
-                              int warps_per_cta, cudaStream_t stream) {
-    if (batch <= 0) return cudaSuccess;
-    const size_t smem = tridiag_smem_bytes(n, warps_per_cta, false);
-    if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
-    static std::once_flag f;
-    set_max_smem_once(k_tridiag<double>, f);
-    const int grid = (batch + warps_per_cta - 1) / warps_per_cta;
-    k_tridiag<double><<<grid, 32 * warps_per_cta, smem, stream>>>(n, batch, ws, W, X, info);
     return cudaGetLastError();
 }
 

@@ -55,8 +55,6 @@ enum BackMode : int {
 // Launchers (asynchronous on `stream`; return cudaSuccess or the launch error).
 cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, int batch,
                           const Workspace& ws, double2* out, int* info, int threads, cudaStream_t stream);
-cudaError_t launch_tridiag_ql(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
-                              int warps_per_cta, cudaStream_t stream);
 // Householder tridiagonalisation of C (lower triangle read, column-major, ld = n) ->
 // reflectors into ws.LV (rows above the superdiagonal), tau, d, e.  Pairs with info != 0 skip.
 cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, const int* info, int threads,
@@ -97,7 +95,6 @@ cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, in
 inline int reduce_kernel_count(int n) { return n <= 56 ? 2 : 1; }
 
 size_t reduce_smem_bytes(int mode, int n);
-size_t tridiag_smem_bytes(int n, int warps_per_cta, bool single);
 size_t ql_chain_smem_bytes(int n, int threads, bool single);
 size_t ql_apply_smem_bytes(int n, int warps_per_cta, bool single);
 size_t back_smem_bytes(int n);

@@ -61,65 +61,6 @@ __device__ int potrf_lower(cplx<R>* L, int ld, int n, R* invd) {
     return 0;
 }
 
-// ============================================================================ trsm (left, lower, no-trans)
-// W <- L^{-1} W for the full n x n tile W (Trsm54Left, geneig_fixed.cu:33-45).
-// Columns are independent: G lanes of one warp share a column, lane g owning the
-// rows i = g (mod G); the solved entry of row k is broadcast by shuffle.
-template <typename R>
-__device__ void trsm_left_lower(const cplx<R>* L, int ldl, const R* invd, cplx<R>* W, int ldw, int n, int G) {
-    using C = cplx<R>;
-    const int tid = threadIdx.x, T = blockDim.x;
-    const int cols_per_pass = T / G;
-    const int g = tid % G;
-    for (int jb = 0; jb < n; jb += cols_per_pass) {
-        const int j = jb + tid / G;
-        const bool valid = j < n;
-        C* w = W + (valid ? j : 0) * ldw;
-        for (int k = 0; k < n; ++k) {
-            const int owner = k % G;
-            C wk = mk<R>(R(0), R(0));
-            if (valid && owner == g) { wk = cscale(w[k], invd[k]); w[k] = wk; }
-            wk = cshfl(wk, owner, G);
-            if (valid) {
-                const C* lk = L + k * ldl;
-                int i0 = k + 1 + ((g - (k + 1)) % G + G) % G;
-                for (int i = i0; i < n; i += G) w[i] = cfms(lk[i], wk, w[i]);
-            }
-        }
-    }
-}
-
-// ============================================================================ trsm (right, lower, conj-trans)
-// W <- W L^{-H}, lower triangle only (Trsm54Right, geneig_fixed.cu:47-59; the
-// result is Hermitian so only C(i, k), k <= i, is formed).  Rows are
-// independent: G lanes share a row, lane g owning the columns kk = g (mod G).
-template <typename R>
-__device__ void trsm_right_lowerH(const cplx<R>* L, int ldl, const R* invd, cplx<R>* W, int ldw, int n, int G) {
-    using C = cplx<R>;
-    const int tid = threadIdx.x, T = blockDim.x;
-    const int rows_per_pass = T / G;
-    const int g = tid % G;
-    const int warp_first = (tid & ~31) / G;             // first row slot of this warp in a pass
-    const int warp_rows = 32 / G;
-    for (int ib = 0; ib < n; ib += rows_per_pass) {
-        const int i = ib + tid / G;
-        const bool valid = i < n;
-        const int kmax = min(n - 1, ib + warp_first + warp_rows - 1);   // uniform per warp
-        for (int k = 0; k <= kmax; ++k) {
-            const int owner = k % G;
-            const bool act = valid && k <= i;
-            C ck = mk<R>(R(0), R(0));
-            if (act && owner == g) { ck = cscale(W[i + k * ldw], invd[k]); W[i + k * ldw] = ck; }
-            ck = cshfl(ck, owner, G);
-            if (act) {
-                int kk0 = k + 1 + ((g - (k + 1)) % G + G) % G;
-                for (int kk = kk0; kk <= i; kk += G)
-                    W[i + kk * ldw] = cfmsc(ck, L[kk + k * ldl], W[i + kk * ldw]);
-            }
-        }
-    }
-}
-
 // ============================================================================ hetrd (lower)
 // Householder reduction of the Hermitian tile A (lower triangle valid) to real
 // symmetric tridiagonal form T = Q^H A Q, Q = H_0 H_1 ... H_{n-2},
@@ -228,72 +169,6 @@ __device__ void hetrd_lower(cplx<R>* A, int lda, int n, R* d, R* e, cplx<R>* tau
     for (int i = tid; i < n; i += T) d[i] = A[i + i * lda].x;
     if (tid == 0 && n >= 1) e[n - 1] = R(0);
     __syncthreads();
-}
-
-// ============================================================================ Q Z
-// Y <- Q Y with Q = H_0 ... H_{n-2} from hetrd_lower.  The reflectors are read
-// from the rows of the tile LV: component i >= k+2 of v_k sits at LV(k, i) (the
-// strict upper triangle above the superdiagonal, so one tile also holds L in its
-// lower triangle); v_k(k+1) = 1 is implicit.  Applied right to left; columns of
-// Y are independent, G lanes per column reduce v^H y by shuffle.
-template <typename R>
-__device__ void apply_q_left(const cplx<R>* LV, int ld, const cplx<R>* tau, cplx<R>* Y, int ldy, int n, int G) {
-    using C = cplx<R>;
-    const int tid = threadIdx.x, T = blockDim.x;
-    const int cols_per_pass = T / G;
-    const int g = tid % G;
-    for (int jb = 0; jb < n; jb += cols_per_pass) {
-        const int j = jb + tid / G;
-        const bool valid = j < n;
-        C* y = Y + (valid ? j : 0) * ldy;
-        for (int k = n - 2; k >= 0; --k) {
-            const C tk = tau[k];
-            if (tk.x == R(0) && tk.y == R(0)) continue;      // uniform
-            const int m = n - k - 1;
-            const C* v = LV + k + (k + 1) * ld;               // v[i] = LV(k, k+1+i), v[0] = 1
-            C s = mk<R>(R(0), R(0));
-            if (valid) {
-                for (int i = g; i < m; i += G) {
-                    const C vi = (i == 0) ? mk<R>(R(1), R(0)) : v[i * ld];
-                    s = cfmac(vi, y[k + 1 + i], s);
-                }
-            }
-            s.x = group_sum(s.x, G);
-            s.y = group_sum(s.y, G);
-            s = cmul(tk, s);
-            if (valid) {
-                for (int i = g; i < m; i += G) {
-                    const C vi = (i == 0) ? mk<R>(R(1), R(0)) : v[i * ld];
-                    y[k + 1 + i] = cfms(vi, s, y[k + 1 + i]);
-                }
-            }
-        }
-    }
-}
-
-// ============================================================================ trsm (left, lower, conj-trans)
-// Y <- L^{-H} Y (Trsm54LeftConj, geneig_fixed.cu:63-75): backward substitution
-// per column, G lanes per column, lane g owning rows i = g (mod G).
-template <typename R>
-__device__ void trsm_left_lowerH(const cplx<R>* L, int ldl, const R* invd, cplx<R>* Y, int ldy, int n, int G) {
-    using C = cplx<R>;
-    const int tid = threadIdx.x, T = blockDim.x;
-    const int cols_per_pass = T / G;
-    const int g = tid % G;
-    for (int jb = 0; jb < n; jb += cols_per_pass) {
-        const int j = jb + tid / G;
-        const bool valid = j < n;
-        C* y = Y + (valid ? j : 0) * ldy;
-        for (int k = n - 1; k >= 0; --k) {
-            const int owner = k % G;
-            C xk = mk<R>(R(0), R(0));
-            if (valid && owner == g) { xk = cscale(y[k], invd[k]); y[k] = xk; }
-            xk = cshfl(xk, owner, G);
-            if (valid) {
-                for (int i = g; i < k; i += G) y[i] = cfms(cconj(L[k + i * ldl]), xk, y[i]);
-            }
-        }
-    }
 }
 
 // ============================================================================ tridiagonal QL
@@ -698,7 +573,8 @@ __device__ __forceinline__ void seg_trsm_right_lowerH(const C* L, int ldl, const
     }
 }
 
-// y <- Q y with the reflectors along the rows of LV (see apply_q_left).
+// y <- Q y, Q = H_0 ... H_{n-2}, with the reflectors along the rows of LV: component i >= k+2
+// of v_k sits at LV(k, i) (above the superdiagonal); v_k(k+1) = 1 is implicit.
 template <int G, int RM, typename C>
 __device__ __forceinline__ void seg_apply_q(const C* LV, int ld, const C* tau, C (&y)[RM], int n, int g) {
     using R = decltype(C().x);
