@@ -207,6 +207,45 @@ int sbg_queue_bucket(const sbg_queue* q, int i, int* n, int* count, int* chunk, 
 /* How many times the launch graph was captured (1 while the buffers stay the same). */
 int sbg_queue_graph_builds(const sbg_queue* q);
 
+/* ------------------------------------------------------------------ spin-wave q-sweeps */
+/* No counterpart in the reference: the steps either side of the solve when the pairs come from a
+ * linear spin-wave model swept over q.  The reference's intended caller assembles A(q), B(q) on
+ * the host and moves 2 x 16 n^2 bytes per q to the GPU and 16 n^2 bytes of eigenvectors back; a
+ * model held on the GPU takes q (24 bytes) in and gives W and n intensities per q out.
+ *   - Cell: n_sites = N sites, order n = 2N.  Bond k joins sites (i, j) = (sites[2k], sites[2k+1])
+ *     with displacement d = disp[3k..3k+2] and coefficients a = coef[5k] + i coef[5k+1],
+ *     b = coef[5k+2] + i coef[5k+3], c = coef[5k+4].  pos[3i..3i+2] is site i's position
+ *     (NULL: all zero); field is a constant added to the diagonal of B.
+ *   - Per q (q = d_q[3p..3p+2]): P_ij += a/2 e^{i q.d}, P_ji += conj(a/2 e^{i q.d}),
+ *     Q_ij += b/2 e^{i q.d}, Q_ji += b/2 e^{i q.d}, P_ii -= c/2, P_jj -= c/2, summed in bond
+ *     order; A = diag(I_N, -I_N) and B = [[P, Q], [conj Q, conj P]] + field I (column-major, as
+ *     sbg_solver_launch reads them).
+ *   - Intensity of eigenpair m of pair p: I_m = |sum_{i<N} e^{-i q.r_i} (x_m[i] + x_m[N+i])|^2
+ *     / (N |lambda_m|), in W's order (d_I[n p + m]); NaN for a pair whose info != 0.
+ *   - sbg_spinwave_solve runs assembly, the solve and the contraction on `stream`, chunk by
+ *     chunk (the solver's chunk size), with the solver `s` (order 2N, same device).  d_X and d_I
+ *     may each be NULL (eigenvectors / intensities not wanted); W and info are always written.
+ *     Per stream it keeps one chunk of A, B and (when d_X is NULL) X scratch, grown on first
+ *     use: run one sweep of the largest size on a stream before capturing it into a graph.
+ *   - sbg_spinwave_solve_host takes page-locked host q, W, X (or NULL), I (or NULL) and info,
+ *     overlaps the copies with the kernels over num_streams internal streams (chunk_size 0:
+ *     the solver's chunk) and returns when the results are on the host.
+ * All calls return an sbg_status. */
+typedef struct sbg_spinwave sbg_spinwave;
+int sbg_spinwave_create(int n_sites, int n_bonds, const int* sites, const double* coef, const double* disp,
+                        const double* pos, double field, int device_id, sbg_spinwave** out);
+int sbg_spinwave_destroy(sbg_spinwave* m);
+int sbg_spinwave_matrix_size(const sbg_spinwave* m);
+/* A may be NULL (B only). */
+int sbg_spinwave_assemble(sbg_spinwave* m, const double* d_q, int nq, cuDoubleComplex* d_A, cuDoubleComplex* d_B,
+                          cudaStream_t stream);
+int sbg_spinwave_intensities(sbg_spinwave* m, const double* d_q, int nq, const double* d_W,
+                             const cuDoubleComplex* d_X, const int* d_info, double* d_I, cudaStream_t stream);
+int sbg_spinwave_solve(sbg_spinwave* m, sbg_solver* s, const double* d_q, int nq, double* d_W,
+                       cuDoubleComplex* d_X, double* d_I, int* d_info, cudaStream_t stream);
+int sbg_spinwave_solve_host(sbg_spinwave* m, sbg_solver* s, const double* h_q, int nq, double* h_W,
+                            cuDoubleComplex* h_X, double* h_I, int* h_info, int chunk_size, int num_streams);
+
 /* ------------------------------------------------------------------ allocation-free solve */
 /* This entry point has no counterpart in the reference.
  *

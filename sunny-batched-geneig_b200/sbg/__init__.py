@@ -22,7 +22,7 @@ from . import _lib
 from ._lib import SolverOptions, load
 
 __all__ = [
-    "Solver", "SolverError", "Queue", "pack_pairs", "unpack", "solve", "to_colmajor", "from_colmajor", "max_n",
+    "Solver", "SolverError", "Queue", "SpinWave", "pack_pairs", "unpack", "solve", "to_colmajor", "from_colmajor", "max_n",
     "geneig_full_n54_batched", "chol_n54", "reduce_n54", "reduce_eig_n54", "full_n54", "finish_n54",
     "PRECISIONS", "fixed_n54_introspection", "tuning_table_path", "tuning_forget_in_process",
 ]
@@ -281,6 +281,119 @@ class Queue:
                 raise ValueError(f"{name} must be a contiguous CUDA {dt} tensor of {size} elements")
         _check(self._lib.sbg_launch_queue(self._h, _ptr(A), _ptr(B), _ptr(W), _ptr(X), _ptr(info), _stream(stream)),
                "sbg_launch_queue")
+
+
+class SpinWave:
+    """One spin-wave cell held on the GPU (sbg_spinwave_*): assembles A(q), B(q) per q, and
+    contracts each eigenvector to an intensity, around the solve.
+
+    sites: (nb, 2) int site pairs (i, j); coef: (nb, 5) float (Re a, Im a, Re b, Im b, c);
+    disp: (nb, 3) bond displacements; pos: (N, 3) site positions or None; field: constant
+    added to B's diagonal.  Per q: P_ij += a/2 e^{iq.d}, P_ji += conj(a/2 e^{iq.d}),
+    Q_ij = Q_ji += b/2 e^{iq.d}, P_ii, P_jj -= c/2; A = diag(I, -I),
+    B = [[P, Q], [conj Q, conj P]] + field I.  Intensity of eigenpair m:
+    |sum_i e^{-iq.r_i} (x_m[i] + x_m[N+i])|^2 / (N |lambda_m|).
+    q: (nq, 3) float64 tensors (device for the device calls, host for ``solve_host``).
+    """
+
+    def __init__(self, n_sites: int, sites, coef, disp, pos=None, field: float = 0.0, device: int = 0):
+        import numpy as np
+        lib = load()
+        sites = np.ascontiguousarray(np.asarray(sites, dtype=np.int32).reshape(-1, 2))
+        nb = sites.shape[0]
+        coef = np.ascontiguousarray(np.asarray(coef, dtype=np.float64).reshape(nb, 5))
+        disp = np.ascontiguousarray(np.asarray(disp, dtype=np.float64).reshape(nb, 3))
+        posp = None
+        if pos is not None:
+            pos = np.ascontiguousarray(np.asarray(pos, dtype=np.float64).reshape(n_sites, 3))
+            posp = pos.ctypes.data_as(ctypes.c_void_p)
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(device):
+            _check(lib.sbg_spinwave_create(n_sites, nb, sites.ctypes.data_as(ctypes.c_void_p),
+                                           coef.ctypes.data_as(ctypes.c_void_p),
+                                           disp.ctypes.data_as(ctypes.c_void_p), posp, float(field), device,
+                                           ctypes.byref(handle)), "sbg_spinwave_create")
+        self._h = handle
+        self._lib = lib
+        self.n_sites = n_sites
+        self.n = 2 * n_sites
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.sbg_spinwave_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _q(self, q, cuda: bool):
+        if q.dtype != torch.float64 or not q.is_contiguous() or q.dim() != 2 or q.shape[1] != 3 \
+                or q.is_cuda != cuda:
+            raise ValueError(f"q must be a contiguous {'CUDA' if cuda else 'host'} float64 (nq, 3) tensor")
+        return q.shape[0]
+
+    @staticmethod
+    def _buf(name, t, dt, numel, cuda: bool, optional: bool = False):
+        if t is None:
+            if optional:
+                return
+            raise ValueError(f"{name} is required")
+        if t.is_cuda != cuda or t.dtype != dt or not t.is_contiguous() or t.numel() != numel:
+            raise ValueError(f"{name} must be a contiguous {'CUDA' if cuda else 'host'} {dt} tensor "
+                             f"of {numel} elements")
+
+    def assemble(self, q, A=None, B=None, stream=None):
+        """A(q), B(q) of every q into (nq, n*n) column-major device tensors (allocated when None;
+        A is skipped when A is False).  Returns (A, B)."""
+        nq = self._q(q, True)
+        nn = self.n * self.n
+        if B is None:
+            B = torch.empty((nq, nn), dtype=torch.complex128, device=q.device)
+        if A is None:
+            A = torch.empty((nq, nn), dtype=torch.complex128, device=q.device)
+        self._buf("B", B, torch.complex128, nq * nn, True)
+        if A is not False:
+            self._buf("A", A, torch.complex128, nq * nn, True)
+        _check(self._lib.sbg_spinwave_assemble(self._h, _ptr(q), nq, None if A is False else _ptr(A), _ptr(B),
+                                               _stream(stream)), "sbg_spinwave_assemble")
+        return (None if A is False else A), B
+
+    def intensities(self, q, W, X, info, I=None, stream=None):
+        nq = self._q(q, True)
+        if I is None:
+            I = torch.empty((nq, self.n), dtype=torch.float64, device=q.device)
+        self._buf("W", W, torch.float64, nq * self.n, True)
+        self._buf("X", X, torch.complex128, nq * self.n * self.n, True)
+        self._buf("info", info, torch.int32, nq, True)
+        self._buf("I", I, torch.float64, nq * self.n, True)
+        _check(self._lib.sbg_spinwave_intensities(self._h, _ptr(q), nq, _ptr(W), _ptr(X), _ptr(info), _ptr(I),
+                                                  _stream(stream)), "sbg_spinwave_intensities")
+        return I
+
+    def solve(self, solver: Solver, q, W, info, X=None, I=None, stream=None) -> None:
+        """Assemble + solve (+ intensities when I is given) for every q, on the device."""
+        nq = self._q(q, True)
+        self._buf("W", W, torch.float64, nq * self.n, True)
+        self._buf("info", info, torch.int32, nq, True)
+        self._buf("X", X, torch.complex128, nq * self.n * self.n, True, optional=True)
+        self._buf("I", I, torch.float64, nq * self.n, True, optional=True)
+        _check(self._lib.sbg_spinwave_solve(self._h, solver._h, _ptr(q), nq, _ptr(W), _ptr(X), _ptr(I), _ptr(info),
+                                            _stream(stream)), "sbg_spinwave_solve")
+
+    def solve_host(self, solver: Solver, q, W, info, X=None, I=None, chunk_size: int = 0,
+                   num_streams: int = 2) -> None:
+        """The same from (ideally pinned) host q into host W, info, X, I; synchronous."""
+        nq = self._q(q, False)
+        self._buf("W", W, torch.float64, nq * self.n, False)
+        self._buf("info", info, torch.int32, nq, False)
+        self._buf("X", X, torch.complex128, nq * self.n * self.n, False, optional=True)
+        self._buf("I", I, torch.float64, nq * self.n, False, optional=True)
+        _check(self._lib.sbg_spinwave_solve_host(self._h, solver._h, _ptr(q), nq, _ptr(W), _ptr(X), _ptr(I),
+                                                 _ptr(info), chunk_size, num_streams), "sbg_spinwave_solve_host")
 
 
 def pack_pairs(mats):

@@ -15,6 +15,7 @@ I = ctypes.c_int
 U = ctypes.c_uint
 SZ = ctypes.c_size_t
 LL = ctypes.c_longlong
+D = ctypes.c_double
 
 # Every exported symbol with (restype, argtypes); the CPU tests check this list
 # against include/sbg/geneig.h.
@@ -73,6 +74,13 @@ SIGNATURES = {
     "sbg_queue_buckets": (I, [P]),
     "sbg_queue_bucket": (I, [P, I, P, P, P, P, P]),
     "sbg_queue_graph_builds": (I, [P]),
+    "sbg_spinwave_create": (I, [I, I, P, P, P, P, D, I, P]),
+    "sbg_spinwave_destroy": (I, [P]),
+    "sbg_spinwave_matrix_size": (I, [P]),
+    "sbg_spinwave_assemble": (I, [P, P, I, P, P, P]),
+    "sbg_spinwave_intensities": (I, [P, P, I, P, P, P, P, P]),
+    "sbg_spinwave_solve": (I, [P, P, P, I, P, P, P, P, P]),
+    "sbg_spinwave_solve_host": (I, [P, P, P, I, P, P, P, P, I, I]),
 }
 
 

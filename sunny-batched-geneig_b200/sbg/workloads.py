@@ -15,6 +15,10 @@ available), so these generators stand in for it.  All return (A, B) as
   terms u^T J conj(u), u^T J u (u = (1, i, 0)/sqrt 2) times exp(i q.d), with the
   -J_zz/2 on-site terms; B0(q) in the Bogoliubov form, shifted to
   lambda_min = frac * ||B||_2.
+* ``spinwave_cell``: the same cell as a bond table for ``sbg.SpinWave`` (sites, coefficients
+  (Re a, Im a, Re b, Im b, J_zz), displacements) plus seeded site positions in [0, 1)^3; its
+  B(q) = B0(q) + field I, with ``spinwave_field`` choosing the one field of the whole sweep
+  that puts min_q lambda_min(B) at frac * max_q ||B||_2.
 * ``uneven_sizes``: the n of each pair of the uneven batch (proportions over
   {12, 24, 32, 54, 96, 128}), shuffled with the given seed.
 """
@@ -148,6 +152,23 @@ def qsweep(N: int, grid: int = 64, seed: int = 0, frac: float = 1e-3, start: int
     B0 = qsweep_B0(N, q, seed)
     B = _shift(B0, frac, _eigvalsh(B0, eigvalsh))
     return metric_A(N, q.shape[0], device), _colmajor(B)
+
+
+def spinwave_cell(N: int, seed: int = 0) -> dict:
+    """The q-sweep cell of ``qsweep_cell`` as arrays for ``sbg.SpinWave``."""
+    bonds = qsweep_cell(N, seed)
+    sites = np.array([[i, j] for (i, j, a, b, c, d) in bonds], dtype=np.int32).reshape(-1, 2)
+    coef = np.array([[a.real, a.imag, b.real, b.imag, c] for (i, j, a, b, c, d) in bonds],
+                    dtype=np.float64).reshape(-1, 5)
+    disp = np.array([d for (i, j, a, b, c, d) in bonds], dtype=np.float64).reshape(-1, 3)
+    pos = np.random.default_rng(seed + 7919).uniform(0.0, 1.0, (N, 3))
+    return dict(n_sites=N, sites=sites, coef=coef, disp=disp, pos=pos)
+
+
+def spinwave_field(lmin: float, lmax: float, frac: float) -> float:
+    """Field h with min_q lambda_min(B0 + h I) = frac * max_q lambda_max(B0 + h I), from the sweep's
+    extreme eigenvalues of B0 (h = (frac lmax - lmin) / (1 - frac), as ``_shift`` per pair)."""
+    return (frac * lmax - lmin) / (1.0 - frac)
 
 
 UNEVEN_SIZES = (12, 24, 32, 54, 96, 128)
