@@ -144,10 +144,14 @@ int sbg_solver_reserve(sbg_solver* s, int pairs, int stream_slots);
  * launch_chunked, nvrtc_solver.cpp:1078-1107, applied to host<->device traffic).
  * Synchronous: returns once W, X and info are on the host.  Host buffers should be
  * page-locked (cudaHostAlloc) for the copies to overlap.  Device staging buffers are
- * owned by the solver and grow on demand. */
+ * owned by the solver and grow on demand.  Only B's lower triangle crosses the host link
+ * when h_B lies in one pinned, device-mapped allocation (cudaHostAlloc memory on 64-bit
+ * systems): a kernel reads it in place; otherwise all of B is copied. */
 int sbg_solver_solve_host(sbg_solver* s, const cuDoubleComplex* h_A, const cuDoubleComplex* h_B,
                           double* h_W, cuDoubleComplex* h_X, int* h_info, int batch,
                           int chunk_size, int num_streams);
+/* Bytes the solver's last sbg_solver_solve_host moved host -> device and device -> host. */
+int sbg_solver_host_transfer_bytes(const sbg_solver* s, long long* h2d_bytes, long long* d2h_bytes);
 
 /* Per-stage timing: when enabled, every launch records CUDA events around each stage
  * kernel on the launch stream.  sbg_solver_read_stage_times synchronizes on them and

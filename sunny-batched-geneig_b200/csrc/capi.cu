@@ -189,6 +189,14 @@ int sbg_solver_solve_host(sbg_solver* s, const cuDoubleComplex* h_A, const cuDou
     });
 }
 
+int sbg_solver_host_transfer_bytes(const sbg_solver* s, long long* h2d_bytes, long long* d2h_bytes) {
+    return guarded([&] {
+        if (!s) throw Error(SBG_ERR_INVALID_VALUE, "solver == NULL");
+        if (h2d_bytes) *h2d_bytes = s->last_h2d_bytes;
+        if (d2h_bytes) *d2h_bytes = s->last_d2h_bytes;
+    });
+}
+
 int sbg_solver_enable_stage_timing(sbg_solver* s, int enable) {
     return guarded([&] {
         if (!s) throw Error(SBG_ERR_INVALID_VALUE, "solver == NULL");

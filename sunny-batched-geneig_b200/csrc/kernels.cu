@@ -17,6 +17,7 @@
 #include "stages.cuh"
 #include "colsolve.cuh"
 
+#include <algorithm>
 #include <cstdlib>
 #include <mutex>
 
@@ -1121,6 +1122,45 @@ template <int NMAX>
 void run_back_col(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info, size_t smem,
                   cudaStream_t stream) {
     run_back_col_g<NMAX, 1>(mode, n, batch, ws, X, info, smem, stream);
+}
+
+// ----------------------------------------------------------------------------- k_pull_pairs
+// Pairs are walked grid-stride, each by the whole CTA; every thread keeps 4 independent 16-byte
+// loads in flight (their latency is the host link's, about a microsecond), then stores them.
+constexpr int kPullThreads = 256;
+constexpr int kPullDepth = 4;
+
+__global__ void __launch_bounds__(kPullThreads) k_pull_pairs(const double2* __restrict__ src,
+                                                             double2* __restrict__ dst, int count, int n,
+                                                             int lower) {
+    const int nn = n * n;
+    for (int p = blockIdx.x; p < count; p += gridDim.x) {
+        const double2* s = src + static_cast<size_t>(nn) * p;
+        double2* d = dst + static_cast<size_t>(nn) * p;
+        for (int base = 0; base < nn; base += kPullDepth * kPullThreads) {
+            double2 v[kPullDepth];
+            int at[kPullDepth];
+#pragma unroll
+            for (int u = 0; u < kPullDepth; ++u) {
+                const int e = base + u * kPullThreads + threadIdx.x;
+                const int col = e / n, row = e - col * n;
+                at[u] = (e < nn && (!lower || row >= col)) ? e : -1;
+                if (at[u] >= 0) v[u] = s[e];
+            }
+#pragma unroll
+            for (int u = 0; u < kPullDepth; ++u)
+                if (at[u] >= 0) d[at[u]] = v[u];
+        }
+    }
+}
+
+cudaError_t launch_pull_pairs(const double2* src, double2* dst, int count, int n, bool lower, cudaStream_t stream) {
+    if (count <= 0) return cudaSuccess;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_pull_pairs<<<std::min(count, sms), kPullThreads, 0, stream>>>(src, dst, count, n, lower ? 1 : 0);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,

@@ -67,6 +67,11 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
 cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
                                  int refine_steps, int chain_threads, int apply_warps, int refine_threads,
                                  cudaStream_t stream);
+// Host-buffer path: copies `count` pairs of n x n column-major matrices from pinned host memory
+// that the GPU can address (src is its device-side address) into device memory, either every
+// element or only rows j..n-1 of each column j (lower, for B, whose upper triangle no kernel
+// reads).  The kernel's loads cross the host link; one CTA per SM keeps enough of them in flight.
+cudaError_t launch_pull_pairs(const double2* src, double2* dst, int count, int n, bool lower, cudaStream_t stream);
 cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
                         int threads, cudaStream_t stream);
 

@@ -154,6 +154,14 @@ class Solver:
         _check(self._lib.sbg_solver_solve_host(self._h, _ptr(A), _ptr(B), _ptr(W), _ptr(X), _ptr(info), batch,
                                                chunk_size, num_streams), "sbg_solver_solve_host")
 
+    def host_transfer_bytes(self):
+        """(host->device, device->host) bytes of the last ``solve_host``: B's lower triangle only
+        when B is pinned, device-mapped host memory (pulled by a kernel), all of B otherwise."""
+        h2d, d2h = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(self._lib.sbg_solver_host_transfer_bytes(self._h, ctypes.byref(h2d), ctypes.byref(d2h)),
+               "sbg_solver_host_transfer_bytes")
+        return h2d.value, d2h.value
+
     def enable_stage_timing(self, enable: bool = True) -> None:
         _check(self._lib.sbg_solver_enable_stage_timing(self._h, int(enable)), "sbg_solver_enable_stage_timing")
 

@@ -50,6 +50,7 @@ SIGNATURES = {
     "sbg_solver_launch_chunked": (I, [P, P, P, P, P, P, I, I, I, P]),
     "sbg_solver_reserve": (I, [P, I, I]),
     "sbg_solver_solve_host": (I, [P, P, P, P, P, P, I, I, I]),
+    "sbg_solver_host_transfer_bytes": (I, [P, P, P]),
     "sbg_solver_enable_stage_timing": (I, [P, I]),
     "sbg_solver_read_stage_times": (I, [P, P, P]),
     "sbg_workspace_bytes_per_pair": (SZ, [I, I]),

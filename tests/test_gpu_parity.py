@@ -247,3 +247,40 @@ def test_near_goldstone_both_forms(oracle_mod):
         # kappa(B) ~ 1e8 for any FP64 Cholesky-based solver); hold ours to LAPACK's level
         assert s["residual"] < max(1e-12, 4.0 * res_ref), (prec, s, res_ref)
         assert s["orth"] < max(1e-9, 4.0 * orth_ref), (prec, s, orth_ref)       # zhegv: ~4e-9 here
+
+
+@pytest.mark.parametrize("n", [12, 54, 96])
+def test_solve_host_paths_match_device_launch(n):
+    """sbg_solver_solve_host from pinned host buffers (B's lower triangle pulled by a kernel) and
+    from pageable ones (whole matrices copied) equals the device launch bit for bit, with NaN in
+    B's strict upper triangle (never read), and reports the bytes it moved."""
+    N = n // 2
+    batch = 300
+    A, B = wl.bogoliubov(N, batch, seed=11, frac=1e-2)
+    Bm = B.reshape(batch, n, n)                   # [b, j, i] = B(i, j)
+    upper = torch.triu(torch.ones(n, n, dtype=torch.bool), diagonal=1).T   # i < j, in [j, i] indexing
+    Bm[:, upper] = complex("nan+nanj")
+    B = Bm.reshape(batch, n * n).contiguous()
+    s = sbg.Solver(n)
+    dW = torch.empty((batch, n), dtype=torch.float64, device="cuda")
+    dX = torch.empty((batch, n * n), dtype=torch.complex128, device="cuda")
+    dI = torch.empty(batch, dtype=torch.int32, device="cuda")
+    s.launch(A.cuda(), B.cuda(), dW, dX, dI)
+    torch.cuda.synchronize()
+    assert (dI == 0).all() and torch.isfinite(dW).all()
+    nn = n * n
+    for pinned in (True, False):
+        hA = A.clone().pin_memory() if pinned else A.clone()
+        hB = B.clone().pin_memory() if pinned else B.clone()
+        hW = torch.empty((batch, n), dtype=torch.float64)
+        hX = torch.empty((batch, nn), dtype=torch.complex128)
+        hI = torch.empty(batch, dtype=torch.int32)
+        if pinned:
+            hW, hX, hI = hW.pin_memory(), hX.pin_memory(), hI.pin_memory()
+        s.solve_host(hA, hB, hW, hX, hI, chunk_size=64, num_streams=3)
+        assert torch.equal(hW, dW.cpu()) and torch.equal(hX, dX.cpu()) and torch.equal(hI, dI.cpu()), pinned
+        h2d, d2h = s.host_transfer_bytes()
+        b_bytes = 8 * n * (n + 1) if pinned else 16 * nn
+        assert h2d == (16 * nn + b_bytes) * batch, (pinned, h2d)
+        assert d2h == (16 * nn + 8 * n + 4) * batch
+    s.close()
