@@ -65,8 +65,9 @@ __device__ __forceinline__ double2 entry_sum(const int* map, const int* ptr, con
     return v;
 }
 
-// One CTA per q: the bond phases into shared memory, then every entry of B(q) (and,
-// when A != nullptr, of the metric A) written column-major, coalesced.
+// One CTA per q: the bond phases into shared memory, then every entry of B(q) (and, when
+// A != nullptr, of the metric A) written column-major: each warp takes whole columns, its lanes
+// the rows, so the stores of a column are contiguous and no index is divided.
 __global__ void __launch_bounds__(kAssembleThreads) k_sw_assemble(SwTables T, const double* __restrict__ qv, int nq,
                                                                    double2* __restrict__ A, double2* __restrict__ B) {
     const int p = blockIdx.x;
@@ -84,25 +85,27 @@ __global__ void __launch_bounds__(kAssembleThreads) k_sw_assemble(SwTables T, co
         tb[k] = sbg::cmul(T.half_b[k], ph);
     }
     __syncthreads();
-    const int N = T.N, n = 2 * N, nn = n * n;
-    double2* Bp = B + static_cast<size_t>(nn) * p;
-    double2* Ap = A ? A + static_cast<size_t>(nn) * p : nullptr;
-    for (int e = threadIdx.x; e < nn; e += kAssembleThreads) {
-        const int col = e / n, row = e - col * n;
-        const int br = row >= N, bc = col >= N;
-        const int r = row - br * N, c = col - bc * N;
-        double2 v;
-        if (br == bc) {                                   // P (top left) or conj(P) (bottom right)
-            v = entry_sum(T.mapP, T.ptrP, T.listP, r + N * c, ta, true);
-            if (r == c) v.x += T.onsite[r];
-            if (br) v.y = -v.y;
-            if (r == c) v.x += T.field;
-        } else {                                          // Q (top right) or conj(Q) (bottom left)
-            v = entry_sum(T.mapQ, T.ptrQ, T.listQ, r + N * c, tb, false);
-            if (br) v.y = -v.y;
+    const int N = T.N, n = 2 * N;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double2* Bp = B + static_cast<size_t>(n) * n * p;
+    double2* Ap = A ? A + static_cast<size_t>(n) * n * p : nullptr;
+    for (int col = warp; col < n; col += kAssembleThreads / 32) {
+        const int bc = col >= N, c = col - bc * N;
+        for (int row = lane; row < n; row += 32) {
+            const int br = row >= N, r = row - br * N;
+            double2 v;
+            if (br == bc) {                               // P (top left) or conj(P) (bottom right)
+                v = entry_sum(T.mapP, T.ptrP, T.listP, r + N * c, ta, true);
+                if (r == c) v.x += T.onsite[r];
+                if (br) v.y = -v.y;
+                if (r == c) v.x += T.field;
+            } else {                                      // Q (top right) or conj(Q) (bottom left)
+                v = entry_sum(T.mapQ, T.ptrQ, T.listQ, r + N * c, tb, false);
+                if (br) v.y = -v.y;
+            }
+            Bp[static_cast<size_t>(col) * n + row] = v;
+            if (Ap) Ap[static_cast<size_t>(col) * n + row] = make_double2(row == col ? (row < N ? 1.0 : -1.0) : 0.0, 0.0);
         }
-        Bp[e] = v;
-        if (Ap) Ap[e] = make_double2(row == col ? (row < N ? 1.0 : -1.0) : 0.0, 0.0);
     }
 }
 
