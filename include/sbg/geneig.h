@@ -112,7 +112,9 @@ typedef struct {
     int tuning_mode;          /* SBG_TUNING_*  (hpp:101) */
     int cache_mode;           /* SBG_CACHE_*   (hpp:102) */
     int precision;            /* SBG_PRECISION_FP64 (plain drop-in) or SBG_PRECISION_MIXED */
-    int refine_steps;         /* mixed form: Ogita-Aishima steps, 0 = default (3; the last only orthogonalises near-degenerate pairs) */
+    int refine_steps;         /* mixed form: most Ogita-Aishima steps, 0 = default (5): full steps until the largest
+                                 correction is <= 1e-8 (at least two), then one that only orthogonalises
+                                 near-degenerate pairs; typically 3 run */
     int workspace_pairs;      /* pairs per internal chunk; 0 = default */
 } sbg_solver_options;
 

@@ -72,7 +72,7 @@ void sbgi::create_solver(int n, int device, const sbg_solver_options* o, sbg_sol
     s->n = n;
     s->device = device;
     s->precision = opts.precision;
-    s->refine_steps = opts.refine_steps > 0 ? opts.refine_steps : 3;
+    s->refine_steps = opts.refine_steps > 0 ? opts.refine_steps : 5;
     s->chunk_pairs = opts.workspace_pairs > 0 ? opts.workspace_pairs : default_chunk_pairs(n);
     sbg::TuneRequest req;
     req.n = n;

@@ -524,12 +524,24 @@ __global__ void __launch_bounds__(T) k_refine(int n, int batch, Workspace ws, do
         eT[i] = ws.e[static_cast<size_t>(n) * b + i];
     }
     __syncthreads();
-    // The correction stalls at ~eps ||T|| / gap for nearly degenerate pairs instead of
-    // vanishing, so every step runs; the last one only orthogonalises pairs closer
-    // than 1e-2 ||T||_F (see oa_refine_step).
+    // Full steps until the largest correction |E_ij| is <= 1e-8 (at least two), then one step that
+    // only orthogonalises pairs closer than 1e-2 ||T||_F (see oa_refine_step); max_steps counts
+    // them all.  Z + Z E is orthonormal only to second order in E, and the correction of
+    // eigenvalues at a relative distance of ~1e-5 is large late: the first step, while the FP32
+    // residual still exceeds their gap, treats them as a cluster, the next rotates them by ~1e-3,
+    // and a schedule that stopped there left X^H B X - I at ~1e-12 on 0.01-0.1 % of q-sweep
+    // pairs.  The correction of a converged pair stalls at ~eps ||T|| / gap instead of vanishing,
+    // which the final orthogonalising step absorbs.
     for (int step = 0; step < max_steps; ++step) {
-        oa_refine_step<2>(n, dT, eT, Za, ld, TZ, Rm, Sm, Zb, lam, red, step + 1 == max_steps ? 1e-2 : 0.0);
+        const bool last = step + 1 == max_steps;
+        const double em = oa_refine_step<2>(n, dT, eT, Za, ld, TZ, Rm, Sm, Zb, lam, red, last ? 1e-2 : 0.0);
         double* t = Za; Za = Zb; Zb = t;
+        if (last) break;
+        if (step >= 1 && em <= 1e-8) {          // converged (em is the same on every thread)
+            oa_refine_step<2>(n, dT, eT, Za, ld, TZ, Rm, Sm, Zb, lam, red, 1e-2);
+            t = Za; Za = Zb; Zb = t;
+            break;
+        }
     }
     // Acceptance: every refined pair must satisfy ||T z - lam z|| <= 256 eps ||T||_F ||z||.  When the
     // FP32 start was too coarse for the refinement to separate eigenvalues (e.g. small eigenvalues

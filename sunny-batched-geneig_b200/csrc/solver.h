@@ -120,7 +120,7 @@ struct sbg_solver {
     int n = 0;
     int device = 0;
     int precision = SBG_PRECISION_FP64;
-    int refine_steps = 2;
+    int refine_steps = 5;
     int chunk_pairs = 0;
     sbg::Schedule sched;
     bool autotuned = false;
