@@ -815,6 +815,208 @@ __global__ void k_ql_apply_reg(int n, int batch, Workspace ws, double* __restric
     }
 }
 
+// ----------------------------------------------------------------------------- k_ql_values
+// The QL chain of k_ql_chain (one thread per pair) for the eigenvalues only: no rotation log,
+// no permutation; W ascending.  Feeds k_tridiag_invit.
+__global__ void k_ql_values(int n, int batch, Workspace ws, double* __restrict__ W, int* __restrict__ info) {
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int b = blockIdx.x * T + tid;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double* d = reinterpret_cast<double*>(smem) + tid;
+    double* e = reinterpret_cast<double*>(smem) + static_cast<size_t>(n) * T + tid;
+    if (b >= batch) return;
+    double* Wb = W + static_cast<size_t>(n) * b;
+    if (info[b] != 0) {
+        for (int i = 0; i < n; ++i) Wb[i] = __longlong_as_double(0x7ff8000000000000ll);
+        return;
+    }
+    for (int i = 0; i < n; ++i) {
+        d[i * T] = ws.d[static_cast<size_t>(n) * b + i];
+        e[i * T] = ws.e[static_cast<size_t>(n) * b + i];
+    }
+    const int r = ql_chain<double, false>(n, d, e, T, nullptr, 0, nullptr, Wb);
+    if (r > 0) info[b] = r;
+}
+
+// ----------------------------------------------------------------------------- k_tridiag_invit
+// Eigenvectors of the tridiagonal T (d, e) from its FP64 eigenvalues (k_ql_values) by inverse
+// iteration, one warp per pair, one lane per eigenvector at a time (LAPACK dstein's method):
+// T - lambda_j I = L U without pivoting, a pivot below eps ||T|| replaced by that size, two
+// solves from a fixed pseudo-random start, each followed by normalisation.  That is O(n) work
+// per vector against the O(n^2) of applying every QL rotation to it.  The vectors of
+// eigenvalues closer than kInvitOrtol ||T|| (a cluster) are computed in order, one lane per
+// cluster, with three solves each orthogonalised against the cluster's earlier vectors
+// (modified Gram-Schmidt); the other vectors' orthogonality is ~eps ||T|| / gap.  Every
+// vector must pass ||T z - lambda z|| <= kInvitTol ||T||; a pair with a failed vector, a
+// cluster of more than kInvitMaxCluster eigenvalues (a spectrum dominated by one huge
+// eigenvalue), or a QL chain that did not converge is recomputed by the warp QL instead.
+// Per-lane scratch (1/u and the vector) is interleaved [i * 32 + lane]: lane-parallel
+// recurrences read consecutive words.  Z goes to the caller's X buffer, column k = vector k.
+constexpr int kInvitMaxN = 63;
+constexpr double kInvitOrtol = 3e-4;
+constexpr int kInvitMaxCluster = 8;
+constexpr double kInvitTol = 256.0 * 1.1102230246251565e-16;
+
+struct InvitSmem {
+    size_t scr, dd, ee, lam, cls, flag, per_warp;
+    __host__ __device__ explicit InvitSmem(int n) {
+        size_t o = 0;
+        const size_t lanes = 2 * 32 * static_cast<size_t>(n), tile = static_cast<size_t>(n) * tile_ld(n);
+        scr = o;  o += 8 * (lanes > tile ? lanes : tile);     // also the fallback QL's Z tile
+        dd = o;   o += 8 * static_cast<size_t>(n);
+        ee = o;   o += 8 * static_cast<size_t>(n);
+        lam = o;  o += 8 * static_cast<size_t>(n);
+        cls = o;  o += align_up(4 * static_cast<size_t>(n), 16);
+        flag = o; o += 16;
+        per_warp = o;
+    }
+};
+
+__device__ __forceinline__ double invit_start(int j, int i) {
+    unsigned h = static_cast<unsigned>(i + 1) * 0x9E3779B1u ^ static_cast<unsigned>(j + 1) * 0x85EBCA77u;
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    return static_cast<double>(h & 0xFFFFFu) * (2.0 / 1048575.0) - 1.0;
+}
+
+// Eigenvector j into Zg column j; orthogonalised against columns lo .. j-1 when lo < j.
+// Returns false if the vector fails the residual test or is not finite.
+__device__ bool invit_vector(int n, int j, int lo, const double* dd, const double* ee, const double* lam,
+                             double tnorm, double* invu, double* z, double* Zg) {
+    const int lane = threadIdx.x & 31;
+    const double lj = lam[j];
+    const double tiny = 1.1102230246251565e-16 * tnorm;
+#define IU(i) invu[(i) * 32 + lane]
+#define ZV(i) z[(i) * 32 + lane]
+    double u = dd[0] - lj;
+    if (fabs(u) < tiny) u = copysign(tiny, u);
+    double iu = 1.0 / u;
+    IU(0) = iu;
+    for (int i = 1; i < n; ++i) {
+        const double ei = ee[i - 1];
+        u = (dd[i] - lj) - ei * ei * iu;
+        if (fabs(u) < tiny) u = copysign(tiny, u);
+        iu = 1.0 / u;
+        IU(i) = iu;
+    }
+    for (int i = 0; i < n; ++i) ZV(i) = invit_start(j, i);
+    const int iters = lo < j ? 3 : 2;
+    bool ok = true;
+    for (int it = 0; it < iters; ++it) {
+        double y = ZV(0);
+        for (int i = 1; i < n; ++i) {                  // L y = x  (L(i, i-1) = e_{i-1} / u_{i-1})
+            y = ZV(i) - ee[i - 1] * IU(i - 1) * y;
+            ZV(i) = y;
+        }
+        double zn = y * IU(n - 1);                     // U z = y  (U(i, i+1) = e_i)
+        ZV(n - 1) = zn;
+        for (int i = n - 2; i >= 0; --i) {
+            zn = (ZV(i) - ee[i] * zn) * IU(i);
+            ZV(i) = zn;
+        }
+        for (int p = lo; p < j; ++p) {                 // modified Gram-Schmidt in the cluster
+            const double* zp = Zg + static_cast<size_t>(p) * n;
+            double c = 0.0;
+            for (int i = 0; i < n; ++i) c = fma(zp[i], ZV(i), c);
+            for (int i = 0; i < n; ++i) ZV(i) = fma(-c, zp[i], ZV(i));
+        }
+        double s2 = 0.0;
+        for (int i = 0; i < n; ++i) s2 = fma(ZV(i), ZV(i), s2);
+        if (!(s2 > 0.0) || !isfinite(s2)) { ok = false; break; }
+        const double inv = 1.0 / sqrt(s2);
+        for (int i = 0; i < n; ++i) ZV(i) *= inv;
+    }
+    if (ok) {
+        double r2 = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double v = (dd[i] - lj) * ZV(i);
+            if (i > 0) v = fma(ee[i - 1], ZV(i - 1), v);
+            if (i + 1 < n) v = fma(ee[i], ZV(i + 1), v);
+            r2 = fma(v, v, r2);
+        }
+        ok = sqrt(r2) <= kInvitTol * tnorm;
+    }
+    double* zc = Zg + static_cast<size_t>(j) * n;
+    for (int i = 0; i < n; ++i) zc[i] = ZV(i);
+#undef IU
+#undef ZV
+    return ok;
+}
+
+__global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspace ws, double* __restrict__ W,
+                                                      double2* __restrict__ X, int* __restrict__ info) {
+    const int b = blockIdx.x, lane = threadIdx.x & 31;
+    if (b >= batch) return;
+    const int inf = info[b];
+    if (inf > n || inf < 0) return;                   // an earlier stage failed: W and X are NaN
+    extern __shared__ __align__(16) unsigned char smem[];
+    const InvitSmem lay(n);
+    double* scr = reinterpret_cast<double*>(smem + lay.scr);
+    double* dd = reinterpret_cast<double*>(smem + lay.dd);
+    double* ee = reinterpret_cast<double*>(smem + lay.ee);
+    double* lam = reinterpret_cast<double*>(smem + lay.lam);
+    int* cls = reinterpret_cast<int*>(smem + lay.cls);
+    int* sflag = reinterpret_cast<int*>(smem + lay.flag);
+    double* Wb = W + static_cast<size_t>(n) * b;
+    double* Zg = reinterpret_cast<double*>(X + static_cast<size_t>(n) * n * b);
+    double rs = 0.0;
+    for (int i = lane; i < n; i += 32) {
+        dd[i] = ws.d[static_cast<size_t>(n) * b + i];
+        ee[i] = ws.e[static_cast<size_t>(n) * b + i];
+        lam[i] = Wb[i];
+    }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {
+        double v = fabs(dd[i]);
+        if (i > 0) v += fabs(ee[i - 1]);
+        if (i + 1 < n) v += fabs(ee[i]);
+        rs = fmax(rs, v);
+    }
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) rs = fmax(rs, shfl_xor(rs, m));
+    const double tnorm = rs > 0.0 && isfinite(rs) ? rs : 1.0;
+    if (lane == 0) {                                  // clusters: cls[j] = index of the first member
+        int start = 0, biggest = 1;
+        for (int j = 0; j < n; ++j) {
+            if (j > 0 && !(lam[j] - lam[j - 1] <= kInvitOrtol * tnorm)) start = j;
+            cls[j] = start;
+            biggest = max(biggest, j - start + 1);
+        }
+        *sflag = biggest;
+    }
+    __syncwarp();
+    bool fallback = inf != 0 || *sflag > kInvitMaxCluster;
+    if (!fallback) {
+        bool ok = true;
+        for (int j = lane; j < n; j += 32)
+            if (cls[j] == j) ok &= invit_vector(n, j, j, dd, ee, lam, tnorm, scr, scr + 32 * n, Zg);
+        __syncwarp();                                 // every cluster's first vector is in Zg
+        for (int s0 = lane; s0 < n; s0 += 32)
+            if (cls[s0] == s0)
+                for (int j = s0 + 1; j < n && cls[j] == s0; ++j)
+                    ok &= invit_vector(n, j, s0, dd, ee, lam, tnorm, scr, scr + 32 * n, Zg);
+        fallback = !__all_sync(0xffffffffu, ok);
+    }
+    if (fallback) {                                   // the warp QL, Z tile over the lane scratch
+        const int ldz = tile_ld(n);
+        __syncwarp();
+        for (int r = lane; r < n; r += 32)
+            for (int c = 0; c < n; ++c) scr[r * ldz + c] = (r == c) ? 1.0 : 0.0;
+        for (int i = lane; i < n; i += 32) {
+            dd[i] = ws.d[static_cast<size_t>(n) * b + i];
+            ee[i] = ws.e[static_cast<size_t>(n) * b + i];
+        }
+        __syncwarp();
+        const int unconv = tridiag_ql<double>(n, dd, ee, scr, ldz);
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) Wb[i] = dd[i];
+        for (int r = lane; r < n; r += 32)
+            for (int k = 0; k < n; ++k) Zg[r + static_cast<size_t>(k) * n] = scr[r * ldz + k];
+        if (lane == 0) info[b] = unconv;
+    }
+}
+
 // ----------------------------------------------------------------------------- k_back
 // One CTA per pair: X = L^{-H} Q Z.  Column j of Z is held in registers by a group
 // of G lanes (lane g owns rows g + G r), read straight from the X buffer; only the
@@ -1059,6 +1261,15 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
     if (batch <= 0) return cudaSuccess;
     if (!W || !X || !info || !ws.d || !ws.e || !ws.log || !ws.perm || !ws.flag) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) return launch_ql_rows(n, batch, ws, W, X, info, single, chain_threads, stream);
+    if (!single && n <= kInvitMaxN) {                               // eigenvalues by QL, vectors by inverse iteration
+        const size_t vs = ql_chain_smem_bytes(n, chain_threads, false);
+        if (vs > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+        static std::once_flag fv;
+        set_max_smem_once(k_ql_values, fv);
+        k_ql_values<<<(batch + chain_threads - 1) / chain_threads, chain_threads, vs, stream>>>(n, batch, ws, W, info);
+        k_tridiag_invit<<<batch, 32, InvitSmem(n).per_warp, stream>>>(n, batch, ws, W, X, info);
+        return cudaGetLastError();
+    }
     const size_t cs = ql_chain_smem_bytes(n, chain_threads, single);
     const size_t as = ql_apply_smem_bytes(n, apply_warps, single);
     if (cs > static_cast<size_t>(max_smem_optin()) || as > static_cast<size_t>(max_smem_optin()))

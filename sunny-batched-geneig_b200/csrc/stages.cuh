@@ -433,7 +433,8 @@ __device__ double oa_refine_step(int n, const double* dT, const double* eT, cons
 // receives the pre-sort column index of eigenvalue k.
 // Returns the number of unconverged off-diagonals, or -1 if the log capacity
 // (cap entries) would be exceeded (the caller then falls back to tridiag_ql).
-template <typename R>
+// LOG = false: eigenvalues only (no log, no permutation; log, cap and perm are ignored).
+template <typename R, bool LOG = true>
 __device__ int ql_chain(int n, R* d, R* e, int stride, cplx<R>* log, int cap, int* perm, double* W) {
     using C = cplx<R>;
     const R eps = sizeof(R) == 8 ? R(1.1102230246251565e-16) : R(5.9604645e-08);
@@ -462,8 +463,11 @@ __device__ int ql_chain(int n, R* d, R* e, int stride, cplx<R>* log, int cap, in
             if (m == l) break;
             if (iter == maxit) { ++unconverged; break; }
             ++iter;
-            if (pos + (m - l) + 2 > cap) return -1;
-            const int hdr = pos++;
+            int hdr = 0;
+            if constexpr (LOG) {
+                if (pos + (m - l) + 2 > cap) return -1;
+                hdr = pos++;
+            }
             const R el = E(l), dl = D(l);
             R g = (D(l + 1) - dl) / (R(2) * el);
             R r = sqrt(fma(g, g, R(1)));
@@ -488,24 +492,24 @@ __device__ int ql_chain(int n, R* d, R* e, int stride, cplx<R>* log, int cap, in
                 p = s * r;
                 D(i + 1) = g + p;
                 g = fma(c, r, -b);
-                log[pos++] = mk<R>(c, s);
+                if constexpr (LOG) log[pos++] = mk<R>(c, s);
                 ei = ei_next; di = di_next;
             }
-            log[hdr] = mk<R>(R(m - 1), R(early ? (m - 1 - i) : (m - l)));
+            if constexpr (LOG) log[hdr] = mk<R>(R(m - 1), R(early ? (m - 1 - i) : (m - l)));
             if (early) continue;
             D(l) -= p; E(l) = g; E(m) = R(0);
         }
     }
-    log[pos] = mk<R>(R(-1), R(0));
+    if constexpr (LOG) log[pos] = mk<R>(R(-1), R(0));
     // selection sort with the permutation recorded
-    for (int k = 0; k < n; ++k) perm[k] = k;
+    if constexpr (LOG) for (int k = 0; k < n; ++k) perm[k] = k;
     for (int k = 0; k + 1 < n; ++k) {
         int j = k;
         R pmin = D(k);
         for (int t = k + 1; t < n; ++t) if (D(t) < pmin) { j = t; pmin = D(t); }
         if (j != k) {
             D(j) = D(k); D(k) = pmin;
-            const int tp = perm[k]; perm[k] = perm[j]; perm[j] = tp;
+            if constexpr (LOG) { const int tp = perm[k]; perm[k] = perm[j]; perm[j] = tp; }
         }
     }
     for (int k = 0; k < n; ++k) W[k] = static_cast<double>(D(k) * anorm);
