@@ -850,23 +850,26 @@ __global__ void k_ql_values(int n, int batch, Workspace ws, double* __restrict__
 // vector must pass ||T z - lambda z|| <= kInvitTol ||T||; a pair with a failed vector, a
 // cluster of more than kInvitMaxCluster eigenvalues (a spectrum dominated by one huge
 // eigenvalue), or a QL chain that did not converge is recomputed by the warp QL instead.
-// Per-lane scratch (1/u and the vector) is interleaved [i * 32 + lane]: lane-parallel
-// recurrences read consecutive words.  Z goes to the caller's X buffer, column k = vector k.
+// Per-lane scratch (1/u and the vector) is interleaved [i * 33 + lane]: lane-parallel
+// recurrences read consecutive words, and the warp's column-by-column copy to the caller's X
+// buffer (Z, column k = vector k) reads it across lanes without bank conflicts.
 constexpr int kInvitMaxN = 63;
 constexpr double kInvitOrtol = 3e-4;
 constexpr int kInvitMaxCluster = 8;
 constexpr double kInvitTol = 256.0 * 1.1102230246251565e-16;
+constexpr int kInvitLd = 33;            // lane scratch [i * 33 + lane]: rows also read across lanes
 
 struct InvitSmem {
-    size_t scr, dd, ee, lam, cls, flag, per_warp;
+    size_t scr, dd, ee, lam, cls, mem, flag, per_warp;
     __host__ __device__ explicit InvitSmem(int n) {
         size_t o = 0;
-        const size_t lanes = 2 * 32 * static_cast<size_t>(n), tile = static_cast<size_t>(n) * tile_ld(n);
+        const size_t lanes = 2 * kInvitLd * static_cast<size_t>(n), tile = static_cast<size_t>(n) * tile_ld(n);
         scr = o;  o += 8 * (lanes > tile ? lanes : tile);     // also the fallback QL's Z tile
         dd = o;   o += 8 * static_cast<size_t>(n);
         ee = o;   o += 8 * static_cast<size_t>(n);
         lam = o;  o += 8 * static_cast<size_t>(n);
         cls = o;  o += align_up(4 * static_cast<size_t>(n), 16);
+        mem = o;  o += 4 * 32;
         flag = o; o += 16;
         per_warp = o;
     }
@@ -880,69 +883,65 @@ __device__ __forceinline__ double invit_start(int j, int i) {
     return static_cast<double>(h & 0xFFFFFu) * (2.0 / 1048575.0) - 1.0;
 }
 
-// Eigenvector j into Zg column j; orthogonalised against columns lo .. j-1 when lo < j.
-// Returns false if the vector fails the residual test or is not finite.
-__device__ bool invit_vector(int n, int j, int lo, const double* dd, const double* ee, const double* lam,
-                             double tnorm, double* invu, double* z, double* Zg) {
+// Per-lane pieces of inverse iteration on T - lam I; invu and z are the lane's columns of the
+// interleaved scratch ([i * kInvitLd + lane]).
+#define SBG_IU(i) invu[(i) * kInvitLd + lane]
+#define SBG_ZV(i) z[(i) * kInvitLd + lane]
+// T - lam I = L U without pivoting (pivots below `tiny` raised to it): keeps 1/u_i.
+__device__ __forceinline__ void invit_factor(int n, double lam, const double* dd, const double* ee, double tiny,
+                                             double* invu) {
     const int lane = threadIdx.x & 31;
-    const double lj = lam[j];
-    const double tiny = 1.1102230246251565e-16 * tnorm;
-#define IU(i) invu[(i) * 32 + lane]
-#define ZV(i) z[(i) * 32 + lane]
-    double u = dd[0] - lj;
+    double u = dd[0] - lam;
     if (fabs(u) < tiny) u = copysign(tiny, u);
     double iu = 1.0 / u;
-    IU(0) = iu;
+    SBG_IU(0) = iu;
     for (int i = 1; i < n; ++i) {
         const double ei = ee[i - 1];
-        u = (dd[i] - lj) - ei * ei * iu;
+        u = (dd[i] - lam) - ei * ei * iu;
         if (fabs(u) < tiny) u = copysign(tiny, u);
         iu = 1.0 / u;
-        IU(i) = iu;
+        SBG_IU(i) = iu;
     }
-    for (int i = 0; i < n; ++i) ZV(i) = invit_start(j, i);
-    const int iters = lo < j ? 3 : 2;
-    bool ok = true;
-    for (int it = 0; it < iters; ++it) {
-        double y = ZV(0);
-        for (int i = 1; i < n; ++i) {                  // L y = x  (L(i, i-1) = e_{i-1} / u_{i-1})
-            y = ZV(i) - ee[i - 1] * IU(i - 1) * y;
-            ZV(i) = y;
-        }
-        double zn = y * IU(n - 1);                     // U z = y  (U(i, i+1) = e_i)
-        ZV(n - 1) = zn;
-        for (int i = n - 2; i >= 0; --i) {
-            zn = (ZV(i) - ee[i] * zn) * IU(i);
-            ZV(i) = zn;
-        }
-        for (int p = lo; p < j; ++p) {                 // modified Gram-Schmidt in the cluster
-            const double* zp = Zg + static_cast<size_t>(p) * n;
-            double c = 0.0;
-            for (int i = 0; i < n; ++i) c = fma(zp[i], ZV(i), c);
-            for (int i = 0; i < n; ++i) ZV(i) = fma(-c, zp[i], ZV(i));
-        }
-        double s2 = 0.0;
-        for (int i = 0; i < n; ++i) s2 = fma(ZV(i), ZV(i), s2);
-        if (!(s2 > 0.0) || !isfinite(s2)) { ok = false; break; }
-        const double inv = 1.0 / sqrt(s2);
-        for (int i = 0; i < n; ++i) ZV(i) *= inv;
-    }
-    if (ok) {
-        double r2 = 0.0;
-        for (int i = 0; i < n; ++i) {
-            double v = (dd[i] - lj) * ZV(i);
-            if (i > 0) v = fma(ee[i - 1], ZV(i - 1), v);
-            if (i + 1 < n) v = fma(ee[i], ZV(i + 1), v);
-            r2 = fma(v, v, r2);
-        }
-        ok = sqrt(r2) <= kInvitTol * tnorm;
-    }
-    double* zc = Zg + static_cast<size_t>(j) * n;
-    for (int i = 0; i < n; ++i) zc[i] = ZV(i);
-#undef IU
-#undef ZV
-    return ok;
 }
+// z <- (T - lam I)^{-1} z with the factors above.
+__device__ __forceinline__ void invit_solve(int n, const double* ee, const double* invu, double* z) {
+    const int lane = threadIdx.x & 31;
+    double y = SBG_ZV(0);
+    for (int i = 1; i < n; ++i) {                      // L y = x  (L(i, i-1) = e_{i-1} / u_{i-1})
+        y = SBG_ZV(i) - ee[i - 1] * SBG_IU(i - 1) * y;
+        SBG_ZV(i) = y;
+    }
+    double zn = y * SBG_IU(n - 1);                     // U z = y  (U(i, i+1) = e_i)
+    SBG_ZV(n - 1) = zn;
+    for (int i = n - 2; i >= 0; --i) {
+        zn = (SBG_ZV(i) - ee[i] * zn) * SBG_IU(i);
+        SBG_ZV(i) = zn;
+    }
+}
+__device__ __forceinline__ bool invit_normalise(int n, double* z) {
+    const int lane = threadIdx.x & 31;
+    double s2 = 0.0;
+    for (int i = 0; i < n; ++i) s2 = fma(SBG_ZV(i), SBG_ZV(i), s2);
+    if (!(s2 > 0.0) || !isfinite(s2)) return false;
+    const double inv = 1.0 / sqrt(s2);
+    for (int i = 0; i < n; ++i) SBG_ZV(i) *= inv;
+    return true;
+}
+// ||T z - lam z|| <= kInvitTol ||T|| for the lane's (unit) vector.
+__device__ __forceinline__ bool invit_residual_ok(int n, double lam, const double* dd, const double* ee,
+                                                  const double* z, double tnorm) {
+    const int lane = threadIdx.x & 31;
+    double r2 = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double v = (dd[i] - lam) * SBG_ZV(i);
+        if (i > 0) v = fma(ee[i - 1], SBG_ZV(i - 1), v);
+        if (i + 1 < n) v = fma(ee[i], SBG_ZV(i + 1), v);
+        r2 = fma(v, v, r2);
+    }
+    return sqrt(r2) <= kInvitTol * tnorm;
+}
+#undef SBG_IU
+#undef SBG_ZV
 
 __global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspace ws, double* __restrict__ W,
                                                       double2* __restrict__ X, int* __restrict__ info) {
@@ -957,6 +956,7 @@ __global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspac
     double* ee = reinterpret_cast<double*>(smem + lay.ee);
     double* lam = reinterpret_cast<double*>(smem + lay.lam);
     int* cls = reinterpret_cast<int*>(smem + lay.cls);
+    int* members = reinterpret_cast<int*>(smem + lay.mem);
     int* sflag = reinterpret_cast<int*>(smem + lay.flag);
     double* Wb = W + static_cast<size_t>(n) * b;
     double* Zg = reinterpret_cast<double*>(X + static_cast<size_t>(n) * n * b);
@@ -976,26 +976,91 @@ __global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspac
 #pragma unroll
     for (int m = 16; m >= 1; m >>= 1) rs = fmax(rs, shfl_xor(rs, m));
     const double tnorm = rs > 0.0 && isfinite(rs) ? rs : 1.0;
+    const double tiny = 1.1102230246251565e-16 * tnorm;
     if (lane == 0) {                                  // clusters: cls[j] = index of the first member
-        int start = 0, biggest = 1;
+        int start = 0, biggest = 1, cnt = 0;
         for (int j = 0; j < n; ++j) {
             if (j > 0 && !(lam[j] - lam[j - 1] <= kInvitOrtol * tnorm)) start = j;
             cls[j] = start;
             biggest = max(biggest, j - start + 1);
+            if (start != j) { if (cnt < 32) members[cnt] = j; ++cnt; }
         }
-        *sflag = biggest;
+        sflag[0] = biggest;
+        sflag[1] = cnt;
     }
     __syncwarp();
-    bool fallback = inf != 0 || *sflag > kInvitMaxCluster;
+    const int cnt = sflag[1];
+    bool fallback = inf != 0 || sflag[0] > kInvitMaxCluster || cnt > 32;
     if (!fallback) {
         bool ok = true;
-        for (int j = lane; j < n; j += 32)
-            if (cls[j] == j) ok &= invit_vector(n, j, j, dd, ee, lam, tnorm, scr, scr + 32 * n, Zg);
-        __syncwarp();                                 // every cluster's first vector is in Zg
-        for (int s0 = lane; s0 < n; s0 += 32)
-            if (cls[s0] == s0)
-                for (int j = s0 + 1; j < n && cls[j] == s0; ++j)
-                    ok &= invit_vector(n, j, s0, dd, ee, lam, tnorm, scr, scr + 32 * n, Zg);
+        double* invu = scr;
+        double* zs = scr + kInvitLd * n;
+        // (1) each cluster's first vector and every singleton: factor, two solves from a fixed
+        // pseudo-random start, residual test; 32 at a time, then copied out column by column
+        for (int base = 0; base < n; base += 32) {
+            const int j = base + lane;
+            if (j < n && cls[j] == j) {
+                invit_factor(n, lam[j], dd, ee, tiny, invu);
+                for (int i = 0; i < n; ++i) zs[i * kInvitLd + lane] = invit_start(j, i);
+                invit_solve(n, ee, invu, zs);
+                ok &= invit_normalise(n, zs);
+                invit_solve(n, ee, invu, zs);
+                ok &= invit_normalise(n, zs);
+                ok &= invit_residual_ok(n, lam[j], dd, ee, zs, tnorm);
+            }
+            __syncwarp();
+            const int top = min(32, n - base);
+            for (int L = 0; L < top; ++L) {
+                const int jj = base + L;
+                if (cls[jj] != jj) continue;          // uniform
+                double* zc = Zg + static_cast<size_t>(jj) * n;
+                for (int i = lane; i < n; i += 32) zc[i] = zs[i * kInvitLd + L];
+            }
+            __syncwarp();
+        }
+        ok = __all_sync(0xffffffffu, ok);              // from here on `ok` is the same on every lane
+        // (2) the other cluster members, one lane each, all at once: three rounds of a solve
+        // (every lane its own member) and modified Gram-Schmidt in index order (the whole warp,
+        // lanes over rows) against the cluster's first vector and its earlier members
+        if (ok && cnt > 0) {
+            const int jm = lane < cnt ? members[lane] : -1;
+            if (jm >= 0) {
+                invit_factor(n, lam[jm], dd, ee, tiny, invu);
+                for (int i = 0; i < n; ++i) zs[i * kInvitLd + lane] = invit_start(jm, i);
+            }
+            for (int it = 0; it < 3 && ok; ++it) {
+                if (jm >= 0) invit_solve(n, ee, invu, zs);
+                __syncwarp();
+                for (int m = 0; m < cnt && ok; ++m) {
+                    const int j = members[m], s0 = cls[j];
+                    const double* q0 = Zg + static_cast<size_t>(s0) * n;
+                    double c = 0.0;
+                    for (int i = lane; i < n; i += 32) c = fma(q0[i], zs[i * kInvitLd + m], c);
+                    c = warp_sum(c);
+                    for (int i = lane; i < n; i += 32) zs[i * kInvitLd + m] = fma(-c, q0[i], zs[i * kInvitLd + m]);
+                    for (int m2 = 0; m2 < m; ++m2) {
+                        if (cls[members[m2]] != s0) continue;     // uniform
+                        double c2 = 0.0;
+                        for (int i = lane; i < n; i += 32) c2 = fma(zs[i * kInvitLd + m2], zs[i * kInvitLd + m], c2);
+                        c2 = warp_sum(c2);
+                        for (int i = lane; i < n; i += 32)
+                            zs[i * kInvitLd + m] = fma(-c2, zs[i * kInvitLd + m2], zs[i * kInvitLd + m]);
+                    }
+                    double s2 = 0.0;
+                    for (int i = lane; i < n; i += 32) s2 = fma(zs[i * kInvitLd + m], zs[i * kInvitLd + m], s2);
+                    s2 = warp_sum(s2);
+                    if (!(s2 > 0.0) || !isfinite(s2)) { ok = false; break; }     // uniform
+                    const double inv = 1.0 / sqrt(s2);
+                    for (int i = lane; i < n; i += 32) zs[i * kInvitLd + m] *= inv;
+                }
+                __syncwarp();
+            }
+            if (jm >= 0 && ok) ok &= invit_residual_ok(n, lam[jm], dd, ee, zs, tnorm);
+            for (int m = 0; m < cnt; ++m) {
+                double* zc = Zg + static_cast<size_t>(members[m]) * n;
+                for (int i = lane; i < n; i += 32) zc[i] = zs[i * kInvitLd + m];
+            }
+        }
         fallback = !__all_sync(0xffffffffu, ok);
     }
     if (fallback) {                                   // the warp QL, Z tile over the lane scratch
