@@ -887,34 +887,44 @@ __device__ __forceinline__ double invit_start(int j, int i) {
 // interleaved scratch ([i * kInvitLd + lane]).
 #define SBG_IU(i) invu[(i) * kInvitLd + lane]
 #define SBG_ZV(i) z[(i) * kInvitLd + lane]
-// T - lam I = L U without pivoting (pivots below `tiny` raised to it): keeps 1/u_i.
-__device__ __forceinline__ void invit_factor(int n, double lam, const double* dd, const double* ee, double tiny,
-                                             double* invu) {
+// T - lam I = L U without pivoting (pivots below `tiny` raised to it): keeps 1/u_i.  Each step's
+// operands are loaded one step ahead, so the dependent chain is only the recurrence itself.
+__device__ __forceinline__ void invit_factor(int n, double lam, const double* __restrict__ dd,
+                                             const double* __restrict__ ee, double tiny, double* __restrict__ invu) {
     const int lane = threadIdx.x & 31;
     double u = dd[0] - lam;
     if (fabs(u) < tiny) u = copysign(tiny, u);
     double iu = 1.0 / u;
     SBG_IU(0) = iu;
+    double dn = n > 1 ? dd[1] - lam : 0.0, en = n > 1 ? ee[0] * ee[0] : 0.0;
     for (int i = 1; i < n; ++i) {
-        const double ei = ee[i - 1];
-        u = (dd[i] - lam) - ei * ei * iu;
+        const double di = dn, e2 = en;
+        if (i + 1 < n) { dn = dd[i + 1] - lam; en = ee[i] * ee[i]; }
+        u = fma(-e2, iu, di);
         if (fabs(u) < tiny) u = copysign(tiny, u);
         iu = 1.0 / u;
         SBG_IU(i) = iu;
     }
 }
-// z <- (T - lam I)^{-1} z with the factors above.
-__device__ __forceinline__ void invit_solve(int n, const double* ee, const double* invu, double* z) {
+// z <- (T - lam I)^{-1} z with the factors above (operands loaded one step ahead).
+__device__ __forceinline__ void invit_solve(int n, const double* __restrict__ ee, const double* __restrict__ invu,
+                                            double* __restrict__ z) {
     const int lane = threadIdx.x & 31;
     double y = SBG_ZV(0);
+    double xn = n > 1 ? SBG_ZV(1) : 0.0, cn = n > 1 ? ee[0] * SBG_IU(0) : 0.0;
     for (int i = 1; i < n; ++i) {                      // L y = x  (L(i, i-1) = e_{i-1} / u_{i-1})
-        y = SBG_ZV(i) - ee[i - 1] * SBG_IU(i - 1) * y;
+        const double x = xn, c = cn;
+        if (i + 1 < n) { xn = SBG_ZV(i + 1); cn = ee[i] * SBG_IU(i); }
+        y = fma(-c, y, x);
         SBG_ZV(i) = y;
     }
     double zn = y * SBG_IU(n - 1);                     // U z = y  (U(i, i+1) = e_i)
     SBG_ZV(n - 1) = zn;
+    double yp = n > 1 ? SBG_ZV(n - 2) : 0.0, ep = n > 1 ? ee[n - 2] : 0.0, ip = n > 1 ? SBG_IU(n - 2) : 0.0;
     for (int i = n - 2; i >= 0; --i) {
-        zn = (SBG_ZV(i) - ee[i] * zn) * SBG_IU(i);
+        const double yi = yp, ei = ep, ii = ip;
+        if (i > 0) { yp = SBG_ZV(i - 1); ep = ee[i - 1]; ip = SBG_IU(i - 1); }
+        zn = fma(-ei, zn, yi) * ii;
         SBG_ZV(i) = zn;
     }
 }
