@@ -906,49 +906,52 @@ __device__ __forceinline__ void invit_factor(int n, double lam, const double* __
         SBG_IU(i) = iu;
     }
 }
-// z <- (T - lam I)^{-1} z with the factors above (operands loaded one step ahead).
-__device__ __forceinline__ void invit_solve(int n, const double* __restrict__ ee, const double* __restrict__ invu,
-                                            double* __restrict__ z) {
+// z <- (T - lam I)^{-1} x with the factors above, x = sc z, or (GEN) the start vector of eigenvalue
+// j; returns ||z||^2 (summed in the backward pass).  Operands are loaded one step ahead.
+template <bool GEN>
+__device__ __forceinline__ double invit_solve(int n, const double* __restrict__ ee, const double* __restrict__ invu,
+                                              double* __restrict__ z, double sc, int j) {
     const int lane = threadIdx.x & 31;
-    double y = SBG_ZV(0);
-    double xn = n > 1 ? SBG_ZV(1) : 0.0, cn = n > 1 ? ee[0] * SBG_IU(0) : 0.0;
+    auto xin = [&](int i) { if constexpr (GEN) return invit_start(j, i); else return sc * SBG_ZV(i); };
+    double y = xin(0);
+    SBG_ZV(0) = y;
+    double xn = n > 1 ? xin(1) : 0.0, cn = n > 1 ? ee[0] * SBG_IU(0) : 0.0;
     for (int i = 1; i < n; ++i) {                      // L y = x  (L(i, i-1) = e_{i-1} / u_{i-1})
         const double x = xn, c = cn;
-        if (i + 1 < n) { xn = SBG_ZV(i + 1); cn = ee[i] * SBG_IU(i); }
+        if (i + 1 < n) { xn = xin(i + 1); cn = ee[i] * SBG_IU(i); }
         y = fma(-c, y, x);
         SBG_ZV(i) = y;
     }
     double zn = y * SBG_IU(n - 1);                     // U z = y  (U(i, i+1) = e_i)
     SBG_ZV(n - 1) = zn;
+    double s2 = zn * zn;
     double yp = n > 1 ? SBG_ZV(n - 2) : 0.0, ep = n > 1 ? ee[n - 2] : 0.0, ip = n > 1 ? SBG_IU(n - 2) : 0.0;
     for (int i = n - 2; i >= 0; --i) {
         const double yi = yp, ei = ep, ii = ip;
         if (i > 0) { yp = SBG_ZV(i - 1); ep = ee[i - 1]; ip = SBG_IU(i - 1); }
         zn = fma(-ei, zn, yi) * ii;
         SBG_ZV(i) = zn;
+        s2 = fma(zn, zn, s2);
     }
+    return s2;
 }
-__device__ __forceinline__ bool invit_normalise(int n, double* z) {
+// z <- sc z in place; returns ||T z - lam z||^2 of the scaled vector (one pass).
+__device__ __forceinline__ double invit_scale_residual(int n, double lam, const double* __restrict__ dd,
+                                                       const double* __restrict__ ee, double* __restrict__ z,
+                                                       double sc) {
     const int lane = threadIdx.x & 31;
-    double s2 = 0.0;
-    for (int i = 0; i < n; ++i) s2 = fma(SBG_ZV(i), SBG_ZV(i), s2);
-    if (!(s2 > 0.0) || !isfinite(s2)) return false;
-    const double inv = 1.0 / sqrt(s2);
-    for (int i = 0; i < n; ++i) SBG_ZV(i) *= inv;
-    return true;
-}
-// ||T z - lam z|| <= kInvitTol ||T|| for the lane's (unit) vector.
-__device__ __forceinline__ bool invit_residual_ok(int n, double lam, const double* dd, const double* ee,
-                                                  const double* z, double tnorm) {
-    const int lane = threadIdx.x & 31;
-    double r2 = 0.0;
+    double zp = 0.0, zc = SBG_ZV(0), r2 = 0.0;
     for (int i = 0; i < n; ++i) {
-        double v = (dd[i] - lam) * SBG_ZV(i);
-        if (i > 0) v = fma(ee[i - 1], SBG_ZV(i - 1), v);
-        if (i + 1 < n) v = fma(ee[i], SBG_ZV(i + 1), v);
+        const double zx = i + 1 < n ? SBG_ZV(i + 1) : 0.0;
+        double v = (dd[i] - lam) * zc;
+        if (i > 0) v = fma(ee[i - 1], zp, v);
+        if (i + 1 < n) v = fma(ee[i], zx, v);
         r2 = fma(v, v, r2);
+        SBG_ZV(i) = zc * sc;
+        zp = zc;
+        zc = zx;
     }
-    return sqrt(r2) <= kInvitTol * tnorm;
+    return r2 * sc * sc;
 }
 #undef SBG_IU
 #undef SBG_ZV
@@ -1011,12 +1014,12 @@ __global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspac
             const int j = base + lane;
             if (j < n && cls[j] == j) {
                 invit_factor(n, lam[j], dd, ee, tiny, invu);
-                for (int i = 0; i < n; ++i) zs[i * kInvitLd + lane] = invit_start(j, i);
-                invit_solve(n, ee, invu, zs);
-                ok &= invit_normalise(n, zs);
-                invit_solve(n, ee, invu, zs);
-                ok &= invit_normalise(n, zs);
-                ok &= invit_residual_ok(n, lam[j], dd, ee, zs, tnorm);
+                double s2 = invit_solve<true>(n, ee, invu, zs, 1.0, j);
+                const bool f1 = s2 > 0.0 && isfinite(s2);
+                s2 = invit_solve<false>(n, ee, invu, zs, f1 ? 1.0 / sqrt(s2) : 1.0, j);
+                const bool f2 = s2 > 0.0 && isfinite(s2);
+                const double r2 = invit_scale_residual(n, lam[j], dd, ee, zs, f2 ? 1.0 / sqrt(s2) : 1.0);
+                ok &= f1 && f2 && sqrt(r2) <= kInvitTol * tnorm;
             }
             __syncwarp();
             const int top = min(32, n - base);
@@ -1036,10 +1039,12 @@ __global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspac
             const int jm = lane < cnt ? members[lane] : -1;
             if (jm >= 0) {
                 invit_factor(n, lam[jm], dd, ee, tiny, invu);
-                for (int i = 0; i < n; ++i) zs[i * kInvitLd + lane] = invit_start(jm, i);
             }
-            for (int it = 0; it < 3 && ok; ++it) {
-                if (jm >= 0) invit_solve(n, ee, invu, zs);
+            for (int it = 0; it < 3 && ok; ++it) {        // each round's input is unit (Gram-Schmidt below)
+                if (jm >= 0) {
+                    if (it == 0) invit_solve<true>(n, ee, invu, zs, 1.0, jm);
+                    else invit_solve<false>(n, ee, invu, zs, 1.0, jm);
+                }
                 __syncwarp();
                 for (int m = 0; m < cnt && ok; ++m) {
                     const int j = members[m], s0 = cls[j];
@@ -1065,7 +1070,7 @@ __global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspac
                 }
                 __syncwarp();
             }
-            if (jm >= 0 && ok) ok &= invit_residual_ok(n, lam[jm], dd, ee, zs, tnorm);
+            if (jm >= 0 && ok) ok &= sqrt(invit_scale_residual(n, lam[jm], dd, ee, zs, 1.0)) <= kInvitTol * tnorm;
             for (int m = 0; m < cnt; ++m) {
                 double* zc = Zg + static_cast<size_t>(members[m]) * n;
                 for (int i = lane; i < n; i += 32) zc[i] = zs[i * kInvitLd + m];
