@@ -57,7 +57,7 @@ STAGE_BYTES = {"reduce": 32 * N * N, "tridiag": 0, "eig": 16 * N, "back": 16 * N
 # DRAM bytes (read + write) per pair of each FP64 stage at n = 54, from one ncu capture of a
 # 16,384-pair solve (profiles/ncu_stage_kernels_qsweep_n54_16384pairs.md); DRAM traffic grows in
 # proportion to the pairs a launch processes, so traffic per launch = this x pairs per launch.
-TRAFFIC_PER_PAIR_N54 = {"reduce": 51.4e3 + 120.0e3, "tridiag": 52.2e3, "eig": 52.8e3 + 76.2e3, "back": 114.0e3}
+TRAFFIC_PER_PAIR_N54 = {"reduce": 51.4e3 + 120.0e3, "tridiag": 52.3e3, "eig": 0.9e3 + 21.4e3, "back": 114.4e3}
 
 # The other configurations (bench.py --workload NAME): fixed-n Bogoliubov / q-sweep batches and the
 # uneven-n batch through the queue.  Each prints one JSON line of the same shape as the headline.
