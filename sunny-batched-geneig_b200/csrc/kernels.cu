@@ -855,7 +855,6 @@ __global__ void k_ql_values(int n, int batch, Workspace ws, double* __restrict__
 // Per-lane scratch (1/u and the vector) is interleaved [i * 33 + lane]: lane-parallel
 // recurrences read consecutive words, and the warp's column-by-column copy to the caller's X
 // buffer (Z, column k = vector k) reads it across lanes without bank conflicts.
-constexpr int kInvitMaxN = 63;
 constexpr double kInvitOrtol = 3e-4;
 constexpr int kInvitMaxCluster = 8;
 constexpr double kInvitTol = 256.0 * 1.1102230246251565e-16;
@@ -1356,7 +1355,7 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
     if (batch <= 0) return cudaSuccess;
     if (!W || !X || !info || !ws.d || !ws.e || !ws.log || !ws.perm || !ws.flag) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) return launch_ql_rows(n, batch, ws, W, X, info, single, chain_threads, stream);
-    if (!single && n <= kInvitMaxN) {                               // eigenvalues by QL, vectors by inverse iteration
+    if (eig_by_inverse_iteration(n, single)) {                      // eigenvalues by QL, vectors by inverse iteration
         const size_t vs = ql_chain_smem_bytes(n, chain_threads, false);
         if (vs > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
         static std::once_flag fv;

@@ -98,6 +98,10 @@ cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, in
 // Kernels one full reduce launch (kReduceFull) issues for order n: the warp Cholesky and the
 // column hegst kernel for n <= 56, one kernel otherwise.
 inline int reduce_kernel_count(int n) { return n <= 56 ? 2 : 1; }
+// FP64 eigenvectors by inverse iteration for n <= kInvitMaxN (k_ql_values + k_tridiag_invit); the
+// rotation-log QL (k_ql_chain + k_ql_apply*) above it and for the mixed form.
+constexpr int kInvitMaxN = 63;
+inline bool eig_by_inverse_iteration(int n, bool single) { return !single && n <= kInvitMaxN; }
 
 size_t reduce_smem_bytes(int mode, int n);
 size_t ql_chain_smem_bytes(int n, int threads, bool single);

@@ -252,7 +252,11 @@ bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double&
     cudaMemcpy(bench.B.p, hB.data(), 16 * bench.nn * count, cudaMemcpyHostToDevice);
     const Schedule base = default_schedule(n, precision);
     const std::vector<int> thread_opts = req.force_threads ? std::vector<int>{req.force_threads} : std::vector<int>{128, 256};
-    const std::vector<int> warp_opts = req.force_ql_warps ? std::vector<int>{req.force_ql_warps} : std::vector<int>{1, 2, 4, 8};
+    // pairs per CTA of the rotation apply; the inverse-iteration path has no such parameter
+    const std::vector<int> warp_opts =
+        req.force_ql_warps ? std::vector<int>{req.force_ql_warps}
+        : eig_by_inverse_iteration(n, precision == SBG_PRECISION_MIXED) ? std::vector<int>{base.ql_warps}
+                                                                         : std::vector<int>{1, 2, 4, 8};
     Schedule win = base;
     double t_total = 0.0;
     // k_reduce
