@@ -109,7 +109,12 @@ def clusters(w, cluster_gap: float):
 
 
 def cluster_sin(B, Xg, Xr, Wr, n: int, cluster_gap: float = 1e-6) -> np.ndarray:
-    """Largest B-principal-angle sine between candidate and oracle cluster subspaces."""
+    """Largest B-principal-angle sine between candidate and oracle cluster subspaces.
+
+    Computed directly as the B-norm of the candidate basis' component outside the oracle's
+    subspace, E = G - R (R^H B G), sin = sqrt(lambda_max(E^H B E)) (both bases B-orthonormal).
+    The cosine route, sqrt(1 - sigma_min(R^H B G)^2), cannot resolve angles below
+    sqrt(2 eps) = 1.5e-8."""
     Bm = as_mats(B, n)
     G = as_mats(Xg, n)
     R = as_mats(Xr, n)
@@ -117,10 +122,11 @@ def cluster_sin(B, Xg, Xr, Wr, n: int, cluster_gap: float = 1e-6) -> np.ndarray:
     out = np.zeros(G.shape[0])
     for b in range(G.shape[0]):
         for lo, hi in clusters(Wr[b], cluster_gap):
-            M = R[b][:, lo:hi].conj().T @ Bm[b] @ G[b][:, lo:hi]
-            s = np.linalg.svd(M, compute_uv=False)
-            smin = min(1.0, float(s.min()))
-            out[b] = max(out[b], float(np.sqrt(max(0.0, 1.0 - smin * smin))))
+            Gc, Rc = G[b][:, lo:hi], R[b][:, lo:hi]
+            E = Gc - Rc @ (Rc.conj().T @ Bm[b] @ Gc)
+            S = E.conj().T @ Bm[b] @ E
+            lmax = float(np.linalg.eigvalsh(0.5 * (S + S.conj().T))[-1])
+            out[b] = max(out[b], float(np.sqrt(max(0.0, lmax))))
     return out
 
 
