@@ -47,14 +47,14 @@ struct SwTables {
     const int* mapQ = nullptr;
     const int* ptrQ = nullptr;
     const int* listQ = nullptr;
+    const int* entP = nullptr;          // list index k -> its entry r + N c (P, then Q)
+    const int* entQ = nullptr;
+    int nP = 0, nQ = 0;                 // entries with contributions
 };
 
-// Sum of the listed contributions t[k] (conjugated where flagged) to one entry.
-__device__ __forceinline__ double2 entry_sum(const int* map, const int* ptr, const int* list, int idx,
-                                             const double2* t, bool flagged) {
+// Sum of the contributions t[list[ptr[k] ..]] (conjugated where flagged) of list entry k.
+__device__ __forceinline__ double2 list_sum(const int* ptr, const int* list, int k, const double2* t, bool flagged) {
     double2 v = make_double2(0.0, 0.0);
-    const int k = map[idx];
-    if (k < 0) return v;
     for (int j = ptr[k]; j < ptr[k + 1]; ++j) {
         const int e = list[j];
         double2 c = t[flagged ? (e >> 1) : e];
@@ -65,9 +65,9 @@ __device__ __forceinline__ double2 entry_sum(const int* map, const int* ptr, con
     return v;
 }
 
-// One CTA per q: the bond phases into shared memory, then every entry of B(q) (and, when
-// A != nullptr, of the metric A) written column-major: each warp takes whole columns, its lanes
-// the rows, so the stores of a column are contiguous and no index is divided.
+// One CTA per q: the bond phases into shared memory; B(q) (and, when A != nullptr, the metric A)
+// zero-filled with plain coalesced stores, then only the entries with bond contributions and the
+// diagonal written (a third of B at n = 54): each a fixed-order sum, so B is bit-reproducible.
 __global__ void __launch_bounds__(kAssembleThreads) k_sw_assemble(SwTables T, const double* __restrict__ qv, int nq,
                                                                    double2* __restrict__ A, double2* __restrict__ B) {
     const int p = blockIdx.x;
@@ -84,28 +84,39 @@ __global__ void __launch_bounds__(kAssembleThreads) k_sw_assemble(SwTables T, co
         ta[k] = sbg::cmul(T.half_a[k], ph);
         tb[k] = sbg::cmul(T.half_b[k], ph);
     }
-    __syncthreads();
-    const int N = T.N, n = 2 * N;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double2* Bp = B + static_cast<size_t>(n) * n * p;
-    double2* Ap = A ? A + static_cast<size_t>(n) * n * p : nullptr;
-    for (int col = warp; col < n; col += kAssembleThreads / 32) {
-        const int bc = col >= N, c = col - bc * N;
-        for (int row = lane; row < n; row += 32) {
-            const int br = row >= N, r = row - br * N;
-            double2 v;
-            if (br == bc) {                               // P (top left) or conj(P) (bottom right)
-                v = entry_sum(T.mapP, T.ptrP, T.listP, r + N * c, ta, true);
-                if (r == c) v.x += T.onsite[r];
-                if (br) v.y = -v.y;
-                if (r == c) v.x += T.field;
-            } else {                                      // Q (top right) or conj(Q) (bottom left)
-                v = entry_sum(T.mapQ, T.ptrQ, T.listQ, r + N * c, tb, false);
-                if (br) v.y = -v.y;
-            }
-            Bp[static_cast<size_t>(col) * n + row] = v;
-            if (Ap) Ap[static_cast<size_t>(col) * n + row] = make_double2(row == col ? (row < N ? 1.0 : -1.0) : 0.0, 0.0);
+    const int N = T.N, n = 2 * N, nn = n * n;
+    double2* Bp = B + static_cast<size_t>(nn) * p;
+    double2* Ap = A ? A + static_cast<size_t>(nn) * p : nullptr;
+    const double2 zero = make_double2(0.0, 0.0);
+    for (int e = threadIdx.x; e < nn; e += kAssembleThreads) {
+        Bp[e] = zero;
+        if (Ap) Ap[e] = zero;
+    }
+    __syncthreads();                    // phases ready; zeros ordered before the values below
+    const size_t ldn = static_cast<size_t>(n);
+    for (int k = threadIdx.x; k < T.nP; k += kAssembleThreads) {      // P off the diagonal: P, conj(P) blocks
+        const int idx = T.entP[k], c = idx / N, r = idx - c * N;
+        if (r == c) continue;
+        const double2 v = list_sum(T.ptrP, T.listP, k, ta, true);
+        Bp[r + ldn * c] = v;
+        Bp[(N + r) + ldn * (N + c)] = make_double2(v.x, -v.y);
+    }
+    for (int r = threadIdx.x; r < N; r += kAssembleThreads) {         // the diagonal: bonds, on-site, field
+        const int k = T.mapP[r + N * r];
+        double2 v = k >= 0 ? list_sum(T.ptrP, T.listP, k, ta, true) : zero;
+        v.x += T.onsite[r];
+        Bp[r + ldn * r] = make_double2(v.x + T.field, v.y);
+        Bp[(N + r) + ldn * (N + r)] = make_double2(v.x + T.field, -v.y);
+        if (Ap) {
+            Ap[r + ldn * r] = make_double2(1.0, 0.0);
+            Ap[(N + r) + ldn * (N + r)] = make_double2(-1.0, 0.0);
         }
+    }
+    for (int k = threadIdx.x; k < T.nQ; k += kAssembleThreads) {      // Q and conj(Q) blocks
+        const int idx = T.entQ[k], c = idx / N, r = idx - c * N;
+        const double2 v = list_sum(T.ptrQ, T.listQ, k, tb, false);
+        Bp[r + ldn * (N + c)] = v;
+        Bp[(N + r) + ldn * c] = make_double2(v.x, -v.y);
     }
 }
 
@@ -319,11 +330,11 @@ namespace {
 
 // Entry (r, c) -> ordered contributions, for one N x N block.
 struct EntryLists {
-    std::vector<int> map, ptr, list;
+    std::vector<int> map, ptr, list, ent;
     explicit EntryLists(int N) : map(static_cast<size_t>(N) * N, -1), ptr(1, 0) {}
     std::vector<std::vector<int>> pending;
     void add(int idx, int v) {
-        if (map[idx] < 0) { map[idx] = static_cast<int>(pending.size()); pending.emplace_back(); }
+        if (map[idx] < 0) { map[idx] = static_cast<int>(pending.size()); pending.emplace_back(); ent.push_back(idx); }
         pending[map[idx]].push_back(v);
     }
     void finish() {
@@ -396,7 +407,8 @@ void create_spinwave(int N, int nb, const int* sites, const double* coef, const 
 
     // One allocation: doubles (a/2, b/2, d, onsite, r), then ints (maps, ptrs, lists).
     const size_t nd = half_a.size() + half_b.size() + 3 * static_cast<size_t>(nb) + onsite.size() + posv.size();
-    const size_t ni = P.map.size() + P.ptr.size() + P.list.size() + Q.map.size() + Q.ptr.size() + Q.list.size();
+    const size_t ni = P.map.size() + P.ptr.size() + P.list.size() + Q.map.size() + Q.ptr.size() + Q.list.size() +
+                      P.ent.size() + Q.ent.size();
     std::vector<unsigned char> host(8 * nd + 4 * ni);
     std::unique_ptr<sbg_spinwave> m(new sbg_spinwave);
     m->device = device;
@@ -426,6 +438,10 @@ void create_spinwave(int N, int nb, const int* sites, const double* coef, const 
     T.mapQ = static_cast<const int*>(put(Q.map.data(), 4 * Q.map.size()));
     T.ptrQ = static_cast<const int*>(put(Q.ptr.data(), 4 * Q.ptr.size()));
     T.listQ = static_cast<const int*>(put(Q.list.data(), 4 * Q.list.size()));
+    T.entP = static_cast<const int*>(put(P.ent.data(), 4 * P.ent.size()));
+    T.entQ = static_cast<const int*>(put(Q.ent.data(), 4 * Q.ent.size()));
+    T.nP = static_cast<int>(P.ent.size());
+    T.nQ = static_cast<int>(Q.ent.size());
     check_cuda(cudaMemcpy(m->d_tables, host.data(), host.size(), cudaMemcpyHostToDevice), "H2D spin-wave tables");
     m->assemble_smem = smem;
     {
