@@ -148,7 +148,8 @@ int sbg_solver_reserve(sbg_solver* s, int pairs, int stream_slots);
  * page-locked (cudaHostAlloc) for the copies to overlap.  Device staging buffers are
  * owned by the solver and grow on demand.  Only B's lower triangle crosses the host link
  * when h_B lies in one pinned, device-mapped allocation (cudaHostAlloc memory on 64-bit
- * systems): a kernel reads it in place; otherwise all of B is copied. */
+ * systems): a kernel reads it in place; otherwise all of B is copied.  Calls on one solver are
+ * serialised (they share its staging buffers); use one solver per host thread for overlap. */
 int sbg_solver_solve_host(sbg_solver* s, const cuDoubleComplex* h_A, const cuDoubleComplex* h_B,
                           double* h_W, cuDoubleComplex* h_X, int* h_info, int batch,
                           int chunk_size, int num_streams);
@@ -235,7 +236,8 @@ int sbg_queue_graph_builds(const sbg_queue* q);
  *     use: run one sweep of the largest size on a stream before capturing it into a graph.
  *   - sbg_spinwave_solve_host takes page-locked host q, W, X (or NULL), I (or NULL) and info,
  *     overlaps the copies with the kernels over num_streams internal streams (chunk_size 0:
- *     the solver's chunk) and returns when the results are on the host.
+ *     the solver's chunk) and returns when the results are on the host; calls on one model are
+ *     serialised (they share its staging buffers).
  * All calls return an sbg_status. */
 typedef struct sbg_spinwave sbg_spinwave;
 int sbg_spinwave_create(int n_sites, int n_bonds, const int* sites, const double* coef, const double* disp,

@@ -139,6 +139,7 @@ struct sbg_solver {
                      int capacity = 0; cudaStream_t stream = nullptr; cudaStream_t pull = nullptr;
                      cudaEvent_t pulled = nullptr; cudaEvent_t consumed = nullptr; };
     std::vector<Staging> staging;
+    std::mutex host_mu;                 // one solve_host at a time: they share the staging buffers
     // bytes the last solve_host moved over the host link, each way
     long long last_h2d_bytes = 0, last_d2h_bytes = 0;
     // per-stage event timing
@@ -237,6 +238,7 @@ struct sbg_solver {
     void solve_host(const double2* hA, const double2* hB, double* hW, double2* hX, int* hinfo, int batch,
                     int chunk, int nstreams) {
         if (batch < 0 || chunk <= 0 || nstreams <= 0) throw Error(SBG_ERR_INVALID_VALUE, "bad solve_host arguments");
+        std::lock_guard<std::mutex> serial(host_mu);
         last_h2d_bytes = last_d2h_bytes = 0;
         if (batch == 0) return;
         if (!hA || !hB || !hW || !hX || !hinfo) throw Error(SBG_ERR_INVALID_VALUE, "null host pointer");

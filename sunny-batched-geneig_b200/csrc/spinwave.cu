@@ -189,6 +189,7 @@ struct sbg_spinwave {
     struct Staging { cudaStream_t stream = nullptr; double* q = nullptr; double* W = nullptr; double* I = nullptr;
                      int* info = nullptr; int capacity = 0; };
     std::vector<Staging> staging;
+    std::mutex host_mu;                 // one solve_host at a time: they share the staging buffers
 
     ~sbg_spinwave() {
         int prev = 0;
@@ -278,6 +279,7 @@ struct sbg_spinwave {
                     int chunk, int nstreams) {
         if (!sv) throw Error(SBG_ERR_INVALID_VALUE, "solver == NULL");
         if (nq < 0 || chunk < 0 || nstreams <= 0) throw Error(SBG_ERR_INVALID_VALUE, "bad solve_host arguments");
+        std::lock_guard<std::mutex> serial(host_mu);
         if (nq == 0) return;
         if (!hq || !hW || !hinfo) throw Error(SBG_ERR_INVALID_VALUE, "null host pointer");
         if (chunk == 0) chunk = sv->chunk_pairs;
