@@ -144,8 +144,9 @@ class Solver:
         _check(self._lib.sbg_solver_launch_chunked(self._h, _ptr(A), _ptr(B), _ptr(W), _ptr(X), _ptr(info), batch,
                                                    chunk_size, len(streams), arr), "sbg_solver_launch_chunked")
 
-    def solve_host(self, A, B, W, X, info, chunk_size: int = 16384, num_streams: int = 2) -> None:
-        """End-to-end solve of host (ideally pinned) CPU tensors; synchronous."""
+    def solve_host(self, A, B, W, X, info, chunk_size: int = 16384, num_streams: int = 4) -> None:
+        """End-to-end solve of host (ideally pinned) CPU tensors; synchronous.  With B pinned
+        (``pin_memory()``) only its lower triangle crosses the host link."""
         for name, t, dt in (("A", A, torch.complex128), ("B", B, torch.complex128), ("W", W, torch.float64),
                             ("X", X, torch.complex128), ("info", info, torch.int32)):
             if t.is_cuda or t.dtype != dt or not t.is_contiguous():
