@@ -700,13 +700,15 @@ __host__ __device__ inline size_t ql_rows_bytes(int n) {
            big_align(sizeof(R) * 2 * static_cast<size_t>(n), 16);
 }
 
+// redo: only the pairs flagged by k_tridiag_invit (ws.flag 2, or 3 after a log overflow).
 template <typename R>
 __global__ void __launch_bounds__(32) k_ql_apply_rows(int n, int batch, Workspace ws, double* __restrict__ W,
-                                                      double2* __restrict__ X, int* __restrict__ info) {
+                                                      double2* __restrict__ X, int* __restrict__ info, int redo) {
     using C = cplx<R>;
     const int nrb = (n + 31) / 32;                     // row blocks per pair
     const int b = blockIdx.x / nrb, rb = blockIdx.x - b * nrb, lane = threadIdx.x;
     if (b >= batch) return;
+    if (redo && ws.flag[b] < 2) return;
     if (info[b] > n || info[b] < 0) return;            // B not positive definite: the back stage writes NaN
     extern __shared__ __align__(16) unsigned char smem[];
     const int ldz = tile_ld(n);
@@ -716,7 +718,7 @@ __global__ void __launch_bounds__(32) k_ql_apply_rows(int n, int batch, Workspac
     R* ee = dd + n;
     const size_t mat = static_cast<size_t>(n) * n;
     R* Zg = reinterpret_cast<R*>(X + mat * b);
-    if (ws.flag[b] != 0) {                             // log overflow: warp QL on block 0
+    if (ws.flag[b] != 0 && ws.flag[b] != 2) {          // log overflow: warp QL on block 0
         if (rb != 0) return;
         R* Zs = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(X + mat * b) + 8 * mat);   // row-major, ld n
         for (size_t idx = lane; idx < mat; idx += 32) Zs[idx] = (idx / n == idx % n) ? R(1) : R(0);
@@ -994,16 +996,23 @@ cudaError_t launch_ql_rows(int n, int batch, const Workspace& ws, double* W, dou
     const size_t as = ql_rows_smem_bytes(n, single);
     if (cs > static_cast<size_t>(max_smem_optin()) || as > static_cast<size_t>(max_smem_optin()))
         return cudaErrorInvalidValue;
-    cudaError_t err = launch_ql_chain(n, batch, ws, W, info, single, chain_threads, stream);
+    // FP64 up to kInvitBigMaxN: inverse iteration for every pair it can take, then the rotation-log
+    // QL below for the pairs it flagged only
+    const bool redo = eig_by_inverse_iteration(n, single);
+    if (redo) {
+        cudaError_t err = launch_eig_invit(n, batch, ws, W, X, info, chain_threads, true, stream);
+        if (err != cudaSuccess) return err;
+    }
+    cudaError_t err = launch_ql_chain(n, batch, ws, W, info, single, chain_threads, stream, redo);
     if (err != cudaSuccess) return err;
     const int grid = ((n + 31) / 32) * batch;
     static std::once_flag fd, ff;
     if (single) {
         set_big_smem_once(k_ql_apply_rows<float>, ff, static_cast<size_t>(max_smem_optin()));
-        k_ql_apply_rows<float><<<grid, 32, as, stream>>>(n, batch, ws, W, X, info);
+        k_ql_apply_rows<float><<<grid, 32, as, stream>>>(n, batch, ws, W, X, info, 0);
     } else {
         set_big_smem_once(k_ql_apply_rows<double>, fd, static_cast<size_t>(max_smem_optin()));
-        k_ql_apply_rows<double><<<grid, 32, as, stream>>>(n, batch, ws, W, X, info);
+        k_ql_apply_rows<double><<<grid, 32, as, stream>>>(n, batch, ws, W, X, info, redo ? 1 : 0);
     }
     return cudaGetLastError();
 }

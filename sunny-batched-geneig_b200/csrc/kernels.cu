@@ -619,17 +619,23 @@ __global__ void __launch_bounds__(T) k_refine(int n, int batch, Workspace ws, do
 // One THREAD per pair: the scalar QL recurrence with (d, e) in shared memory
 // interleaved over the CTA, rotations appended to the pair's log.  All 32 lanes of
 // a warp do useful work, so the FP64 pipe runs the chains of 32 pairs at once.
+// redo: only the pairs k_tridiag_invit flagged (ws.flag == 2); they keep 2, or 3 on a log overflow.
 template <typename R>
-__global__ void k_ql_chain(int n, int batch, Workspace ws, double* __restrict__ W, int* __restrict__ info) {
+__global__ void k_ql_chain(int n, int batch, Workspace ws, double* __restrict__ W, int* __restrict__ info,
+                           int redo) {
     const int tid = threadIdx.x, T = blockDim.x;
     const int b = blockIdx.x * T + tid;
     extern __shared__ __align__(16) unsigned char smem[];
     R* d = reinterpret_cast<R*>(smem) + tid;
     R* e = reinterpret_cast<R*>(smem) + static_cast<size_t>(n) * T + tid;
     if (b >= batch) return;
+    if (redo) {
+        if (ws.flag[b] != 2) return;
+        if (info[b] > 0 && info[b] <= n) info[b] = 0;          // QL non-convergence: run it again here
+    }
     double* Wb = W + static_cast<size_t>(n) * b;
     cplx<R>* log = reinterpret_cast<cplx<R>*>(ws.log) + static_cast<size_t>(ws.log_cap) * b;
-    ws.flag[b] = 0;
+    if (!redo) ws.flag[b] = 0;
     if (info[b] != 0) {
         for (int i = 0; i < n; ++i) Wb[i] = __longlong_as_double(0x7ff8000000000000ll);
         log[0] = mk<R>(R(-1), R(0));
@@ -640,7 +646,7 @@ __global__ void k_ql_chain(int n, int batch, Workspace ws, double* __restrict__ 
         e[i * T] = static_cast<R>(ws.e[static_cast<size_t>(n) * b + i]);
     }
     const int r = ql_chain<R>(n, d, e, T, log, ws.log_cap, ws.perm + static_cast<size_t>(n) * b, Wb);
-    if (r < 0) ws.flag[b] = 1;
+    if (r < 0) ws.flag[b] = redo ? 3 : 1;
     else if (r > 0) info[b] = r;
 }
 
@@ -862,10 +868,11 @@ constexpr int kInvitLd = 33;            // lane scratch [i * 33 + lane]: rows al
 
 struct InvitSmem {
     size_t scr, dd, ee, lam, cls, mem, flag, per_warp;
-    __host__ __device__ explicit InvitSmem(int n) {
+    // with_tile: the scratch also holds the in-kernel fallback QL's Z tile
+    __host__ __device__ explicit InvitSmem(int n, bool with_tile = true) {
         size_t o = 0;
         const size_t lanes = 2 * kInvitLd * static_cast<size_t>(n), tile = static_cast<size_t>(n) * tile_ld(n);
-        scr = o;  o += 8 * (lanes > tile ? lanes : tile);     // also the fallback QL's Z tile
+        scr = o;  o += 8 * (with_tile && tile > lanes ? tile : lanes);
         dd = o;   o += 8 * static_cast<size_t>(n);
         ee = o;   o += 8 * static_cast<size_t>(n);
         lam = o;  o += 8 * static_cast<size_t>(n);
@@ -970,14 +977,18 @@ __device__ __forceinline__ double invit_scale_residual(int n, double lam, const 
 #undef SBG_IU
 #undef SBG_ZV
 
+// flag_redo: a pair the kernel cannot take gets ws.flag = 2 and no output (the rotation-log QL is
+// then run for the flagged pairs); otherwise the warp QL runs here, on a Z tile in the scratch.
 __global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspace ws, double* __restrict__ W,
-                                                      double2* __restrict__ X, int* __restrict__ info) {
+                                                      double2* __restrict__ X, int* __restrict__ info,
+                                                      int flag_redo) {
     const int b = blockIdx.x, lane = threadIdx.x & 31;
     if (b >= batch) return;
+    if (flag_redo && lane == 0) ws.flag[b] = 0;
     const int inf = info[b];
     if (inf > n || inf < 0) return;                   // an earlier stage failed: W and X are NaN
     extern __shared__ __align__(16) unsigned char smem[];
-    const InvitSmem lay(n);
+    const InvitSmem lay(n, !flag_redo);
     double* scr = reinterpret_cast<double*>(smem + lay.scr);
     double* dd = reinterpret_cast<double*>(smem + lay.dd);
     double* ee = reinterpret_cast<double*>(smem + lay.ee);
@@ -1091,6 +1102,10 @@ __global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspac
             }
         }
         fallback = !__all_sync(0xffffffffu, ok);
+    }
+    if (fallback && flag_redo) {
+        if (lane == 0) ws.flag[b] = 2;
+        return;
     }
     if (fallback) {                                   // the warp QL, Z tile over the lane scratch
         const int ldz = tile_ld(n);
@@ -1333,7 +1348,7 @@ size_t ql_apply_smem_bytes(int n, int pairs_per_cta, bool single) {
 }
 
 cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, int* info, bool single,
-                            int chain_threads, cudaStream_t stream) {
+                            int chain_threads, cudaStream_t stream, bool redo) {
     if (batch <= 0) return cudaSuccess;
     if (!W || !info || !ws.d || !ws.e || !ws.log || !ws.perm || !ws.flag) return cudaErrorInvalidValue;
     const size_t cs = ql_chain_smem_bytes(n, chain_threads, single);
@@ -1342,11 +1357,27 @@ cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, in
     static std::once_flag fcd, fcf;
     if (single) {
         set_max_smem_once(k_ql_chain<float>, fcf);
-        k_ql_chain<float><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info);
+        k_ql_chain<float><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info, redo ? 1 : 0);
     } else {
         set_max_smem_once(k_ql_chain<double>, fcd);
-        k_ql_chain<double><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info);
+        k_ql_chain<double><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info, redo ? 1 : 0);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eig_invit(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                             int chain_threads, bool flag_redo, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    if (!W || !X || !info || !ws.d || !ws.e || !ws.flag) return cudaErrorInvalidValue;
+    const size_t vs = ql_chain_smem_bytes(n, chain_threads, false);
+    const size_t is = InvitSmem(n, !flag_redo).per_warp;
+    if (vs > static_cast<size_t>(max_smem_optin()) || is > static_cast<size_t>(max_smem_optin()))
+        return cudaErrorInvalidValue;
+    static std::once_flag fv, fi;
+    set_max_smem_once(k_ql_values, fv);
+    set_max_smem_once(k_tridiag_invit, fi);
+    k_ql_values<<<(batch + chain_threads - 1) / chain_threads, chain_threads, vs, stream>>>(n, batch, ws, W, info);
+    k_tridiag_invit<<<batch, 32, is, stream>>>(n, batch, ws, W, X, info, flag_redo ? 1 : 0);
     return cudaGetLastError();
 }
 
@@ -1355,15 +1386,8 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
     if (batch <= 0) return cudaSuccess;
     if (!W || !X || !info || !ws.d || !ws.e || !ws.log || !ws.perm || !ws.flag) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) return launch_ql_rows(n, batch, ws, W, X, info, single, chain_threads, stream);
-    if (eig_by_inverse_iteration(n, single)) {                      // eigenvalues by QL, vectors by inverse iteration
-        const size_t vs = ql_chain_smem_bytes(n, chain_threads, false);
-        if (vs > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
-        static std::once_flag fv;
-        set_max_smem_once(k_ql_values, fv);
-        k_ql_values<<<(batch + chain_threads - 1) / chain_threads, chain_threads, vs, stream>>>(n, batch, ws, W, info);
-        k_tridiag_invit<<<batch, 32, InvitSmem(n).per_warp, stream>>>(n, batch, ws, W, X, info);
-        return cudaGetLastError();
-    }
+    if (eig_by_inverse_iteration(n, single))                        // eigenvalues by QL, vectors by inverse iteration
+        return launch_eig_invit(n, batch, ws, W, X, info, chain_threads, false, stream);
     const size_t cs = ql_chain_smem_bytes(n, chain_threads, single);
     const size_t as = ql_apply_smem_bytes(n, apply_warps, single);
     if (cs > static_cast<size_t>(max_smem_optin()) || as > static_cast<size_t>(max_smem_optin()))
@@ -1392,12 +1416,12 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
     if (single) {
         set_max_smem_once(k_ql_chain<float>, fcf);
         set_max_smem_once(k_ql_apply<float>, faf);
-        k_ql_chain<float><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info);
+        k_ql_chain<float><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info, 0);
         k_ql_apply<float><<<agrid, athreads, as, stream>>>(n, batch, ws, W, X, info);
     } else {
         set_max_smem_once(k_ql_chain<double>, fcd);
         set_max_smem_once(k_ql_apply<double>, fad);
-        k_ql_chain<double><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info);
+        k_ql_chain<double><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info, 0);
         k_ql_apply<double><<<agrid, athreads, as, stream>>>(n, batch, ws, W, X, info);
     }
     return cudaGetLastError();

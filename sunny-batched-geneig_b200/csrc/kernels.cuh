@@ -92,16 +92,33 @@ cudaError_t launch_ql_rows(int n, int batch, const Workspace& ws, double* W, dou
 cudaError_t launch_back_big(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
                             cudaStream_t stream);
 // The QL scalar chain alone (thread per pair): W, the rotation log, perm, flag.
+// redo: only pairs with ws.flag == 2 (flagged by launch_eig_invit); they keep 2, or get 3 on a
+// log overflow.
 cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, int* info, bool single,
-                            int chain_threads, cudaStream_t stream);
+                            int chain_threads, cudaStream_t stream, bool redo = false);
 
 // Kernels one full reduce launch (kReduceFull) issues for order n: the warp Cholesky and the
 // column hegst kernel for n <= 56, one kernel otherwise.
 inline int reduce_kernel_count(int n) { return n <= 56 ? 2 : 1; }
-// FP64 eigenvectors by inverse iteration for n <= kInvitMaxN (k_ql_values + k_tridiag_invit); the
-// rotation-log QL (k_ql_chain + k_ql_apply*) above it and for the mixed form.
+// FP64 eigenvectors by inverse iteration (k_ql_values + k_tridiag_invit) for n <= kInvitMaxN, with
+// the warp QL inside the kernel for pairs it cannot take, and for kSmallMaxN < n <= kInvitBigMaxN,
+// where such pairs are flagged and the rotation-log QL (k_ql_chain + k_ql_apply_rows) redone for
+// them only; the rotation-log QL for every other n and for the mixed form.
 constexpr int kInvitMaxN = 63;
-inline bool eig_by_inverse_iteration(int n, bool single) { return !single && n <= kInvitMaxN; }
+constexpr int kInvitBigMaxN = 128;
+inline bool eig_by_inverse_iteration(int n, bool single) {
+    return !single && (n <= kInvitMaxN || (n > kSmallMaxN && n <= kInvitBigMaxN));
+}
+// Kernels one eigensolve stage launches for order n.
+inline int eig_kernel_count(int n, bool single) {
+    if (single) return 3;
+    if (n <= kInvitMaxN) return 2;
+    return n > kSmallMaxN && n <= kInvitBigMaxN ? 4 : 2;
+}
+// Eigenvalues (k_ql_values) and inverse-iteration eigenvectors (k_tridiag_invit) of every pair;
+// flag_redo: pairs it cannot take get ws.flag = 2 (and no output) instead of the in-kernel QL.
+cudaError_t launch_eig_invit(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                             int chain_threads, bool flag_redo, cudaStream_t stream);
 
 size_t reduce_smem_bytes(int mode, int n);
 size_t ql_chain_smem_bytes(int n, int threads, bool single);

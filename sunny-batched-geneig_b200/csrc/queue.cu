@@ -228,7 +228,14 @@ void create_queue(const int* n_host, int count, int device, const sbg_solver_opt
     check_cuda(cudaMemcpy(q->d_vec_off, vec_off.data(), sizeof(long long) * count, cudaMemcpyHostToDevice), "H2D");
     check_cuda(cudaStreamCreateWithFlags(&q->capture_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     check_cuda(cudaEventCreateWithFlags(&q->fork, cudaEventDisableTiming), "cudaEventCreate");
-    const size_t budget = size_t(1) << 30;           // about 1 GiB of staging + workspace per bucket
+    // Staging + workspace per bucket: half of the free device memory shared by the buckets, between
+    // 1 and 8 GiB.  Bigger chunks mean fewer, fuller launches per bucket: with 1 GiB the n = 128
+    // bucket of the 500,000-pair uneven batch ran ~36 chunks of ~700 pairs (2.4 waves of its
+    // one-CTA-per-pair kernels) back to back.
+    size_t free_b = 0, total_b = 0;
+    check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const size_t budget = std::min<size_t>(size_t(8) << 30,
+                                           std::max<size_t>(size_t(1) << 30, free_b / 2 / by_n.size()));
     for (auto& kv : by_n) {
         q->buckets.emplace_back();
         Bucket& b = q->buckets.back();

@@ -224,7 +224,7 @@ struct sbg_solver {
         else
             check_cuda(sbg::launch_ql_logged(n, cnt, ws, W, X, info, false, sched.chain_threads, sched.ql_warps,
                                              stream), "QL kernels");
-        stage_end(stream, ev, 2, precision == SBG_PRECISION_MIXED ? 3 : 2);
+        stage_end(stream, ev, 2, sbg::eig_kernel_count(n, precision == SBG_PRECISION_MIXED));
         stage_begin(stream, &ev);
         check_cuda(sbg::launch_back(sbg::kBackFull, n, cnt, ws, X, info, sched.back_threads, stream),
                    "back-transform kernel");
