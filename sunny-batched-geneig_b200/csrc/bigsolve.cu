@@ -22,6 +22,9 @@
 //   k_ql_apply_rows  the QL rotation log applied to one 32-row block of Z per CTA (a pair's
 //                    n x n Z does not fit one SM here); a pair whose log overflowed is solved
 //                    by the warp QL of its first block with Z in the X buffer's second half.
+//                    In FP64 for n <= 128 the eigenvectors come from inverse iteration
+//                    (k_tridiag_invit, kernels.cu) and this kernel, with the log, only redoes
+//                    the pairs inverse iteration flagged.
 //   k_back_big       a cluster of ceil(n / 32) CTAs per pair, each CTA a contiguous block of
 //                    32 columns: X = L^{-H} Q Z with 8 (n <= 160) or 16 lanes per column
 //                    (a column's rows in registers across its lane group), the

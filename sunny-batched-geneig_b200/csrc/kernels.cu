@@ -5,11 +5,12 @@
 //            C = L^{-1} A L^{-H}; L into the workspace, C into the caller's X buffer.
 //   hetrd    k_hetrd_warp (n <= 65) or k_hetrd: Householder tridiagonalisation of C,
 //            reflectors and (d, e, tau) into the workspace.
-//   eig      FP64, n <= 63: k_ql_values (the implicit-QL recurrence, one thread per pair,
-//            eigenvalues only) and k_tridiag_invit (eigenvectors by inverse iteration, one
-//            warp per pair).  Otherwise k_ql_chain logs the recurrence's rotations and
-//            k_ql_apply / k_ql_apply_reg replay the log onto Z (W ascending); the mixed form
-//            runs the recurrence in FP32 and refines with k_refine.
+//   eig      FP64, n <= 63 (and 85..128, launched from bigsolve.cu): k_ql_values (the
+//            implicit-QL recurrence, one thread per pair, eigenvalues only) and
+//            k_tridiag_invit (eigenvectors by inverse iteration, one warp per pair).
+//            Otherwise k_ql_chain logs the recurrence's rotations and k_ql_apply /
+//            k_ql_apply_reg replay the log onto Z (W ascending); the mixed form runs the
+//            recurrence in FP32 and refines with k_refine.
 //   back     k_back_col (n <= 56) or k_back: X = L^{-H} Q Z, written over Z.
 //
 // The split follows where the work is latency bound: the QL recurrence is a
