@@ -194,7 +194,9 @@ int sbg_max_n(int precision);
  *   - Every n gets its own solver with the per-n schedule (opts->tuning_mode as in
  *     sbg_solver_create: the table, or the autotuner); opts->precision = MIXED applies to the
  *     n that the mixed form supports (sbg_max_n) and the others run FP64 (sbg_queue_bucket reports
- *     which); opts->workspace_pairs > 0 caps the pairs per internal chunk.
+ *     which); each bucket's chunk (staging + solver scratch) is sized from half the free device
+ *     memory at creation, split over the buckets, 1 to 8 GiB each; opts->workspace_pairs > 0
+ *     sets the pairs per chunk instead (for callers that must bound the queue's memory).
  *   - sbg_launch_queue is asynchronous on `stream`: it replays one CUDA graph in which all n run
  *     concurrently (captured on the first launch, and again when the buffers change).
  * All calls return an sbg_status. */
