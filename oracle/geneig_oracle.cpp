@@ -23,7 +23,9 @@
 // LAPACK itself comes from the OpenBLAS 0.3.15 shipped in this image.
 //
 // Every batch routine partitions the pairs over `nthreads` host threads, one pair
-// per task, with OpenBLAS forced to one thread, as the baseline plan asks.
+// per task, with OpenBLAS forced to one thread (the reference's own CPU loop,
+// tests/test_full_batched_n54.cpp:238-256, solves one pair per LAPACKE call; the
+// threads run such calls side by side without oversubscribing the cores).
 
 #include <lapacke.h>
 
