@@ -108,7 +108,65 @@ def parse():
                     help="pairs for --workload other than qsweep54 (0 = the configuration's own count)")
     ap.add_argument("--workload", default="qsweep54", choices=["qsweep54"] + sorted(OTHER_WORKLOADS),
                     help="qsweep54 is the headline line; the others measure the remaining configurations")
+    ap.add_argument("--strong", action="store_true",
+                    help="strong scaling: the ranks split one --pairs batch (contiguous shards) instead of each "
+                         "solving --pairs pairs of its own")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="rank plumbing only: process group, barrier, max-over-ranks timing of an empty step")
     return ap.parse_args()
+
+
+def relaunch(args) -> int:
+    """--gpus N (N > 1) started without a launcher: re-run this command as N ranks on this node
+    (torch.distributed.run, rendezvous on 127.0.0.1) and return its exit code.  Never silently
+    runs one rank for N."""
+    import socket
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
+def world_from_env(args):
+    """(world, rank, local_rank) of this process.  Under a launcher WORLD_SIZE wins; a --gpus that
+    disagrees with it is an error rather than a mislabelled line."""
+    world = env_int("WORLD_SIZE", 1)
+    if "WORLD_SIZE" in os.environ and args.gpus not in (1, world):
+        raise SystemExit(f"--gpus {args.gpus} but the launcher started {world} ranks")
+    return world, env_int("RANK", 0), env_int("LOCAL_RANK", 0)
+
+
+def run_dry(args):
+    """The multi-rank plumbing of every line without GPU work: process group (NCCL on GPUs, gloo
+    on the host), barrier, an empty timed step, the max over ranks; rank 0 prints n_gpus."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    world, rank, local = world_from_env(args)
+    on_gpu = torch.cuda.is_available()
+    if world > 1:
+        if on_gpu:
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local) if on_gpu else torch.device("cpu")
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        if world > 1:
+            dist.barrier()
+    dt = torch.tensor([(time.perf_counter() - t0) / max(1, args.steps)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(dt, op=dist.ReduceOp.MAX)
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "n_gpus": world, "ranks": world, "steps": args.steps,
+                          "backend": (dist.get_backend() if world > 1 else None),
+                          "ms_per_step": 1e3 * float(dt.item())}), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
 
 
 # ------------------------------------------------------------------ clocks
@@ -165,9 +223,10 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ workload
 
-def make_workload(torch, sbg, pairs: int, seed: int, device, n_sites: int = N_SITES):
-    """q-sweep pairs on the device; the shift uses the eigenvalues of B0, computed by
-    the FP64 solver itself with B = I (a standard Hermitian eigenproblem)."""
+def make_workload(torch, sbg, pairs: int, seed: int, device, n_sites: int = N_SITES, start: int = 0):
+    """q-sweep pairs on the device (q points start, start + 1, ... of the grid); the shift uses the
+    eigenvalues of B0, computed by the FP64 solver itself with B = I (a standard Hermitian
+    eigenproblem)."""
     from sbg import workloads as wl
     n = 2 * n_sites
     nn = n * n
@@ -178,7 +237,7 @@ def make_workload(torch, sbg, pairs: int, seed: int, device, n_sites: int = N_SI
     chunk = 16384
     for off in range(0, pairs, chunk):
         cnt = min(chunk, pairs - off)
-        q = wl.qsweep_points(GRID, off % GRID ** 3, cnt, device)
+        q = wl.qsweep_points(GRID, (start + off) % GRID ** 3, cnt, device)
         B0 = wl.qsweep_B0(n_sites, q, seed)
         Bc = wl._colmajor(B0)
         I = eye.expand(cnt, nn).contiguous()
@@ -253,6 +312,10 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch(args))
+    if args.dry_run:
+        return run_dry(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload != "qsweep54":
@@ -261,9 +324,7 @@ def main():
     import torch.distributed as dist
     import sbg
 
-    world = env_int("WORLD_SIZE", 1)
-    rank = env_int("RANK", 0)
-    local = env_int("LOCAL_RANK", 0)
+    world, rank, local = world_from_env(args)
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     if world > 1:
@@ -283,11 +344,17 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    pairs = args.pairs
-    A, B = make_workload(torch, sbg, pairs, seed=rank, device=device)
+    if args.strong:                      # one global batch split over the ranks (one cell, seed 0)
+        from sbg.sharding import shard_bounds
+        q0, pairs = shard_bounds(args.pairs, world, rank)
+        A, B = make_workload(torch, sbg, pairs, seed=0, device=device, start=q0)
+    else:                                # weak scaling: every rank its own q-sweep (cell seed = rank)
+        pairs = args.pairs
+        A, B = make_workload(torch, sbg, pairs, seed=rank, device=device)
     W = torch.empty((pairs, N), dtype=torch.float64, device=device)
     X = torch.empty_like(B)
     info = torch.empty(pairs, dtype=torch.int32, device=device)
+    job_pairs = args.pairs if args.strong else world * pairs      # pairs all ranks solve per step
     forms = [f for f in args.forms.split(",") if f]
     chunk = 65536
     solvers = {f: sbg.Solver(N, local, precision=f, workspace_pairs=chunk) for f in forms}
@@ -343,7 +410,7 @@ def main():
         torch.cuda.synchronize()
         st = s.read_stage_times()
         s.enable_stage_timing(False)
-        results[f] = dict(ms=ms, value=world * pairs / (ms / 1e3), acc=acc, info_nonzero=bad, clocks=clocks,
+        results[f] = dict(ms=ms, value=job_pairs / (ms / 1e3), acc=acc, info_nonzero=bad, clocks=clocks,
                           stages={k: (v[0] / 2, v[1] / 2) for k, v in st.items()})
 
     # choose the headline form: fastest that meets the gate on the sample
@@ -396,17 +463,19 @@ def main():
         except Exception:
             pass
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        hbm_src = "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
         fp64_peak = fp64_peak_tflops(torch)
         stages = R["stages"]
         top = max(stages, key=lambda k: stages[k][0])
         ms_top = stages[top][0] / max(1, stages[top][1])            # average launch duration
-        pairs_per_launch = pairs / max(1, stages[top][1] / 2 * 2) if False else None
         launches_top = stages[top][1]
         units = pairs / max(1, launches_top)
         achieved = STAGE_FLOPS[top] * units / (ms_top / 1e3) / 1e12
         hbm_achieved = BYTES_PER_SOLVE * R["value"] / world / 1e9
         roofline = {"bound": "fp64", "kernel": top, "achieved": achieved, "peak": fp64_peak["tflops"],
                     "unit": "TFLOP/s", "frac": achieved / fp64_peak["tflops"],
+                    "peak_nominal": fp64_peak["nominal_tflops"],
+                    "frac_of_nominal": achieved / fp64_peak["nominal_tflops"],
                     "traffic": TRAFFIC_PER_PAIR_N54[top] * units if best == "fp64" else None,
                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per pair, 16,384-pair "
                                       "capture, scaled to the launch's pairs",
@@ -414,16 +483,18 @@ def main():
                     "algorithmic_flops_per_pair": STAGE_FLOPS[top], "pairs_per_launch": units,
                     "avg_launch_ms": ms_top,
                     "hbm": {"achieved_gbs": hbm_achieved, "peak_gbs": hbm_peak,
-                            "frac": hbm_achieved / hbm_peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
+                            "frac": hbm_achieved / hbm_peak, "peak_source": hbm_src},
                     "whole_solve": {"achieved_tflops": FLOPS_PER_SOLVE * R["value"] / world / 1e12,
                                     "frac": FLOPS_PER_SOLVE * R["value"] / world / 1e12 / fp64_peak["tflops"]}}
         launches = sum(v[1] for v in R["stages"].values()) * args.steps
         line = {
             "metric": METRIC, "value": R["value"], "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": R["ms"], "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": R["ms"], "higher_is_better": True,
+            "scaling": "strong" if args.strong else "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": {"workload": f"q-sweep n={N} (N={N_SITES} sites, 4 bonds/site, 64^3 grid), "
                                    f"lambda_min(B)=1e-3||B||, A=diag(I,-I)", "pairs_per_gpu": pairs,
+                       "pairs_per_step": job_pairs,
                        "form": best, "l2": "inputs (24 GB) larger than L2; no flush", "chunk_pairs": chunk},
             "forms": {f: {"value": r["value"], "ms_per_step": r["ms"], "accuracy": r["acc"],
                           "info_nonzero": r["info_nonzero"],
@@ -481,9 +552,7 @@ def run_other(args):
     cfg = OTHER_WORKLOADS[args.workload]
     if cfg["kind"] == "spinwave":
         return run_spinwave(args, cfg)
-    world = env_int("WORLD_SIZE", 1)
-    rank = env_int("RANK", 0)
-    local = env_int("LOCAL_RANK", 0)
+    world, rank, local = world_from_env(args)
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     if world > 1:
@@ -711,9 +780,7 @@ def run_spinwave(args, cfg):
     from sbg import workloads as wl
     from oracle import metrics as Mx
 
-    world = env_int("WORLD_SIZE", 1)
-    rank = env_int("RANK", 0)
-    local = env_int("LOCAL_RANK", 0)
+    world, rank, local = world_from_env(args)
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     if world > 1:
@@ -911,19 +978,58 @@ def run_spinwave(args, cfg):
         dist.destroy_process_group()
 
 
+_FP64_PEAK = {}
+
+
 def fp64_peak_tflops(torch):
-    """FP64 FMA peak of this GPU: SMs x 64 FP64 FMA/clk x 2 flops x max SM clock (the B200's
-    FP64 rate; MEASURED_PEAKS.json holds no FP64 figure)."""
-    p = torch.cuda.get_device_properties(torch.cuda.current_device())
-    mhz = None
+    """FP64 peak of this GPU, MEASURED: the library's FP64 FMA probe (sbg_selftest_fp64_fma: 8
+    CTAs of 256 threads per SM, 8 independent FMA chains per thread), timed with CUDA events on its
+    stream, best of 3 after a warm-up, with the SM clock sampled while it runs.  The nominal figure
+    (SMs x 64 FP64 FMA/clk x 2 x max SM clock) is reported beside it."""
+    dev = torch.cuda.current_device()
+    if dev in _FP64_PEAK:
+        return _FP64_PEAK[dev]
+    import ctypes
+    from sbg import _lib
+    p = torch.cuda.get_device_properties(dev)
+    mhz = 1965.0
     try:
         out = subprocess.run(["nvidia-smi", "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits",
-                              f"--id={torch.cuda.current_device()}"], capture_output=True, text=True, timeout=10)
+                              f"--id={dev}"], capture_output=True, text=True, timeout=10)
         mhz = float(out.stdout.strip().splitlines()[0])
     except Exception:
-        mhz = 1965.0
-    return {"tflops": p.multi_processor_count * 64 * 2 * mhz * 1e6 / 1e12,
-            "source": f"nominal: {p.multi_processor_count} SMs x 64 FP64 FMA/clk x 2 x {mhz:.0f} MHz (no measured FP64 peak)"}
+        pass
+    nominal = p.multi_processor_count * 64 * 2 * mhz * 1e6 / 1e12
+    lib = _lib.load()
+    blocks, iters = 8 * p.multi_processor_count, 40000
+    out_buf = torch.empty(blocks * 256, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    flops = float(blocks) * 256 * 64 * iters
+    clock = ClockSampler(dev)
+    lib.sbg_selftest_fp64_fma(ctypes.c_void_p(out_buf.data_ptr()), blocks, iters, sp)
+    torch.cuda.synchronize()
+    clock.start()
+    best = None
+    for _ in range(3):
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = lib.sbg_selftest_fp64_fma(ctypes.c_void_p(out_buf.data_ptr()), blocks, iters, sp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if st != 0:
+            raise RuntimeError(lib.sbg_last_error().decode())
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    clocks = clock.stop()
+    measured = flops / (best / 1e3) / 1e12
+    _FP64_PEAK[dev] = {
+        "tflops": measured, "nominal_tflops": nominal,
+        "source": f"measured: FP64 FMA probe (sbg_selftest_fp64_fma, {blocks} CTAs x 256 threads x 8 chains, "
+                  f"{best:.2f} ms, SM clock median {clocks.get('sm_mhz')} MHz); nominal {nominal:.2f} TFLOP/s = "
+                  f"{p.multi_processor_count} SMs x 64 FP64 FMA/clk x 2 x {mhz:.0f} MHz",
+        "probe_ms": best, "probe_sm_mhz": clocks.get("sm_mhz")}
+    return _FP64_PEAK[dev]
 
 
 if __name__ == "__main__":

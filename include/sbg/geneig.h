@@ -167,6 +167,10 @@ int sbg_solver_read_stage_times(sbg_solver* s, double* ms_out4, int* launches_ou
 
 /* Device bytes of workspace per pair for a given n and precision. */
 size_t sbg_workspace_bytes_per_pair(int n, int precision);
+/* Exact device bytes of the workspace a solver allocates for `pairs` pairs of order n: the
+ * per-pair bytes times pairs plus the 256-byte alignment of its seven regions (at most
+ * 7 * 256 bytes more). */
+size_t sbg_workspace_bytes(int n, int precision, int pairs);
 
 /* Getters (nvrtc_solver.hpp:128-145). */
 int sbg_solver_matrix_size(const sbg_solver* s);
@@ -267,11 +271,13 @@ int sbg_spinwave_solve_host(sbg_spinwave* m, sbg_solver* s, const double* h_q, i
  * SBG_NOALLOC_SCRATCH_BYTES long, which every GPU that loads the library keeps until process
  * exit.  The caller still provides A, B, W, X and info.
  *   - It allocates nothing (no cudaMalloc, cudaFree or allocating library call).
- *   - Limit: batch * sbg_workspace_bytes_per_pair(n, SBG_PRECISION_FP64) + 1792 must fit in
+ *   - Limit: sbg_workspace_bytes(n, SBG_PRECISION_FP64, batch) must fit in
  *     SBG_NOALLOC_SCRATCH_BYTES (at n = 54 that is 533 pairs); larger batches are rejected with
  *     SBG_ERR_INVALID_VALUE and a message in sbg_last_error() — split them into slices.
  *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress)
- *     and caches it; make that first call before any stream capture.
+ *     and caches it; make that first call before any stream capture.  The cached address
+ *     belongs to the device's current context: cudaDeviceReset on that device after the first
+ *     call is not supported (the array would move and the cached address dangle).
  *   - All calls share the one array and it keeps the last call's contents (nothing in it needs
  *     to start at zero).  Calls that overlap on the GPU race on it: order them on one stream.
  * Returns an sbg_status. */
@@ -287,6 +293,18 @@ int sbg_geneig_full_noalloc_launch(int n, const cuDoubleComplex* d_A, const cuDo
 int sbg_tuning_table_path(int device_id, char* buf, size_t buflen);
 /* Forgets the in-process autotune memo (the next autotuned construction reads the file). */
 int sbg_tuning_forget_in_process(void);
+
+/* ------------------------------------------------------------------ device self-test */
+/* No counterpart in the reference.  Writes d_r[i] = the reciprocal of d_u[i] as the inverse
+ * iteration computes it (Newton-Raphson from the hardware estimate, not a correctly rounded
+ * division), i < count, on `stream`, so a test can compare it with 1.0 / u.  Returns an
+ * sbg_status. */
+int sbg_selftest_reciprocal(const double* d_u, double* d_r, int count, cudaStream_t stream);
+/* No counterpart in the reference.  FP64 FMA throughput probe for the roofline's denominator:
+ * `blocks` CTAs of 256 threads; every thread runs 8 independent dependent FMA chains of 4 * iters
+ * FMAs each, so one launch executes blocks * 256 * 64 * iters FP64 flops.  d_out receives
+ * blocks * 256 doubles (the chains' sums).  Time it with CUDA events on `stream`. */
+int sbg_selftest_fp64_fma(double* d_out, int blocks, int iters, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

@@ -32,12 +32,28 @@ GEIG_VERSION = 1
 _lib = None
 
 
+def reference_dir() -> str:
+    """Where the reference tree is read from when it is present (build time only): the
+    SBG_REFERENCE_DIR environment variable, else the default the Makefile also uses."""
+    return os.environ.get("SBG_REFERENCE_DIR", "/root/reference")
+
+
+REF_DRIVERS = ("test_full_batched_n54", "test_full_n54", "test_chol_n54", "test_reduce_n54",
+               "test_reduce_eig_n54")
+
+
 def build(quiet: bool = True) -> None:
-    """Compile libsbg_oracle.so (and _ref/ when the reference tree is present)."""
+    """Compile libsbg_oracle.so and, when the reference tree is present, _ref/: the reference's
+    fixture generator and its own n = 54 test drivers linked against libsbg_geneig.so (which
+    must be built first)."""
     targets = ["all"]
-    if os.path.isdir("/root/reference/tests"):
+    ref = reference_dir()
+    if os.path.isdir(os.path.join(ref, "tests")):
         targets.append("ref")
-    subprocess.run(["make", "-C", HERE, *targets], check=True,
+        lib_so = os.path.join(os.path.dirname(HERE), "sunny-batched-geneig_b200", "sbg", "libsbg_geneig.so")
+        if os.path.exists(lib_so):
+            targets.append("drivers")
+    subprocess.run(["make", "-C", HERE, f"SBG_REFERENCE_DIR={ref}", *targets], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
 
 

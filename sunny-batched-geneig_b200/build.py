@@ -17,6 +17,7 @@ REPO = os.path.dirname(PKG_DIR)
 CSRC = os.path.join(PKG_DIR, "csrc")
 INCLUDE = os.path.join(REPO, "include")
 LIB = os.path.join(PKG_DIR, "sbg", "libsbg_geneig.so")
+BUILD_DIR = os.path.join(PKG_DIR, "_build")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -46,10 +47,28 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _compile(src: str, obj: str, verbose: bool) -> None:
+    flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    cmd = [nvcc(), *flags, f"-I{INCLUDE}", f"-I{CSRC}", "-c", src, "-o", obj + ".tmp"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(obj + ".tmp", obj)
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles each source to an object in _build/ (in parallel), then links the library."""
     if not force and not _stale():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", *sources(), "-o", LIB + ".tmp"]
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    objs = [os.path.join(BUILD_DIR, os.path.basename(s)[:-3] + ".o") for s in sources()]
+    workers = max(1, min(len(objs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(workers) as ex:
+        for f in [ex.submit(_compile, s, o, verbose) for s, o in zip(sources(), objs)]:
+            f.result()
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", LIB + ".tmp"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

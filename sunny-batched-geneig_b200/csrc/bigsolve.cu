@@ -894,10 +894,8 @@ __global__ void __launch_bounds__(kBigThreads) k_back_big(int mode, int n, int b
 }
 
 template <class K>
-void set_big_smem_once(K kernel, std::once_flag& flag, size_t bytes) {
-    std::call_once(flag, [&]() {
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
-    });
+void set_big_smem_once(K kernel, SmemOptIn& rec, size_t bytes) {
+    set_smem_limit(reinterpret_cast<const void*>(kernel), rec, static_cast<int>(bytes));
 }
 
 template <typename... KArgs, typename... Args>
@@ -933,7 +931,7 @@ template <int CS, int RM>
 void run_reduce_big(cudaError_t* err, const double2* A, const double2* B, int n, int batch, const Workspace& ws,
                     double2* X, int* info, cudaStream_t stream) {
     const size_t smem = BigReduceSmem(n, CS).total;
-    static std::once_flag f;
+    static SmemOptIn f;
     set_big_smem_once(k_reduce_big<CS, RM>, f, static_cast<size_t>(max_smem_optin()));
     *err = launch_clustered(k_reduce_big<CS, RM>, CS, batch * CS, kBigThreads, smem, stream, A, B, n, batch, ws, X,
                             info);
@@ -943,7 +941,7 @@ template <int CS, int G, int RM, int NCW>
 void run_back_big(cudaError_t* err, int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
                   cudaStream_t stream) {
     const size_t smem = BigBackSmem(n).total;
-    static std::once_flag f;
+    static SmemOptIn f;
     set_big_smem_once(k_back_big<CS, G, RM, NCW>, f, static_cast<size_t>(max_smem_optin()));
     *err = launch_clustered(k_back_big<CS, G, RM, NCW>, CS, batch * CS, kBigThreads, smem, stream, mode, n, batch,
                             ws, X, info);
@@ -957,7 +955,7 @@ constexpr int kMidMaxN = 160;             // the packed tile + buffers fit 227 K
 template <int RM>
 void run_reduce_mid(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X, int* info,
                     cudaStream_t stream) {
-    static std::once_flag f;
+    static SmemOptIn f;
     set_big_smem_once(k_reduce_mid<RM>, f, static_cast<size_t>(max_smem_optin()));
     k_reduce_mid<RM><<<batch, kMidThreads, MidSmem(n).total, stream>>>(A, B, n, batch, ws, X, info);
 }
@@ -1009,7 +1007,7 @@ cudaError_t launch_ql_rows(int n, int batch, const Workspace& ws, double* W, dou
     cudaError_t err = launch_ql_chain(n, batch, ws, W, info, single, chain_threads, stream, redo);
     if (err != cudaSuccess) return err;
     const int grid = ((n + 31) / 32) * batch;
-    static std::once_flag fd, ff;
+    static SmemOptIn fd, ff;
     if (single) {
         set_big_smem_once(k_ql_apply_rows<float>, ff, static_cast<size_t>(max_smem_optin()));
         k_ql_apply_rows<float><<<grid, 32, as, stream>>>(n, batch, ws, W, X, info, 0);

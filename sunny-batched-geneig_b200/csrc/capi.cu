@@ -239,6 +239,25 @@ size_t sbg_workspace_bytes_per_pair(int n, int /*precision*/) {
     return n > 0 ? sbg::workspace_bytes_per_pair(n) : 0;
 }
 
+int sbg_selftest_reciprocal(const double* d_u, double* d_r, int count, cudaStream_t stream) {
+    return guarded([&] {
+        if (count < 0) throw Error(SBG_ERR_INVALID_VALUE, "count < 0");
+        if (count > 0 && (!d_u || !d_r)) throw Error(SBG_ERR_INVALID_VALUE, "null device pointer");
+        check_cuda(sbg::launch_selftest_recip(d_u, d_r, count, stream), "reciprocal self-test kernel");
+    });
+}
+
+int sbg_selftest_fp64_fma(double* d_out, int blocks, int iters, cudaStream_t stream) {
+    return guarded([&] {
+        if (!d_out || blocks <= 0 || iters <= 0) throw Error(SBG_ERR_INVALID_VALUE, "bad FMA probe arguments");
+        check_cuda(sbg::launch_selftest_fp64_fma(d_out, blocks, iters, stream), "FP64 FMA probe kernel");
+    });
+}
+
+size_t sbg_workspace_bytes(int n, int /*precision*/, int pairs) {
+    return n > 0 && pairs > 0 ? sbg::workspace_bytes(n, pairs) : 0;
+}
+
 int sbg_solver_matrix_size(const sbg_solver* s) { return s ? s->n : 0; }
 int sbg_solver_batches_per_block(const sbg_solver* s) { return s ? s->sched.ql_warps : 0; }
 int sbg_solver_block_dim_x(const sbg_solver* s) { return s ? s->sched.reduce_threads : 0; }

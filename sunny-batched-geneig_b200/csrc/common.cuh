@@ -127,4 +127,21 @@ constexpr uint32_t kMaxPolls = 1u << 24;   // far beyond any real copy; a timeou
 // LAPACK conventions happens (kept above any n + i value).
 constexpr int kInfoCopyTimeout = 1 << 29;
 
+// ----------------------------------------------------------------------------- reciprocal
+
+// 1/u by Newton-Raphson iteration for the reciprocal (the textbook method: each step
+// r <- r + r (1 - u r) squares the relative error) from the hardware reciprocal estimate
+// (rcp.approx.ftz.f64); two steps.  Used by the inverse iteration's factorization, where it is
+// shorter than a correctly rounded division in the dependent chain and no correct rounding is
+// needed (every vector's residual is checked); |u| >= eps ||T|| there keeps u normal.
+// sbg_selftest_reciprocal exposes it so a test can compare it with the correctly rounded 1.0 / u.
+__device__ __forceinline__ double recip_nr(double u) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(u));
+    double e = fma(-u, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-u, r, 1.0);
+    return fma(r, e, r);
+}
+
 }  // namespace sbg

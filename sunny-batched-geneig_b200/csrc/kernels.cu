@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <atomic>
 #include <mutex>
 
 namespace sbg {
@@ -46,10 +47,13 @@ struct ReduceSmem {
 
 
 // Waits for the bulk copies of this CTA; on the (never expected) timeout it flags
-// the pair and waits once more, bounded, so no copy lands after the CTA exits.
+// the pair (every thread that timed out ORs the bit into the pair's info word, when one is
+// given) and waits once more, bounded, so no copy lands after the CTA exits.  The stage then
+// runs on whatever landed; the flag (info > n) makes the back-transform write NaN for the pair
+// and every later stage skip it.
 __device__ inline bool wait_copies(uint64_t* bar, int* info_word) {
     if (mbar_wait_bounded(bar, 0, kMaxPolls)) return true;
-    if (threadIdx.x == 0 && info_word) atomicOr(info_word, kInfoCopyTimeout);
+    if (info_word) atomicOr(info_word, kInfoCopyTimeout);
     mbar_wait_bounded(bar, 0, kMaxPolls);
     return false;
 }
@@ -91,7 +95,8 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_reduce(int mode, const d
             if (need_a) bulk_g2s(As + static_cast<size_t>(j) * ld, Ab + static_cast<size_t>(j) * n, 16u * n, bar);
         }
     }
-    wait_copies(bar, info + b);
+    // the first stage: info[b] is written only at the end (with the timeout bit of thread 0's wait)
+    const int copy_status = wait_copies(bar, nullptr) ? 0 : kInfoCopyTimeout;
 
     int st = 0;
     if (mode == kReduceFromLM) {
@@ -101,7 +106,7 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_reduce(int mode, const d
         st = potrf_lower(Ls, ld, n, invd);
     }
     if (st != 0) {
-        if (tid == 0) info[b] = (mode == kReduceFull) ? n + st : st;
+        if (tid == 0) info[b] = ((mode == kReduceFull) ? n + st : st) | copy_status;
         return;
     }
     if (mode == kReduceChol) {
@@ -109,7 +114,7 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_reduce(int mode, const d
             const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
             out[mat * b + idx] = (i >= j) ? Ls[i + j * ld] : make_double2(0.0, 0.0);
         }
-        if (tid == 0) info[b] = 0;
+        if (tid == 0) info[b] = copy_status;
         return;
     }
     if (mode != kReduceFromLM) {
@@ -170,7 +175,7 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_reduce(int mode, const d
             if (i >= j) LVg[idx] = Ls[i + j * ld];
         }
     }
-    if (tid == 0) info[b] = 0;
+    if (tid == 0) info[b] = copy_status;
 }
 
 struct BackSmem {
@@ -215,10 +220,11 @@ __global__ void __launch_bounds__(32 * kPotrfWarpsPerCta) k_potrf_warp(int mode,
     __syncwarp();
     for (int j = lane; j < n; j += 32)
         bulk_g2s(P + pk(j, n), Bb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
-    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) mbar_wait_bounded(bar, 0, kMaxPolls);
+    // the first stage: info[b] is written only at the end, with the timeout bit of lane 0's wait
+    const int copy_status = wait_copies(bar, nullptr) ? 0 : kInfoCopyTimeout;
     const int st = potrf_warp_packed<double>(P, n, invd);
     if (st != 0) {
-        if (lane == 0) info[b] = (mode == kReduceFull) ? n + st : st;
+        if (lane == 0) info[b] = ((mode == kReduceFull) ? n + st : st) | copy_status;
         return;
     }
     __syncwarp();
@@ -230,7 +236,7 @@ __global__ void __launch_bounds__(32 * kPotrfWarpsPerCta) k_potrf_warp(int mode,
             else if (mode == kReduceChol) dst[i + static_cast<size_t>(j) * n] = make_double2(0.0, 0.0);
         }
     }
-    if (lane == 0) info[b] = 0;
+    if (lane == 0) info[b] = copy_status;
 }
 
 // ----------------------------------------------------------------------------- k_hegst_col
@@ -248,7 +254,7 @@ __host__ __device__ inline size_t hegst_col_bytes(int n) {
 template <int NMAX, bool EXACT>
 __global__ void __launch_bounds__(NMAX, 4) k_hegst_col(int mode, const double2* __restrict__ A, const Workspace ws,
                                                     double2* __restrict__ out, int n_arg, int batch,
-                                                    const int* __restrict__ info) {
+                                                    int* __restrict__ info) {
     const int n = EXACT ? NMAX : n_arg;
     const int b = blockIdx.x;
     if (b >= batch) return;
@@ -275,7 +281,7 @@ __global__ void __launch_bounds__(NMAX, 4) k_hegst_col(int mode, const double2* 
 #pragma unroll
     for (int i = 0; i < NMAX; ++i)
         y[i] = (own && i < n) ? Ab[i + static_cast<size_t>(tid) * n] : make_double2(0.0, 0.0);
-    wait_copies(bar, nullptr);
+    wait_copies(bar, info + b);
     for (int i = tid; i < n; i += NMAX) invd[i] = 1.0 / Lp[pk(i, n)].x;
     __syncthreads();
     if (own) col_trsm_lower<NMAX>(Lp, invd, y, n, [&](int k, double2 w) { Ob[k + static_cast<size_t>(tid) * n] = w; });
@@ -305,7 +311,7 @@ __host__ __device__ constexpr int back_col_threads() { return (NMAX * G + 31) / 
 template <int NMAX, int G, bool EXACT>
 __global__ void __launch_bounds__(back_col_threads<NMAX, G>(), G == 1 ? 4 : 3) k_back_col(int mode, int n_arg, int batch,
                                                                             Workspace ws, double2* __restrict__ X,
-                                                                            const int* __restrict__ info) {
+                                                                            int* __restrict__ info) {
     const int n = EXACT ? NMAX : n_arg;              // EXACT: n is a compile-time constant
     constexpr int T = back_col_threads<NMAX, G>();
     constexpr int RM = (NMAX + G - 1) / G;
@@ -347,7 +353,7 @@ __global__ void __launch_bounds__(back_col_threads<NMAX, G>(), G == 1 ? 4 : 3) k
         y[r] = make_double2((own && i < n) ? Zg[i + static_cast<size_t>(col) * n] : 0.0, 0.0);
     }
     for (int i = tid; i < n; i += T) tau_s[i] = ws.tau[static_cast<size_t>(n) * b + i];
-    wait_copies(bar, nullptr);
+    wait_copies(bar, info + b);
     for (int i = tid; i < n; i += T) invd[i] = 1.0 / LVs[i + i * ld].x;
     __syncthreads();               // all of Z is in registers before any X is stored over it
     grp_apply_q<G, RM, double>(LVs, ld, tau_s, y, n, g);
@@ -385,7 +391,7 @@ struct HetrdSmem {
 };
 template <int T>
 __global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __restrict__ C, Workspace ws,
-                                             const int* __restrict__ info) {
+                                             int* __restrict__ info) {
     const int b = blockIdx.x;
     if (b >= batch) return;
     if (info[b] != 0) return;
@@ -411,7 +417,7 @@ __global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __
         for (int j = tid; j < n; j += 32)
             bulk_g2s(As + j + static_cast<size_t>(j) * ld, Cb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
     }
-    wait_copies(bar, nullptr);
+    wait_copies(bar, info + b);
     hetrd_lower(As, ld, n, d_s, e_s, tau_s, vw, pbuf, ww);
     // reflector k, component i >= k+2, sits at A(i, k); it goes to LV(k, i)
     double2* LVg = ws.LV + mat * b;
@@ -438,7 +444,7 @@ constexpr int kHetrdWarpsPerCta = 2;
 constexpr int kHetrdWarpMaxN = 65;
 
 __global__ void __launch_bounds__(32 * kHetrdWarpsPerCta) k_hetrd_warp(int n, int batch, const double2* __restrict__ C,
-                                                                      Workspace ws, const int* __restrict__ info) {
+                                                                      Workspace ws, int* __restrict__ info) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * kHetrdWarpsPerCta + warp;
     if (b >= batch) return;
@@ -460,7 +466,7 @@ __global__ void __launch_bounds__(32 * kHetrdWarpsPerCta) k_hetrd_warp(int n, in
     __syncwarp();
     for (int j = lane; j < n; j += 32)
         bulk_g2s(P + pk(j, n), Cb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
-    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) mbar_wait_bounded(bar, 0, kMaxPolls);
+    wait_copies(bar, info + b);
     hetrd_warp_packed<double>(P, n, d_s, e_s, tau_s, vb, wb);
     double2* LVg = ws.LV + mat * b;
     for (int k = 0; k + 1 < n; ++k) {                    // LV(k, k+1) = v_k(k+1) = 1
@@ -896,19 +902,6 @@ __device__ __forceinline__ double invit_start(int j, int i) {
 // interleaved scratch ([i * kInvitLd + lane]).
 #define SBG_IU(i) invu[(i) * kInvitLd + lane]
 #define SBG_ZV(i) z[(i) * kInvitLd + lane]
-// 1/u by Newton-Raphson from the hardware reciprocal estimate (rcp.approx.ftz.f64): each step
-// r <- r + r (1 - u r) squares the relative error; with two, the result equalled 1.0 / u bit for
-// bit on 2^24 random u spanning 2^-998 .. 2^998 on a B200.  Shorter than a correctly
-// rounded division in the factorization's dependent chain; the factorization needs no correct
-// rounding (every vector's residual is checked), and |u| >= eps ||T|| keeps u normal.
-__device__ __forceinline__ double invit_recip(double u) {
-    double r;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(u));
-    double e = fma(-u, r, 1.0);
-    r = fma(r, e, r);
-    e = fma(-u, r, 1.0);
-    return fma(r, e, r);
-}
 // T - lam I = L U without pivoting (pivots below `tiny` raised to it): keeps 1/u_i.  Each step's
 // operands are loaded one step ahead, so the dependent chain is only the recurrence itself.
 __device__ __forceinline__ void invit_factor(int n, double lam, const double* __restrict__ dd,
@@ -916,7 +909,7 @@ __device__ __forceinline__ void invit_factor(int n, double lam, const double* __
     const int lane = threadIdx.x & 31;
     double u = dd[0] - lam;
     if (fabs(u) < tiny) u = copysign(tiny, u);
-    double iu = invit_recip(u);
+    double iu = recip_nr(u);
     SBG_IU(0) = iu;
     double dn = n > 1 ? dd[1] - lam : 0.0, en = n > 1 ? ee[0] * ee[0] : 0.0;
     for (int i = 1; i < n; ++i) {
@@ -924,7 +917,7 @@ __device__ __forceinline__ void invit_factor(int n, double lam, const double* __
         if (i + 1 < n) { dn = dd[i + 1] - lam; en = ee[i] * ee[i]; }
         u = fma(-e2, iu, di);
         if (fabs(u) < tiny) u = copysign(tiny, u);
-        iu = invit_recip(u);
+        iu = recip_nr(u);
         SBG_IU(i) = iu;
     }
 }
@@ -1135,7 +1128,7 @@ __global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspac
 
 template <int T, int G, int RM>
 __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_back(int mode, int n, int batch, Workspace ws,
-                                            double2* __restrict__ X, const int* __restrict__ info) {
+                                            double2* __restrict__ X, int* __restrict__ info) {
     const int b = blockIdx.x;
     if (b >= batch) return;
     const size_t mat = static_cast<size_t>(n) * n;
@@ -1173,7 +1166,7 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_back(int mode, int n, in
         y[r] = make_double2((valid && i < n) ? Zg[i + static_cast<size_t>(j) * n] : 0.0, 0.0);
     }
     for (int i = tid; i < n; i += T) tau_s[i] = ws.tau[static_cast<size_t>(n) * b + i];
-    wait_copies(bar, nullptr);
+    wait_copies(bar, info + b);
     for (int i = tid; i < n; i += T) invd[i] = 1.0 / LVs[i + i * ld].x;
     __syncthreads();              // also: every thread has read its Z before any X is written
     seg_apply_q<G, RM>(LVs, ld, tau_s, y, n, g);
@@ -1188,10 +1181,8 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_back(int mode, int n, in
 }
 
 template <class K>
-void set_max_smem_once(K kernel, std::once_flag& flag) {
-    std::call_once(flag, [&]() {
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem_optin());
-    });
+void set_max_smem_once(K kernel, SmemOptIn& rec) {
+    set_smem_limit(reinterpret_cast<const void*>(kernel), rec, max_smem_optin());
 }
 
 }  // namespace
@@ -1213,32 +1204,76 @@ size_t workspace_bytes_per_pair(int n) {
     return 16 * nn + 16 * n + 8 * n * 2 + 16 * cap + 4 * n + 4;
 }
 
+namespace {
+// Byte offsets of the workspace's seven regions from its base, each rounded up to 256 bytes.
+struct WorkspaceLayout {
+    size_t LV, tau, d, e, log, perm, flag, end;
+    int log_cap;
+    WorkspaceLayout(int n, int capacity) {
+        const size_t nn = static_cast<size_t>(n) * n, cap = static_cast<size_t>(capacity);
+        log_cap = ql_log_capacity(n);
+        size_t o = 0;
+        auto take = [&](size_t bytes) { const size_t q = o; o += align_up(bytes, 256); return q; };
+        LV = take(16 * nn * cap);
+        tau = take(16 * n * cap);
+        d = take(8 * n * cap);
+        e = take(8 * n * cap);
+        log = take(16 * static_cast<size_t>(log_cap) * cap);
+        perm = take(4 * n * cap);
+        flag = take(4 * cap);
+        end = o;
+    }
+};
+}  // namespace
+
+size_t workspace_bytes(int n, int capacity) { return WorkspaceLayout(n, capacity).end; }
+
 Workspace carve_workspace(void* base, int n, int capacity) {
+    const WorkspaceLayout lay(n, capacity);
+    char* p = static_cast<char*>(base);
     Workspace w;
     w.n = n;
     w.capacity = capacity;
-    const size_t nn = static_cast<size_t>(n) * n, cap = static_cast<size_t>(capacity);
-    char* p = static_cast<char*>(base);
-    auto take = [&](size_t bytes) { char* q = p; p += align_up(bytes, 256); return q; };
-    w.LV = reinterpret_cast<double2*>(take(16 * nn * cap));
-    w.tau = reinterpret_cast<double2*>(take(16 * n * cap));
-    w.d = reinterpret_cast<double*>(take(8 * n * cap));
-    w.e = reinterpret_cast<double*>(take(8 * n * cap));
-    w.log_cap = ql_log_capacity(n);
-    w.log = take(16 * static_cast<size_t>(w.log_cap) * cap);
-    w.perm = reinterpret_cast<int*>(take(4 * n * cap));
-    w.flag = reinterpret_cast<int*>(take(4 * cap));
+    w.LV = reinterpret_cast<double2*>(p + lay.LV);
+    w.tau = reinterpret_cast<double2*>(p + lay.tau);
+    w.d = reinterpret_cast<double*>(p + lay.d);
+    w.e = reinterpret_cast<double*>(p + lay.e);
+    w.log_cap = lay.log_cap;
+    w.log = p + lay.log;
+    w.perm = reinterpret_cast<int*>(p + lay.perm);
+    w.flag = reinterpret_cast<int*>(p + lay.flag);
     return w;
 }
 
 int max_smem_optin() {
-    static int value = [] {
-        int dev = 0, v = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        return v;
-    }();
-    return value;
+    // per device ordinal (devices can differ); 0 = not yet queried
+    static std::atomic<int> cache[SmemOptIn::kDevices];
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return 0; }
+    if (dev >= 0 && dev < SmemOptIn::kDevices && (v = cache[dev].load(std::memory_order_relaxed)) > 0) return v;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (dev >= 0 && dev < SmemOptIn::kDevices) cache[dev].store(v, std::memory_order_relaxed);
+    return v;
+}
+
+void set_smem_limit(const void* kernel, SmemOptIn& rec, int bytes) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) { cudaGetLastError(); return; }
+    const bool tracked = dev >= 0 && dev < SmemOptIn::kDevices;
+    if (tracked && rec.raised[dev].load(std::memory_order_acquire) >= bytes) return;
+    // Idempotent: two threads that race here both set the same limit.  A failure is left for
+    // the launch to report (it fails with the limit unraised).
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    if (!tracked) return;
+    int cur = rec.raised[dev].load(std::memory_order_relaxed);
+    while (cur < bytes && !rec.raised[dev].compare_exchange_weak(cur, bytes, std::memory_order_acq_rel)) {
+    }
 }
 
 size_t reduce_smem_bytes(int, int n) { return ReduceSmem(n).total; }
@@ -1256,23 +1291,23 @@ size_t back_smem_bytes(int n) { return BackSmem(n).total; }
 template <int T, int G, int RM>
 void run_reduce(int mode, const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* out,
                 int* info, size_t smem, cudaStream_t stream) {
-    static std::once_flag f;
+    static SmemOptIn f;
     set_max_smem_once(k_reduce<T, G, RM>, f);
     k_reduce<T, G, RM><<<batch, T, smem, stream>>>(mode, A, B, n, batch, ws, out, info);
 }
 
 template <int T, int G, int RM>
-void run_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info, size_t smem,
+void run_back(int mode, int n, int batch, const Workspace& ws, double2* X, int* info, size_t smem,
               cudaStream_t stream) {
-    static std::once_flag f;
+    static SmemOptIn f;
     set_max_smem_once(k_back<T, G, RM>, f);
     k_back<T, G, RM><<<batch, T, smem, stream>>>(mode, n, batch, ws, X, info);
 }
 
 template <int NMAX, bool EXACT = false>
-void run_hegst_col(int mode, const double2* A, const Workspace& ws, double2* out, int n, int batch, const int* info,
+void run_hegst_col(int mode, const double2* A, const Workspace& ws, double2* out, int n, int batch, int* info,
                    cudaStream_t stream) {
-    static std::once_flag f;
+    static SmemOptIn f;
     set_max_smem_once(k_hegst_col<NMAX, EXACT>, f);
     k_hegst_col<NMAX, EXACT><<<batch, NMAX, hegst_col_bytes(n), stream>>>(mode, A, ws, out, n, batch, info);
 }
@@ -1291,7 +1326,7 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
     // The two-kernel path hands L from k_potrf_warp to k_hegst_col through ws.LV, so it
     // needs a workspace (the staged Cholesky alone does not).
     if (n <= kColMaxN && mode != kReduceFromLM && (mode == kReduceChol || ws.LV != nullptr)) {
-        static std::once_flag fp;
+        static SmemOptIn fp;
         set_max_smem_once(k_potrf_warp, fp);
         const int grid = (batch + kPotrfWarpsPerCta - 1) / kPotrfWarpsPerCta;
         k_potrf_warp<<<grid, 32 * kPotrfWarpsPerCta, potrf_warp_bytes(n) * kPotrfWarpsPerCta, stream>>>(
@@ -1312,14 +1347,14 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
 
 size_t hetrd_smem_bytes(int n, int threads) { return HetrdSmem(n, threads).total; }
 
-cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, const int* info, int threads,
+cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, int* info, int threads,
                          cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!C || !info || !ws.LV || !ws.d || !ws.e || !ws.tau) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) return big_path(n) ? cudaSuccess : cudaErrorInvalidValue;   // done by the reduce kernel
     if (n <= kHetrdWarpMaxN) {
         const size_t smem = hetrd_warp_bytes(n) * kHetrdWarpsPerCta;
-        static std::once_flag fw;
+        static SmemOptIn fw;
         set_max_smem_once(k_hetrd_warp, fw);
         const int grid = (batch + kHetrdWarpsPerCta - 1) / kHetrdWarpsPerCta;
         k_hetrd_warp<<<grid, 32 * kHetrdWarpsPerCta, smem, stream>>>(n, batch, C, ws, info);
@@ -1327,7 +1362,7 @@ cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws
     }
     const size_t smem = hetrd_smem_bytes(n, threads == 128 ? 128 : 256);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
-    static std::once_flag f128, f256;
+    static SmemOptIn f128, f256;
     if (threads == 128) {
         set_max_smem_once(k_hetrd<128>, f128);
         k_hetrd<128><<<batch, 128, smem, stream>>>(n, batch, C, ws, info);
@@ -1355,7 +1390,7 @@ cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, in
     const size_t cs = ql_chain_smem_bytes(n, chain_threads, single);
     if (cs > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     const int cgrid = (batch + chain_threads - 1) / chain_threads;
-    static std::once_flag fcd, fcf;
+    static SmemOptIn fcd, fcf;
     if (single) {
         set_max_smem_once(k_ql_chain<float>, fcf);
         k_ql_chain<float><<<cgrid, chain_threads, cs, stream>>>(n, batch, ws, W, info, redo ? 1 : 0);
@@ -1374,7 +1409,7 @@ cudaError_t launch_eig_invit(int n, int batch, const Workspace& ws, double* W, d
     const size_t is = InvitSmem(n, !flag_redo).per_warp;
     if (vs > static_cast<size_t>(max_smem_optin()) || is > static_cast<size_t>(max_smem_optin()))
         return cudaErrorInvalidValue;
-    static std::once_flag fv, fi;
+    static SmemOptIn fv, fi;
     set_max_smem_once(k_ql_values, fv);
     set_max_smem_once(k_tridiag_invit, fi);
     k_ql_values<<<(batch + chain_threads - 1) / chain_threads, chain_threads, vs, stream>>>(n, batch, ws, W, info);
@@ -1404,7 +1439,7 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
         // one pair per CTA: ~150 registers a lane, so small CTAs pack the SM best
         const size_t rs = single ? ql_apply_reg_pair_bytes<float>(n) : ql_apply_reg_pair_bytes<double>(n);
         const int rgrid = batch, rthreads = 32 * ((n + 31) / 32);
-        static std::once_flag r32d, r32f;
+        static SmemOptIn r32d, r32f;
 #define SBG_RUN_REG(NM, R, FLAG)                                                                 \
         { set_max_smem_once(k_ql_apply_reg<NM, R>, FLAG);                                          \
           k_ql_apply_reg<NM, R><<<rgrid, rthreads, rs, stream>>>(n, batch, ws, W, X, info); }
@@ -1413,7 +1448,7 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
 #undef SBG_RUN_REG
         return cudaGetLastError();
     }
-    static std::once_flag fcd, fcf, fad, faf;
+    static SmemOptIn fcd, fcf, fad, faf;
     if (single) {
         set_max_smem_once(k_ql_chain<float>, fcf);
         set_max_smem_once(k_ql_apply<float>, faf);
@@ -1437,7 +1472,7 @@ cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* 
     if (rsmem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     cudaError_t err = launch_ql_logged(n, batch, ws, W, X, info, true, chain_threads, apply_warps, stream);
     if (err != cudaSuccess) return err;
-    static std::once_flag f128, f256;
+    static SmemOptIn f128, f256;
     if (refine_threads == 128) {
         set_max_smem_once(k_refine<128>, f128);
         k_refine<128><<<batch, 128, rsmem, stream>>>(n, batch, ws, W, X, info, refine_steps);
@@ -1449,9 +1484,9 @@ cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* 
 }
 
 template <int NMAX, int G, bool EXACT = false>
-void run_back_col_g(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info, size_t smem,
+void run_back_col_g(int mode, int n, int batch, const Workspace& ws, double2* X, int* info, size_t smem,
                     cudaStream_t stream) {
-    static std::once_flag f;
+    static SmemOptIn f;
     set_max_smem_once(k_back_col<NMAX, G, EXACT>, f);
     smem = BackSmem(n, (((NMAX | 1) & 7) == 7) ? (NMAX | 1) + 2 : (NMAX | 1)).total;
     k_back_col<NMAX, G, EXACT><<<batch, back_col_threads<NMAX, G>(), smem, stream>>>(mode, n, batch, ws, X, info);
@@ -1461,7 +1496,7 @@ void run_back_col_g(int mode, int n, int batch, const Workspace& ws, double2* X,
 // per SM) gives the same time as G = 1 (4 CTAs per SM); the per-lane chain halves but the
 // shuffles and the lower occupancy eat the gain.
 template <int NMAX>
-void run_back_col(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info, size_t smem,
+void run_back_col(int mode, int n, int batch, const Workspace& ws, double2* X, int* info, size_t smem,
                   cudaStream_t stream) {
     run_back_col_g<NMAX, 1>(mode, n, batch, ws, X, info, smem, stream);
 }
@@ -1505,7 +1540,7 @@ cudaError_t launch_pull_pairs(const double2* src, double2* dst, int count, int n
     return cudaGetLastError();
 }
 
-cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
+cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, int* info,
                         int /*threads*/, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
@@ -1521,6 +1556,46 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
         return cudaGetLastError();
     }
     SBG_DISPATCH_BY_N(n, run_back, mode, n, batch, ws, X, info, smem, stream);
+    return cudaGetLastError();
+}
+
+// Device self-test of recip_nr (the inverse iteration's reciprocal): r[i] = recip_nr(u[i]).
+__global__ void k_selftest_recip(const double* __restrict__ u, double* __restrict__ r, int count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) r[i] = recip_nr(u[i]);
+}
+
+cudaError_t launch_selftest_recip(const double* u, double* r, int count, cudaStream_t stream) {
+    if (count <= 0) return cudaSuccess;
+    const int blocks = std::min((count + 255) / 256, 148 * 8);
+    k_selftest_recip<<<blocks, 256, 0, stream>>>(u, r, count);
+    return cudaGetLastError();
+}
+
+// FP64 FMA throughput probe: every thread runs kFmaChains independent dependent chains of
+// fma(a, x, y) (x, y runtime values, so nothing folds) for `iters` rounds and stores their sum.
+// Flops = 2 * kFmaChains * iters * threads.  Enough independent chains per warp cover the FMA
+// latency, so the FP64 pipe, not the chain, bounds it.
+constexpr int kFmaChains = 8;
+__global__ void __launch_bounds__(256) k_selftest_fp64_fma(double* __restrict__ out, int iters, double x, double y) {
+    double a[kFmaChains];
+#pragma unroll
+    for (int c = 0; c < kFmaChains; ++c) a[c] = threadIdx.x * 1e-3 + c;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+            for (int c = 0; c < kFmaChains; ++c) a[c] = fma(a[c], x, y);
+        }
+    }
+    double sum = 0.0;
+#pragma unroll
+    for (int c = 0; c < kFmaChains; ++c) sum += a[c];
+    out[blockIdx.x * blockDim.x + threadIdx.x] = sum;
+}
+
+cudaError_t launch_selftest_fp64_fma(double* out, int blocks, int iters, cudaStream_t stream) {
+    if (blocks <= 0 || iters <= 0) return cudaErrorInvalidValue;
+    k_selftest_fp64_fma<<<blocks, 256, 0, stream>>>(out, iters, 0.999999, 1e-7);
     return cudaGetLastError();
 }
 

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstddef>
 
 namespace sbg {
@@ -38,8 +39,12 @@ struct Workspace {
 int ql_log_capacity(int n);
 
 size_t workspace_bytes_per_pair(int n);
-// Carves a Workspace for `capacity` pairs of size n out of `base` (256-byte aligned).
+// Carves a Workspace for `capacity` pairs of size n out of `base` (256-byte aligned).  Each of
+// its seven regions starts on a 256-byte boundary.
 Workspace carve_workspace(void* base, int n, int capacity);
+// Exact bytes carve_workspace(base, n, capacity) spans from base: every allocation that backs a
+// workspace is sized by this (at most workspace_bytes_per_pair(n) * capacity + 7 * 256).
+size_t workspace_bytes(int n, int capacity);
 
 enum ReduceMode : int {
     kReduceFull = 0,      // potrf + hegst          -> L into ws.LV (lower), C lower into out
@@ -57,7 +62,7 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
                           const Workspace& ws, double2* out, int* info, int threads, cudaStream_t stream);
 // Householder tridiagonalisation of C (lower triangle read, column-major, ld = n) ->
 // reflectors into ws.LV (rows above the superdiagonal), tau, d, e.  Pairs with info != 0 skip.
-cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, const int* info, int threads,
+cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, int* info, int threads,
                          cudaStream_t stream);
 size_t hetrd_smem_bytes(int n, int threads);
 // Two-kernel QL: thread-per-pair scalar chain logging rotations, then a warp-per-pair
@@ -72,7 +77,7 @@ cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* 
 // element or only rows j..n-1 of each column j (lower, for B, whose upper triangle no kernel
 // reads).  The kernel's loads cross the host link; one CTA per SM keeps enough of them in flight.
 cudaError_t launch_pull_pairs(const double2* src, double2* dst, int count, int n, bool lower, cudaStream_t stream);
-cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,
+cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, int* info,
                         int threads, cudaStream_t stream);
 
 // Pairs with n <= kSmallMaxN are solved by CTA-per-pair (or warp-per-pair) stage kernels;
@@ -125,6 +130,24 @@ size_t ql_chain_smem_bytes(int n, int threads, bool single);
 size_t ql_apply_smem_bytes(int n, int warps_per_cta, bool single);
 size_t back_smem_bytes(int n);
 size_t refine_smem_bytes(int n, int threads);
+// r[i] = recip_nr(u[i]) for i < count (device self-test of the inverse iteration's reciprocal).
+cudaError_t launch_selftest_recip(const double* u, double* r, int count, cudaStream_t stream);
+// FP64 FMA throughput probe: `blocks` CTAs of 256 threads, each thread 8 chains x 4 x iters FMAs;
+// out holds blocks * 256 doubles.
+cudaError_t launch_selftest_fp64_fma(double* out, int blocks, int iters, cudaStream_t stream);
+// Largest dynamic shared memory a block may opt into on the CURRENT device (queried once per
+// device ordinal; 0 if the query fails).
 int max_smem_optin();
+
+// Per-kernel record of the dynamic shared-memory limit raised on each device.
+// cudaFuncSetAttribute acts on the device current at the call, so one process that launches on
+// several GPUs has to raise it on each of them.  Ordinals beyond kDevices are raised every call.
+struct SmemOptIn {
+    static constexpr int kDevices = 64;
+    std::atomic<int> raised[kDevices] = {};
+};
+// Raises `kernel`'s dynamic shared-memory limit to `bytes` on the current device unless the
+// record shows it done there already.
+void set_smem_limit(const void* kernel, SmemOptIn& rec, int bytes);
 
 }  // namespace sbg

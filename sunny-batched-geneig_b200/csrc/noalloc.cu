@@ -13,7 +13,9 @@
 // Rules the implementation follows:
 //   * host code never hands the array's name to a kernel (on the host it is only a
 //     stand-in symbol, not a device address); the device address comes from
-//     cudaGetSymbolAddress, taken once per device with that device current and cached;
+//     cudaGetSymbolAddress, taken once per device with that device current and cached
+//     (so cudaDeviceReset of that device after the first call is not supported: the
+//     array moves with the new context and the cached address would dangle);
 //   * nothing in the scratch has to start at zero: every stage writes what the next
 //     one reads for every pair of the call, so the previous call's leftovers are
 //     harmless;
@@ -50,10 +52,14 @@ cudaError_t scratch_address(void** out) {
     return cudaSuccess;
 }
 
-// Bytes of scratch a batch needs: the per-pair workspace plus the 256-byte alignment
-// slack of its seven sub-arrays.
-size_t scratch_needed(int n, int batch) {
-    return sbg::workspace_bytes_per_pair(n) * static_cast<size_t>(batch) + 7 * 256;
+// Bytes of scratch a batch needs: exactly what carve_workspace spans.
+size_t scratch_needed(int n, int batch) { return sbg::workspace_bytes(n, batch); }
+
+// Largest batch of order n the fixed array holds.
+size_t max_pairs(int n) {
+    size_t p = (static_cast<size_t>(SBG_NOALLOC_SCRATCH_BYTES) - 7 * 256) / sbg::workspace_bytes_per_pair(n);
+    while (scratch_needed(n, static_cast<int>(p + 1)) <= static_cast<size_t>(SBG_NOALLOC_SCRATCH_BYTES)) ++p;
+    return p;
 }
 
 int fail(int status, const std::string& msg) {
@@ -75,13 +81,11 @@ extern "C" int sbg_geneig_full_noalloc_launch(int n, const cuDoubleComplex* d_A,
         return fail(SBG_ERR_UNSUPPORTED, "n = " + std::to_string(n) + " exceeds the supported maximum");
     const size_t need = scratch_needed(n, batch);
     if (need > static_cast<size_t>(SBG_NOALLOC_SCRATCH_BYTES)) {
-        const size_t per = sbg::workspace_bytes_per_pair(n);
-        const size_t max_pairs = (static_cast<size_t>(SBG_NOALLOC_SCRATCH_BYTES) - 7 * 256) / per;
         return fail(SBG_ERR_INVALID_VALUE,
                     "batch " + std::to_string(batch) + " at n = " + std::to_string(n) + " needs " +
                         std::to_string(need) + " bytes of scratch; the fixed no-allocation scratch holds " +
                         std::to_string(SBG_NOALLOC_SCRATCH_BYTES) + " bytes, i.e. at most " +
-                        std::to_string(max_pairs) + " pairs at this n (split the batch)");
+                        std::to_string(max_pairs(n)) + " pairs at this n (split the batch)");
     }
     void* base = nullptr;
     cudaError_t e = scratch_address(&base);

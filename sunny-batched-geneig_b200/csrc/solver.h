@@ -197,7 +197,7 @@ struct sbg_solver {
                 throw Error(SBG_ERR_CAPTURING, "workspace must grow while the stream is capturing; "
                                                "call sbg_solver_reserve before capture");
             if (s.ptr) { check_cuda(cudaFree(s.ptr), "cudaFree"); s.ptr = nullptr; s.capacity = 0; }
-            const size_t bytes = sbg::workspace_bytes_per_pair(n) * static_cast<size_t>(pairs) + 5 * 256;
+            const size_t bytes = sbg::workspace_bytes(n, pairs);
             check_cuda(cudaMalloc(&s.ptr, bytes), "cudaMalloc(workspace)");
             s.bytes = bytes;
             s.capacity = pairs;

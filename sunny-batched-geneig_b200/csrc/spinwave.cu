@@ -348,8 +348,9 @@ struct EntryLists {
     }
 };
 
-std::mutex g_assemble_attr_mu;
-size_t g_assemble_attr_bytes = 48 * 1024;
+// k_sw_assemble's dynamic shared-memory limit, raised per device to the largest bond table a
+// model on that device needs.
+sbg::SmemOptIn g_assemble_attr;
 
 void create_spinwave(int N, int nb, const int* sites, const double* coef, const double* disp, const double* pos,
                      double field, int device, sbg_spinwave** out) {
@@ -446,15 +447,8 @@ void create_spinwave(int N, int nb, const int* sites, const double* coef, const 
     T.nQ = static_cast<int>(Q.ent.size());
     check_cuda(cudaMemcpy(m->d_tables, host.data(), host.size(), cudaMemcpyHostToDevice), "H2D spin-wave tables");
     m->assemble_smem = smem;
-    {
-        // The attribute is per kernel: raise it to the largest bond table any model needs.
-        std::lock_guard<std::mutex> lock(g_assemble_attr_mu);
-        if (smem > g_assemble_attr_bytes) {
-            check_cuda(cudaFuncSetAttribute(k_sw_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            static_cast<int>(smem)), "cudaFuncSetAttribute");
-            g_assemble_attr_bytes = smem;
-        }
-    }
+    if (smem > 48 * 1024)      // the attribute is per kernel and device (this one is current)
+        sbg::set_smem_limit(reinterpret_cast<const void*>(k_sw_assemble), g_assemble_attr, static_cast<int>(smem));
     *out = m.release();
 }
 

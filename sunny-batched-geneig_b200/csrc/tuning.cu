@@ -199,7 +199,7 @@ struct Bench {
         : n(n_), precision(prec), count(count_), nn(static_cast<size_t>(n_) * n_),
           A(16 * nn * count_), B(16 * nn * count_), W(8 * static_cast<size_t>(n_) * count_), X(16 * nn * count_),
           Z(16 * nn * count_), info(4 * static_cast<size_t>(count_)),
-          wsbuf(workspace_bytes_per_pair(n_) * count_ + 5 * 256) {
+          wsbuf(workspace_bytes(n_, count_)) {
         cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
         ws = carve_workspace(wsbuf.p, n, count);
     }

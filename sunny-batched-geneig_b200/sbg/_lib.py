@@ -54,6 +54,9 @@ SIGNATURES = {
     "sbg_solver_enable_stage_timing": (I, [P, I]),
     "sbg_solver_read_stage_times": (I, [P, P, P]),
     "sbg_workspace_bytes_per_pair": (SZ, [I, I]),
+    "sbg_workspace_bytes": (SZ, [I, I, I]),
+    "sbg_selftest_reciprocal": (I, [P, P, I, P]),
+    "sbg_selftest_fp64_fma": (I, [P, I, I, P]),
     "sbg_solver_matrix_size": (I, [P]),
     "sbg_solver_batches_per_block": (I, [P]),
     "sbg_solver_block_dim_x": (I, [P]),

@@ -1,8 +1,9 @@
 """Distils the reference's GEIG v1 fixtures into the compact golden vectors kept here.
 
-Run in a checkout that has the reference tree (default /root/reference):
+Run in a checkout that has the reference tree (its location from --ref, else the
+SBG_REFERENCE_DIR environment variable, else oracle.reference_dir()'s default):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref DIR]
 
 Sources:
   * tests/data/n{16,32,48,54,64,96}_b8_s42_{random,nearid}.bin of the reference
@@ -43,7 +44,7 @@ def sha(a: np.ndarray) -> str:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=O.reference_dir())
     args = ap.parse_args()
     files = sorted(glob.glob(os.path.join(args.ref, "tests", "data", "*.bin")))
     entries = {}

@@ -8,8 +8,11 @@ of cudaMalloc/cudaFree.  Its scratch is a fixed array compiled into the library.
 These tests call it through the C ABI (ctypes) and compare it with the regular
 entry point, sbg_solver_launch, on the same inputs, for two calls in a row (the
 second call finds the first call's data still in the shared scratch), using the
-tolerances of the other parity tests.  The file is named so that pytest collects
-it last; it also runs on its own in a fresh process.
+tolerances of the other parity tests; check it against LAPACK zhegv directly at
+every kernel family it routes to (register-row n <= 32, warp / column kernels
+n <= 56, one CTA per pair for 85..160, clusters above 160); and check that a call
+leaves the device's free memory unchanged.  The file is named so that pytest
+collects it last; it also runs on its own in a fresh process.
 """
 from __future__ import annotations
 
@@ -65,8 +68,12 @@ def _scratch_bytes():
 
 
 def _max_pairs(n):
-    per = int(_lib.load().sbg_workspace_bytes_per_pair(n, 0))
-    return (_scratch_bytes() - 7 * 256) // per
+    lib = _lib.load()
+    per = int(lib.sbg_workspace_bytes_per_pair(n, 0))
+    p = (_scratch_bytes() - 7 * 256) // per
+    while int(lib.sbg_workspace_bytes(n, 0, p + 1)) <= _scratch_bytes():
+        p += 1
+    return p
 
 
 def test_noalloc_matches_regular_entry_point_two_calls():
@@ -95,3 +102,42 @@ def test_noalloc_rejects_batches_beyond_its_scratch():
     assert st == 1                                       # SBG_ERR_INVALID_VALUE
     msg = lib.sbg_last_error().decode()
     assert "scratch" in msg and str(_max_pairs(N)) in msg
+
+
+@pytest.mark.parametrize("N", [6, 16, 27, 48, 96])
+def test_noalloc_against_zhegv_every_kernel_family(N, oracle_mod):
+    """n = 12, 32, 54, 96, 192 against LAPACK zhegv with the parity gates, two calls in a row
+    with different pairs (the second finds the first's leftovers in the shared scratch)."""
+    from test_gpu_parity import check
+    n = 2 * N
+    batch = min(48 if n <= 96 else 8, _max_pairs(n))
+    for seed in (N, N + 1000):
+        A, B = wl.bogoliubov(N, batch, seed=seed)
+        st, W, X, info = _noalloc(A.cuda(), B.cuda(), n)
+        assert st == 0, _lib.load().sbg_last_error().decode()
+        torch.cuda.synchronize()
+        a, b = A.numpy(), B.numpy()
+        Wr, Xr, _ = oracle_mod.hegv(a, b, n, nthreads=8)
+        check(a, b, W.cpu().numpy(), X.cpu().numpy(), info.cpu().numpy(), Wr, Xr, n, relative=True)
+
+
+def test_noalloc_allocates_nothing():
+    """After one warm-up call (which may load the module and look up the scratch address),
+    further calls leave cudaMemGetInfo's free bytes exactly where they were."""
+    A, B = wl.bogoliubov(27, 64, seed=3)
+    dA, dB = A.cuda(), B.cuda()
+    st, W, X, info = _noalloc(dA, dB, N)
+    assert st == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    lib = _lib.load()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for _ in range(2):
+        st = lib.sbg_geneig_full_noalloc_launch(N, ctypes.c_void_p(dA.data_ptr()), ctypes.c_void_p(dB.data_ptr()),
+                                                ctypes.c_void_p(W.data_ptr()), ctypes.c_void_p(X.data_ptr()),
+                                                ctypes.c_void_p(info.data_ptr()), 64, stream)
+        assert st == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert (info.cpu().numpy() == 0).all()
