@@ -34,7 +34,7 @@ int supported_max_n(int precision) {
     const bool single = precision == SBG_PRECISION_MIXED;
     for (int n = 1; n <= sbg::kBigMaxN; ++n) {
         if (n > sbg::kSmallMaxN) {          // cluster kernels
-            if (single) break;              // the refinement kernel holds five n x n tiles: small n only
+            if (single) break;
             size_t need = std::max(sbg::big_reduce_smem_bytes(n), sbg::ql_rows_smem_bytes(n, false));
             need = std::max(need, sbg::ql_chain_smem_bytes(n, 32, false));
             if (sbg::big_path(n) && need <= lim) best = n;
@@ -42,9 +42,14 @@ int supported_max_n(int precision) {
         }
         size_t need = std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, n), sbg::back_smem_bytes(n));
         need = std::max(need, sbg::hetrd_smem_bytes(n, 128));
-        need = std::max(need, sbg::ql_apply_smem_bytes(n, 1, precision == SBG_PRECISION_MIXED));
-        need = std::max(need, sbg::ql_chain_smem_bytes(n, 32, precision == SBG_PRECISION_MIXED));
-        if (precision == SBG_PRECISION_MIXED) need = std::max(need, sbg::refine_smem_bytes(n, 128));
+        need = std::max(need, sbg::ql_apply_smem_bytes(n, 1, false));
+        need = std::max(need, sbg::ql_chain_smem_bytes(n, 32, false));
+        if (single) {                       // complex64 Householder + FP64 tensor-core refinement
+            if (n > sbg::kMixedMaxN) break;
+            need = std::max(need, sbg::refine_c_smem_bytes(n));
+            need = std::max(need, sbg::mixed_fallback_smem_bytes(n));
+            need = std::max(need, sbg::hetrd_c64_smem_bytes(n));
+        }
         if (need <= lim) best = n;
     }
     return best;

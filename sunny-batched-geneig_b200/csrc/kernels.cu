@@ -4,14 +4,16 @@
 //   reduce   k_potrf_warp + k_hegst_col (n <= 56) or k_reduce (57..84): B = L L^H and
 //            C = L^{-1} A L^{-H}; L into the workspace, C into the caller's X buffer.
 //   hetrd    k_hetrd_warp (n <= 65) or k_hetrd: Householder tridiagonalisation of C,
-//            reflectors and (d, e, tau) into the workspace.
+//            reflectors and (d, e, tau) into the workspace; the mixed form (n <= 56) runs it
+//            in complex64 (k_hetrd_warp_c64).
 //   eig      FP64, n <= 63 (and 85..128, launched from bigsolve.cu): k_ql_values (the
 //            implicit-QL recurrence, one thread per pair, eigenvalues only) and
 //            k_tridiag_invit (eigenvectors by inverse iteration, one warp per pair).
 //            Otherwise k_ql_chain logs the recurrence's rotations and k_ql_apply /
-//            k_ql_apply_reg replay the log onto Z (W ascending); the mixed form runs the
-//            recurrence in FP32 and refines with k_refine.
-//   back     k_back_col (n <= 56) or k_back: X = L^{-H} Q Z, written over Z.
+//            k_ql_apply_reg replay the log onto Z (W ascending).  The mixed form refines
+//            Y = Q Z against C afterwards (refine.cu).
+//   back     k_back_col (n <= 56) or k_back: X = L^{-H} Q Z, written over Z (the mixed
+//            form: Y = Q Z, then X = L^{-H} Y after the refinement).
 //
 // The split follows where the work is latency bound: the QL recurrence is a
 // dependent scalar chain per pair, so it runs with many pairs per SM, while the
@@ -347,18 +349,26 @@ __global__ void __launch_bounds__(back_col_threads<NMAX, G>(), G == 1 ? 4 : 3) k
     const bool own = col < n;
     const double* Zg = reinterpret_cast<const double*>(Xb);
     double2 y[RM];
+    if (mode == kBackLOnly) {                        // complex Y in the X buffer
 #pragma unroll
-    for (int r = 0; r < RM; ++r) {
-        const int i = G * r + g;
-        y[r] = make_double2((own && i < n) ? Zg[i + static_cast<size_t>(col) * n] : 0.0, 0.0);
+        for (int r = 0; r < RM; ++r) {
+            const int i = G * r + g;
+            y[r] = (own && i < n) ? Xb[i + static_cast<size_t>(col) * n] : make_double2(0.0, 0.0);
+        }
+    } else {                                         // real Z in the X buffer
+#pragma unroll
+        for (int r = 0; r < RM; ++r) {
+            const int i = G * r + g;
+            y[r] = make_double2((own && i < n) ? Zg[i + static_cast<size_t>(col) * n] : 0.0, 0.0);
+        }
     }
     for (int i = tid; i < n; i += T) tau_s[i] = ws.tau[static_cast<size_t>(n) * b + i];
     wait_copies(bar, info + b);
     for (int i = tid; i < n; i += T) invd[i] = 1.0 / LVs[i + i * ld].x;
     __syncthreads();               // all of Z is in registers before any X is stored over it
-    grp_apply_q<G, RM, double>(LVs, ld, tau_s, y, n, g);
+    if (mode != kBackLOnly) grp_apply_q<G, RM, double>(LVs, ld, tau_s, y, n, g);
     double2* xcol = Xb + static_cast<size_t>(col) * n;
-    if (mode == kBackFull) {
+    if (mode == kBackFull || mode == kBackLOnly) {
         grp_trsm_lowerH<G, RM>(LVs, ld, invd, y, n, g, [&](int k, double2 x) { if (own) xcol[k] = x; });
     } else if (own) {
 #pragma unroll
@@ -481,145 +491,84 @@ __global__ void __launch_bounds__(32 * kHetrdWarpsPerCta) k_hetrd_warp(int n, in
     }
 }
 
-// ----------------------------------------------------------------------------- k_refine
-// Mixed path, second half: FP64 Ogita-Aishima refinement of the FP32 tridiagonal
-// eigenpairs.  Reads Z (float, column-major) from the X region and (d, e) from
-// the workspace; writes the refined Z (double) over it and W.
-struct RefineSmem {
-    size_t Z0, Z1, TZ, Rm, Sm, d, e, lam, red, total;
-    __host__ __device__ RefineSmem(int n, int nwarps) {
-        const size_t tile = align_up(8 * static_cast<size_t>(n) * tile_ld(n), 16);
-        size_t o = 0;
-        Z0 = o; o += tile;
-        Z1 = o; o += tile;
-        TZ = o; o += tile;
-        Rm = o; o += tile;
-        Sm = o; o += tile;
-        d = o;  o += align_up(8 * n, 16);
-        e = o;  o += align_up(8 * n, 16);
-        lam = o; o += align_up(8 * n, 16);
-        red = o; o += 32 * nwarps;
-        total = o;
-    }
-};
+// ----------------------------------------------------------------------------- k_hetrd_warp_c64
+// Mixed form, Householder stage in complex64: one WARP per pair (n <= 65).  C's lower triangle
+// (FP64, in the X buffer) is rounded to complex64 into a packed tile (8 B per entry: 11.9 KB at
+// n = 54, half of k_hetrd_warp's, so twice the pairs fit an SM) and tridiagonalised by
+// hetrd_warp_packed<float>.  Outputs go where k_hetrd_warp puts them, promoted to FP64, so the
+// FP64 eigen- and back-transform kernels run on them unchanged: reflectors in LV's rows above the
+// superdiagonal, (d, e), and tau rescaled in FP64 so that each H = I - tau v v^H is unitary to
+// FP64 rounding for the promoted v (|tau|^2 ||v||^2 = 2 Re tau; the FP32 tau satisfies it only to
+// ~1e-7), which keeps the refinement's Y = Q Z orthonormal to the level of Z.  C itself (FP64) is
+// also written to the pair's stash in the refinement's tile format (refine_stash_entries), since
+// X, where the reduction left it, is overwritten before the refinement runs.
+__host__ __device__ inline size_t hetrd_c64_bytes(int n) {
+    return align_up(8 * static_cast<size_t>(n) * (n + 1) / 2, 16) + 8 * 2 * n + 2 * align_up(4 * n, 16) +
+           align_up(8 * n, 16) + 16;
+}
+constexpr int kHetrdC64WarpsPerCta = 2;
 
-template <int T>
-__global__ void __launch_bounds__(T) k_refine(int n, int batch, Workspace ws, double* __restrict__ W,
-                                              double2* __restrict__ X, int* __restrict__ info,
-                                              int max_steps) {
-    const int b = blockIdx.x;
+__device__ __forceinline__ double2* refine_stash(const Workspace& ws, int b) {
+    return reinterpret_cast<double2*>(static_cast<char*>(ws.log) + 16 * static_cast<size_t>(ws.log_stride) * b);
+}
+
+__global__ void __launch_bounds__(32 * kHetrdC64WarpsPerCta) k_hetrd_warp_c64(int n, int batch,
+                                                                              const double2* __restrict__ C,
+                                                                              Workspace ws, int* __restrict__ info) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * kHetrdC64WarpsPerCta + warp;
     if (b >= batch) return;
-    if (info[b] > n || info[b] < 0) return;          // B not positive definite: W already NaN
+    if (info[b] != 0) return;
     extern __shared__ __align__(16) unsigned char smem[];
-    const RefineSmem lay(n, T / 32);
-    const int ld = tile_ld(n), tid = threadIdx.x;
-    double* Za = reinterpret_cast<double*>(smem + lay.Z0);
-    double* Zb = reinterpret_cast<double*>(smem + lay.Z1);
-    double* TZ = reinterpret_cast<double*>(smem + lay.TZ);
-    double* Rm = reinterpret_cast<double*>(smem + lay.Rm);
-    double* Sm = reinterpret_cast<double*>(smem + lay.Sm);
-    double* dT = reinterpret_cast<double*>(smem + lay.d);
-    double* eT = reinterpret_cast<double*>(smem + lay.e);
-    double* lam = reinterpret_cast<double*>(smem + lay.lam);
-    double* red = reinterpret_cast<double*>(smem + lay.red);
+    unsigned char* base = smem + hetrd_c64_bytes(n) * warp;
+    float2* P = reinterpret_cast<float2*>(base);
+    float2* vb = reinterpret_cast<float2*>(base + align_up(8 * static_cast<size_t>(n) * (n + 1) / 2, 16));
+    float2* wb = vb + n;
+    float* d_s = reinterpret_cast<float*>(wb + n);
+    float* e_s = d_s + align_up(4 * n, 16) / 4;
+    float2* tau_s = reinterpret_cast<float2*>(e_s + align_up(4 * n, 16) / 4);
     const size_t mat = static_cast<size_t>(n) * n;
-    const float* Z32 = reinterpret_cast<const float*>(X + mat * b);
-    for (size_t idx = tid; idx < mat; idx += T) {
-        const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
-        Za[r + c * ld] = static_cast<double>(Z32[idx]);
-    }
-    for (int i = tid; i < n; i += T) {
-        dT[i] = ws.d[static_cast<size_t>(n) * b + i];
-        eT[i] = ws.e[static_cast<size_t>(n) * b + i];
-    }
-    __syncthreads();
-    // Full steps until the largest correction |E_ij| is <= 1e-8 (at least two), then one step that
-    // only orthogonalises pairs closer than 1e-2 ||T||_F (see oa_refine_step); max_steps counts
-    // them all.  Z + Z E is orthonormal only to second order in E, and the correction of
-    // eigenvalues at a relative distance of ~1e-5 is large late: the first step, while the FP32
-    // residual still exceeds their gap, treats them as a cluster, the next rotates them by ~1e-3,
-    // and a schedule that stopped there left X^H B X - I at ~1e-12 on 0.01-0.1 % of q-sweep
-    // pairs.  The correction of a converged pair stalls at ~eps ||T|| / gap instead of vanishing,
-    // which the final orthogonalising step absorbs.
-    for (int step = 0; step < max_steps; ++step) {
-        const bool last = step + 1 == max_steps;
-        const double em = oa_refine_step<2>(n, dT, eT, Za, ld, TZ, Rm, Sm, Zb, lam, red, last ? 1e-2 : 0.0);
-        double* t = Za; Za = Zb; Zb = t;
-        if (last) break;
-        if (step >= 1 && em <= 1e-8) {          // converged (em is the same on every thread)
-            oa_refine_step<2>(n, dT, eT, Za, ld, TZ, Rm, Sm, Zb, lam, red, 1e-2);
-            t = Za; Za = Zb; Zb = t;
-            break;
+    const double2* Cb = C + mat * b;
+    // stash: C full Hermitian, planar (re plane, then im plane), column-major, ld = LD, zero padded
+    const int NP = refine_np(n), LD = refine_ld(n);
+    double* sre = reinterpret_cast<double*>(refine_stash(ws, b));
+    double* sim = sre + static_cast<size_t>(NP) * LD;
+    for (int j = 0; j < NP; ++j) {
+        float2* col = P + pk(j, n) - j;
+        for (int i = j + lane; i < NP; i += 32) {
+            const bool in = i < n && j < n;
+            double2 v = in ? Cb[i + static_cast<size_t>(j) * n] : make_double2(0.0, 0.0);
+            if (i == j) v.y = 0.0;
+            if (in) col[i] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+            sre[j * LD + i] = v.x;
+            sim[j * LD + i] = v.y;
+            if (i != j) { sre[i * LD + j] = v.x; sim[i * LD + j] = -v.y; }
         }
     }
-    // Acceptance: every refined pair must satisfy ||T z - lam z|| <= 256 eps ||T||_F ||z||.  When the
-    // FP32 start was too coarse for the refinement to separate eigenvalues (e.g. small eigenvalues
-    // of a T with a wide spectrum: FP32 resolves them only to ~6e-8 ||T||), the pair is solved by
-    // the FP64 QL here instead.
-    double worst = 0.0, tn = 0.0;
-    for (int i = tid; i < n; i += T) tn = fma(dT[i], dT[i], (i + 1 < n) ? fma(2.0 * eT[i], eT[i], tn) : tn);
-    for (int c = tid; c < n; c += T) {
-        const double* z = Za + c * ld;
-        double r2 = 0.0, z2 = 0.0;
-        for (int i = 0; i < n; ++i) {
-            double v = (dT[i] - lam[c]) * z[i];
-            if (i > 0) v = fma(eT[i - 1], z[i - 1], v);
-            if (i + 1 < n) v = fma(eT[i], z[i + 1], v);
-            r2 = fma(v, v, r2);
-            z2 = fma(z[i], z[i], z2);
+    __syncwarp();
+    hetrd_warp_packed<float>(P, n, d_s, e_s, tau_s, vb, wb);
+    double2* LVg = ws.LV + mat * b;
+    for (int k = 0; k + 1 < n; ++k) {                    // LV(k, k+1) = v_k(k+1) = 1
+        const float2* col = P + pk(k, n) - k;            // col[i] = v_k(i), i >= k + 2
+        double s2 = 0.0;
+        for (int i = k + 1 + lane; i < n; i += 32) {
+            const double2 v = (i == k + 1) ? make_double2(1.0, 0.0)
+                                           : make_double2(static_cast<double>(col[i].x), static_cast<double>(col[i].y));
+            LVg[k + static_cast<size_t>(i) * n] = v;
+            s2 = fma(v.x, v.x, fma(v.y, v.y, s2));
         }
-        worst = fmax(worst, sqrt(r2 / fmax(z2, 1e-300)));
-    }
-    tn = warp_sum(tn);
-#pragma unroll
-    for (int m = 16; m >= 1; m >>= 1) worst = fmax(worst, shfl_xor(worst, m));
-    if ((tid & 31) == 0) { red[4 * (tid >> 5)] = tn; red[4 * (tid >> 5) + 1] = worst; }
-    __syncthreads();
-    double tnorm = 0.0, rmax = 0.0;
-    for (int w = 0; w < T / 32; ++w) { tnorm += red[4 * w]; rmax = fmax(rmax, red[4 * w + 1]); }
-    __syncthreads();
-    const bool fallback = !(rmax <= 256.0 * 1.1102230246251565e-16 * sqrt(tnorm));
-    if (fallback) {
-        // FP64 QL on (d, e) with Za read as a row-major tile (Za[r * ld + c] = Z(r, c))
-        for (int idx = tid; idx < n * ld; idx += T) Za[idx] = 0.0;
-        __syncthreads();
-        for (int i = tid; i < n; i += T) Za[i * ld + i] = 1.0;
-        __syncthreads();
-        if (tid < 32) {
-            const int unconv = tridiag_ql<double>(n, dT, eT, Za, ld);
-            if (tid == 0 && unconv) info[b] = unconv;
-        }
-        __syncthreads();
-        const size_t mat2 = static_cast<size_t>(n) * n;
-        double* Zg2 = reinterpret_cast<double*>(X + mat2 * b);
-        for (size_t idx = tid; idx < mat2; idx += T) {
-            const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
-            Zg2[idx] = Za[r * ld + c];
-        }
-        for (int i = tid; i < n; i += T) W[static_cast<size_t>(n) * b + i] = dT[i];
-        return;
-    }
-    // ascending order (the FP32 order can differ for near-equal eigenvalues)
-    if (tid == 0) {
-        for (int i = 0; i + 1 < n; ++i) {
-            int k = i;
-            for (int j = i + 1; j < n; ++j) if (lam[j] < lam[k]) k = j;
-            if (k != i) { const double t = lam[i]; lam[i] = lam[k]; lam[k] = t; }
-            reinterpret_cast<int*>(TZ)[i] = k;       // swap record
+        s2 = warp_sum(s2);
+        if (lane == 0) {
+            const double tr = tau_s[k].x, ti = tau_s[k].y, t2 = tr * tr + ti * ti;
+            const double sc = t2 > 0.0 ? 2.0 * tr / (t2 * s2) : 0.0;
+            ws.tau[static_cast<size_t>(n) * b + k] = make_double2(tr * sc, ti * sc);
         }
     }
-    __syncthreads();
-    for (int i = 0; i + 1 < n; ++i) {
-        const int k = reinterpret_cast<int*>(TZ)[i];
-        if (k != i) for (int r = tid; r < n; r += T) { const double t = Za[r + i * ld]; Za[r + i * ld] = Za[r + k * ld]; Za[r + k * ld] = t; }
-        __syncthreads();
+    for (int i = lane; i < n; i += 32) {
+        ws.d[static_cast<size_t>(n) * b + i] = d_s[i];
+        ws.e[static_cast<size_t>(n) * b + i] = (i + 1 < n) ? static_cast<double>(e_s[i]) : 0.0;
+        if (i + 1 == n) ws.tau[static_cast<size_t>(n) * b + i] = make_double2(0.0, 0.0);
     }
-    double* Zg = reinterpret_cast<double*>(X + mat * b);
-    for (size_t idx = tid; idx < mat; idx += T) {
-        const int c = static_cast<int>(idx / n), r = static_cast<int>(idx - static_cast<size_t>(c) * n);
-        Zg[idx] = Za[r + c * ld];
-    }
-    for (int i = tid; i < n; i += T) W[static_cast<size_t>(n) * b + i] = lam[i];
 }
 
 // ----------------------------------------------------------------------------- k_ql_chain
@@ -1200,7 +1149,8 @@ int ql_log_capacity(int n) {
 
 size_t workspace_bytes_per_pair(int n) {
     const size_t nn = static_cast<size_t>(n) * n;
-    const size_t cap = static_cast<size_t>((3 * n * n) / 2 + 8 * n + 16);    // the default (largest) capacity
+    // the default (largest) rotation-log capacity, or the mixed form's stash if that is larger
+    const size_t cap = static_cast<size_t>(std::max((3 * n * n) / 2 + 8 * n + 16, refine_stash_entries(n)));
     return 16 * nn + 16 * n + 8 * n * 2 + 16 * cap + 4 * n + 4;
 }
 
@@ -1208,17 +1158,18 @@ namespace {
 // Byte offsets of the workspace's seven regions from its base, each rounded up to 256 bytes.
 struct WorkspaceLayout {
     size_t LV, tau, d, e, log, perm, flag, end;
-    int log_cap;
+    int log_cap, log_stride;
     WorkspaceLayout(int n, int capacity) {
         const size_t nn = static_cast<size_t>(n) * n, cap = static_cast<size_t>(capacity);
         log_cap = ql_log_capacity(n);
+        log_stride = std::max(log_cap, refine_stash_entries(n));
         size_t o = 0;
         auto take = [&](size_t bytes) { const size_t q = o; o += align_up(bytes, 256); return q; };
         LV = take(16 * nn * cap);
         tau = take(16 * n * cap);
         d = take(8 * n * cap);
         e = take(8 * n * cap);
-        log = take(16 * static_cast<size_t>(log_cap) * cap);
+        log = take(16 * static_cast<size_t>(log_stride) * cap);
         perm = take(4 * n * cap);
         flag = take(4 * cap);
         end = o;
@@ -1239,6 +1190,7 @@ Workspace carve_workspace(void* base, int n, int capacity) {
     w.d = reinterpret_cast<double*>(p + lay.d);
     w.e = reinterpret_cast<double*>(p + lay.e);
     w.log_cap = lay.log_cap;
+    w.log_stride = lay.log_stride;
     w.log = p + lay.log;
     w.perm = reinterpret_cast<int*>(p + lay.perm);
     w.flag = reinterpret_cast<int*>(p + lay.flag);
@@ -1373,7 +1325,6 @@ cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws
     return cudaGetLastError();
 }
 
-size_t refine_smem_bytes(int n, int threads) { return RefineSmem(n, threads / 32).total; }
 
 size_t ql_chain_smem_bytes(int n, int threads, bool single) {
     return (single ? 4 : 8) * 2 * static_cast<size_t>(n) * threads;
@@ -1463,23 +1414,18 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
     return cudaGetLastError();
 }
 
-cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
-                                 int refine_steps, int chain_threads, int apply_warps, int refine_threads,
-                                 cudaStream_t stream) {
+size_t hetrd_c64_smem_bytes(int n) { return hetrd_c64_bytes(n) * kHetrdC64WarpsPerCta; }
+
+cudaError_t launch_hetrd_c64(int n, int batch, const double2* C, const Workspace& ws, int* info, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
-    if (n > kSmallMaxN) return cudaErrorInvalidValue;
-    const size_t rsmem = refine_smem_bytes(n, refine_threads);
-    if (rsmem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
-    cudaError_t err = launch_ql_logged(n, batch, ws, W, X, info, true, chain_threads, apply_warps, stream);
-    if (err != cudaSuccess) return err;
-    static SmemOptIn f128, f256;
-    if (refine_threads == 128) {
-        set_max_smem_once(k_refine<128>, f128);
-        k_refine<128><<<batch, 128, rsmem, stream>>>(n, batch, ws, W, X, info, refine_steps);
-    } else {
-        set_max_smem_once(k_refine<256>, f256);
-        k_refine<256><<<batch, 256, rsmem, stream>>>(n, batch, ws, W, X, info, refine_steps);
-    }
+    if (n < 1 || n > kMixedMaxN || !C || !info || !ws.LV || ws.log_stride < refine_stash_entries(n))
+        return cudaErrorInvalidValue;
+    const size_t smem = hetrd_c64_smem_bytes(n);
+    if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+    static SmemOptIn f;
+    set_max_smem_once(k_hetrd_warp_c64, f);
+    k_hetrd_warp_c64<<<(batch + kHetrdC64WarpsPerCta - 1) / kHetrdC64WarpsPerCta, 32 * kHetrdC64WarpsPerCta, smem,
+                       stream>>>(n, batch, C, ws, info);
     return cudaGetLastError();
 }
 
@@ -1544,6 +1490,7 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
                         int /*threads*/, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
+    if (mode == kBackLOnly && n > kColMaxN) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) return launch_back_big(mode, n, batch, ws, X, info, stream);
     const size_t smem = back_smem_bytes(n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;

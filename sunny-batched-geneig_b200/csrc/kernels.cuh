@@ -28,7 +28,8 @@ struct Workspace {
     void* log = nullptr;
     int* perm = nullptr;
     int* flag = nullptr;
-    int log_cap = 0;    // entries per pair
+    int log_cap = 0;    // entries per pair the QL may log
+    int log_stride = 0; // entries per pair of the log region (>= log_cap; the mixed form's stash lives there)
     int capacity = 0;   // pairs
     int n = 0;
 };
@@ -37,6 +38,15 @@ struct Workspace {
 // eigenvalue); pairs that need more fall back to the warp-per-pair QL.  The environment
 // variable SBG_QL_LOG_CAPACITY lowers it (a testing knob that forces the fallback).
 int ql_log_capacity(int n);
+
+// Mixed form: the FP64 refinement's tiles are n padded to a multiple of 8 (the FP64 MMA shape),
+// stored planar (re and im planes), column-major with leading dimension refine_ld(n) (which keeps
+// the MMA fragment loads free of bank conflicts).  Its copy of C (both planes, full Hermitian,
+// zero padding) is the pair's stash: refine_stash_entries(n) 16-byte entries of the log region.
+__host__ __device__ constexpr int refine_np(int n) { return (n + 7) / 8 * 8; }
+__host__ __device__ constexpr int refine_ld(int n) { return refine_np(n) + 4; }
+__host__ __device__ constexpr int refine_stash_entries(int n) { return refine_np(n) * refine_ld(n); }
+constexpr int kMixedMaxN = 56;
 
 size_t workspace_bytes_per_pair(int n);
 // Carves a Workspace for `capacity` pairs of size n out of `base` (256-byte aligned).  Each of
@@ -55,6 +65,7 @@ enum ReduceMode : int {
 enum BackMode : int {
     kBackFull = 0,        // X = L^{-H} Q Z
     kBackQOnly = 1,       // V = Q Z (eigenvectors of the reduced matrix)
+    kBackLOnly = 2,       // X = L^{-H} Y, Y complex in the X buffer (mixed form; n <= 56 only)
 };
 
 // Launchers (asynchronous on `stream`; return cudaSuccess or the launch error).
@@ -69,9 +80,22 @@ size_t hetrd_smem_bytes(int n, int threads);
 // application of the log to Z (single = FP32 chain and Z, the mixed form's first half).
 cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
                              bool single, int chain_threads, int apply_warps, cudaStream_t stream);
-cudaError_t launch_tridiag_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
-                                 int refine_steps, int chain_threads, int apply_warps, int refine_threads,
-                                 cudaStream_t stream);
+// Mixed form (n <= kMixedMaxN), after the FP64 reduction left C in X:
+//   launch_hetrd_c64     complex64 Householder (warp per pair); FP64-promoted reflectors, tau (made
+//                        unitary in FP64) and T into the workspace, C into the pair's stash;
+//   launch_eig_mixed     eigenpairs of that T (launch_eig_invit, FP64), Y = Q Z
+//                        (launch_back(kBackQOnly)), then launch_refine_mixed: FP64 Ogita-Aishima
+//                        refinement of (W, Y) against the stashed C on the FP64 tensor cores, and
+//                        the FP64 fallback for pairs it cannot take;
+//   launch_back(kBackLOnly)  X = L^{-H} Y.
+cudaError_t launch_hetrd_c64(int n, int batch, const double2* C, const Workspace& ws, int* info, cudaStream_t stream);
+cudaError_t launch_refine_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                                int refine_steps, cudaStream_t stream);
+cudaError_t launch_eig_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                             int refine_steps, int chain_threads, cudaStream_t stream);
+size_t hetrd_c64_smem_bytes(int n);
+size_t refine_c_smem_bytes(int n);
+size_t mixed_fallback_smem_bytes(int n);
 // Host-buffer path: copies `count` pairs of n x n column-major matrices from pinned host memory
 // that the GPU can address (src is its device-side address) into device memory, either every
 // element or only rows j..n-1 of each column j (lower, for B, whose upper triangle no kernel
@@ -116,7 +140,7 @@ inline bool eig_by_inverse_iteration(int n, bool single) {
 }
 // Kernels one eigensolve stage launches for order n.
 inline int eig_kernel_count(int n, bool single) {
-    if (single) return 3;
+    if (single) return 5;          // k_ql_values, k_tridiag_invit, Q-apply, refinement, fallback
     if (n <= kInvitMaxN) return 2;
     return n > kSmallMaxN && n <= kInvitBigMaxN ? 4 : 2;
 }
@@ -129,7 +153,6 @@ size_t reduce_smem_bytes(int mode, int n);
 size_t ql_chain_smem_bytes(int n, int threads, bool single);
 size_t ql_apply_smem_bytes(int n, int warps_per_cta, bool single);
 size_t back_smem_bytes(int n);
-size_t refine_smem_bytes(int n, int threads);
 // r[i] = recip_nr(u[i]) for i < count (device self-test of the inverse iteration's reciprocal).
 cudaError_t launch_selftest_recip(const double* u, double* r, int count, cudaStream_t stream);
 // FP64 FMA throughput probe: `blocks` CTAs of 256 threads, each thread 8 chains x 4 x iters FMAs;

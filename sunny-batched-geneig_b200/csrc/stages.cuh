@@ -280,148 +280,6 @@ __device__ int tridiag_ql(int n, R* d, R* e, R* Z, int ldz) {
     return unconverged;
 }
 
-// ============================================================================ Ogita-Aishima refinement
-// One refinement step for the eigen-decomposition of the real symmetric
-// tridiagonal T = tridiag(e, d, e) from an approximate eigenvector matrix Z
-// (column-major tile, ld), following Ogita & Aishima, "Iterative refinement for
-// symmetric eigenvalue decomposition" (Japan J. Indust. Appl. Math. 35, 2018),
-// Algorithm 1:
-//   R = I - Z^T Z,  S = Z^T T Z,  lam_i = S_ii / (1 - R_ii),
-//   delta = 2 (||S - diag(lam)|| + ||T|| ||R||)  (Frobenius norms bound the 2-norms),
-//   E_ij = (S_ij + lam_j R_ij) / (lam_j - lam_i)  if |lam_i - lam_j| > delta, else R_ij / 2,
-//   Z' = Z + Z E.
-// Every product runs in FP64.  TZ, Rm, Sm are n x n scratch tiles (same ld);
-// Znew receives Z'.  red is 4 doubles of scratch per warp.  Returns
-// max_{i != j} |E_ij| (the size of the correction), identical on every thread.
-// floor_rel > 0 raises delta to at least floor_rel ||T||_F: pairs closer than that are
-// then only orthogonalised (E_ij = R_ij / 2).  The formula's division by the gap turns
-// the O(eps ||T||) rounding of S_ij into an O(eps ||T|| / gap) error of E_ij, which
-// breaks the orthogonality of nearly degenerate pairs; their directions are already
-// accurate to that level, so a final step with the floor restores Z^T Z = I to O(R^2)
-// and keeps the residual at O(eps ||T||).
-template <int TB>
-__device__ double oa_refine_step(int n, const double* dT, const double* eT, const double* Z, int ld,
-                                 double* TZ, double* Rm, double* Sm, double* Znew, double* lam,
-                                 double* red, double floor_rel) {
-    const int tid = threadIdx.x, T = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = T >> 5;
-    // TZ = T Z
-    for (int idx = tid; idx < n * n; idx += T) {
-        const int j = idx / n, i = idx - j * n;
-        const double* z = Z + j * ld;
-        double v = dT[i] * z[i];
-        if (i > 0) v = fma(eT[i - 1], z[i - 1], v);
-        if (i + 1 < n) v = fma(eT[i], z[i + 1], v);
-        TZ[i + j * ld] = v;
-    }
-    __syncthreads();
-    // Rm = I - Z^T Z, Sm = Z^T (T Z): TB x TB register tiles
-    const int nb = (n + TB - 1) / TB;
-    for (int blk = tid; blk < nb * nb; blk += T) {
-        const int bj = blk / nb, bi = blk - bj * nb;
-        double r[TB][TB], sacc[TB][TB];
-#pragma unroll
-        for (int a = 0; a < TB; ++a)
-#pragma unroll
-            for (int c = 0; c < TB; ++c) { r[a][c] = 0.0; sacc[a][c] = 0.0; }
-        int ci[TB], cj[TB];
-#pragma unroll
-        for (int a = 0; a < TB; ++a) { ci[a] = min(bi * TB + a, n - 1); cj[a] = min(bj * TB + a, n - 1); }
-        for (int k = 0; k < n; ++k) {
-            double zi[TB], zj[TB], tj[TB];
-#pragma unroll
-            for (int a = 0; a < TB; ++a) { zi[a] = Z[k + ci[a] * ld]; zj[a] = Z[k + cj[a] * ld]; tj[a] = TZ[k + cj[a] * ld]; }
-#pragma unroll
-            for (int a = 0; a < TB; ++a)
-#pragma unroll
-                for (int c = 0; c < TB; ++c) { r[a][c] = fma(zi[a], zj[c], r[a][c]); sacc[a][c] = fma(zi[a], tj[c], sacc[a][c]); }
-        }
-#pragma unroll
-        for (int a = 0; a < TB; ++a)
-#pragma unroll
-            for (int c = 0; c < TB; ++c) {
-                const int i = bi * TB + a, j = bj * TB + c;
-                if (i < n && j < n) {
-                    Rm[i + j * ld] = (i == j ? 1.0 : 0.0) - r[a][c];
-                    Sm[i + j * ld] = sacc[a][c];
-                }
-            }
-    }
-    __syncthreads();
-    for (int i = tid; i < n; i += T) lam[i] = Sm[i + i * ld] / (1.0 - Rm[i + i * ld]);
-    // Frobenius norms of S - diag(lam), R and T
-    double s_off = 0.0, r_n = 0.0, t_n = 0.0;
-    for (int idx = tid; idx < n * n; idx += T) {
-        const int j = idx / n, i = idx - j * n;
-        const double sv = Sm[i + j * ld], rv = Rm[i + j * ld];
-        if (i != j) s_off = fma(sv, sv, s_off);
-        r_n = fma(rv, rv, r_n);
-    }
-    for (int i = tid; i < n; i += T) {
-        t_n = fma(dT[i], dT[i], t_n);
-        if (i + 1 < n) t_n = fma(2.0 * eT[i], eT[i], t_n);
-    }
-    __syncthreads();
-    for (int i = tid; i < n; i += T) {
-        const double dv = Sm[i + i * ld] - lam[i];
-        s_off = fma(dv, dv, s_off);
-    }
-    s_off = warp_sum(s_off); r_n = warp_sum(r_n); t_n = warp_sum(t_n);
-    if (lane == 0) { red[4 * warp] = s_off; red[4 * warp + 1] = r_n; red[4 * warp + 2] = t_n; }
-    __syncthreads();
-    double S2 = 0.0, R2 = 0.0, T2 = 0.0;
-    for (int w = 0; w < nw; ++w) { S2 += red[4 * w]; R2 += red[4 * w + 1]; T2 += red[4 * w + 2]; }
-    const double delta = fmax(2.0 * (sqrt(S2) + sqrt(T2) * sqrt(R2)), floor_rel * sqrt(T2));
-    // E (over Sm)
-    double emax = 0.0;
-    for (int idx = tid; idx < n * n; idx += T) {
-        const int j = idx / n, i = idx - j * n;
-        const double rij = Rm[i + j * ld];
-        double eij;
-        const double gap = lam[j] - lam[i];
-        if (i != j && fabs(gap) > delta) eij = (Sm[i + j * ld] + lam[j] * rij) / gap;
-        else eij = 0.5 * rij;
-        if (i != j) emax = fmax(emax, fabs(eij));
-        TZ[i + j * ld] = eij;                  // E kept in TZ (T Z is no longer needed)
-    }
-    __syncthreads();
-    // Znew = Z + Z E
-    for (int blk = tid; blk < nb * nb; blk += T) {
-        const int bj = blk / nb, bi = blk - bj * nb;
-        double acc[TB][TB];
-        int ri[TB], cj[TB];
-#pragma unroll
-        for (int a = 0; a < TB; ++a) { ri[a] = min(bi * TB + a, n - 1); cj[a] = min(bj * TB + a, n - 1); }
-#pragma unroll
-        for (int a = 0; a < TB; ++a)
-#pragma unroll
-            for (int c = 0; c < TB; ++c) acc[a][c] = Z[ri[a] + cj[c] * ld];
-        for (int k = 0; k < n; ++k) {
-            double zr[TB], ek[TB];
-#pragma unroll
-            for (int a = 0; a < TB; ++a) { zr[a] = Z[ri[a] + k * ld]; ek[a] = TZ[k + cj[a] * ld]; }
-#pragma unroll
-            for (int a = 0; a < TB; ++a)
-#pragma unroll
-                for (int c = 0; c < TB; ++c) acc[a][c] = fma(zr[a], ek[c], acc[a][c]);
-        }
-#pragma unroll
-        for (int a = 0; a < TB; ++a)
-#pragma unroll
-            for (int c = 0; c < TB; ++c) {
-                const int i = bi * TB + a, j = bj * TB + c;
-                if (i < n && j < n) Znew[i + j * ld] = acc[a][c];
-            }
-    }
-#pragma unroll
-    for (int m = 16; m >= 1; m >>= 1) emax = fmax(emax, shfl_xor(emax, m));
-    if (lane == 0) red[4 * warp + 3] = emax;
-    __syncthreads();
-    double em = 0.0;
-    for (int w = 0; w < nw; ++w) em = fmax(em, red[4 * w + 3]);
-    __syncthreads();
-    return em;
-}
-
 // ============================================================================ QL, scalar chain only
 // The same implicit QL as tridiag_ql, run by ONE thread for one pair, with d and
 // e in shared memory interleaved over the CTA (element i of thread t at

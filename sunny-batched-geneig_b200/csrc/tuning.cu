@@ -40,10 +40,12 @@ bool fits(int n, int precision, const Schedule& s) {
                ql_chain_smem_bytes(n, s.chain_threads, false) <= lim;
     }
     if (reduce_smem_bytes(kReduceFull, n) > lim || back_smem_bytes(n) > lim || hetrd_smem_bytes(n, s.hetrd_threads) > lim) return false;
-    const bool single = precision == SBG_PRECISION_MIXED;
-    if (ql_chain_smem_bytes(n, s.chain_threads, single) > lim) return false;
-    if (ql_apply_smem_bytes(n, s.ql_warps, single) > lim) return false;
-    if (precision == SBG_PRECISION_MIXED && refine_smem_bytes(n, s.refine_threads) > lim) return false;
+    if (ql_chain_smem_bytes(n, s.chain_threads, false) > lim) return false;
+    if (ql_apply_smem_bytes(n, s.ql_warps, false) > lim) return false;
+    if (precision == SBG_PRECISION_MIXED &&
+        (n > kMixedMaxN || refine_c_smem_bytes(n) > lim || mixed_fallback_smem_bytes(n) > lim ||
+         hetrd_c64_smem_bytes(n) > lim))
+        return false;
     return true;
 }
 
@@ -210,17 +212,19 @@ struct Bench {
     double* w() { return static_cast<double*>(W.p); }
     double2* x() { return static_cast<double2*>(X.p); }
     int* inf() { return static_cast<int*>(info.p); }
+    bool mixed() const { return precision == SBG_PRECISION_MIXED; }
     void eig(const Schedule& s) {
-        if (precision == SBG_PRECISION_MIXED)
-            launch_tridiag_mixed(n, count, ws, w(), x(), inf(), 3, s.chain_threads, s.ql_warps, s.refine_threads, st);
+        if (mixed())
+            launch_eig_mixed(n, count, ws, w(), x(), inf(), 5, s.chain_threads, st);
         else
             launch_ql_logged(n, count, ws, w(), x(), inf(), false, s.chain_threads, s.ql_warps, st);
     }
     void full(const Schedule& s) {
         launch_reduce(kReduceFull, a(), b(), n, count, ws, x(), inf(), s.reduce_threads, st);
-        launch_hetrd(n, count, x(), ws, inf(), s.hetrd_threads, st);
+        if (mixed()) launch_hetrd_c64(n, count, x(), ws, inf(), st);
+        else launch_hetrd(n, count, x(), ws, inf(), s.hetrd_threads, st);
         eig(s);
-        launch_back(kBackFull, n, count, ws, x(), inf(), s.back_threads, st);
+        launch_back(mixed() ? kBackLOnly : kBackFull, n, count, ws, x(), inf(), s.back_threads, st);
     }
 };
 

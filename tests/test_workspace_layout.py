@@ -13,9 +13,11 @@ def _align(x, a=256):
 
 def carve_end(n, pairs):
     """End of the last region: LV (n*n complex), tau (n complex), d, e (n real), the QL rotation
-    log ((3n^2)/2 + 8n + 16 entries of 16 B), perm (n int), flag (1 int), per pair, each region
-    rounded up to 256 bytes."""
-    cap = (3 * n * n) // 2 + 8 * n + 16
+    log ((3n^2)/2 + 8n + 16 entries of 16 B, or the mixed form's stash of C, NP (NP + 4) entries
+    with NP = n rounded up to a multiple of 8, if that is larger), perm (n int), flag (1 int), per
+    pair, each region rounded up to 256 bytes."""
+    np_ = (n + 7) // 8 * 8
+    cap = max((3 * n * n) // 2 + 8 * n + 16, np_ * (np_ + 4))
     regions = [16 * n * n * pairs, 16 * n * pairs, 8 * n * pairs, 8 * n * pairs, 16 * cap * pairs,
                4 * n * pairs, 4 * pairs]
     return sum(_align(r) for r in regions)
