@@ -107,8 +107,10 @@ enum { SBG_CACHE_AUTO = 0, SBG_CACHE_NO_DISK = 1, SBG_CACHE_NONE = 2 }; /* Cache
 enum { SBG_PRECISION_FP64 = 0, SBG_PRECISION_MIXED = 1 };
 
 typedef struct {
-    int batches_per_block;    /* pairs per CTA of the QL stage; 0 = auto (ctor arg, hpp:99) */
-    int force_block_dim_x;    /* threads per CTA of the reduce/back stages; 0 = auto (hpp:100) */
+    int batches_per_block;    /* pairs per CTA; 0 = auto (ctor arg, hpp:99): of the warp-per-pair Cholesky and
+                                 Householder kernels for n <= 65 (1, 2 or 4), of the QL rotation stage above */
+    int force_block_dim_x;    /* threads per CTA of the CTA-per-pair Householder (66 <= n <= 84): 128 or 256;
+                                 0 = auto (hpp:100) */
     int tuning_mode;          /* SBG_TUNING_*  (hpp:101) */
     int cache_mode;           /* SBG_CACHE_*   (hpp:102) */
     int precision;            /* SBG_PRECISION_FP64 (plain drop-in) or SBG_PRECISION_MIXED */
@@ -171,6 +173,16 @@ size_t sbg_workspace_bytes_per_pair(int n, int precision);
  * per-pair bytes times pairs plus the 256-byte alignment of its seven regions (at most
  * 7 * 256 bytes more). */
 size_t sbg_workspace_bytes(int n, int precision, int pairs);
+
+/* The solver's schedule as six ints (no counterpart in the reference, whose schedule is its
+ * (batches per block, block size) pair): [0] threads per CTA of the CTA-per-pair Householder,
+ * [1] pairs per CTA of the warp-per-pair Cholesky / Householder kernels, [2] 1 = the exact-n
+ * column kernels where they exist (n = 32, 54), [3] lanes per column of the column back-transform
+ * (1 or 2), [4] pairs per CTA of the QL rotation stage, [5] pairs per CTA of the QL scalar
+ * chain.  set_schedule replaces it (values checked against their ranges and the device's shared
+ * memory; SBG_ERR_INVALID_VALUE otherwise), for callers that tune outside the library. */
+int sbg_solver_schedule(const sbg_solver* s, int* out6);
+int sbg_solver_set_schedule(sbg_solver* s, const int* in6);
 
 /* Getters (nvrtc_solver.hpp:128-145). */
 int sbg_solver_matrix_size(const sbg_solver* s);

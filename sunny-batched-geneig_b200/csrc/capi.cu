@@ -84,7 +84,7 @@ void sbgi::create_solver(int n, int device, const sbg_solver_options* o, sbg_sol
     req.device = device;
     req.precision = opts.precision;
     req.force_threads = opts.force_block_dim_x;
-    req.force_ql_warps = opts.batches_per_block;
+    req.force_bpb = opts.batches_per_block;
     req.autotune = opts.tuning_mode == SBG_TUNING_AUTOTUNE;
     req.cache_mode = opts.cache_mode;
     sbg::TuneResult tr = sbg::select_schedule(req);
@@ -264,8 +264,44 @@ size_t sbg_workspace_bytes(int n, int /*precision*/, int pairs) {
 }
 
 int sbg_solver_matrix_size(const sbg_solver* s) { return s ? s->n : 0; }
-int sbg_solver_batches_per_block(const sbg_solver* s) { return s ? s->sched.ql_warps : 0; }
-int sbg_solver_block_dim_x(const sbg_solver* s) { return s ? s->sched.reduce_threads : 0; }
+int sbg_solver_schedule(const sbg_solver* s, int* out6) {
+    return guarded([&] {
+        if (!s || !out6) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
+        const sbg::Schedule& c = s->sched;
+        const int v[6] = {c.hetrd_threads, c.pair_warps, c.col_exact, c.back_lanes, c.ql_warps, c.chain_threads};
+        for (int i = 0; i < 6; ++i) out6[i] = v[i];
+    });
+}
+
+int sbg_solver_set_schedule(sbg_solver* s, const int* in6) {
+    return guarded([&] {
+        if (!s || !in6) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
+        sbg::Schedule c;
+        c.hetrd_threads = in6[0];
+        c.pair_warps = in6[1];
+        c.col_exact = in6[2];
+        c.back_lanes = in6[3];
+        c.ql_warps = in6[4];
+        c.chain_threads = in6[5];
+        const bool ok = (c.hetrd_threads == 128 || c.hetrd_threads == 256) &&
+                        (c.pair_warps == 1 || c.pair_warps == 2 || c.pair_warps == 4) &&
+                        (c.col_exact == 0 || c.col_exact == 1) && (c.back_lanes == 1 || c.back_lanes == 2) &&
+                        c.ql_warps >= 1 && c.ql_warps <= 16 &&
+                        (c.chain_threads == 32 || c.chain_threads == 64 || c.chain_threads == 128 ||
+                         c.chain_threads == 256);
+        if (!ok) throw Error(SBG_ERR_INVALID_VALUE, "schedule value out of range");
+        DeviceGuard g(s->device);
+        if (!sbg::schedule_fits(s->n, s->precision, c))
+            throw Error(SBG_ERR_INVALID_VALUE, "schedule exceeds the device's shared memory for this n");
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->sched = c;
+    });
+}
+
+int sbg_solver_batches_per_block(const sbg_solver* s) {
+    return s ? (s->n <= 65 ? s->sched.pair_warps : s->sched.ql_warps) : 0;
+}
+int sbg_solver_block_dim_x(const sbg_solver* s) { return s ? s->sched.hetrd_threads : 0; }
 unsigned int sbg_solver_shared_mem_bytes(const sbg_solver* s) {
     if (!s) return 0;
     size_t m = std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, s->n), sbg::back_smem_bytes(s->n));
@@ -304,7 +340,7 @@ void geneig_full_n54_batched_launch(const cuDoubleComplex* d_H, const cuDoubleCo
         default_n54_solver()->launch(c2(d_H), c2(d_S), d_W, c2(d_U), d_info, batch_size, stream);
     }));
 }
-unsigned int geneig_full_n54_batched_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads; }
+unsigned int geneig_full_n54_batched_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).hetrd_threads; }
 unsigned int geneig_full_n54_batched_shared_mem_bytes(void) {
     return static_cast<unsigned>(std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, 54), sbg::back_smem_bytes(54)));
 }
@@ -313,11 +349,11 @@ void chol_n54_launch(const cuDoubleComplex* d_S, cuDoubleComplex* d_L, int* d_in
     report_void(guarded([&] {
         sbg::Workspace none;
         check_cuda(sbg::launch_reduce(sbg::kReduceChol, nullptr, c2(d_S), 54, 1, none, c2(d_L), d_info,
-                                      sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads, stream),
+                                      sbg::default_schedule(54, SBG_PRECISION_FP64).shape(), stream),
                    "chol kernel");
     }));
 }
-unsigned int chol_n54_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads; }
+unsigned int chol_n54_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).hetrd_threads; }
 unsigned int chol_n54_shared_mem_bytes(void) { return static_cast<unsigned>(sbg::reduce_smem_bytes(sbg::kReduceChol, 54)); }
 
 void geneig_reduce_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComplex* d_S, cuDoubleComplex* d_M,
@@ -325,11 +361,11 @@ void geneig_reduce_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComplex*
     report_void(guarded([&] {
         sbg::Workspace none;
         check_cuda(sbg::launch_reduce(sbg::kReduceHegst, c2(d_H), c2(d_S), 54, 1, none, c2(d_M), d_info,
-                                      sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads, stream),
+                                      sbg::default_schedule(54, SBG_PRECISION_FP64).shape(), stream),
                    "reduce kernel");
     }));
 }
-unsigned int geneig_reduce_n54_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads; }
+unsigned int geneig_reduce_n54_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).hetrd_threads; }
 unsigned int geneig_reduce_n54_shared_mem_bytes(void) { return static_cast<unsigned>(sbg::reduce_smem_bytes(sbg::kReduceHegst, 54)); }
 
 void geneig_reduce_eig_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComplex* d_S, double* d_W,
@@ -338,15 +374,15 @@ void geneig_reduce_eig_n54_launch(const cuDoubleComplex* d_H, const cuDoubleComp
         sbg_solver* s = default_n54_solver();
         sbg::Workspace ws = s->workspace(0, 1, stream);
         check_cuda(sbg::launch_reduce(sbg::kReduceFull, c2(d_H), c2(d_S), 54, 1, ws, c2(d_V), d_info,
-                                      s->sched.reduce_threads, stream), "reduce kernel");
-        check_cuda(sbg::launch_hetrd(54, 1, c2(d_V), ws, d_info, s->sched.hetrd_threads, stream), "hetrd kernel");
+                                      s->sched.shape(), stream), "reduce kernel");
+        check_cuda(sbg::launch_hetrd(54, 1, c2(d_V), ws, d_info, s->sched.shape(), stream), "hetrd kernel");
         check_cuda(sbg::launch_ql_logged(54, 1, ws, d_W, c2(d_V), d_info, false, s->sched.chain_threads,
                                          s->sched.ql_warps, stream), "QL kernels");
-        check_cuda(sbg::launch_back(sbg::kBackQOnly, 54, 1, ws, c2(d_V), d_info, s->sched.back_threads, stream),
+        check_cuda(sbg::launch_back(sbg::kBackQOnly, 54, 1, ws, c2(d_V), d_info, s->sched.shape(), stream),
                    "back kernel");
     }));
 }
-unsigned int geneig_reduce_eig_n54_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).reduce_threads; }
+unsigned int geneig_reduce_eig_n54_block_dim_x(void) { return sbg::default_schedule(54, SBG_PRECISION_FP64).hetrd_threads; }
 unsigned int geneig_reduce_eig_n54_shared_mem_bytes(void) { return geneig_full_n54_batched_shared_mem_bytes(); }
 unsigned int geneig_reduce_eig_n54_chol_smem_bytes(void) { return static_cast<unsigned>(sbg::reduce_smem_bytes(sbg::kReduceFull, 54)); }
 unsigned int geneig_reduce_eig_n54_heev_smem_bytes(void) {
@@ -374,13 +410,13 @@ void geneig_finish_n54_launch(const cuDoubleComplex* d_L, const cuDoubleComplex*
         for (int off = 0; off < batch_size; off += ws.capacity) {
             const int cnt = std::min(ws.capacity, batch_size - off);
             check_cuda(sbg::launch_reduce(sbg::kReduceFromLM, nullptr, c2(d_L) + nn * off, 54, cnt, ws,
-                                          nullptr, d_info + off, s->sched.reduce_threads, stream), "reduce kernel");
-            check_cuda(sbg::launch_hetrd(54, cnt, c2(d_M) + nn * off, ws, d_info + off, s->sched.hetrd_threads, stream),
+                                          nullptr, d_info + off, s->sched.shape(), stream), "reduce kernel");
+            check_cuda(sbg::launch_hetrd(54, cnt, c2(d_M) + nn * off, ws, d_info + off, s->sched.shape(), stream),
                        "hetrd kernel");
             check_cuda(sbg::launch_ql_logged(54, cnt, ws, d_W + 54 * off, c2(d_U) + nn * off, d_info + off, false,
                                              s->sched.chain_threads, s->sched.ql_warps, stream), "QL kernels");
             check_cuda(sbg::launch_back(sbg::kBackFull, 54, cnt, ws, c2(d_U) + nn * off, d_info + off,
-                                        s->sched.back_threads, stream), "back kernel");
+                                        s->sched.shape(), stream), "back kernel");
         }
     }));
 }

@@ -200,14 +200,14 @@ struct BackSmem {
 __host__ __device__ inline size_t potrf_warp_bytes(int n) {
     return align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16) + align_up(8 * n, 16) + 16;
 }
-constexpr int kPotrfWarpsPerCta = 2;
+constexpr int kMaxPairWarps = 4;      // warp-per-pair kernels: 1, 2 or 4 pairs (warps) per CTA
 constexpr int kColMaxN = 56;      // column-per-thread kernels: y[NMAX] in registers, NMAX in {32, 48, 56}
 
-__global__ void __launch_bounds__(32 * kPotrfWarpsPerCta) k_potrf_warp(int mode, const double2* __restrict__ B, int n,
+__global__ void __launch_bounds__(32 * kMaxPairWarps) k_potrf_warp(int mode, const double2* __restrict__ B, int n,
                                                                       int batch, Workspace ws, double2* __restrict__ out,
                                                                       int* __restrict__ info) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * kPotrfWarpsPerCta + warp;
+    const int b = blockIdx.x * (blockDim.x >> 5) + warp;
     if (b >= batch) return;
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char* base = smem + potrf_warp_bytes(n) * warp;
@@ -450,13 +450,12 @@ __global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __
 __host__ __device__ inline size_t hetrd_warp_bytes(int n) {
     return align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16) + 16 * 2 * n + 2 * align_up(8 * n, 16) + 16 * n + 16;
 }
-constexpr int kHetrdWarpsPerCta = 2;
 constexpr int kHetrdWarpMaxN = 65;
 
-__global__ void __launch_bounds__(32 * kHetrdWarpsPerCta) k_hetrd_warp(int n, int batch, const double2* __restrict__ C,
+__global__ void __launch_bounds__(32 * kMaxPairWarps) k_hetrd_warp(int n, int batch, const double2* __restrict__ C,
                                                                       Workspace ws, int* __restrict__ info) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * kHetrdWarpsPerCta + warp;
+    const int b = blockIdx.x * (blockDim.x >> 5) + warp;
     if (b >= batch) return;
     if (info[b] != 0) return;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -506,17 +505,16 @@ __host__ __device__ inline size_t hetrd_c64_bytes(int n) {
     return align_up(8 * static_cast<size_t>(n) * (n + 1) / 2, 16) + 8 * 2 * n + 2 * align_up(4 * n, 16) +
            align_up(8 * n, 16) + 16;
 }
-constexpr int kHetrdC64WarpsPerCta = 2;
 
 __device__ __forceinline__ double2* refine_stash(const Workspace& ws, int b) {
     return reinterpret_cast<double2*>(static_cast<char*>(ws.log) + 16 * static_cast<size_t>(ws.log_stride) * b);
 }
 
-__global__ void __launch_bounds__(32 * kHetrdC64WarpsPerCta) k_hetrd_warp_c64(int n, int batch,
+__global__ void __launch_bounds__(32 * kMaxPairWarps) k_hetrd_warp_c64(int n, int batch,
                                                                               const double2* __restrict__ C,
                                                                               Workspace ws, int* __restrict__ info) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = blockIdx.x * kHetrdC64WarpsPerCta + warp;
+    const int b = blockIdx.x * (blockDim.x >> 5) + warp;
     if (b >= batch) return;
     if (info[b] != 0) return;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1129,6 +1127,11 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_back(int mode, int n, in
     }
 }
 
+// Pairs (warps) per CTA of the warp-per-pair kernels: 1, 2 or 4 (anything else: the default 2).
+inline int pair_warps_of(const LaunchShape& s) {
+    return (s.pair_warps == 1 || s.pair_warps == 2 || s.pair_warps == 4) ? s.pair_warps : 2;
+}
+
 template <class K>
 void set_max_smem_once(K kernel, SmemOptIn& rec) {
     set_smem_limit(reinterpret_cast<const void*>(kernel), rec, max_smem_optin());
@@ -1265,7 +1268,7 @@ void run_hegst_col(int mode, const double2* A, const Workspace& ws, double2* out
 }
 
 cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, int batch,
-                          const Workspace& ws, double2* out, int* info, int /*threads*/, cudaStream_t stream) {
+                          const Workspace& ws, double2* out, int* info, const LaunchShape& shape, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!B || !info) return cudaErrorInvalidValue;
     if ((mode == kReduceChol || mode == kReduceHegst || mode == kReduceFull) && !out) return cudaErrorInvalidValue;
@@ -1278,14 +1281,14 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
     // The two-kernel path hands L from k_potrf_warp to k_hegst_col through ws.LV, so it
     // needs a workspace (the staged Cholesky alone does not).
     if (n <= kColMaxN && mode != kReduceFromLM && (mode == kReduceChol || ws.LV != nullptr)) {
+        const int pw = pair_warps_of(shape);
         static SmemOptIn fp;
         set_max_smem_once(k_potrf_warp, fp);
-        const int grid = (batch + kPotrfWarpsPerCta - 1) / kPotrfWarpsPerCta;
-        k_potrf_warp<<<grid, 32 * kPotrfWarpsPerCta, potrf_warp_bytes(n) * kPotrfWarpsPerCta, stream>>>(
-            mode, B, n, batch, ws, out, info);
+        const int grid = (batch + pw - 1) / pw;
+        k_potrf_warp<<<grid, 32 * pw, potrf_warp_bytes(n) * pw, stream>>>(mode, B, n, batch, ws, out, info);
         if (mode == kReduceChol) return cudaGetLastError();
-        if (n == 32) run_hegst_col<32, true>(mode, A, ws, out, n, batch, info, stream);
-        else if (n == 54) run_hegst_col<54, true>(mode, A, ws, out, n, batch, info, stream);
+        if (n == 32 && shape.col_exact) run_hegst_col<32, true>(mode, A, ws, out, n, batch, info, stream);
+        else if (n == 54 && shape.col_exact) run_hegst_col<54, true>(mode, A, ws, out, n, batch, info, stream);
         else if (n <= 32) run_hegst_col<32>(mode, A, ws, out, n, batch, info, stream);
         else if (n <= 48) run_hegst_col<48>(mode, A, ws, out, n, batch, info, stream);
         else run_hegst_col<56>(mode, A, ws, out, n, batch, info, stream);
@@ -1299,17 +1302,19 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
 
 size_t hetrd_smem_bytes(int n, int threads) { return HetrdSmem(n, threads).total; }
 
-cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, int* info, int threads,
+cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, int* info, const LaunchShape& shape,
                          cudaStream_t stream) {
+    const int threads = shape.threads;
     if (batch <= 0) return cudaSuccess;
     if (!C || !info || !ws.LV || !ws.d || !ws.e || !ws.tau) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) return big_path(n) ? cudaSuccess : cudaErrorInvalidValue;   // done by the reduce kernel
     if (n <= kHetrdWarpMaxN) {
-        const size_t smem = hetrd_warp_bytes(n) * kHetrdWarpsPerCta;
+        const int pw = pair_warps_of(shape);
+        const size_t smem = hetrd_warp_bytes(n) * pw;
+        if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
         static SmemOptIn fw;
         set_max_smem_once(k_hetrd_warp, fw);
-        const int grid = (batch + kHetrdWarpsPerCta - 1) / kHetrdWarpsPerCta;
-        k_hetrd_warp<<<grid, 32 * kHetrdWarpsPerCta, smem, stream>>>(n, batch, C, ws, info);
+        k_hetrd_warp<<<(batch + pw - 1) / pw, 32 * pw, smem, stream>>>(n, batch, C, ws, info);
         return cudaGetLastError();
     }
     const size_t smem = hetrd_smem_bytes(n, threads == 128 ? 128 : 256);
@@ -1414,18 +1419,24 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
     return cudaGetLastError();
 }
 
-size_t hetrd_c64_smem_bytes(int n) { return hetrd_c64_bytes(n) * kHetrdC64WarpsPerCta; }
+size_t hetrd_c64_smem_bytes(int n) { return hetrd_c64_bytes(n) * kMaxPairWarps; }
 
-cudaError_t launch_hetrd_c64(int n, int batch, const double2* C, const Workspace& ws, int* info, cudaStream_t stream) {
+size_t pair_kernels_smem_bytes(int n, int pair_warps) {
+    const size_t per = std::max(potrf_warp_bytes(n), std::max(hetrd_warp_bytes(n), hetrd_c64_bytes(n)));
+    return per * static_cast<size_t>(pair_warps);
+}
+
+cudaError_t launch_hetrd_c64(int n, int batch, const double2* C, const Workspace& ws, int* info,
+                             const LaunchShape& shape, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (n < 1 || n > kMixedMaxN || !C || !info || !ws.LV || ws.log_stride < refine_stash_entries(n))
         return cudaErrorInvalidValue;
-    const size_t smem = hetrd_c64_smem_bytes(n);
+    const int pw = pair_warps_of(shape);
+    const size_t smem = hetrd_c64_bytes(n) * pw;
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     static SmemOptIn f;
     set_max_smem_once(k_hetrd_warp_c64, f);
-    k_hetrd_warp_c64<<<(batch + kHetrdC64WarpsPerCta - 1) / kHetrdC64WarpsPerCta, 32 * kHetrdC64WarpsPerCta, smem,
-                       stream>>>(n, batch, C, ws, info);
+    k_hetrd_warp_c64<<<(batch + pw - 1) / pw, 32 * pw, smem, stream>>>(n, batch, C, ws, info);
     return cudaGetLastError();
 }
 
@@ -1438,14 +1449,6 @@ void run_back_col_g(int mode, int n, int batch, const Workspace& ws, double2* X,
     k_back_col<NMAX, G, EXACT><<<batch, back_col_threads<NMAX, G>(), smem, stream>>>(mode, n, batch, ws, X, info);
 }
 
-// One lane per column: measured at n = 54, splitting a column over 2 lanes (G = 2, 3 CTAs
-// per SM) gives the same time as G = 1 (4 CTAs per SM); the per-lane chain halves but the
-// shuffles and the lower occupancy eat the gain.
-template <int NMAX>
-void run_back_col(int mode, int n, int batch, const Workspace& ws, double2* X, int* info, size_t smem,
-                  cudaStream_t stream) {
-    run_back_col_g<NMAX, 1>(mode, n, batch, ws, X, info, smem, stream);
-}
 
 // ----------------------------------------------------------------------------- k_pull_pairs
 // Pairs are walked grid-stride, each by the whole CTA; every thread keeps 4 independent 16-byte
@@ -1487,7 +1490,7 @@ cudaError_t launch_pull_pairs(const double2* src, double2* dst, int count, int n
 }
 
 cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, int* info,
-                        int /*threads*/, cudaStream_t stream) {
+                        const LaunchShape& shape, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
     if (mode == kBackLOnly && n > kColMaxN) return cudaErrorInvalidValue;
@@ -1495,11 +1498,23 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
     const size_t smem = back_smem_bytes(n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     if (n <= kColMaxN) {
-        if (n == 32) run_back_col_g<32, 1, true>(mode, n, batch, ws, X, info, smem, stream);
-        else if (n == 54) run_back_col_g<54, 1, true>(mode, n, batch, ws, X, info, smem, stream);
-        else if (n <= 32) run_back_col<32>(mode, n, batch, ws, X, info, smem, stream);
-        else if (n <= 48) run_back_col<48>(mode, n, batch, ws, X, info, smem, stream);
-        else run_back_col<56>(mode, n, batch, ws, X, info, smem, stream);
+        const bool two = shape.back_lanes == 2;
+        if (n == 32 && shape.col_exact) {
+            if (two) run_back_col_g<32, 2, true>(mode, n, batch, ws, X, info, smem, stream);
+            else run_back_col_g<32, 1, true>(mode, n, batch, ws, X, info, smem, stream);
+        } else if (n == 54 && shape.col_exact) {
+            if (two) run_back_col_g<54, 2, true>(mode, n, batch, ws, X, info, smem, stream);
+            else run_back_col_g<54, 1, true>(mode, n, batch, ws, X, info, smem, stream);
+        } else if (n <= 32) {
+            if (two) run_back_col_g<32, 2>(mode, n, batch, ws, X, info, smem, stream);
+            else run_back_col_g<32, 1>(mode, n, batch, ws, X, info, smem, stream);
+        } else if (n <= 48) {
+            if (two) run_back_col_g<48, 2>(mode, n, batch, ws, X, info, smem, stream);
+            else run_back_col_g<48, 1>(mode, n, batch, ws, X, info, smem, stream);
+        } else {
+            if (two) run_back_col_g<56, 2>(mode, n, batch, ws, X, info, smem, stream);
+            else run_back_col_g<56, 1>(mode, n, batch, ws, X, info, smem, stream);
+        }
         return cudaGetLastError();
     }
     SBG_DISPATCH_BY_N(n, run_back, mode, n, batch, ws, X, info, smem, stream);

@@ -68,12 +68,26 @@ enum BackMode : int {
     kBackLOnly = 2,       // X = L^{-H} Y, Y complex in the X buffer (mixed form; n <= 56 only)
 };
 
+// Launch shape of the stage kernels, the part of a schedule the autotuner varies:
+//   threads     threads per CTA of k_hetrd (66 <= n <= 84): 128 or 256
+//   pair_warps  pairs (one warp each) per CTA of k_potrf_warp, k_hetrd_warp, k_hetrd_warp_c64
+//               (n <= 65): 1, 2 or 4 -- the reference's "batches per block"
+//   col_exact   k_hegst_col / k_back_col: the exact-n instantiation where one exists (n = 32, 54)
+//               instead of the one for the next larger NMAX
+//   back_lanes  lanes per column of k_back_col (n <= 56): 1 or 2
+struct LaunchShape {
+    int threads = 256;
+    int pair_warps = 2;
+    int col_exact = 1;
+    int back_lanes = 1;
+};
+
 // Launchers (asynchronous on `stream`; return cudaSuccess or the launch error).
 cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, int batch,
-                          const Workspace& ws, double2* out, int* info, int threads, cudaStream_t stream);
+                          const Workspace& ws, double2* out, int* info, const LaunchShape& shape, cudaStream_t stream);
 // Householder tridiagonalisation of C (lower triangle read, column-major, ld = n) ->
 // reflectors into ws.LV (rows above the superdiagonal), tau, d, e.  Pairs with info != 0 skip.
-cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, int* info, int threads,
+cudaError_t launch_hetrd(int n, int batch, const double2* C, const Workspace& ws, int* info, const LaunchShape& shape,
                          cudaStream_t stream);
 size_t hetrd_smem_bytes(int n, int threads);
 // Two-kernel QL: thread-per-pair scalar chain logging rotations, then a warp-per-pair
@@ -88,12 +102,16 @@ cudaError_t launch_ql_logged(int n, int batch, const Workspace& ws, double* W, d
 //                        refinement of (W, Y) against the stashed C on the FP64 tensor cores, and
 //                        the FP64 fallback for pairs it cannot take;
 //   launch_back(kBackLOnly)  X = L^{-H} Y.
-cudaError_t launch_hetrd_c64(int n, int batch, const double2* C, const Workspace& ws, int* info, cudaStream_t stream);
+cudaError_t launch_hetrd_c64(int n, int batch, const double2* C, const Workspace& ws, int* info,
+                             const LaunchShape& shape, cudaStream_t stream);
 cudaError_t launch_refine_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
                                 int refine_steps, cudaStream_t stream);
 cudaError_t launch_eig_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
-                             int refine_steps, int chain_threads, cudaStream_t stream);
+                             int refine_steps, int chain_threads, const LaunchShape& shape, cudaStream_t stream);
 size_t hetrd_c64_smem_bytes(int n);
+// Dynamic shared memory of a CTA of the warp-per-pair kernels (k_potrf_warp, k_hetrd_warp,
+// k_hetrd_warp_c64) with pair_warps pairs.
+size_t pair_kernels_smem_bytes(int n, int pair_warps);
 size_t refine_c_smem_bytes(int n);
 size_t mixed_fallback_smem_bytes(int n);
 // Host-buffer path: copies `count` pairs of n x n column-major matrices from pinned host memory
@@ -102,7 +120,7 @@ size_t mixed_fallback_smem_bytes(int n);
 // reads).  The kernel's loads cross the host link; one CTA per SM keeps enough of them in flight.
 cudaError_t launch_pull_pairs(const double2* src, double2* dst, int count, int n, bool lower, cudaStream_t stream);
 cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2* X, int* info,
-                        int threads, cudaStream_t stream);
+                        const LaunchShape& shape, cudaStream_t stream);
 
 // Pairs with n <= kSmallMaxN are solved by CTA-per-pair (or warp-per-pair) stage kernels;
 // kSmallMaxN < n <= kBigMaxN by the cluster kernels of bigsolve.cu.  For those the reduce

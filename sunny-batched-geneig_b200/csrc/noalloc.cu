@@ -95,11 +95,11 @@ extern "C" int sbg_geneig_full_noalloc_launch(int n, const cuDoubleComplex* d_A,
     const double2* A = reinterpret_cast<const double2*>(d_A);
     const double2* B = reinterpret_cast<const double2*>(d_B);
     double2* X = reinterpret_cast<double2*>(d_X);
-    e = sbg::launch_reduce(sbg::kReduceFull, A, B, n, batch, ws, X, d_info, sch.reduce_threads, stream);
-    if (e == cudaSuccess) e = sbg::launch_hetrd(n, batch, X, ws, d_info, sch.hetrd_threads, stream);
+    e = sbg::launch_reduce(sbg::kReduceFull, A, B, n, batch, ws, X, d_info, sch.shape(), stream);
+    if (e == cudaSuccess) e = sbg::launch_hetrd(n, batch, X, ws, d_info, sch.shape(), stream);
     if (e == cudaSuccess)
         e = sbg::launch_ql_logged(n, batch, ws, d_W, X, d_info, false, sch.chain_threads, sch.ql_warps, stream);
-    if (e == cudaSuccess) e = sbg::launch_back(sbg::kBackFull, n, batch, ws, X, d_info, sch.back_threads, stream);
+    if (e == cudaSuccess) e = sbg::launch_back(sbg::kBackFull, n, batch, ws, X, d_info, sch.shape(), stream);
     if (e != cudaSuccess) return fail(SBG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
     return SBG_OK;
 }

@@ -509,9 +509,9 @@ cudaError_t launch_refine_mixed(int n, int batch, const Workspace& ws, double* W
 }
 
 cudaError_t launch_eig_mixed(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
-                             int refine_steps, int chain_threads, cudaStream_t stream) {
+                             int refine_steps, int chain_threads, const LaunchShape& shape, cudaStream_t stream) {
     cudaError_t err = launch_eig_invit(n, batch, ws, W, X, info, chain_threads, false, stream);
-    if (err == cudaSuccess) err = launch_back(kBackQOnly, n, batch, ws, X, info, 0, stream);
+    if (err == cudaSuccess) err = launch_back(kBackQOnly, n, batch, ws, X, info, shape, stream);
     if (err == cudaSuccess) err = launch_refine_mixed(n, batch, ws, W, X, info, refine_steps, stream);
     return err;
 }

@@ -210,26 +210,27 @@ struct sbg_solver {
                    const sbg::Workspace& ws, cudaStream_t stream) {
         cudaEvent_t ev;
         stage_begin(stream, &ev);
-        check_cuda(sbg::launch_reduce(sbg::kReduceFull, A, B, n, cnt, ws, X, info,
-                                      sched.reduce_threads, stream), "reduce kernel");
+        check_cuda(sbg::launch_reduce(sbg::kReduceFull, A, B, n, cnt, ws, X, info, sched.shape(), stream),
+                   "reduce kernel");
         stage_end(stream, ev, 0, sbg::reduce_kernel_count(n));
         const bool mixed = precision == SBG_PRECISION_MIXED;
         stage_begin(stream, &ev);
         if (mixed)
-            check_cuda(sbg::launch_hetrd_c64(n, cnt, X, ws, info, stream), "complex64 hetrd kernel");
+            check_cuda(sbg::launch_hetrd_c64(n, cnt, X, ws, info, sched.shape(), stream), "complex64 hetrd kernel");
         else
-            check_cuda(sbg::launch_hetrd(n, cnt, X, ws, info, sched.hetrd_threads, stream), "hetrd kernel");
+            check_cuda(sbg::launch_hetrd(n, cnt, X, ws, info, sched.shape(), stream), "hetrd kernel");
         stage_end(stream, ev, 1, n > sbg::kSmallMaxN ? 0 : 1);       // large n: inside the reduce kernel
         stage_begin(stream, &ev);
         if (mixed)             // eigenpairs of the complex64 T, Y = Q Z, FP64 refinement against C
-            check_cuda(sbg::launch_eig_mixed(n, cnt, ws, W, X, info, refine_steps, sched.chain_threads, stream),
+            check_cuda(sbg::launch_eig_mixed(n, cnt, ws, W, X, info, refine_steps, sched.chain_threads, sched.shape(),
+                                             stream),
                        "mixed eigensolve kernels");
         else
             check_cuda(sbg::launch_ql_logged(n, cnt, ws, W, X, info, false, sched.chain_threads, sched.ql_warps,
                                              stream), "QL kernels");
         stage_end(stream, ev, 2, sbg::eig_kernel_count(n, mixed));
         stage_begin(stream, &ev);
-        check_cuda(sbg::launch_back(mixed ? sbg::kBackLOnly : sbg::kBackFull, n, cnt, ws, X, info, sched.back_threads,
+        check_cuda(sbg::launch_back(mixed ? sbg::kBackLOnly : sbg::kBackFull, n, cnt, ws, X, info, sched.shape(),
                                     stream), "back-transform kernel");
         stage_end(stream, ev, 3, 1);
     }

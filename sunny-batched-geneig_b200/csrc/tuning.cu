@@ -26,8 +26,8 @@ namespace sbg {
 namespace {
 
 constexpr const char* kTableMagic = "SBGTUNE";
-constexpr int kTableVersion = 3;
-constexpr const char* kLibVersion = "sbg-geneig-0.1";
+constexpr int kTableVersion = 4;
+constexpr const char* kLibVersion = "sbg-geneig-0.2";
 
 std::mutex g_mu;
 std::map<std::tuple<int, int, int>, Schedule> g_in_process;   // (device, n, precision)
@@ -42,6 +42,7 @@ bool fits(int n, int precision, const Schedule& s) {
     if (reduce_smem_bytes(kReduceFull, n) > lim || back_smem_bytes(n) > lim || hetrd_smem_bytes(n, s.hetrd_threads) > lim) return false;
     if (ql_chain_smem_bytes(n, s.chain_threads, false) > lim) return false;
     if (ql_apply_smem_bytes(n, s.ql_warps, false) > lim) return false;
+    if (n <= 65 && pair_kernels_smem_bytes(n, s.pair_warps) > lim) return false;
     if (precision == SBG_PRECISION_MIXED &&
         (n > kMixedMaxN || refine_c_smem_bytes(n) > lim || mixed_fallback_smem_bytes(n) > lim ||
          hetrd_c64_smem_bytes(n) > lim))
@@ -97,8 +98,8 @@ bool load_table(const std::string& path, const std::string& key, std::vector<Tab
         std::istringstream es(lines[i]);
         std::string tag;
         TableEntry e{};
-        es >> tag >> e.n >> e.precision >> e.s.reduce_threads >> e.s.hetrd_threads >> e.s.back_threads >> e.s.ql_warps >>
-            e.s.chain_threads >> e.s.refine_threads >> e.us;
+        es >> tag >> e.n >> e.precision >> e.s.hetrd_threads >> e.s.pair_warps >> e.s.col_exact >> e.s.back_lanes >>
+            e.s.ql_warps >> e.s.chain_threads >> e.us;
         if (tag != "entry" || !es) { out.clear(); return false; }
         out.push_back(e);
     }
@@ -125,9 +126,9 @@ void save_table(const std::string& path, const std::string& key, const std::vect
     body << kTableMagic << " " << kTableVersion << "\n";
     body << "device " << key << "\n";
     for (const auto& e : entries)
-        body << "entry " << e.n << " " << e.precision << " " << e.s.reduce_threads << " " << e.s.hetrd_threads << " "
-             << e.s.back_threads << " "
-             << e.s.ql_warps << " " << e.s.chain_threads << " " << e.s.refine_threads << " " << e.us << "\n";
+        body << "entry " << e.n << " " << e.precision << " " << e.s.hetrd_threads << " " << e.s.pair_warps << " "
+             << e.s.col_exact << " " << e.s.back_lanes << " " << e.s.ql_warps << " " << e.s.chain_threads << " "
+             << e.us << "\n";
     const std::string b = body.str();
     char buf[32];
     std::snprintf(buf, sizeof(buf), "%016llx", static_cast<unsigned long long>(fnv1a(b)));
@@ -213,19 +214,21 @@ struct Bench {
     double2* x() { return static_cast<double2*>(X.p); }
     int* inf() { return static_cast<int*>(info.p); }
     bool mixed() const { return precision == SBG_PRECISION_MIXED; }
+    void reduce(const Schedule& s) { launch_reduce(kReduceFull, a(), b(), n, count, ws, x(), inf(), s.shape(), st); }
+    void tridiag(const Schedule& s) {
+        if (mixed()) launch_hetrd_c64(n, count, x(), ws, inf(), s.shape(), st);
+        else launch_hetrd(n, count, x(), ws, inf(), s.shape(), st);
+    }
     void eig(const Schedule& s) {
         if (mixed())
-            launch_eig_mixed(n, count, ws, w(), x(), inf(), 5, s.chain_threads, st);
+            launch_eig_mixed(n, count, ws, w(), x(), inf(), 5, s.chain_threads, s.shape(), st);
         else
             launch_ql_logged(n, count, ws, w(), x(), inf(), false, s.chain_threads, s.ql_warps, st);
     }
-    void full(const Schedule& s) {
-        launch_reduce(kReduceFull, a(), b(), n, count, ws, x(), inf(), s.reduce_threads, st);
-        if (mixed()) launch_hetrd_c64(n, count, x(), ws, inf(), st);
-        else launch_hetrd(n, count, x(), ws, inf(), s.hetrd_threads, st);
-        eig(s);
-        launch_back(mixed() ? kBackLOnly : kBackFull, n, count, ws, x(), inf(), s.back_threads, st);
+    void back(const Schedule& s) {
+        launch_back(mixed() ? kBackLOnly : kBackFull, n, count, ws, x(), inf(), s.shape(), st);
     }
+    void full(const Schedule& s) { reduce(s); tridiag(s); eig(s); back(s); }
 };
 
 // Host residual ||A x - lam B x||_inf / (||A||_F ||x||_2) for one column.
@@ -255,62 +258,68 @@ bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double&
     cudaMemcpy(bench.A.p, hA.data(), 16 * bench.nn * count, cudaMemcpyHostToDevice);
     cudaMemcpy(bench.B.p, hB.data(), 16 * bench.nn * count, cudaMemcpyHostToDevice);
     const Schedule base = default_schedule(n, precision);
-    const std::vector<int> thread_opts = req.force_threads ? std::vector<int>{req.force_threads} : std::vector<int>{128, 256};
-    // pairs per CTA of the rotation apply; the inverse-iteration path has no such parameter
-    const std::vector<int> warp_opts =
-        req.force_ql_warps ? std::vector<int>{req.force_ql_warps}
-        : eig_by_inverse_iteration(n, precision == SBG_PRECISION_MIXED) ? std::vector<int>{base.ql_warps}
-                                                                         : std::vector<int>{1, 2, 4, 8};
+    const bool small = n <= kSmallMaxN;
+    // pairs per CTA of the warp-per-pair kernels (the reference's batches per block, its BPB
+    // sweep over {16, 8, 4, 2, 1}); here at most 4 warps share a CTA
+    const std::vector<int> bpb_opts = req.force_bpb && n <= 65 ? std::vector<int>{req.force_bpb}
+                                      : n <= 65 ? std::vector<int>{1, 2, 4} : std::vector<int>{base.pair_warps};
+    const std::vector<int> exact_opts = (n == 32 || n == 54) ? std::vector<int>{1, 0} : std::vector<int>{base.col_exact};
+    const std::vector<int> thread_opts = req.force_threads ? std::vector<int>{req.force_threads}
+                                         : (small && n > 65) ? std::vector<int>{128, 256}
+                                                             : std::vector<int>{base.hetrd_threads};
+    // pairs per CTA of the rotation apply; the inverse-iteration paths have no such parameter
+    const bool invit = eig_by_inverse_iteration(n, false);
+    const std::vector<int> warp_opts = req.force_bpb && n > 65 ? std::vector<int>{req.force_bpb}
+                                       : invit ? std::vector<int>{base.ql_warps} : std::vector<int>{1, 2, 4, 8};
     Schedule win = base;
     double t_total = 0.0;
-    // k_reduce
+    // reduction + tridiagonalisation together (pair_warps is shared by their warp-per-pair kernels)
     {
         double bt = 1e30;
-        for (int t : thread_opts) {
-            double ms = median_ms([&] { launch_reduce(kReduceFull, bench.a(), bench.b(), n, count, bench.ws, bench.x(),
-                                                      bench.inf(), t, bench.st); }, 3, bench.st);
-            if (ms < bt) { bt = ms; win.reduce_threads = t; }
-        }
-        t_total += bt;
-    }
-    // k_hetrd (reads C from X, which k_reduce just wrote; idempotent)
-    {
-        double bt = 1e30;
-        for (int t : thread_opts) {
-            double ms = median_ms([&] { launch_hetrd(n, count, bench.x(), bench.ws, bench.inf(), t, bench.st); },
-                                  3, bench.st);
-            if (ms < bt) { bt = ms; win.hetrd_threads = t; }
-        }
-        t_total += bt;
-    }
-    // eigensolve of the tridiagonal (k_reduce's output stays valid in the workspace)
-    {
-        double bt = 1e30;
-        std::vector<int> refine_opts = precision == SBG_PRECISION_MIXED ? std::vector<int>{128, 256} : std::vector<int>{256};
-        for (int ct : {64, 128, 256})
-            for (int w : warp_opts)
-                for (int rt : refine_opts) {
+        for (int pw : bpb_opts)
+            for (int ex : exact_opts)
+                for (int t : thread_opts) {
                     Schedule s = win;
-                    s.ql_warps = w;
-                    s.chain_threads = ct;
-                    s.refine_threads = rt;
+                    s.pair_warps = pw;
+                    s.col_exact = ex;
+                    s.hetrd_threads = t;
                     if (!fits(n, precision, s)) continue;
-                    double ms = median_ms([&] { bench.eig(s); }, 3, bench.st);
-                    if (ms < bt) { bt = ms; win.ql_warps = w; win.chain_threads = ct; win.refine_threads = rt; }
+                    const double ms = median_ms([&] { bench.reduce(s); bench.tridiag(s); }, 3, bench.st);
+                    if (ms < bt) { bt = ms; win.pair_warps = pw; win.col_exact = ex; win.hetrd_threads = t; }
                 }
         t_total += bt;
+        bench.reduce(win);
+        bench.tridiag(win);
     }
-    // k_back (restores Z before every run: the kernel overwrites it with X)
+    // eigensolve of the tridiagonal (the workspace keeps T; idempotent)
+    {
+        double bt = 1e30;
+        for (int ct : {64, 128, 256})
+            for (int w : warp_opts) {
+                Schedule s = win;
+                s.ql_warps = w;
+                s.chain_threads = ct;
+                if (!fits(n, precision, s)) continue;
+                // the mixed form's refinement reads C from its stash and rewrites X: restore X first
+                const double ms = median_ms([&] { bench.eig(s); }, 3, bench.st);
+                if (ms < bt) { bt = ms; win.ql_warps = w; win.chain_threads = ct; }
+            }
+        t_total += bt;
+    }
+    // back-transform (restores its input before every run: the kernel overwrites it with X)
     {
         bench.eig(win);
         cudaMemcpyAsync(bench.Z.p, bench.X.p, 16 * bench.nn * count, cudaMemcpyDeviceToDevice, bench.st);
         double bt = 1e30;
-        for (int t : thread_opts) {
-            double ms = median_ms([&] {
+        const std::vector<int> lane_opts = n <= 56 ? std::vector<int>{1, 2} : std::vector<int>{base.back_lanes};
+        for (int gl : lane_opts) {
+            Schedule s = win;
+            s.back_lanes = gl;
+            const double ms = median_ms([&] {
                 cudaMemcpyAsync(bench.X.p, bench.Z.p, 16 * bench.nn * count, cudaMemcpyDeviceToDevice, bench.st);
-                launch_back(kBackFull, n, count, bench.ws, bench.x(), bench.inf(), t, bench.st);
+                bench.back(s);
             }, 3, bench.st);
-            if (ms < bt) { bt = ms; win.back_threads = t; }
+            if (ms < bt) { bt = ms; win.back_lanes = gl; }
         }
         t_total += bt;
     }
@@ -346,21 +355,22 @@ bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double&
     }
     best = win;
     best_us = 1e3 * t_total / count;
-    std::fprintf(stderr, "[sbg autotune] n=%d precision=%d: reduce=%d hetrd=%d back=%d ql_chain=%d ql_apply_warps=%d "
-                 "refine=%d (%.3f us/pair)\n", n, precision, win.reduce_threads, win.hetrd_threads, win.back_threads,
-                 win.chain_threads,
-                 win.ql_warps, win.refine_threads, best_us);
+    std::fprintf(stderr, "[sbg autotune] n=%d precision=%d: pairs/CTA=%d exact=%d hetrd_threads=%d back_lanes=%d "
+                 "ql_chain=%d ql_apply_warps=%d (%.3f us/pair)\n", n, precision, win.pair_warps, win.col_exact,
+                 win.hetrd_threads, win.back_lanes, win.chain_threads, win.ql_warps, best_us);
     return true;
 }
 
 }  // namespace
 
+bool schedule_fits(int n, int precision, const Schedule& s) { return fits(n, precision, s); }
+
 Schedule default_schedule(int n, int precision) {
     Schedule s;
-    s.reduce_threads = n > 24 ? 256 : 128;
     s.hetrd_threads = n > 24 ? 256 : 128;
-    s.back_threads = n > 24 ? 256 : 128;
-    s.refine_threads = n > 24 ? 256 : 128;
+    s.pair_warps = 2;
+    s.col_exact = 1;
+    s.back_lanes = 1;
     s.ql_warps = n <= 32 ? 8 : (n <= 64 ? 4 : 2);
     s.chain_threads = 128;
     while (s.chain_threads > 32 && !fits(n, precision, s)) s.chain_threads /= 2;
@@ -394,14 +404,19 @@ TuneResult select_schedule(const TuneRequest& req) {
     if (req.force_threads) {
         if (req.force_threads != 128 && req.force_threads != 256)
             throw std::runtime_error("force_block_dim_x must be 128 or 256");
-        r.sched.reduce_threads = r.sched.hetrd_threads = r.sched.back_threads = r.sched.refine_threads =
-            req.force_threads;
+        r.sched.hetrd_threads = req.force_threads;
     }
-    if (req.force_ql_warps) {
-        if (req.force_ql_warps < 1 || req.force_ql_warps > 16) throw std::runtime_error("batches_per_block must be 1..16");
-        r.sched.ql_warps = req.force_ql_warps;
+    if (req.force_bpb) {
+        if (req.n <= 65) {            // pairs per CTA of the warp-per-pair kernels
+            if (req.force_bpb != 1 && req.force_bpb != 2 && req.force_bpb != 4)
+                throw std::runtime_error("batches_per_block must be 1, 2 or 4 for n <= 65");
+            r.sched.pair_warps = req.force_bpb;
+        } else {                      // pairs per CTA of the QL rotation apply
+            if (req.force_bpb < 1 || req.force_bpb > 16) throw std::runtime_error("batches_per_block must be 1..16");
+            r.sched.ql_warps = req.force_bpb;
+        }
         if (!fits(req.n, req.precision, r.sched))
-            throw std::runtime_error("batches_per_block=" + std::to_string(req.force_ql_warps) +
+            throw std::runtime_error("batches_per_block=" + std::to_string(req.force_bpb) +
                                      " exceeds the shared-memory budget for n=" + std::to_string(req.n));
     }
     if (!req.autotune) return r;

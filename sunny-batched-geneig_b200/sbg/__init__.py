@@ -180,6 +180,22 @@ class Solver:
     def reserve(self, pairs: int, stream_slots: int = 1) -> None:
         _check(self._lib.sbg_solver_reserve(self._h, pairs, stream_slots), "sbg_solver_reserve")
 
+    SCHEDULE_FIELDS = ("hetrd_threads", "pairs_per_cta", "col_exact", "back_lanes", "ql_warps", "chain_threads")
+
+    @property
+    def schedule(self) -> dict:
+        """The launch schedule (sbg_solver_schedule): CTA shapes of the stage kernels."""
+        out = (ctypes.c_int * 6)()
+        _check(self._lib.sbg_solver_schedule(self._h, out), "sbg_solver_schedule")
+        return dict(zip(self.SCHEDULE_FIELDS, list(out)))
+
+    @schedule.setter
+    def schedule(self, sched: dict) -> None:
+        cur = self.schedule
+        cur.update(sched)
+        vals = (ctypes.c_int * 6)(*[int(cur[k]) for k in self.SCHEDULE_FIELDS])
+        _check(self._lib.sbg_solver_set_schedule(self._h, vals), "sbg_solver_set_schedule")
+
     @property
     def batches_per_block(self) -> int:
         return int(self._lib.sbg_solver_batches_per_block(self._h))

@@ -57,6 +57,8 @@ SIGNATURES = {
     "sbg_workspace_bytes": (SZ, [I, I, I]),
     "sbg_selftest_reciprocal": (I, [P, P, I, P]),
     "sbg_selftest_fp64_fma": (I, [P, I, I, P]),
+    "sbg_solver_schedule": (I, [P, P]),
+    "sbg_solver_set_schedule": (I, [P, P]),
     "sbg_solver_matrix_size": (I, [P]),
     "sbg_solver_batches_per_block": (I, [P]),
     "sbg_solver_block_dim_x": (I, [P]),
