@@ -114,9 +114,10 @@ typedef struct {
     int tuning_mode;          /* SBG_TUNING_*  (hpp:101) */
     int cache_mode;           /* SBG_CACHE_*   (hpp:102) */
     int precision;            /* SBG_PRECISION_FP64 (plain drop-in) or SBG_PRECISION_MIXED */
-    int refine_steps;         /* mixed form: most Ogita-Aishima steps, 0 = default (5): full steps until the largest
-                                 correction is <= 1e-8 (at least two), then one that only orthogonalises
-                                 near-degenerate pairs; typically 3 run */
+    int refine_steps;         /* mixed form: most Ogita-Aishima updates, 0 = default (5).  Each pass checks every
+                                 residual (<= 256 eps ||C||_F) and the orthonormality (<= 1e-13) first and stops
+                                 there; from complex64 two updates are typical.  A pair still short after the
+                                 last update is solved again by the FP64 fallback */
     int workspace_pairs;      /* pairs per internal chunk; 0 = default */
 } sbg_solver_options;
 

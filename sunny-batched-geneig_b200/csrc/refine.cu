@@ -6,9 +6,10 @@
 //                        eigenvector matrix Y = Q Z (from the X buffer) held in shared memory as
 //                        planar FP64 tiles (re and im planes, column-major, ld = NP + 4, zero
 //                        padded to NP = n rounded up to 8).  Warp w owns rows 8w..8w+7 of every
-//                        product, all NP columns: P = C Y, then G = Y^H Y and S = Y^H P together,
-//                        the correction E, and Y' = Y + Y E.  Writes the refined Y over X and W,
-//                        or flags the pair (ws.flag = 2).
+//                        strip product (all NP columns): P = C Y and Y' = Y + Y E; the Hermitian
+//                        G = Y^H Y and S = Y^H P are computed as lower-triangle 8 x 8 blocks dealt
+//                        round-robin over the warps.  Writes the refined Y over X and W, or flags
+//                        the pair (ws.flag = 2).
 //   k_mixed_fallback     flagged pairs only: FP64 Householder, FP64 QL and Y = Q Z in one CTA,
 //                        from the stashed C (Y into X, W).  The back-transform X = L^{-H} Y runs
 //                        after both, for every pair.
@@ -89,28 +90,54 @@ __device__ __forceinline__ void cgemm(Strip<NB>& acc, const double* __restrict__
     }
 }
 
-// G += Y^H Y and S += Y^H P in one pass (both share the A operand Y^H).
+// The lower-triangle 8 x 8 blocks of the Hermitian products G = Y^H Y and S = Y^H P:
+// NB (NB + 1) / 2 blocks, block q being (row block r, column block c), r >= c, in row-major order of
+// the lower triangle, dealt round-robin to the NB warps (warp w takes q = w, w + NB, ...; at most KB).
 template <int NB>
-__device__ __forceinline__ void cgemm_gram(Strip<NB>& G, Strip<NB>& S, const double* __restrict__ Yre,
-                                           const double* __restrict__ Yim, const double* __restrict__ Pre,
-                                           const double* __restrict__ Pim, int ld, int row0) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+struct Gram {
+    static constexpr int kTotal = NB * (NB + 1) / 2;
+    static constexpr int KB = (kTotal + NB - 1) / NB;
+    double gre[KB][2], gim[KB][2], sre[KB][2], sim[KB][2];
+};
+
+__device__ __forceinline__ void lower_block(int q, int& r, int& c) {
+    r = 0;
+    while ((r + 1) * (r + 2) / 2 <= q) ++r;
+    c = q - r * (r + 1) / 2;
+}
+
+// G and S (lower blocks of this warp) in one pass: both share the A operand Y^H.
+template <int NB>
+__device__ __forceinline__ void gram_lower(Gram<NB>& gm, const double* __restrict__ Yre, const double* __restrict__ Yim,
+                                           const double* __restrict__ Pre, const double* __restrict__ Pim, int ld) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    int ra[Gram<NB>::KB], cb[Gram<NB>::KB];
+#pragma unroll
+    for (int k = 0; k < Gram<NB>::KB; ++k) {
+        const int q = w + k * NB;
+        ra[k] = 0;
+        cb[k] = 0;
+        if (q < Gram<NB>::kTotal) lower_block(q, ra[k], cb[k]);
+        gm.gre[k][0] = gm.gre[k][1] = gm.gim[k][0] = gm.gim[k][1] = 0.0;
+        gm.sre[k][0] = gm.sre[k][1] = gm.sim[k][0] = gm.sim[k][1] = 0.0;
+    }
 #pragma unroll 2
     for (int k0 = 0; k0 < 8 * NB; k0 += 4) {
-        const int ia = (row0 + g) * ld + k0 + t;
-        const double ar = Yre[ia], ai = -Yim[ia];
 #pragma unroll
-        for (int c = 0; c < NB; ++c) {
-            const int ib = (8 * c + g) * ld + k0 + t;
+        for (int k = 0; k < Gram<NB>::KB; ++k) {
+            if (w + k * NB >= Gram<NB>::kTotal) continue;          // uniform over the warp
+            const int ia = (8 * ra[k] + g) * ld + k0 + t;
+            const int ib = (8 * cb[k] + g) * ld + k0 + t;
+            const double ar = Yre[ia], ai = -Yim[ia];
             const double yr = Yre[ib], yi = Yim[ib], pr = Pre[ib], pi = Pim[ib];
-            dmma(G.re[c][0], G.re[c][1], ar, yr);
-            dmma(G.re[c][0], G.re[c][1], -ai, yi);
-            dmma(G.im[c][0], G.im[c][1], ar, yi);
-            dmma(G.im[c][0], G.im[c][1], ai, yr);
-            dmma(S.re[c][0], S.re[c][1], ar, pr);
-            dmma(S.re[c][0], S.re[c][1], -ai, pi);
-            dmma(S.im[c][0], S.im[c][1], ar, pi);
-            dmma(S.im[c][0], S.im[c][1], ai, pr);
+            dmma(gm.gre[k][0], gm.gre[k][1], ar, yr);
+            dmma(gm.gre[k][0], gm.gre[k][1], -ai, yi);
+            dmma(gm.gim[k][0], gm.gim[k][1], ar, yi);
+            dmma(gm.gim[k][0], gm.gim[k][1], ai, yr);
+            dmma(gm.sre[k][0], gm.sre[k][1], ar, pr);
+            dmma(gm.sre[k][0], gm.sre[k][1], -ai, pi);
+            dmma(gm.sim[k][0], gm.sim[k][1], ar, pi);
+            dmma(gm.sim[k][0], gm.sim[k][1], ai, pr);
         }
     }
 }
@@ -134,6 +161,22 @@ __device__ __forceinline__ void block_sum4(double (&v)[4], double* red) {
     __syncthreads();
 }
 
+// Block-wide sums of v[0], v[1] and max of v[2] (same slots as block_sum4).
+template <int NW>
+__device__ __forceinline__ void block_sum2_max(double (&v)[4], double* red) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    v[0] = warp_sum(v[0]);
+    v[1] = warp_sum(v[1]);
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) v[2] = fmax(v[2], shfl_xor(v[2], m));
+    if (lane == 0) { red[4 * w] = v[0]; red[4 * w + 1] = v[1]; red[4 * w + 2] = v[2]; }
+    __syncthreads();
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int i = 0; i < NW; ++i) { a += red[4 * i]; b += red[4 * i + 1]; c = fmax(c, red[4 * i + 2]); }
+    v[0] = a; v[1] = b; v[2] = c;
+    __syncthreads();
+}
+
 template <int NP>
 struct RefineCSmem {
     static constexpr int LD = NP + 4;
@@ -141,101 +184,138 @@ struct RefineCSmem {
     static constexpr size_t Cre = 0, Cim = plane, Yre = 2 * plane, Yim = 3 * plane, Pre = 4 * plane,
                             Pim = 5 * plane, lam = 6 * plane;
     static constexpr size_t red = lam + align16(sizeof(double) * NP);
-    static constexpr size_t colacc = red + align16(sizeof(double) * 4 * (NP / 8));
-    static constexpr size_t bar = colacc + align16(sizeof(double) * 2 * NP * (NP / 8));
+    static constexpr size_t order = red + align16(sizeof(double) * 4 * (NP / 8));
+    static constexpr size_t bar = order + align16(sizeof(int) * NP);
     static constexpr size_t total = bar + 16;
 };
 
 constexpr double kEps = 1.1102230246251565e-16;
+constexpr double kOrthTol = 1e-13;       // max |(Y^H Y - I)_ij| accepted
 
-// One Ogita-Aishima step on Y (shared tiles): P = C Y; G = Y^H Y, S = Y^H P;
-// lam_i = S_ii / G_ii; delta = max(2 (||S - diag lam||_F + ||C||_F ||I - G||_F), floor_rel ||C||_F);
-// E_ij = (S_ij + lam_j R_ij) / (lam_j - lam_i) where |lam_j - lam_i| > delta, else R_ij / 2
-// (R = I - G); Y <- Y + Y E.  Returns max_{i != j} |E_ij| (the same on every thread).
-// Ogita & Aishima, "Iterative refinement for symmetric eigenvalue decomposition", Japan J.
-// Indust. Appl. Math. 35 (2018), Algorithm 1, here for a Hermitian C.
+// The Ogita-Aishima iteration on Y (Ogita & Aishima, "Iterative refinement for symmetric
+// eigenvalue decomposition", Japan J. Indust. Appl. Math. 35 (2018), Algorithm 1, here for a
+// Hermitian C), arranged so that the products of each pass also decide whether to stop:
+//   P = C Y;  G = Y^H Y, S = Y^H P (lower blocks);  lam_i = S_ii / G_ii  (Rayleigh quotients);
+//   stop when every column has ||P_j - lam_j y_j|| <= 256 eps ||C||_F ||y_j|| and
+//   max |R_ij| <= kOrthTol (R = I - G);
+//   else delta = max(2 (||S - diag lam||_F + ||C||_F ||R||_F), floor ||C||_F),
+//   E_ij = (S_ij + lam_j R_ij) / (lam_j - lam_i) where |lam_j - lam_i| > delta, else R_ij / 2,
+//   Y <- Y + Y E.  floor = 1e-2 once only the orthogonality is missing: eigenvalues closer than
+//   1e-2 ||C||_F are then only orthogonalised (their O(eps ||C|| / gap) corrections would undo it).
+// A start from complex64 typically stops after one update (two passes of products).  Returns
+// true when it stopped converged within max_updates updates.
 template <int NP>
-__device__ double refine_step(int n, const double* Cre, const double* Cim, double* Yre, double* Yim, double* Pre,
-                              double* Pim, double* lam, double* red, double cnorm, double floor_rel) {
-    constexpr int NB = NP / 8, LD = NP + 4;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-    const int row0 = 8 * w, i = row0 + g;
-    {
-        Strip<NB> P;
-        P.zero();
-        cgemm<NB, false>(P, Cre, Cim, Yre, Yim, LD, row0);
-        P.store(Pre, Pim, LD, row0);          // the P tile is free: the previous step's E was consumed
-    }
-    __syncthreads();
-    Strip<NB> G, S;
-    G.zero();
-    S.zero();
-    cgemm_gram<NB>(G, S, Yre, Yim, Pre, Pim, LD, row0);
-#pragma unroll
-    for (int c = 0; c < NB; ++c)
-#pragma unroll
-        for (int q = 0; q < 2; ++q)
-            if (c == w && 2 * t + q == g && i < n) lam[i] = S.re[c][q] / G.re[c][q];
-    __syncthreads();                           // lam visible; every warp is done reading P
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};      // ||S - diag lam||^2, ||R||^2
-#pragma unroll
-    for (int c = 0; c < NB; ++c)
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int j = 8 * c + 2 * t + q;
-            if (i < n && j < n) {
-                const double sr = (i == j) ? S.re[c][q] - lam[i] : S.re[c][q];
-                const double rr = (i == j ? 1.0 : 0.0) - G.re[c][q];
-                acc[0] = fma(sr, sr, fma(S.im[c][q], S.im[c][q], acc[0]));
-                acc[1] = fma(rr, rr, fma(G.im[c][q], G.im[c][q], acc[1]));
-            }
+__device__ bool refine(int n, const double* Cre, const double* Cim, double* Yre, double* Yim, double* Pre, double* Pim,
+                       double* lam, double* red, double cnorm, int max_updates) {
+    constexpr int NB = NP / 8, LD = NP + 4, NT = NP * 4;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = lane >> 2, t = lane & 3;
+    const int row0 = 8 * w;
+    for (int it = 0;; ++it) {
+        {
+            Strip<NB> P;
+            P.zero();
+            cgemm<NB, false>(P, Cre, Cim, Yre, Yim, LD, row0);
+            P.store(Pre, Pim, LD, row0);      // the P tile is free: the previous E was consumed
         }
-    block_sum4<NB>(acc, red);
-    const double delta = fmax(2.0 * (sqrt(acc[0]) + cnorm * sqrt(acc[1])), floor_rel * cnorm);
-    // E in G's registers, then over the P tile (P is no longer read)
-    double em = 0.0;
+        __syncthreads();
+        Gram<NB> gm;
+        gram_lower<NB>(gm, Yre, Yim, Pre, Pim, LD);
+        int rb[Gram<NB>::KB], cbk[Gram<NB>::KB];
 #pragma unroll
-    for (int c = 0; c < NB; ++c)
+        for (int k = 0; k < Gram<NB>::KB; ++k) {
+            rb[k] = cbk[k] = 0;
+            if (w + k * NB < Gram<NB>::kTotal) lower_block(w + k * NB, rb[k], cbk[k]);
+        }
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int j = 8 * c + 2 * t + q;
-            double er = 0.0, ei = 0.0;
-            if (i < n && j < n) {
-                const double rr = (i == j ? 1.0 : 0.0) - G.re[c][q], ri = -G.im[c][q];
-                const double gap = lam[j] - lam[i];
-                if (i != j && fabs(gap) > delta) {
-                    const double inv = 1.0 / gap;
-                    er = fma(lam[j], rr, S.re[c][q]) * inv;
-                    ei = fma(lam[j], ri, S.im[c][q]) * inv;
-                } else {
-                    er = 0.5 * rr;
-                    ei = 0.5 * ri;
+        for (int k = 0; k < Gram<NB>::KB; ++k)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int i = 8 * rb[k] + g;
+                if (w + k * NB < Gram<NB>::kTotal && rb[k] == cbk[k] && 2 * t + q == g && i < n)
+                    lam[i] = gm.sre[k][q] / gm.gre[k][q];
+            }
+        __syncthreads();                       // lam visible; every warp is done reading P as an operand
+        // norms and the largest departure from orthonormality (lower blocks; off-diagonal blocks twice)
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};  // ||S - diag lam||^2, ||R||^2, max|R_ij|, -
+#pragma unroll
+        for (int k = 0; k < Gram<NB>::KB; ++k)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int i = 8 * rb[k] + g, j = 8 * cbk[k] + 2 * t + q;
+                if (w + k * NB < Gram<NB>::kTotal && i < n && j < n) {
+                    const double wgt = rb[k] == cbk[k] ? 1.0 : 2.0;
+                    const double sr = (i == j) ? gm.sre[k][q] - lam[i] : gm.sre[k][q];
+                    const double rr = (i == j ? 1.0 : 0.0) - gm.gre[k][q], ri = gm.gim[k][q];
+                    acc[0] += wgt * fma(sr, sr, gm.sim[k][q] * gm.sim[k][q]);
+                    acc[1] += wgt * fma(rr, rr, ri * ri);
+                    acc[2] = fmax(acc[2], fabs(rr) + fabs(ri));
                 }
-                if (i != j) em = fmax(em, fabs(er) + fabs(ei));
             }
-            G.re[c][q] = er;
-            G.im[c][q] = ei;
+        // residual of every column: ||P_j - lam_j y_j||^2 against (256 eps ||C||_F)^2 ||y_j||^2
+        bool res_ok = true;
+        for (int j = tid; j < n; j += NT) {
+            double rr = 0.0, yy = 0.0;
+            const double lj = lam[j];
+            for (int i = 0; i < n; ++i) {
+                const double yr = Yre[j * LD + i], yi = Yim[j * LD + i];
+                const double dr = fma(-lj, yr, Pre[j * LD + i]), di = fma(-lj, yi, Pim[j * LD + i]);
+                rr = fma(dr, dr, fma(di, di, rr));
+                yy = fma(yr, yr, fma(yi, yi, yy));
+            }
+            const double tol = 256.0 * kEps * cnorm;
+            if (!(rr <= tol * tol * yy)) res_ok = false;
         }
-    G.store(Pre, Pim, LD, row0);
+        res_ok = __syncthreads_and(res_ok);
+        block_sum2_max<NB>(acc, red);           // acc[0], acc[1] summed, acc[2] the block's max
+        const bool orth_ok = acc[2] <= kOrthTol;
+        if (res_ok && orth_ok) return true;
+        if (it >= max_updates) return false;
+        const double floor_rel = res_ok ? 1e-2 : 0.0;
+        const double delta = fmax(2.0 * (sqrt(acc[0]) + cnorm * sqrt(acc[1])), floor_rel * cnorm);
+        // E over the P tile (P is no longer read): each lower block gives E_ij and, mirrored, E_ji
 #pragma unroll
-    for (int m = 16; m >= 1; m >>= 1) em = fmax(em, shfl_xor(em, m));
-    if (lane == 0) red[4 * w + 3] = em;
-    __syncthreads();                           // E visible; the max slots written
-    em = 0.0;
-    for (int q = 0; q < NB; ++q) em = fmax(em, red[4 * q + 3]);
-    Strip<NB> Yn;
-    Yn.load(Yre, Yim, LD, row0);
-    cgemm<NB, false>(Yn, Yre, Yim, Pre, Pim, LD, row0);
-    __syncthreads();                           // every warp is done reading Y
-    Yn.store(Yre, Yim, LD, row0);
-    __syncthreads();
-    return em;
+        for (int k = 0; k < Gram<NB>::KB; ++k) {
+            if (w + k * NB >= Gram<NB>::kTotal) continue;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int i = 8 * rb[k] + g, j = 8 * cbk[k] + 2 * t + q;
+                double er = 0.0, ei = 0.0, fr = 0.0, fi = 0.0;     // E_ij, E_ji
+                if (i < n && j < n) {
+                    const double rr = (i == j ? 1.0 : 0.0) - gm.gre[k][q], ri = -gm.gim[k][q];
+                    const double gap = lam[j] - lam[i];
+                    if (i != j && fabs(gap) > delta) {
+                        const double inv = 1.0 / gap;
+                        er = fma(lam[j], rr, gm.sre[k][q]) * inv;
+                        ei = fma(lam[j], ri, gm.sim[k][q]) * inv;
+                        fr = -fma(lam[i], rr, gm.sre[k][q]) * inv;  // (conj S_ij + lam_i conj R_ij) / (lam_i - lam_j)
+                        fi = fma(lam[i], ri, gm.sim[k][q]) * inv;
+                    } else {
+                        er = 0.5 * rr; ei = 0.5 * ri;
+                        fr = 0.5 * rr; fi = -0.5 * ri;
+                    }
+                }
+                Pre[j * LD + i] = er;
+                Pim[j * LD + i] = ei;
+                if (rb[k] != cbk[k]) {
+                    Pre[i * LD + j] = fr;
+                    Pim[i * LD + j] = fi;
+                }
+            }
+        }
+        __syncthreads();                       // E visible
+        Strip<NB> Yn;
+        Yn.load(Yre, Yim, LD, row0);
+        cgemm<NB, false>(Yn, Yre, Yim, Pre, Pim, LD, row0);
+        __syncthreads();                       // every warp is done reading Y
+        Yn.store(Yre, Yim, LD, row0);
+        __syncthreads();
+    }
 }
 
 template <int NP>
 __global__ void __launch_bounds__(NP * 4, 1) k_refine_c(int n, int batch, Workspace ws, double* __restrict__ W,
                                                       double2* __restrict__ X, int* __restrict__ info,
-                                                      int max_steps) {
+                                                      int max_updates) {
     constexpr int NB = NP / 8, LD = NP + 4, NT = NP * 4;
     using L = RefineCSmem<NP>;
     const int b = blockIdx.x;
@@ -256,7 +336,7 @@ __global__ void __launch_bounds__(NP * 4, 1) k_refine_c(int n, int batch, Worksp
     double* Pim = reinterpret_cast<double*>(smem + L::Pim);
     double* lam = reinterpret_cast<double*>(smem + L::lam);
     double* red = reinterpret_cast<double*>(smem + L::red);
-    double* colacc = reinterpret_cast<double*>(smem + L::colacc);
+    int* order = reinterpret_cast<int*>(smem + L::order);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::bar);
     const size_t mat = static_cast<size_t>(n) * n;
     double2* Xb = X + mat * b;
@@ -286,62 +366,13 @@ __global__ void __launch_bounds__(NP * 4, 1) k_refine_c(int n, int batch, Worksp
     }
     block_sum4<NB>(cn, red);
     const double cnorm = sqrt(cn[0]);
-    // ---- steps: full steps until the largest correction is <= 1e-8 (at least two), then one step
-    // that only orthogonalises eigenvalues closer than 1e-2 ||C||_F; max_steps counts them all.
-    // Y + Y E is orthonormal only to second order in E, and the correction of close eigenvalues
-    // comes late (the first step, while the FP32 residual exceeds their gap, treats them as a
-    // cluster); the final orthogonalising step absorbs the O(eps ||C|| / gap) stall of converged
-    // pairs.
-    for (int step = 0; step < max_steps; ++step) {
-        const bool last = step + 1 == max_steps;
-        const double em = refine_step<NP>(n, Cre, Cim, Yre, Yim, Pre, Pim, lam, red, cnorm, last ? 1e-2 : 0.0);
-        if (last) break;
-        if (step >= 1 && em <= 1e-8) {
-            refine_step<NP>(n, Cre, Cim, Yre, Yim, Pre, Pim, lam, red, cnorm, 1e-2);
-            break;
-        }
-    }
-    // ---- acceptance: ||C y_j - lam_j y_j|| <= 256 eps ||C||_F ||y_j|| for every column, with lam
-    // from the last step (its error is second order in the step's input error)
-    {
-        const int lane = tid & 31, w = tid >> 5, g = lane >> 2, t = lane & 3, row0 = 8 * w, i = row0 + g;
-        Strip<NB> P;
-        P.zero();
-        cgemm<NB, false>(P, Cre, Cim, Yre, Yim, LD, row0);
-        // per-column partial sums over this warp's 8 rows: lanes with equal t share columns
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const int j = 8 * c + 2 * t + q;
-                const int yi = j * LD + i;
-                double rr = 0.0, yy = 0.0;
-                if (i < n && j < n) {
-                    const double dr = fma(-lam[j], Yre[yi], P.re[c][q]), di = fma(-lam[j], Yim[yi], P.im[c][q]);
-                    rr = fma(dr, dr, di * di);
-                    yy = fma(Yre[yi], Yre[yi], Yim[yi] * Yim[yi]);
-                }
-                for (int m = 4; m <= 16; m <<= 1) { rr += shfl_xor(rr, m); yy += shfl_xor(yy, m); }
-                if (g == 0) { colacc[(2 * w) * NP + j] = rr; colacc[(2 * w + 1) * NP + j] = yy; }
-            }
-        __syncthreads();
-        bool bad = false;
-        for (int j = tid; j < n; j += NT) {
-            double rr = 0.0, yy = 0.0;
-            for (int q = 0; q < NB; ++q) { rr += colacc[(2 * q) * NP + j]; yy += colacc[(2 * q + 1) * NP + j]; }
-            const double tol = 256.0 * kEps * cnorm;
-            if (!(rr <= tol * tol * yy)) bad = true;
-        }
-        bad = __syncthreads_or(bad);
-        if (bad) {                             // the FP64 fallback redoes this pair
-            if (tid == 0) ws.flag[b] = 2;
-            return;
-        }
+    if (!refine<NP>(n, Cre, Cim, Yre, Yim, Pre, Pim, lam, red, cnorm, max_updates)) {
+        if (tid == 0) ws.flag[b] = 2;          // the FP64 fallback redoes this pair
+        return;
     }
     if (tid == 0) ws.flag[b] = 0;
     // ---- outputs: W ascending and Y's columns alike (a swap can only come from eigenvalues the
-    // FP32 start ordered within its rounding; the columns follow their eigenvalues)
-    int* order = reinterpret_cast<int*>(colacc);           // the column sums are consumed
+    // complex64 start ordered within its rounding; the columns follow their eigenvalues)
     if (tid == 0) {
         for (int j = 0; j < n; ++j) order[j] = j;
         for (int j = 1; j < n; ++j) {                      // insertion sort by lam (stable)
