@@ -1110,14 +1110,17 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_back(int mode, int n, in
 #pragma unroll
     for (int r = 0; r < RM; ++r) {
         const int i = g + G * r;
-        y[r] = make_double2((valid && i < n) ? Zg[i + static_cast<size_t>(j) * n] : 0.0, 0.0);
+        if (mode == kBackLOnly)            // complex Y in the X buffer
+            y[r] = (valid && i < n) ? Xb[i + static_cast<size_t>(j) * n] : make_double2(0.0, 0.0);
+        else                               // real Z in the X buffer
+            y[r] = make_double2((valid && i < n) ? Zg[i + static_cast<size_t>(j) * n] : 0.0, 0.0);
     }
     for (int i = tid; i < n; i += T) tau_s[i] = ws.tau[static_cast<size_t>(n) * b + i];
     wait_copies(bar, info + b);
     for (int i = tid; i < n; i += T) invd[i] = 1.0 / LVs[i + i * ld].x;
     __syncthreads();              // also: every thread has read its Z before any X is written
-    seg_apply_q<G, RM>(LVs, ld, tau_s, y, n, g);
-    if (mode == kBackFull) seg_trsm_lowerH<G, RM>(LVs, ld, invd, y, n, g);
+    if (mode != kBackLOnly) seg_apply_q<G, RM>(LVs, ld, tau_s, y, n, g);
+    if (mode == kBackFull || mode == kBackLOnly) seg_trsm_lowerH<G, RM>(LVs, ld, invd, y, n, g);
     if (valid) {
 #pragma unroll
         for (int r = 0; r < RM; ++r) {
@@ -1493,7 +1496,7 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
                         const LaunchShape& shape, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
-    if (mode == kBackLOnly && n > kColMaxN) return cudaErrorInvalidValue;
+    if (mode == kBackLOnly && n > kSmallMaxN) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) return launch_back_big(mode, n, batch, ws, X, info, stream);
     const size_t smem = back_smem_bytes(n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;

@@ -46,7 +46,7 @@ int ql_log_capacity(int n);
 __host__ __device__ constexpr int refine_np(int n) { return (n + 7) / 8 * 8; }
 __host__ __device__ constexpr int refine_ld(int n) { return refine_np(n) + 4; }
 __host__ __device__ constexpr int refine_stash_entries(int n) { return refine_np(n) * refine_ld(n); }
-constexpr int kMixedMaxN = 56;
+constexpr int kMixedMaxN = 63;       // inverse iteration (no rotation log, so the stash is free)
 
 size_t workspace_bytes_per_pair(int n);
 // Carves a Workspace for `capacity` pairs of size n out of `base` (256-byte aligned).  Each of
@@ -65,7 +65,7 @@ enum ReduceMode : int {
 enum BackMode : int {
     kBackFull = 0,        // X = L^{-H} Q Z
     kBackQOnly = 1,       // V = Q Z (eigenvectors of the reduced matrix)
-    kBackLOnly = 2,       // X = L^{-H} Y, Y complex in the X buffer (mixed form; n <= 56 only)
+    kBackLOnly = 2,       // X = L^{-H} Y, Y complex in the X buffer (mixed form; n <= 84)
 };
 
 // Launch shape of the stage kernels, the part of a schedule the autotuner varies:

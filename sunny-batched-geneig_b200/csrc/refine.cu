@@ -507,6 +507,7 @@ size_t refine_c_smem_bytes(int n) {
         case 40: return RefineCSmem<40>::total;
         case 48: return RefineCSmem<48>::total;
         case 56: return RefineCSmem<56>::total;
+        case 64: return RefineCSmem<64>::total;
         default: return 0;
     }
 }
@@ -528,6 +529,7 @@ cudaError_t launch_refine_mixed(int n, int batch, const Workspace& ws, double* W
         case 40: err = run_refine_c<40>(n, batch, ws, W, X, info, refine_steps, stream); break;
         case 48: err = run_refine_c<48>(n, batch, ws, W, X, info, refine_steps, stream); break;
         case 56: err = run_refine_c<56>(n, batch, ws, W, X, info, refine_steps, stream); break;
+        case 64: err = run_refine_c<64>(n, batch, ws, W, X, info, refine_steps, stream); break;
         default: return cudaErrorInvalidValue;
     }
     if (err != cudaSuccess) return err;

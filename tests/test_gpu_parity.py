@@ -132,6 +132,16 @@ def test_qsweep_config(N, precision, oracle_mod):
     check(A, B, W, X, info, Wr, Xr, n, relative=True)
 
 
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 7, 9, 12, 17, 24, 31, 33, 40, 49, 57, 60, 63])
+def test_mixed_form_sizes(n, oracle_mod):
+    """The mixed form (complex64 Householder, FP64 refinement on the tensor cores) at every tile
+    size of its refinement kernel (n padded to 8, 16, ..., 64) and both sides of each."""
+    H, S = oracle_mod.gen_fixture_pairs(n, 6, 13, "random")
+    W, X, info = run(n, H, S, "mixed")
+    Wr, Xr, _ = oracle_mod.hegv(H, S, n, nthreads=4)
+    check(H, S, W, X, info, Wr, Xr, n)
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 5, 7, 12, 17, 24, 31, 33, 63, 65, 77, 83])
 def test_sizes_and_odd_n(n, oracle_mod):
     H, S = oracle_mod.gen_fixture_pairs(n, 6, 11, "random")
