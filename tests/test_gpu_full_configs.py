@@ -116,7 +116,7 @@ def test_qsweep_262144_every_pair(N, oracle_mod, threads):
 
 
 def test_mixed_form_1048576_pairs_streamed(oracle_mod, threads):
-    """The mixed form (FP32 tridiagonal eigensolve + FP64 refinement) on 2^20 q-sweep pairs at
+    """The mixed form (complex64 Householder + FP64 refinement on the tensor cores) on 2^20 q-sweep pairs at
     n = 54: four cells of 262,144 q each (cell seeds 0..3), every pair checked."""
     from bench import make_workload
     worst = (0.0, 0.0)
