@@ -29,27 +29,46 @@
 namespace sbg {
 
 // ---------------------------------------------------------------- potrf, one warp, packed
-// Right-looking lower Cholesky of the packed tile P by one warp (n <= 65): at column k
-// lane L scales row k+1+L (and k+1+m-1-L) of column k, then updates the trailing rows it
-// owns (balanced pairs, as in hetrd_warp_packed).  invd[k] = 1 / L_kk.  Returns 0 or the
-// order of the first non-positive (or NaN) leading minor, the zpotrf convention.
+// Right-looking lower Cholesky of the packed tile P by one warp (n <= 65), two columns per pass:
+// column k is scaled, column k+1 takes column k's update and is scaled, then ONE pass over the
+// trailing triangle (rows and columns >= k+2) subtracts both rank-1 terms, in the order the
+// one-column algorithm would (so the result is the same bit for bit) but reading and writing
+// each trailing entry once per two columns instead of once per column.  Lane L updates the
+// trailing rows L and m-1-L (balanced pairs, as in hetrd_warp_packed).  invd[k] = 1 / L_kk.
+// Returns 0 or the order of the first non-positive (or NaN) leading minor, the zpotrf convention.
 template <typename R>
 __device__ int potrf_warp_packed(cplx<R>* P, int n, R* invd) {
     using C = cplx<R>;
     const int lane = threadIdx.x & 31;
-    for (int k = 0; k < n; ++k) {
+    for (int k = 0; k < n; k += 2) {
         C* colk = P + pk(k, n);                   // colk[i - k] = A(i, k), i >= k
         const R dkk = colk[0].x;
         if (!(dkk > R(0))) return k + 1;          // uniform: every lane reads the same word
         const R dsq = sqrt(dkk);
         const R inv = rsqrt(dkk);                 // in parallel with the square root, not after it
-        const int m = n - k - 1;
+        const int m0 = n - k - 1;
         __syncwarp();
         if (lane == 0) { colk[0] = mk<R>(dsq, R(0)); invd[k] = inv; }
-        for (int i = 1 + lane; i <= m; i += 32) colk[i] = cscale(colk[i], inv);
+        for (int i = 1 + lane; i <= m0; i += 32) colk[i] = cscale(colk[i], inv);
         __syncwarp();
-        // trailing A22(r, j) -= l_r conj(l_j), l = colk[1..m], j <= r
-        const int base = k + 1;
+        if (m0 == 0) break;
+        // column k+1 takes column k's rank-1 term: A(k+1+i, k+1) -= l(k+1+i) conj(l(k+1))
+        C* colk1 = P + pk(k + 1, n);              // colk1[i] = A(k+1+i, k+1)
+        const C lk1 = colk[1];
+        for (int i = lane; i < m0; i += 32) colk1[i] = cfmsc(colk[1 + i], lk1, colk1[i]);
+        __syncwarp();
+        const R d1 = colk1[0].x;
+        if (!(d1 > R(0))) return k + 2;
+        const R dsq1 = sqrt(d1);
+        const R inv1 = rsqrt(d1);
+        const int m = m0 - 1;                     // trailing order (rows / columns >= k + 2)
+        __syncwarp();
+        if (lane == 0) { colk1[0] = mk<R>(dsq1, R(0)); invd[k + 1] = inv1; }
+        for (int i = 1 + lane; i <= m; i += 32) colk1[i] = cscale(colk1[i], inv1);
+        __syncwarp();
+        if (m == 0) break;
+        // trailing A22(r, j) -= l0_r conj(l0_j) + l1_r conj(l1_j), j <= r, l0 = colk[2..], l1 = colk1[1..]
+        const int base = k + 2;
         const int h = (m + 1) >> 1;
         const int r1 = lane, r2 = m - 1 - lane;
         // A22(r, j) at P + pk(base) + r - j + sum_{t<j} (m - t): advances by m - j - 1 per column
@@ -57,11 +76,12 @@ __device__ int potrf_warp_packed(cplx<R>* P, int n, R* invd) {
         if (lane < h) {
             const int tot = (r2 != r1) ? r1 + r2 + 2 : r1 + 1;
             C* a = P + pk(base, n) + r1;
-            C l = colk[1 + r1];
+            C l0 = colk[2 + r1], l1 = colk1[1 + r1];
             int jj = 0;
             for (int t = 0; t < tot; ++t) {
-                if (t == r1 + 1) { a = P + pk(base, n) + r2; l = colk[1 + r2]; jj = 0; }
-                *a = cfmsc(l, colk[1 + jj], *a);
+                if (t == r1 + 1) { a = P + pk(base, n) + r2; l0 = colk[2 + r2]; l1 = colk1[1 + r2]; jj = 0; }
+                C v = cfmsc(l0, colk[2 + jj], *a);
+                *a = cfmsc(l1, colk1[1 + jj], v);
                 a += m - jj - 1;
                 ++jj;
             }

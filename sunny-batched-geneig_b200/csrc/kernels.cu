@@ -448,12 +448,12 @@ __global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __
 // a packed lower-triangular tile (n(n+1)/2 complex; 23.8 KB at n = 54, so eight pairs
 // fit an SM) and reduced by hetrd_warp_packed with warp-level synchronisation only.
 __host__ __device__ inline size_t hetrd_warp_bytes(int n) {
-    return align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16) + 16 * 2 * n + 2 * align_up(8 * n, 16) + 16 * n + 16;
+    return align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16) + 16 * 4 * n + 16;
 }
 constexpr int kHetrdWarpMaxN = 65;
 
 __global__ void __launch_bounds__(32 * kMaxPairWarps) k_hetrd_warp(int n, int batch, const double2* __restrict__ C,
-                                                                      Workspace ws, int* __restrict__ info) {
+                                                                  Workspace ws, int* __restrict__ info) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * (blockDim.x >> 5) + warp;
     if (b >= batch) return;
@@ -463,10 +463,9 @@ __global__ void __launch_bounds__(32 * kMaxPairWarps) k_hetrd_warp(int n, int ba
     double2* P = reinterpret_cast<double2*>(base);
     double2* vb = reinterpret_cast<double2*>(base + align_up(16 * static_cast<size_t>(n) * (n + 1) / 2, 16));
     double2* wb = vb + n;
-    double* d_s = reinterpret_cast<double*>(wb + n);
-    double* e_s = d_s + align_up(8 * n, 16) / 8;
-    double2* tau_s = reinterpret_cast<double2*>(e_s + align_up(8 * n, 16) / 8);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(tau_s + n);
+    double2* vb2 = wb + n;
+    double2* wb2 = vb2 + n;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(wb2 + n);
     const size_t mat = static_cast<size_t>(n) * n;
     const double2* Cb = C + mat * b;
     if (lane == 0) { mbar_init(bar, 1); fence_mbar_init(); }
@@ -476,18 +475,19 @@ __global__ void __launch_bounds__(32 * kMaxPairWarps) k_hetrd_warp(int n, int ba
     for (int j = lane; j < n; j += 32)
         bulk_g2s(P + pk(j, n), Cb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
     wait_copies(bar, info + b);
-    hetrd_warp_packed<double>(P, n, d_s, e_s, tau_s, vb, wb);
+    // d, e and tau go straight to the workspace (global memory): that keeps the per-pair shared
+    // memory at what eight pairs per SM allow
+    double* dg = ws.d + static_cast<size_t>(n) * b;
+    double* eg = ws.e + static_cast<size_t>(n) * b;
+    double2* taug = ws.tau + static_cast<size_t>(n) * b;
+    hetrd_warp_packed<double>(P, n, dg, eg, taug, vb, wb, vb2, wb2);
     double2* LVg = ws.LV + mat * b;
     for (int k = 0; k + 1 < n; ++k) {                    // LV(k, k+1) = v_k(k+1) = 1
         const double2* col = P + pk(k, n) - k;           // col[i] = A(i, k), i >= k
         for (int i = k + 1 + lane; i < n; i += 32)
             LVg[k + static_cast<size_t>(i) * n] = (i == k + 1) ? make_double2(1.0, 0.0) : col[i];
     }
-    for (int i = lane; i < n; i += 32) {
-        ws.d[static_cast<size_t>(n) * b + i] = d_s[i];
-        ws.e[static_cast<size_t>(n) * b + i] = e_s[i];
-        ws.tau[static_cast<size_t>(n) * b + i] = (i + 1 < n) ? tau_s[i] : make_double2(0.0, 0.0);
-    }
+    if (lane == 0) taug[n - 1] = make_double2(0.0, 0.0);
 }
 
 // ----------------------------------------------------------------------------- k_hetrd_warp_c64
@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(32 * kMaxPairWarps) k_hetrd_warp(int n, int ba
 // also written to the pair's stash in the refinement's tile format (refine_stash_entries), since
 // X, where the reduction left it, is overwritten before the refinement runs.
 __host__ __device__ inline size_t hetrd_c64_bytes(int n) {
-    return align_up(8 * static_cast<size_t>(n) * (n + 1) / 2, 16) + 8 * 2 * n + 2 * align_up(4 * n, 16) +
+    return align_up(8 * static_cast<size_t>(n) * (n + 1) / 2, 16) + 8 * 4 * n + 2 * align_up(4 * n, 16) +
            align_up(8 * n, 16) + 16;
 }
 
@@ -522,7 +522,9 @@ __global__ void __launch_bounds__(32 * kMaxPairWarps) k_hetrd_warp_c64(int n, in
     float2* P = reinterpret_cast<float2*>(base);
     float2* vb = reinterpret_cast<float2*>(base + align_up(8 * static_cast<size_t>(n) * (n + 1) / 2, 16));
     float2* wb = vb + n;
-    float* d_s = reinterpret_cast<float*>(wb + n);
+    float2* vb2 = wb + n;
+    float2* wb2 = vb2 + n;
+    float* d_s = reinterpret_cast<float*>(wb2 + n);
     float* e_s = d_s + align_up(4 * n, 16) / 4;
     float2* tau_s = reinterpret_cast<float2*>(e_s + align_up(4 * n, 16) / 4);
     const size_t mat = static_cast<size_t>(n) * n;
@@ -544,7 +546,7 @@ __global__ void __launch_bounds__(32 * kMaxPairWarps) k_hetrd_warp_c64(int n, in
         }
     }
     __syncwarp();
-    hetrd_warp_packed<float>(P, n, d_s, e_s, tau_s, vb, wb);
+    hetrd_warp_packed<float>(P, n, d_s, e_s, tau_s, vb, wb, vb2, wb2);
     double2* LVg = ws.LV + mat * b;
     for (int k = 0; k + 1 < n; ++k) {                    // LV(k, k+1) = v_k(k+1) = 1
         const float2* col = P + pk(k, n) - k;            // col[i] = v_k(i), i >= k + 2

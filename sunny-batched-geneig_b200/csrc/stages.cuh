@@ -544,145 +544,262 @@ __device__ __forceinline__ void ql_log_apply_row(const cplx<R>* log, int cap, cp
 // Column-major packed lower triangle: A(i, j), i >= j, at P[pk(j, n) + i - j].
 __host__ __device__ __forceinline__ int pk(int j, int n) { return j * n - (j * (j - 1)) / 2; }
 
-// The Householder tridiagonalisation of hetrd_lower (LAPACK zhetd2's steps) run by ONE
-// warp on a packed lower triangle, for n <= 65: at step k lane L owns trailing rows
-// L and m-1-L (m = n-k-1), which balances both the Hermitian matvec (m terms per row)
-// and the rank-2 update (r+1 terms for row r).  Only __syncwarp is needed.  The
-// scaled reflector replaces A(k+2:n, k).  vb, wb: m complex of scratch each.
+// ---- warp helpers of hetrd_warp_packed (one warp, packed lower triangle, lane rows L and m-1-L)
+
+// LAPACK zlarfg on x[0..m) (x[0] = alpha): beta, tau, and the scale that turns x[1..m) into the
+// reflector's tail (v = (1, x[1..m) * scale)).  Every lane gets the same values.
 template <typename R>
-__device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, cplx<R>* vb, cplx<R>* wb) {
+struct WarpReflector { cplx<R> tau, scale; R beta; };
+
+template <typename R>
+__device__ __forceinline__ WarpReflector<R> warp_reflector(const cplx<R>* x, int m) {
+    const int lane = threadIdx.x & 31;
+    R s2 = R(0);
+    for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
+    s2 = warp_sum(s2);
+    const cplx<R> alpha = x[0];
+    WarpReflector<R> f;
+    if (s2 == R(0) && alpha.y == R(0)) {
+        f.tau = mk<R>(R(0), R(0)); f.beta = alpha.x; f.scale = mk<R>(R(0), R(0));
+    } else {
+        const R nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
+        f.beta = alpha.x >= R(0) ? -nrm : nrm;
+        const R ib = R(1) / f.beta;                      // two reciprocals instead of four divisions
+        f.tau = mk<R>((f.beta - alpha.x) * ib, -alpha.y * ib);
+        const R ar = alpha.x - f.beta, ai = alpha.y;
+        const R id = R(1) / (ar * ar + ai * ai);
+        f.scale = mk<R>(ar * id, -ai * id);
+    }
+    return f;
+}
+
+// The reflector's vector into vb[0..m) (and its tail over x[1..m)); with tau = 0 (H = I) vb = e_0.
+template <typename R>
+__device__ __forceinline__ void warp_store_reflector(cplx<R>* x, int m, const WarpReflector<R>& f, cplx<R>* vb) {
+    const int lane = threadIdx.x & 31;
+    const bool id = f.tau.x == R(0) && f.tau.y == R(0);
+    __syncwarp();                                        // every lane has read x[0] and the norm terms
+    for (int i = lane; i < m; i += 32) {
+        if (id) { vb[i] = mk<R>(i == 0 ? R(1) : R(0), R(0)); continue; }
+        const cplx<R> v = (i == 0) ? mk<R>(R(1), R(0)) : cmul(x[i], f.scale);
+        vb[i] = v;
+        if (i > 0) x[i] = v;
+    }
+}
+
+// (A22 v)_r for the lane's rows r1 = lane and r2 = m-1-lane of the packed trailing matrix whose
+// column 0 starts at c0 (order m).  Each lane walks its two rows in ONE loop of uniform length (row
+// r1's terms, then row r2's), so no lane waits for the others' longer row: the pair has m-1 terms
+// in the lower row walk, m-1 in the mirrored column walk.  A22(r, j) sits at
+// c0 + r - j + sum_{t<j} (m - t): the address advances by (m - j - 1) from column j to j + 1.
+template <typename R>
+__device__ __forceinline__ void warp_hemv_rows(const cplx<R>* c0, int m, const cplx<R>* vb, cplx<R>& s1, cplx<R>& s2) {
     using C = cplx<R>;
     const int lane = threadIdx.x & 31;
-    for (int k = 0; k + 1 < n; ++k) {
+    const int h = (m + 1) >> 1;
+    const int r1 = lane, r2 = m - 1 - lane;
+    const bool own2 = lane < h && r2 != r1;
+    const C zero = mk<R>(R(0), R(0));
+    s1 = zero;
+    s2 = zero;
+    if (lane >= h) return;
+    const int tot = own2 ? r1 + r2 : r1;                 // lower walk length
+    const int sw = m - 1 - r1;
+    const int tot2 = own2 ? m - 1 : sw;                  // column walk length (== tot when own2)
+    const C* diag1 = c0 + (r1 * m - r1 * (r1 - 1) / 2); // A22(r1, r1)
+    const C* diag2 = c0 + (r2 * m - r2 * (r2 - 1) / 2); // A22(r2, r2)
+    C acc = zero, low1 = zero, u = zero, up1 = zero;
+    const C* pa = c0 + r1;
+    int jj = 0;
+    const C* cp = diag1 + 1;                             // next column-walk element
+    const C* vp = vb + r1 + 1;                           // its partner in v
+    bool lsw = false, usw = false;
+    const int both = tot < tot2 ? tot : tot2;
+    int t = 0;
+    for (; t < both; ++t) {
+        if (t == r1) { low1 = acc; acc = zero; pa = c0 + r2; jj = 0; lsw = true; }
+        if (t == sw) { up1 = u; u = zero; cp = diag2 + 1; vp = vb + r2 + 1; usw = true; }
+        acc = cfma(*pa, vb[jj], acc);
+        u = cfmac(*cp, *vp, u);
+        pa += m - jj - 1;
+        ++jj;
+        ++cp;
+        ++vp;
+    }
+    for (; t < tot; ++t) {                               // (only when the lengths differ)
+        if (t == r1) { low1 = acc; acc = zero; pa = c0 + r2; jj = 0; lsw = true; }
+        acc = cfma(*pa, vb[jj], acc);
+        pa += m - jj - 1;
+        ++jj;
+    }
+    for (; t < tot2; ++t) {
+        if (t == sw) { up1 = u; u = zero; cp = diag2 + 1; vp = vb + r2 + 1; usw = true; }
+        u = cfmac(*cp, *vp, u);
+        ++cp;
+        ++vp;
+    }
+    C low2 = zero, up2 = zero;
+    if (lsw) low2 = acc; else low1 = acc;
+    if (usw) up2 = u; else up1 = u;
+    C a1 = up1;
+    a1.x = fma(diag1[0].x, vb[r1].x, a1.x);
+    a1.y = fma(diag1[0].x, vb[r1].y, a1.y);
+    s1 = cadd(low1, a1);
+    if (own2) {
+        C a2 = up2;
+        a2.x = fma(diag2[0].x, vb[r2].x, a2.x);
+        a2.y = fma(diag2[0].x, vb[r2].y, a2.y);
+        s2 = cadd(low2, a2);
+    }
+}
+
+// A22 -= sum_q (v_q w_q^H + w_q v_q^H), q < NP, on the lane's rows r1 = lane and r2 = m-1-lane of the
+// packed trailing matrix at c0 (order m): r1 + 1 terms of row r1 (diagonal last), then r2 + 1 of row
+// r2, in one loop.  The terms of each entry are applied in q order; the diagonal entries stay real.
+template <typename R, int NP>
+__device__ __forceinline__ void warp_her2_rows(cplx<R>* c0, int m, const cplx<R>* const (&vq)[NP],
+                                               const cplx<R>* const (&wq)[NP]) {
+    using C = cplx<R>;
+    const int lane = threadIdx.x & 31;
+    const int h = (m + 1) >> 1;
+    const int r1 = lane, r2 = m - 1 - lane;
+    if (lane >= h) return;
+    const bool own2 = r2 != r1;
+    const int tot = own2 ? r1 + r2 + 2 : r1 + 1;
+    C* a = c0 + r1;
+    C vr[NP], wr[NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) { vr[q] = vq[q][r1]; wr[q] = wq[q][r1]; }
+    int jj = 0;
+    C* dg1 = nullptr;
+    for (int t = 0; t < tot; ++t) {
+        if (t == r1 + 1) {
+            dg1 = a - (m - jj);
+            a = c0 + r2;
+#pragma unroll
+            for (int q = 0; q < NP; ++q) { vr[q] = vq[q][r2]; wr[q] = wq[q][r2]; }
+            jj = 0;
+        }
+        C tv = *a;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            tv = cfmsc(vr[q], wq[q][jj], tv);
+            tv = cfmsc(wr[q], vq[q][jj], tv);
+        }
+        *a = tv;
+        a += m - jj - 1;
+        ++jj;
+    }
+    // the diagonal entries (each row's last term) stay real
+    if (dg1 == nullptr) dg1 = a - (m - jj);
+    else a[-(m - jj)].y = R(0);
+    dg1->y = R(0);
+}
+
+// The Householder tridiagonalisation of hetrd_lower (LAPACK zhetd2's steps) run by ONE warp on a
+// packed lower triangle, for n <= 65, two steps per pass over the trailing triangle.  At step k
+// lane L owns trailing rows L and m-1-L (m = n-k-1), which balances both the Hermitian matvec
+// (m terms per row) and the rank-2 update (r+1 terms for row r).  Step k's rank-2 update
+// A22 -= v w^H + w v^H is applied at once only to column k+1 (which step k+1 turns into its
+// reflector); step k+1's matvec runs on the trailing matrix without step k's update and corrects
+// it with two dot products, p' = tau' (A22 v' - v^ (w^^H v') - w^ (v^^H v')) (v^, w^: v, w without
+// their first entry), and one pass then applies both steps' updates.  The trailing triangle is so
+// read and written once per two steps instead of once per step (the walks are bound by shared-
+// memory traffic).  Only __syncwarp is needed.  The scaled reflector replaces A(k+2:n, k).
+// d, e, tau may be global memory (written by lane 0 as they are formed, d at the end);
+// vb, wb, vb2, wb2: n complex of shared scratch each.
+template <typename R>
+__device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, cplx<R>* vb, cplx<R>* wb,
+                                  cplx<R>* vb2, cplx<R>* wb2) {
+    using C = cplx<R>;
+    const int lane = threadIdx.x & 31;
+    const C zero = mk<R>(R(0), R(0));
+    int k = 0;
+    while (k + 1 < n) {
         const int m = n - k - 1;
         C* x = P + pk(k, n) + 1;                        // x[i] = A(k+1+i, k)
-        R s2 = R(0);
-        for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
-        s2 = warp_sum(s2);
-        const C alpha = x[0];
-        C tk, scale;
-        R beta;
-        if (s2 == R(0) && alpha.y == R(0)) {
-            tk = mk<R>(R(0), R(0)); beta = alpha.x; scale = mk<R>(R(0), R(0));
-        } else {
-            const R nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
-            beta = alpha.x >= R(0) ? -nrm : nrm;
-            const R ib = R(1) / beta;                    // two reciprocals instead of four divisions
-            tk = mk<R>((beta - alpha.x) * ib, -alpha.y * ib);
-            const R ar = alpha.x - beta, ai = alpha.y;
-            const R id = R(1) / (ar * ar + ai * ai);
-            scale = mk<R>(ar * id, -ai * id);
-        }
-        if (lane == 0) { e[k] = beta; tau[k] = tk; }
-        if (tk.x == R(0) && tk.y == R(0)) continue;
-        for (int i = lane; i < m; i += 32) {
-            const C v = (i == 0) ? mk<R>(R(1), R(0)) : cmul(x[i], scale);
-            vb[i] = v;
-            if (i > 0) x[i] = v;
+        // ---- step k: reflector, p = tau A22 v, w = p - tau/2 (p^H v) v
+        const WarpReflector<R> f = warp_reflector<R>(x, m);
+        if (lane == 0) { e[k] = f.beta; tau[k] = f.tau; }
+        warp_store_reflector<R>(x, m, f, vb);
+        __syncwarp();
+        C* c0 = P + pk(k + 1, n);
+        const int r1 = lane, r2 = m - 1 - lane, h = (m + 1) >> 1;
+        const bool own1 = lane < h, own2 = own1 && r2 != r1;
+        {
+            C s1, s2;
+            warp_hemv_rows<R>(c0, m, vb, s1, s2);
+            const C p1 = cmul(f.tau, s1), p2 = cmul(f.tau, s2);
+            C dot = zero;
+            if (own1) dot = cfmac(p1, vb[r1], dot);
+            if (own2) dot = cfmac(p2, vb[r2], dot);
+            dot.x = warp_sum(dot.x);
+            dot.y = warp_sum(dot.y);
+            const C a2 = cscale(cmul(f.tau, dot), R(-0.5));
+            if (own1) wb[r1] = cfma(a2, vb[r1], p1);     // (tau = 0: p = 0, w = 0)
+            if (own2) wb[r2] = cfma(a2, vb[r2], p2);
         }
         __syncwarp();
-        // trailing matrix A22(r, j) = A(k+1+r, k+1+j): column j starts at P + pk(k+1+j, n)
-        const int base = k + 1;
-        const int h = (m + 1) >> 1;
-        const int r1 = lane, r2 = m - 1 - lane;
-        const bool own1 = lane < h;
-        const bool own2 = lane < h && r2 != r1;
-        // ---- p = tau A22 v for the owned rows.  Each lane walks its two rows in ONE loop of
-        // uniform length (row r1's terms, then row r2's), so no lane waits for the others' longer
-        // row: the pair (r1, r2 = m-1-r1) has m-1 terms in the lower row walk, m-1 in the
-        // mirrored column walk and m+1 in the rank-2 update.
-        // Row walk of the packed lower part: A22(r, j) sits at P + c0 + r - j + sum_{t<j} (n - base - t),
-        // so the address advances by (m - j - 1) from column j to j + 1 (incremental, no pk() per term).
-        C* c0 = P + pk(base, n);
-        C p1 = mk<R>(R(0), R(0)), p2 = mk<R>(R(0), R(0));
-        if (own1) {
-            const C zero = mk<R>(R(0), R(0));
-            // One loop runs both walks (each m-1 terms per lane for a full pair): the lower row
-            // walk (row r1's r1 terms, then row r2's r2) and the mirrored column walk (column r1's
-            // m-1-r1 terms below the diagonal, then column r2's r1) -- shared loop overhead, two
-            // independent FMA chains.
-            const int tot = own2 ? r1 + r2 : r1;              // lower walk length
-            const int sw = m - 1 - r1;
-            const int tot2 = own2 ? m - 1 : sw;               // column walk length (== tot when own2)
-            const C* diag1 = c0 + (r1 * m - r1 * (r1 - 1) / 2);          // A22(r1, r1)
-            const C* diag2 = c0 + (r2 * m - r2 * (r2 - 1) / 2);          // A22(r2, r2)
-            C acc = zero, low1 = zero, u = zero, up1 = zero;
-            const C* pa = c0 + r1;
-            int jj = 0;
-            const C* cp = diag1 + 1;                          // next column-walk element
-            const C* vp = vb + r1 + 1;                        // its partner in v
-            bool lsw = false, usw = false;
-            const int both = tot < tot2 ? tot : tot2;
-            int t = 0;
-            for (; t < both; ++t) {
-                if (t == r1) { low1 = acc; acc = zero; pa = c0 + r2; jj = 0; lsw = true; }
-                if (t == sw) { up1 = u; u = zero; cp = diag2 + 1; vp = vb + r2 + 1; usw = true; }
-                acc = cfma(*pa, vb[jj], acc);
-                u = cfmac(*cp, *vp, u);
-                pa += m - jj - 1;
-                ++jj;
-                ++cp;
-                ++vp;
-            }
-            for (; t < tot; ++t) {                            // (only when the lengths differ)
-                if (t == r1) { low1 = acc; acc = zero; pa = c0 + r2; jj = 0; lsw = true; }
-                acc = cfma(*pa, vb[jj], acc);
-                pa += m - jj - 1;
-                ++jj;
-            }
-            for (; t < tot2; ++t) {
-                if (t == sw) { up1 = u; u = zero; cp = diag2 + 1; vp = vb + r2 + 1; usw = true; }
-                u = cfmac(*cp, *vp, u);
-                ++cp;
-                ++vp;
-            }
-            C low2 = zero, up2 = zero;
-            if (lsw) low2 = acc; else low1 = acc;
-            if (usw) up2 = u; else up1 = u;
-            C a1 = up1;
-            a1.x = fma(diag1[0].x, vb[r1].x, a1.x);
-            a1.y = fma(diag1[0].x, vb[r1].y, a1.y);
-            p1 = cmul(tk, cadd(low1, a1));
-            if (own2) {
-                C a2v = up2;
-                a2v.x = fma(diag2[0].x, vb[r2].x, a2v.x);
-                a2v.y = fma(diag2[0].x, vb[r2].y, a2v.y);
-                p2 = cmul(tk, cadd(low2, a2v));
-            }
+        if (k + 2 >= n) {                               // the last step: apply its update alone
+            const C* vq[1] = {vb};
+            const C* wq[1] = {wb};
+            warp_her2_rows<R, 1>(c0, m, vq, wq);
+            __syncwarp();
+            k += 1;
+            continue;
         }
-        // ---- w = p - tau/2 (p^H v) v
-        C dot = mk<R>(R(0), R(0));
-        if (own1) dot = cfmac(p1, vb[r1], dot);
-        if (own2) dot = cfmac(p2, vb[r2], dot);
-        dot.x = warp_sum(dot.x);
-        dot.y = warp_sum(dot.y);
-        const C a2 = cscale(cmul(tk, dot), R(-0.5));
-        C w1 = mk<R>(R(0), R(0)), w2 = mk<R>(R(0), R(0));
-        if (own1) { w1 = cfma(a2, vb[r1], p1); wb[r1] = w1; }
-        if (own2) { w2 = cfma(a2, vb[r2], p2); wb[r2] = w2; }
-        __syncwarp();
-        // ---- A22 -= v w^H + w v^H on the lower triangle of the owned rows: r1 + 1 terms of
-        // row r1 (diagonal last), then r2 + 1 terms of row r2, in one loop
-        if (own1) {
-            const int tot = own2 ? r1 + r2 + 2 : r1 + 1;
-            C* a = c0 + r1;
-            C vr = vb[r1], wr = w1;
-            int row = r1, jj = 0;
-            C* dg1 = nullptr;
-            for (int t = 0; t < tot; ++t) {
-                if (t == r1 + 1) { dg1 = a - (m - jj); a = c0 + r2; vr = vb[r2]; wr = w2; row = r2; jj = 0; }
-                C tv = cfmsc(vr, wb[jj], *a);
-                tv = cfmsc(wr, vb[jj], tv);
-                *a = tv;
-                a += m - jj - 1;
-                ++jj;
-            }
-            // the diagonal entries (each row's last term) stay real
-            if (dg1 == nullptr) dg1 = a - (m - jj);
-            else a[-(m - jj)].y = R(0);
-            dg1->y = R(0);
+        // ---- column k+1 takes step k's update: A22(r, 0) -= v_r conj(w_0) + w_r conj(v_0)
+        for (int r = lane; r < m; r += 32) {
+            C t = cfmsc(vb[r], wb[0], c0[r]);
+            t = cfmsc(wb[r], vb[0], t);
+            if (r == 0) t.y = R(0);
+            c0[r] = t;
         }
         __syncwarp();
+        // ---- step k+1 on the trailing matrix A22' (rows and columns >= k+2, order m1) without
+        // step k's update: p' = tau' (A22' v' - v^ (w^^H v') - w^ (v^^H v'))
+        const int m1 = m - 1;
+        C* x1 = c0 + 1;                                 // x1[i] = A(k+2+i, k+1)
+        const WarpReflector<R> f1 = warp_reflector<R>(x1, m1);
+        if (lane == 0) { e[k + 1] = f1.beta; tau[k + 1] = f1.tau; }
+        warp_store_reflector<R>(x1, m1, f1, vb2);
+        __syncwarp();
+        C* c1 = P + pk(k + 2, n);
+        const C* vh = vb + 1;                           // v^, w^ over the rows of A22'
+        const C* wh = wb + 1;
+        {
+            C g1 = zero, g2 = zero;                     // w^^H v', v^^H v'
+            for (int i = lane; i < m1; i += 32) {
+                g1 = cfmac(wh[i], vb2[i], g1);
+                g2 = cfmac(vh[i], vb2[i], g2);
+            }
+            g1.x = warp_sum(g1.x); g1.y = warp_sum(g1.y);
+            g2.x = warp_sum(g2.x); g2.y = warp_sum(g2.y);
+            C s1, s2;
+            warp_hemv_rows<R>(c1, m1, vb2, s1, s2);
+            const int q1 = lane, q2 = m1 - 1 - lane, hh = (m1 + 1) >> 1;
+            const bool o1 = lane < hh, o2 = o1 && q2 != q1;
+            C p1 = zero, p2 = zero;
+            if (o1) { s1 = cfms(vh[q1], g1, s1); s1 = cfms(wh[q1], g2, s1); p1 = cmul(f1.tau, s1); }
+            if (o2) { s2 = cfms(vh[q2], g1, s2); s2 = cfms(wh[q2], g2, s2); p2 = cmul(f1.tau, s2); }
+            C dot = zero;
+            if (o1) dot = cfmac(p1, vb2[q1], dot);
+            if (o2) dot = cfmac(p2, vb2[q2], dot);
+            dot.x = warp_sum(dot.x);
+            dot.y = warp_sum(dot.y);
+            const C a2 = cscale(cmul(f1.tau, dot), R(-0.5));
+            if (o1) wb2[q1] = cfma(a2, vb2[q1], p1);
+            if (o2) wb2[q2] = cfma(a2, vb2[q2], p2);
+        }
+        __syncwarp();
+        // ---- both updates on A22': step k's, then step k+1's
+        {
+            const C* vq[2] = {vh, vb2};
+            const C* wq[2] = {wh, wb2};
+            warp_her2_rows<R, 2>(c1, m1, vq, wq);
+        }
+        __syncwarp();
+        k += 2;
     }
     for (int i = lane; i < n; i += 32) d[i] = P[pk(i, n)].x;
     if (lane == 0 && n >= 1) e[n - 1] = R(0);
