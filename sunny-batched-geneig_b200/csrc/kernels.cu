@@ -546,7 +546,7 @@ __global__ void __launch_bounds__(32 * kMaxPairWarps) k_hetrd_warp_c64(int n, in
         }
     }
     __syncwarp();
-    hetrd_warp_packed<float>(P, n, d_s, e_s, tau_s, vb, wb, vb2, wb2);
+    hetrd_warp_packed<float, false>(P, n, d_s, e_s, tau_s, vb, wb, vb2, wb2);
     double2* LVg = ws.LV + mat * b;
     for (int k = 0; k + 1 < n; ++k) {                    // LV(k, k+1) = v_k(k+1) = 1
         const float2* col = P + pk(k, n) - k;            // col[i] = v_k(i), i >= k + 2

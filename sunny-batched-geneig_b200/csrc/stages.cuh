@@ -707,8 +707,12 @@ __device__ __forceinline__ void warp_her2_rows(cplx<R>* c0, int m, const cplx<R>
 // read and written once per two steps instead of once per step (the walks are bound by shared-
 // memory traffic).  Only __syncwarp is needed.  The scaled reflector replaces A(k+2:n, k).
 // d, e, tau may be global memory (written by lane 0 as they are formed, d at the end);
-// vb, wb, vb2, wb2: n complex of shared scratch each.
-template <typename R>
+// vb, wb, vb2, wb2: n complex of shared scratch each (vb2, wb2 unused when !TWO_STEP).
+// TWO_STEP = false runs one step per pass (zhetd2's own order): measured better for complex64,
+// whose walks are bound by instruction issue rather than shared-memory traffic (twice the pairs
+// per SM, half the bytes), so the deferral's extra dot products and column pass cost more than
+// the halved update traffic saves (49.2 against 42.8 ms per 262,144 pairs at n = 54).
+template <typename R, bool TWO_STEP = true>
 __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, cplx<R>* vb, cplx<R>* wb,
                                   cplx<R>* vb2, cplx<R>* wb2) {
     using C = cplx<R>;
@@ -740,7 +744,7 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
             if (own2) wb[r2] = cfma(a2, vb[r2], p2);
         }
         __syncwarp();
-        if (k + 2 >= n) {                               // the last step: apply its update alone
+        if (!TWO_STEP || k + 2 >= n) {                  // one step: apply its update alone
             const C* vq[1] = {vb};
             const C* wq[1] = {wb};
             warp_her2_rows<R, 1>(c0, m, vq, wq);
@@ -748,58 +752,60 @@ __device__ void hetrd_warp_packed(cplx<R>* P, int n, R* d, R* e, cplx<R>* tau, c
             k += 1;
             continue;
         }
-        // ---- column k+1 takes step k's update: A22(r, 0) -= v_r conj(w_0) + w_r conj(v_0)
-        for (int r = lane; r < m; r += 32) {
-            C t = cfmsc(vb[r], wb[0], c0[r]);
-            t = cfmsc(wb[r], vb[0], t);
-            if (r == 0) t.y = R(0);
-            c0[r] = t;
-        }
-        __syncwarp();
-        // ---- step k+1 on the trailing matrix A22' (rows and columns >= k+2, order m1) without
-        // step k's update: p' = tau' (A22' v' - v^ (w^^H v') - w^ (v^^H v'))
-        const int m1 = m - 1;
-        C* x1 = c0 + 1;                                 // x1[i] = A(k+2+i, k+1)
-        const WarpReflector<R> f1 = warp_reflector<R>(x1, m1);
-        if (lane == 0) { e[k + 1] = f1.beta; tau[k + 1] = f1.tau; }
-        warp_store_reflector<R>(x1, m1, f1, vb2);
-        __syncwarp();
-        C* c1 = P + pk(k + 2, n);
-        const C* vh = vb + 1;                           // v^, w^ over the rows of A22'
-        const C* wh = wb + 1;
-        {
-            C g1 = zero, g2 = zero;                     // w^^H v', v^^H v'
-            for (int i = lane; i < m1; i += 32) {
-                g1 = cfmac(wh[i], vb2[i], g1);
-                g2 = cfmac(vh[i], vb2[i], g2);
+        if constexpr (TWO_STEP) {
+            // ---- column k+1 takes step k's update: A22(r, 0) -= v_r conj(w_0) + w_r conj(v_0)
+            for (int r = lane; r < m; r += 32) {
+                C t = cfmsc(vb[r], wb[0], c0[r]);
+                t = cfmsc(wb[r], vb[0], t);
+                if (r == 0) t.y = R(0);
+                c0[r] = t;
             }
-            g1.x = warp_sum(g1.x); g1.y = warp_sum(g1.y);
-            g2.x = warp_sum(g2.x); g2.y = warp_sum(g2.y);
-            C s1, s2;
-            warp_hemv_rows<R>(c1, m1, vb2, s1, s2);
-            const int q1 = lane, q2 = m1 - 1 - lane, hh = (m1 + 1) >> 1;
-            const bool o1 = lane < hh, o2 = o1 && q2 != q1;
-            C p1 = zero, p2 = zero;
-            if (o1) { s1 = cfms(vh[q1], g1, s1); s1 = cfms(wh[q1], g2, s1); p1 = cmul(f1.tau, s1); }
-            if (o2) { s2 = cfms(vh[q2], g1, s2); s2 = cfms(wh[q2], g2, s2); p2 = cmul(f1.tau, s2); }
-            C dot = zero;
-            if (o1) dot = cfmac(p1, vb2[q1], dot);
-            if (o2) dot = cfmac(p2, vb2[q2], dot);
-            dot.x = warp_sum(dot.x);
-            dot.y = warp_sum(dot.y);
-            const C a2 = cscale(cmul(f1.tau, dot), R(-0.5));
-            if (o1) wb2[q1] = cfma(a2, vb2[q1], p1);
-            if (o2) wb2[q2] = cfma(a2, vb2[q2], p2);
+            __syncwarp();
+            // ---- step k+1 on the trailing matrix A22' (rows and columns >= k+2, order m1) without
+            // step k's update: p' = tau' (A22' v' - v^ (w^^H v') - w^ (v^^H v'))
+            const int m1 = m - 1;
+            C* x1 = c0 + 1;                                 // x1[i] = A(k+2+i, k+1)
+            const WarpReflector<R> f1 = warp_reflector<R>(x1, m1);
+            if (lane == 0) { e[k + 1] = f1.beta; tau[k + 1] = f1.tau; }
+            warp_store_reflector<R>(x1, m1, f1, vb2);
+            __syncwarp();
+            C* c1 = P + pk(k + 2, n);
+            const C* vh = vb + 1;                           // v^, w^ over the rows of A22'
+            const C* wh = wb + 1;
+            {
+                C g1 = zero, g2 = zero;                     // w^^H v', v^^H v'
+                for (int i = lane; i < m1; i += 32) {
+                    g1 = cfmac(wh[i], vb2[i], g1);
+                    g2 = cfmac(vh[i], vb2[i], g2);
+                }
+                g1.x = warp_sum(g1.x); g1.y = warp_sum(g1.y);
+                g2.x = warp_sum(g2.x); g2.y = warp_sum(g2.y);
+                C s1, s2;
+                warp_hemv_rows<R>(c1, m1, vb2, s1, s2);
+                const int q1 = lane, q2 = m1 - 1 - lane, hh = (m1 + 1) >> 1;
+                const bool o1 = lane < hh, o2 = o1 && q2 != q1;
+                C p1 = zero, p2 = zero;
+                if (o1) { s1 = cfms(vh[q1], g1, s1); s1 = cfms(wh[q1], g2, s1); p1 = cmul(f1.tau, s1); }
+                if (o2) { s2 = cfms(vh[q2], g1, s2); s2 = cfms(wh[q2], g2, s2); p2 = cmul(f1.tau, s2); }
+                C dot = zero;
+                if (o1) dot = cfmac(p1, vb2[q1], dot);
+                if (o2) dot = cfmac(p2, vb2[q2], dot);
+                dot.x = warp_sum(dot.x);
+                dot.y = warp_sum(dot.y);
+                const C a2 = cscale(cmul(f1.tau, dot), R(-0.5));
+                if (o1) wb2[q1] = cfma(a2, vb2[q1], p1);
+                if (o2) wb2[q2] = cfma(a2, vb2[q2], p2);
+            }
+            __syncwarp();
+            // ---- both updates on A22': step k's, then step k+1's
+            {
+                const C* vq[2] = {vh, vb2};
+                const C* wq[2] = {wh, wb2};
+                warp_her2_rows<R, 2>(c1, m1, vq, wq);
+            }
+            __syncwarp();
+            k += 2;
         }
-        __syncwarp();
-        // ---- both updates on A22': step k's, then step k+1's
-        {
-            const C* vq[2] = {vh, vb2};
-            const C* wq[2] = {wh, wb2};
-            warp_her2_rows<R, 2>(c1, m1, vq, wq);
-        }
-        __syncwarp();
-        k += 2;
     }
     for (int i = lane; i < n; i += 32) d[i] = P[pk(i, n)].x;
     if (lane == 0 && n >= 1) e[n - 1] = R(0);
