@@ -264,28 +264,31 @@ size_t sbg_workspace_bytes(int n, int /*precision*/, int pairs) {
 }
 
 int sbg_solver_matrix_size(const sbg_solver* s) { return s ? s->n : 0; }
-int sbg_solver_schedule(const sbg_solver* s, int* out6) {
+int sbg_solver_schedule(const sbg_solver* s, int* out7) {
     return guarded([&] {
-        if (!s || !out6) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
+        if (!s || !out7) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
         const sbg::Schedule& c = s->sched;
-        const int v[6] = {c.hetrd_threads, c.pair_warps, c.col_exact, c.back_lanes, c.ql_warps, c.chain_threads};
-        for (int i = 0; i < 6; ++i) out6[i] = v[i];
+        const int v[7] = {c.hetrd_threads, c.pair_warps, c.col_exact, c.back_lanes, c.ql_warps, c.chain_threads,
+                          c.back_qpass};
+        for (int i = 0; i < 7; ++i) out7[i] = v[i];
     });
 }
 
-int sbg_solver_set_schedule(sbg_solver* s, const int* in6) {
+int sbg_solver_set_schedule(sbg_solver* s, const int* in7) {
     return guarded([&] {
-        if (!s || !in6) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
+        if (!s || !in7) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
         sbg::Schedule c;
-        c.hetrd_threads = in6[0];
-        c.pair_warps = in6[1];
-        c.col_exact = in6[2];
-        c.back_lanes = in6[3];
-        c.ql_warps = in6[4];
-        c.chain_threads = in6[5];
+        c.hetrd_threads = in7[0];
+        c.pair_warps = in7[1];
+        c.col_exact = in7[2];
+        c.back_lanes = in7[3];
+        c.ql_warps = in7[4];
+        c.chain_threads = in7[5];
+        c.back_qpass = in7[6];
         const bool ok = (c.hetrd_threads == 128 || c.hetrd_threads == 256) &&
                         (c.pair_warps == 1 || c.pair_warps == 2 || c.pair_warps == 4) &&
                         (c.col_exact == 0 || c.col_exact == 1) && (c.back_lanes == 1 || c.back_lanes == 2) &&
+                        (c.back_qpass == 1 || c.back_qpass == 2) &&
                         c.ql_warps >= 1 && c.ql_warps <= 16 &&
                         (c.chain_threads == 32 || c.chain_threads == 64 || c.chain_threads == 128 ||
                          c.chain_threads == 256);

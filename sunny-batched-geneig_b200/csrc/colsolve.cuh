@@ -180,6 +180,89 @@ __device__ __forceinline__ void grp_apply_q(const cplx<R>* LV, int ld, const cpl
     }
 }
 
+// y <- Q y as grp_apply_q, two reflectors per pass.  For the pair (a, b = a - 1), H_a applied
+// first: one pass over the rows forms both dot products s_a = v_a^H y (rows > a) and
+// s_b = v_b^H y (rows >= a), then t_a = tau_a s_a and t_b = tau_b (s_b - c_a t_a) with
+// c_a = v_b^H v_a (cpair[a], formed once per pair of the batch), and one pass subtracts
+// v_a t_a, then v_b t_b, from every row -- the same two reflections, in the same order, with half
+// as many dependent dot-product / update rounds for the column to wait on.  A reflector with
+// tau = 0 contributes t = 0.  The compiler barrier after each block of 8 rows keeps the two
+// vectors' loads from being hoisted ahead en bloc (which spilled the column's registers).
+template <int G, int RM, typename R>
+__device__ __forceinline__ void grp_apply_q2(const cplx<R>* LV, int ld, const cplx<R>* tau, const cplx<R>* cpair,
+                                             cplx<R> (&y)[RM], int n, int g) {
+    using C = cplx<R>;
+    const int nb = ((n - 1) / G) >> 3;               // block of the highest slot any lane holds
+    int k = n - 2;
+#pragma unroll 1
+    for (; k >= 1; k -= 2) {
+        const int a = k;
+        const C* va = LV + a;                        // v_a(i) = va[i * ld], i >= a + 1
+        // v_b(i) = va[i * ld - 1] (row b = a - 1 of the tile), i >= a, v_b(a) = 1: one base pointer,
+        // so every row's two loads are immediate offsets from it
+        const int kb = a / G - 1;                    // slots <= kb hold only rows < a on every lane
+        C sa0 = mk<R>(R(0), R(0)), sa1 = sa0, sb0 = sa0, sb1 = sa0;
+#define SBG_S(I) if constexpr ((I) < RM) { const int i = G * (I) + g; if (i >= a && i < n) { \
+        const C vai = (i > a) ? va[i * ld] : mk<R>(R(0), R(0)); \
+        if (((I) & 1) == 0) { sb0 = cfmac(va[i * ld - 1], y[I], sb0); sa0 = cfmac(vai, y[I], sa0); } \
+        else { sb1 = cfmac(va[i * ld - 1], y[I], sb1); sa1 = cfmac(vai, y[I], sa1); } } }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= kb) break; SBG_ROWS8(SBG_S, B) asm volatile("" ::: "memory");
+        switch (nb) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+        C sa = cadd(sa0, sa1), sb = cadd(sb0, sb1);
+        if constexpr (G > 1) {
+#pragma unroll
+            for (int m = 1; m < G; m <<= 1) {
+                sa.x += shfl_xor(sa.x, m); sa.y += shfl_xor(sa.y, m);
+                sb.x += shfl_xor(sb.x, m); sb.y += shfl_xor(sb.y, m);
+            }
+        }
+        const C ta = cmul(tau[a], sa);
+        const C tb = cmul(tau[a - 1], cfms(cpair[a], ta, sb));
+        asm volatile("" ::: "memory");               // reload v below rather than hold it in registers
+#define SBG_S(I) if constexpr ((I) < RM) { const int i = G * (I) + g; if (i >= a && i < n) { \
+        const C vai = (i > a) ? va[i * ld] : mk<R>(R(0), R(0)); \
+        y[I] = cfms(va[i * ld - 1], tb, cfms(vai, ta, y[I])); } }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= kb) break; SBG_ROWS8(SBG_S, B) asm volatile("" ::: "memory");
+        switch (nb) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+    }
+    if (k == 0) {                                    // an odd count: H_0 alone
+        const C tk = tau[0];
+        C s0 = mk<R>(R(0), R(0)), s1 = s0;
+#define SBG_S(I) if constexpr ((I) < RM) { const int i = G * (I) + g; if (i > 0 && i < n) { \
+        if (((I) & 1) == 0) s0 = cfmac(LV[i * ld], y[I], s0); else s1 = cfmac(LV[i * ld], y[I], s1); } }
+#define SBG_K(B) case B: SBG_ROWS8(SBG_S, B)
+        switch (nb) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+        C s = cadd(s0, s1);
+        if constexpr (G > 1) {
+#pragma unroll
+            for (int m = 1; m < G; m <<= 1) { s.x += shfl_xor(s.x, m); s.y += shfl_xor(s.y, m); }
+        }
+        s = cmul(tk, s);
+#define SBG_S(I) if constexpr ((I) < RM) { const int i = G * (I) + g; if (i > 0 && i < n) y[I] = cfms(LV[i * ld], s, y[I]); }
+#define SBG_K(B) case B: SBG_ROWS8(SBG_S, B)
+        switch (nb) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+    }
+}
+
+// c_a = v_{a-1}^H v_a for a = 1 .. n-2 into cpair[a] (the coupling grp_apply_q2 needs), reflectors
+// along the rows of the LV tile as there; every thread of the CTA calls (T threads).
+template <typename R>
+__device__ __forceinline__ void reflector_couplings(const cplx<R>* LV, int ld, int n, cplx<R>* cpair, int T) {
+    for (int a = 1 + static_cast<int>(threadIdx.x); a + 1 < n; a += T) {
+        cplx<R> c = mk<R>(R(0), R(0));
+        for (int i = a + 1; i < n; ++i) c = cfmac(LV[(a - 1) + i * ld], LV[a + i * ld], c);
+        cpair[a] = c;
+    }
+}
+
 // y <- L^{-1} y (forward substitution) with L packed by columns (Lp, order n): lane g of the
 // group holds rows G r + g.  Each solved w_k stays in its slot of the owning lane.
 template <int G, int RM, typename R>

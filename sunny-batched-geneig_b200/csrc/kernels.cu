@@ -181,13 +181,14 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_reduce(int mode, const d
 }
 
 struct BackSmem {
-    size_t LVs, invd, tau, bar, total;
+    size_t LVs, invd, tau, cpair, bar, total;
     __host__ __device__ BackSmem(int n, int tile_ld_override = 0) {
         const size_t ld = static_cast<size_t>(tile_ld_override > 0 ? tile_ld_override : tile_ld(n));
         size_t o = 0;
         LVs = o;  o += 16 * ld * n;
         invd = o; o += align_up(8 * n, 16);
         tau = o;  o += 16 * n;
+        cpair = o; o += 16 * n;
         bar = o;  o += 16;
         total = o;
     }
@@ -310,7 +311,7 @@ __global__ void __launch_bounds__(NMAX, 4) k_hegst_col(int mode, const double2* 
 template <int NMAX, int G>
 __host__ __device__ constexpr int back_col_threads() { return (NMAX * G + 31) / 32 * 32; }
 
-template <int NMAX, int G, bool EXACT>
+template <int NMAX, int G, bool EXACT, int QP>
 __global__ void __launch_bounds__(back_col_threads<NMAX, G>(), G == 1 ? 4 : 3) k_back_col(int mode, int n_arg, int batch,
                                                                             Workspace ws, double2* __restrict__ X,
                                                                             int* __restrict__ info) {
@@ -365,8 +366,13 @@ __global__ void __launch_bounds__(back_col_threads<NMAX, G>(), G == 1 ? 4 : 3) k
     for (int i = tid; i < n; i += T) tau_s[i] = ws.tau[static_cast<size_t>(n) * b + i];
     wait_copies(bar, info + b);
     for (int i = tid; i < n; i += T) invd[i] = 1.0 / LVs[i + i * ld].x;
+    double2* cpair = reinterpret_cast<double2*>(smem + lay.cpair);
+    if (QP == 2 && mode != kBackLOnly) reflector_couplings<double>(LVs, ld, n, cpair, T);
     __syncthreads();               // all of Z is in registers before any X is stored over it
-    if (mode != kBackLOnly) grp_apply_q<G, RM, double>(LVs, ld, tau_s, y, n, g);
+    if (mode != kBackLOnly) {
+        if constexpr (QP == 2) grp_apply_q2<G, RM, double>(LVs, ld, tau_s, cpair, y, n, g);
+        else grp_apply_q<G, RM, double>(LVs, ld, tau_s, y, n, g);
+    }
     double2* xcol = Xb + static_cast<size_t>(col) * n;
     if (mode == kBackFull || mode == kBackLOnly) {
         grp_trsm_lowerH<G, RM>(LVs, ld, invd, y, n, g, [&](int k, double2 x) { if (own) xcol[k] = x; });
@@ -1447,11 +1453,17 @@ cudaError_t launch_hetrd_c64(int n, int batch, const double2* C, const Workspace
 
 template <int NMAX, int G, bool EXACT = false>
 void run_back_col_g(int mode, int n, int batch, const Workspace& ws, double2* X, int* info, size_t smem,
-                    cudaStream_t stream) {
-    static SmemOptIn f;
-    set_max_smem_once(k_back_col<NMAX, G, EXACT>, f);
+                    cudaStream_t stream, int qpass) {
     smem = BackSmem(n, (((NMAX | 1) & 7) == 7) ? (NMAX | 1) + 2 : (NMAX | 1)).total;
-    k_back_col<NMAX, G, EXACT><<<batch, back_col_threads<NMAX, G>(), smem, stream>>>(mode, n, batch, ws, X, info);
+    if (qpass == 2) {
+        static SmemOptIn f2;
+        set_max_smem_once(k_back_col<NMAX, G, EXACT, 2>, f2);
+        k_back_col<NMAX, G, EXACT, 2><<<batch, back_col_threads<NMAX, G>(), smem, stream>>>(mode, n, batch, ws, X, info);
+    } else {
+        static SmemOptIn f1;
+        set_max_smem_once(k_back_col<NMAX, G, EXACT, 1>, f1);
+        k_back_col<NMAX, G, EXACT, 1><<<batch, back_col_threads<NMAX, G>(), smem, stream>>>(mode, n, batch, ws, X, info);
+    }
 }
 
 
@@ -1504,21 +1516,22 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     if (n <= kColMaxN) {
         const bool two = shape.back_lanes == 2;
+        const int qp = shape.back_qpass == 2 ? 2 : 1;
         if (n == 32 && shape.col_exact) {
-            if (two) run_back_col_g<32, 2, true>(mode, n, batch, ws, X, info, smem, stream);
-            else run_back_col_g<32, 1, true>(mode, n, batch, ws, X, info, smem, stream);
+            if (two) run_back_col_g<32, 2, true>(mode, n, batch, ws, X, info, smem, stream, qp);
+            else run_back_col_g<32, 1, true>(mode, n, batch, ws, X, info, smem, stream, qp);
         } else if (n == 54 && shape.col_exact) {
-            if (two) run_back_col_g<54, 2, true>(mode, n, batch, ws, X, info, smem, stream);
-            else run_back_col_g<54, 1, true>(mode, n, batch, ws, X, info, smem, stream);
+            if (two) run_back_col_g<54, 2, true>(mode, n, batch, ws, X, info, smem, stream, qp);
+            else run_back_col_g<54, 1, true>(mode, n, batch, ws, X, info, smem, stream, qp);
         } else if (n <= 32) {
-            if (two) run_back_col_g<32, 2>(mode, n, batch, ws, X, info, smem, stream);
-            else run_back_col_g<32, 1>(mode, n, batch, ws, X, info, smem, stream);
+            if (two) run_back_col_g<32, 2>(mode, n, batch, ws, X, info, smem, stream, qp);
+            else run_back_col_g<32, 1>(mode, n, batch, ws, X, info, smem, stream, qp);
         } else if (n <= 48) {
-            if (two) run_back_col_g<48, 2>(mode, n, batch, ws, X, info, smem, stream);
-            else run_back_col_g<48, 1>(mode, n, batch, ws, X, info, smem, stream);
+            if (two) run_back_col_g<48, 2>(mode, n, batch, ws, X, info, smem, stream, qp);
+            else run_back_col_g<48, 1>(mode, n, batch, ws, X, info, smem, stream, qp);
         } else {
-            if (two) run_back_col_g<56, 2>(mode, n, batch, ws, X, info, smem, stream);
-            else run_back_col_g<56, 1>(mode, n, batch, ws, X, info, smem, stream);
+            if (two) run_back_col_g<56, 2>(mode, n, batch, ws, X, info, smem, stream, qp);
+            else run_back_col_g<56, 1>(mode, n, batch, ws, X, info, smem, stream, qp);
         }
         return cudaGetLastError();
     }

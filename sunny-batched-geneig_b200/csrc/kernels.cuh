@@ -75,11 +75,13 @@ enum BackMode : int {
 //   col_exact   k_hegst_col / k_back_col: the exact-n instantiation where one exists (n = 32, 54)
 //               instead of the one for the next larger NMAX
 //   back_lanes  lanes per column of k_back_col (n <= 56): 1 or 2
+//   back_qpass  reflectors per pass of k_back_col's Q application (n <= 56): 1 or 2
 struct LaunchShape {
     int threads = 256;
     int pair_warps = 2;
     int col_exact = 1;
     int back_lanes = 1;
+    int back_qpass = 1;
 };
 
 // Launchers (asynchronous on `stream`; return cudaSuccess or the launch error).

@@ -26,7 +26,7 @@ namespace sbg {
 namespace {
 
 constexpr const char* kTableMagic = "SBGTUNE";
-constexpr int kTableVersion = 4;
+constexpr int kTableVersion = 5;
 constexpr const char* kLibVersion = "sbg-geneig-0.2";
 
 std::mutex g_mu;
@@ -99,7 +99,7 @@ bool load_table(const std::string& path, const std::string& key, std::vector<Tab
         std::string tag;
         TableEntry e{};
         es >> tag >> e.n >> e.precision >> e.s.hetrd_threads >> e.s.pair_warps >> e.s.col_exact >> e.s.back_lanes >>
-            e.s.ql_warps >> e.s.chain_threads >> e.us;
+            e.s.back_qpass >> e.s.ql_warps >> e.s.chain_threads >> e.us;
         if (tag != "entry" || !es) { out.clear(); return false; }
         out.push_back(e);
     }
@@ -127,7 +127,8 @@ void save_table(const std::string& path, const std::string& key, const std::vect
     body << "device " << key << "\n";
     for (const auto& e : entries)
         body << "entry " << e.n << " " << e.precision << " " << e.s.hetrd_threads << " " << e.s.pair_warps << " "
-             << e.s.col_exact << " " << e.s.back_lanes << " " << e.s.ql_warps << " " << e.s.chain_threads << " "
+             << e.s.col_exact << " " << e.s.back_lanes << " " << e.s.back_qpass << " " << e.s.ql_warps << " "
+             << e.s.chain_threads << " "
              << e.us << "\n";
     const std::string b = body.str();
     char buf[32];
@@ -312,15 +313,18 @@ bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double&
         cudaMemcpyAsync(bench.Z.p, bench.X.p, 16 * bench.nn * count, cudaMemcpyDeviceToDevice, bench.st);
         double bt = 1e30;
         const std::vector<int> lane_opts = n <= 56 ? std::vector<int>{1, 2} : std::vector<int>{base.back_lanes};
-        for (int gl : lane_opts) {
-            Schedule s = win;
-            s.back_lanes = gl;
-            const double ms = median_ms([&] {
-                cudaMemcpyAsync(bench.X.p, bench.Z.p, 16 * bench.nn * count, cudaMemcpyDeviceToDevice, bench.st);
-                bench.back(s);
-            }, 3, bench.st);
-            if (ms < bt) { bt = ms; win.back_lanes = gl; }
-        }
+        const std::vector<int> qpass_opts = n <= 56 ? std::vector<int>{2, 1} : std::vector<int>{base.back_qpass};
+        for (int gl : lane_opts)
+            for (int qp : qpass_opts) {
+                Schedule s = win;
+                s.back_lanes = gl;
+                s.back_qpass = qp;
+                const double ms = median_ms([&] {
+                    cudaMemcpyAsync(bench.X.p, bench.Z.p, 16 * bench.nn * count, cudaMemcpyDeviceToDevice, bench.st);
+                    bench.back(s);
+                }, 3, bench.st);
+                if (ms < bt) { bt = ms; win.back_lanes = gl; win.back_qpass = qp; }
+            }
         t_total += bt;
     }
     // validate the winner against the built-in schedule and against the residual
@@ -356,8 +360,9 @@ bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double&
     best = win;
     best_us = 1e3 * t_total / count;
     std::fprintf(stderr, "[sbg autotune] n=%d precision=%d: pairs/CTA=%d exact=%d hetrd_threads=%d back_lanes=%d "
-                 "ql_chain=%d ql_apply_warps=%d (%.3f us/pair)\n", n, precision, win.pair_warps, win.col_exact,
-                 win.hetrd_threads, win.back_lanes, win.chain_threads, win.ql_warps, best_us);
+                 "back_qpass=%d ql_chain=%d ql_apply_warps=%d (%.3f us/pair)\n", n, precision, win.pair_warps,
+                 win.col_exact, win.hetrd_threads, win.back_lanes, win.back_qpass, win.chain_threads, win.ql_warps,
+                 best_us);
     return true;
 }
 

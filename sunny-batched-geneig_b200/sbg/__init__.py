@@ -180,12 +180,13 @@ class Solver:
     def reserve(self, pairs: int, stream_slots: int = 1) -> None:
         _check(self._lib.sbg_solver_reserve(self._h, pairs, stream_slots), "sbg_solver_reserve")
 
-    SCHEDULE_FIELDS = ("hetrd_threads", "pairs_per_cta", "col_exact", "back_lanes", "ql_warps", "chain_threads")
+    SCHEDULE_FIELDS = ("hetrd_threads", "pairs_per_cta", "col_exact", "back_lanes", "ql_warps", "chain_threads",
+                       "back_qpass")
 
     @property
     def schedule(self) -> dict:
         """The launch schedule (sbg_solver_schedule): CTA shapes of the stage kernels."""
-        out = (ctypes.c_int * 6)()
+        out = (ctypes.c_int * len(self.SCHEDULE_FIELDS))()
         _check(self._lib.sbg_solver_schedule(self._h, out), "sbg_solver_schedule")
         return dict(zip(self.SCHEDULE_FIELDS, list(out)))
 
@@ -193,7 +194,7 @@ class Solver:
     def schedule(self, sched: dict) -> None:
         cur = self.schedule
         cur.update(sched)
-        vals = (ctypes.c_int * 6)(*[int(cur[k]) for k in self.SCHEDULE_FIELDS])
+        vals = (ctypes.c_int * len(self.SCHEDULE_FIELDS))(*[int(cur[k]) for k in self.SCHEDULE_FIELDS])
         _check(self._lib.sbg_solver_set_schedule(self._h, vals), "sbg_solver_set_schedule")
 
     @property

@@ -3,8 +3,8 @@
 The reference validates an autotuned block size only against its own suggested configuration
 (src/nvrtc/nvrtc_solver.cpp:735-740).  Here every candidate of the sweep -- pairs per CTA of the
 warp-per-pair Cholesky / Householder kernels (the reference's batches per block), exact-n versus
-generic column kernels, one or two lanes per column in the back-transform, the QL chain's CTA
-size -- is set through sbg_solver_set_schedule and its results are compared with zhegv under the
+generic column kernels, one or two lanes per column and one or two reflectors per pass in the
+back-transform, the QL chain's CTA size -- is set through sbg_solver_set_schedule and its results are compared with zhegv under the
 parity gates, and so is the schedule the autotuner picks at n = 32 and 54.
 """
 from __future__ import annotations
@@ -39,19 +39,20 @@ def test_every_candidate_schedule_passes_the_gates(n, precision, pairs_and_oracl
     s = sbg.Solver(n, precision=precision)
     base = s.schedule
     seen = 0
-    for pw, ex, gl, ct in itertools.product((1, 2, 4), (0, 1), (1, 2), (64, 128, 256)):
-        s.schedule = dict(base, pairs_per_cta=pw, col_exact=ex, back_lanes=gl, chain_threads=ct)
+    for pw, ex, gl, qp, ct in itertools.product((1, 2, 4), (0, 1), (1, 2), (1, 2), (64, 128, 256)):
+        s.schedule = dict(base, pairs_per_cta=pw, col_exact=ex, back_lanes=gl, back_qpass=qp, chain_threads=ct)
         assert s.schedule["pairs_per_cta"] == pw and s.batches_per_block == pw
         W, X, info = run(s, A, B)
         check(A, B, W, X, info, Wr, Xr, n, relative=True)
         seen += 1
-    assert seen == 36
+    assert seen == 72
     s.close()
 
 
 def test_schedule_values_are_checked():
     s = sbg.Solver(54)
-    for bad in (dict(pairs_per_cta=3), dict(back_lanes=4), dict(hetrd_threads=96), dict(chain_threads=100)):
+    for bad in (dict(pairs_per_cta=3), dict(back_lanes=4), dict(hetrd_threads=96), dict(chain_threads=100),
+                dict(back_qpass=3)):
         with pytest.raises(sbg.SolverError):
             s.schedule = bad
     s.close()
