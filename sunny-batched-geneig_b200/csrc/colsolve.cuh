@@ -115,6 +115,76 @@ __device__ __forceinline__ void col_trsm_lower(const cplx<R>* Lp, const R* invd,
     }
 }
 
+// col_trsm_lower two steps per sweep: the pivots of k and k+1 are selected together, w_k formed,
+// row k+1 updated by it alone and w_{k+1} formed, then ONE sweep over the rows below subtracts
+// L(i, k) w_k and L(i, k+1) w_{k+1}, in that order (every y[i] takes the same operations as in
+// the one-step sweep).  Since the descending sweep reaches row k+1 last, the next pivot no longer
+// waits for a whole sweep per step.
+template <int NMAX, typename R, typename Out>
+__device__ __forceinline__ void col_trsm_lower2(const cplx<R>* Lp, const R* invd, cplx<R> (&y)[NMAX], int n,
+                                                Out&& out) {
+    using C = cplx<R>;
+    int k = 0;
+    for (; k + 1 < n; k += 2) {
+        C piv = y[0], piv1 = y[0];
+#define SBG_SEL(I) case I: if constexpr ((I) < NMAX) { piv = y[I]; if constexpr ((I) + 1 < NMAX) piv1 = y[(I) + 1]; } break;
+        switch (k) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
+        const C* lk = Lp + pk(k, n) - k;           // lk[i] = L(i, k)
+        const C* lk1 = Lp + pk(k + 1, n) - (k + 1); // lk1[i] = L(i, k + 1)
+        const C wk = cscale(piv, invd[k]);
+        out(k, wk);
+        const C wk1 = cscale(cfms(lk[k + 1], wk, piv1), invd[k + 1]);
+        out(k + 1, wk1);
+#define SBG_S(I) if constexpr ((I) < NMAX) { if ((I) > k + 1 && (I) < n) y[I] = cfms(lk1[I], wk1, cfms(lk[I], wk, y[I])); }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= k + 1) break; SBG_ROWS8(SBG_S, B)
+        switch ((n - 1) >> 3) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+    }
+    if (k < n) {                                  // an odd n: the last row alone
+        C piv = y[0];
+#define SBG_SEL(I) case I: if constexpr ((I) < NMAX) piv = y[I]; break;
+        switch (k) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
+        out(k, cscale(piv, invd[k]));
+    }
+}
+
+// row_trsm_right_lowerH two steps per sweep, as col_trsm_lower2: c_k, then row k+1's value takes
+// c_k's term alone and gives c_{k+1}, then one sweep subtracts both from the columns above.
+template <int NMAX, typename R, typename Out>
+__device__ __forceinline__ void row_trsm_right_lowerH2(const cplx<R>* Lp, const R* invd, cplx<R> (&y)[NMAX], int n,
+                                                       int i, int kmax, Out&& out) {
+    using C = cplx<R>;
+    int k = 0;
+    for (; k + 1 <= kmax; k += 2) {              // kmax: the largest row of the warp (uniform loop)
+        C piv = y[0], piv1 = y[0];
+#define SBG_SEL(I) case I: if constexpr ((I) < NMAX) { piv = y[I]; if constexpr ((I) + 1 < NMAX) piv1 = y[(I) + 1]; } break;
+        switch (k) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
+        const C* lk = Lp + pk(k, n) - k;          // lk[kk] = L(kk, k)
+        const C* lk1 = Lp + pk(k + 1, n) - (k + 1);
+        const C ck = cscale(piv, invd[k]);
+        if (k <= i) out(k, ck);
+        const C ck1 = cscale(cfmsc(ck, lk[k + 1], piv1), invd[k + 1]);
+        if (k + 1 <= i) out(k + 1, ck1);
+#define SBG_S(I) if constexpr ((I) < NMAX) { if ((I) > k + 1 && (I) <= i) y[I] = cfmsc(ck1, lk1[I], cfmsc(ck, lk[I], y[I])); }
+#define SBG_K(B) case B: if ((B) * 8 + 7 <= k + 1) break; SBG_ROWS8(SBG_S, B)
+        switch (kmax >> 3) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+    }
+    if (k <= kmax) {                              // one step left
+        C piv = y[0];
+#define SBG_SEL(I) case I: if constexpr ((I) < NMAX) piv = y[I]; break;
+        switch (k) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
+        const C ck = cscale(piv, invd[k]);
+        if (k <= i) out(k, ck);
+    }
+}
+
 // Row i of C = W L^{-H}, columns kk <= i (the rest is not needed: C is Hermitian).
 // y holds W(i, 0..i); the solved C(i, k) go through out(k, c).
 template <int NMAX, typename R, typename Out>

@@ -287,14 +287,14 @@ __global__ void __launch_bounds__(NMAX, 4) k_hegst_col(int mode, const double2* 
     wait_copies(bar, info + b);
     for (int i = tid; i < n; i += NMAX) invd[i] = 1.0 / Lp[pk(i, n)].x;
     __syncthreads();
-    if (own) col_trsm_lower<NMAX>(Lp, invd, y, n, [&](int k, double2 w) { Ob[k + static_cast<size_t>(tid) * n] = w; });
+    if (own) col_trsm_lower2<NMAX>(Lp, invd, y, n, [&](int k, double2 w) { Ob[k + static_cast<size_t>(tid) * n] = w; });
     __syncthreads();
     if (own) {
         const int i = tid;
 #pragma unroll
         for (int kk = 0; kk < NMAX; ++kk) y[kk] = (kk <= i) ? Ob[i + static_cast<size_t>(kk) * n] : make_double2(0.0, 0.0);
         const int kmax = min(n - 1, (tid | 31));            // the warp's largest row: uniform loop bound
-        row_trsm_right_lowerH<NMAX>(Lp, invd, y, n, i, kmax, [&](int k, double2 c) {
+        row_trsm_right_lowerH2<NMAX>(Lp, invd, y, n, i, kmax, [&](int k, double2 c) {
             if (k == i) c.y = 0.0;
             Ob[i + static_cast<size_t>(k) * n] = c;
         });
