@@ -390,4 +390,50 @@ __device__ __forceinline__ void grp_trsm_lowerH(const cplx<R>* LV, int ld, const
     }
 }
 
+// grp_trsm_lowerH two steps per sweep: rows k and k-1 are selected together, x_k formed, row k-1
+// takes x_k's term alone and gives x_{k-1}, then one sweep over the rows above subtracts
+// conj(L(k, i)) x_k and conj(L(k-1, i)) x_{k-1}, in that order (the same operations per entry as
+// the one-step sweeps, half as many sweeps).
+template <int G, int RM, typename R, typename Out>
+__device__ __forceinline__ void grp_trsm_lowerH2(const cplx<R>* LV, int ld, const R* invd, cplx<R> (&y)[RM], int n,
+                                                 int g, Out&& out) {
+    using C = cplx<R>;
+    const int lane = threadIdx.x & 31;
+    int k = n - 1;
+    for (; k >= 1; k -= 2) {
+        const int rk = k / G, gk = k - rk * G;       // row k: slot rk of lane gk
+        const int rk1 = (k - 1) / G, gk1 = (k - 1) - rk1 * G;
+        C piv = y[0], piv1 = y[0];
+#define SBG_SEL(I) case I: if constexpr ((I) < RM) piv = y[I]; break;
+        switch (rk) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
+#define SBG_SEL(I) case I: if constexpr ((I) < RM) piv1 = y[I]; break;
+        switch (rk1) { SBG_DESC64(SBG_SEL) default: break; }
+#undef SBG_SEL
+        if constexpr (G > 1) {
+            piv = cshfl(piv, (lane & ~(G - 1)) | gk);
+            piv1 = cshfl(piv1, (lane & ~(G - 1)) | gk1);
+        }
+        const C* lrow = LV + k;                      // L(k, i) = lrow[i * ld], i < k
+        const C* lrow1 = LV + k - 1;                 // L(k-1, i) = lrow1[i * ld], i < k - 1
+        const C xk = cscale(piv, invd[k]);
+        if (g == gk) out(k, xk);
+        const C xk1 = cscale(cfms(cconj(lrow[(k - 1) * ld]), xk, piv1), invd[k - 1]);
+        if (g == gk1) out(k - 1, xk1);
+        if (k == 1) { k = -1; break; }
+#define SBG_S(I) if constexpr ((I) < RM) { const int i = G * (I) + g; if (i < k - 1) \
+        y[I] = cfms(cconj(lrow1[i * ld]), xk1, cfms(cconj(lrow[i * ld]), xk, y[I])); }
+#define SBG_K(B) case B: SBG_ROWS8(SBG_S, B)
+        switch (((k - 2) / G) >> 3) { SBG_BLOCKS(SBG_K) default: break; }
+#undef SBG_K
+#undef SBG_S
+    }
+    if (k == 0) {                                    // an odd n: row 0 alone
+        C piv = y[0];
+        if constexpr (G > 1) piv = cshfl(piv, lane & ~(G - 1));
+        const C x0 = cscale(piv, invd[0]);
+        if (g == 0) out(0, x0);
+    }
+}
+
 }  // namespace sbg

@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(back_col_threads<NMAX, G>(), G == 1 ? 4 : 3) k
     }
     double2* xcol = Xb + static_cast<size_t>(col) * n;
     if (mode == kBackFull || mode == kBackLOnly) {
-        grp_trsm_lowerH<G, RM>(LVs, ld, invd, y, n, g, [&](int k, double2 x) { if (own) xcol[k] = x; });
+        grp_trsm_lowerH2<G, RM>(LVs, ld, invd, y, n, g, [&](int k, double2 x) { if (own) xcol[k] = x; });
     } else if (own) {
 #pragma unroll
         for (int r = 0; r < RM; ++r) {
