@@ -426,8 +426,8 @@ struct MidSmem {
 
 // f(a, row, j) on the packed-lower elements A22(row, j), j <= row, of the row pairs
 // (q, m-1-q): each pair's walk (row q's q+1 terms, then row m-1-q's) split into kMidGroup chunks.
-template <class F>
-__device__ __forceinline__ void mid_pair_walk(double2* c0, int m, F&& f) {
+template <class T, class F>
+__device__ __forceinline__ void mid_pair_walk(T* c0, int m, F&& f) {
     const int h = (m + 1) >> 1;
     const int grp = threadIdx.x / kMidGroup, sub = threadIdx.x % kMidGroup;
     for (int q = grp; q < h; q += kMidThreads / kMidGroup) {
@@ -436,7 +436,7 @@ __device__ __forceinline__ void mid_pair_walk(double2* c0, int m, F&& f) {
         const int t0 = sub * tot / kMidGroup, t1 = (sub + 1) * tot / kMidGroup;
         int row = t0 <= r1 ? r1 : r2;
         int jj = t0 <= r1 ? t0 : t0 - r1 - 1;
-        double2* a = c0 + mid_off(jj, m) + row;
+        T* a = c0 + mid_off(jj, m) + row;
         for (int t = t0; t < t1; ++t) {
             if (t == r1 + 1) { row = r2; jj = 0; a = c0 + r2; }
             f(a, row, jj);
@@ -446,13 +446,150 @@ __device__ __forceinline__ void mid_pair_walk(double2* c0, int m, F&& f) {
     }
 }
 
+// zhetd2's steps on the packed lower triangle P (order n, packed by columns) by one CTA of
+// kMidThreads threads, four CTA barriers per step: reflector and v by warp 0 | the Hermitian
+// matvec over the balanced row pairs (row walk and mirrored column walk split over kMidGroup
+// threads, combined by shuffles) with the dot product's per-warp partials | w | rank-2 update.
+// Reflector k stays in column k below the diagonal (its first component, 1, at A(k+1, k)); d, e
+// and tau go to dout, eout, tout as they are formed.  R = double for the plain form
+// (k_reduce_mid), float for the mixed form's complex64 Householder (k_hetrd_c64_big).
+template <typename R, typename RD, typename CT>
+__device__ void mid_hetrd(cplx<R>* P, int n, cplx<R>* vb, cplx<R>* wb, cplx<R>* pb, R* red, cplx<R>* s_tk,
+                          RD* dout, RD* eout, CT* tout) {
+    using C = cplx<R>;
+    const C zero = mk<R>(R(0), R(0));
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int grp = tid / kMidGroup, sub = tid % kMidGroup;
+    for (int k = 0; k + 1 < n; ++k) {
+        const int m = n - k - 1;
+        C* x = P + pk(k, n) + 1;                            // x[i] = A(k+1+i, k)
+        if (warp == 0) {
+            R s2 = R(0);
+            for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
+            s2 = warp_sum(s2);
+            const C alpha = x[0];
+            C tk, scale;
+            R beta;
+            if (s2 == R(0) && alpha.y == R(0)) {
+                tk = zero; beta = alpha.x; scale = zero;
+            } else {
+                const R nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
+                beta = alpha.x >= R(0) ? -nrm : nrm;
+                tk = mk<R>((beta - alpha.x) / beta, -alpha.y / beta);
+                const R ar = alpha.x - beta, ai = alpha.y, den = ar * ar + ai * ai;
+                scale = mk<R>(ar / den, -ai / den);
+            }
+            if (tk.x != R(0) || tk.y != R(0)) {
+                __syncwarp();                                     // every lane has read alpha
+                for (int i = lane; i < m; i += 32) {
+                    const C v = (i == 0) ? mk<R>(R(1), R(0)) : cmul(x[i], scale);
+                    vb[i] = v;
+                    x[i] = v;
+                }
+            }
+            if (lane == 0) {
+                s_tk[k & 1] = tk;
+                dout[k] = P[pk(k, n)].x;
+                eout[k] = beta;
+                tout[k] = tk;
+            }
+        }
+        __syncthreads();
+        const C tk = s_tk[k & 1];
+        if (tk.x == R(0) && tk.y == R(0)) continue;                 // H_k = I (uniform)
+        // p = tau A22 v over the row pairs; warp-uniform loop (the group shuffles need whole warps)
+        C* c0 = P + pk(k + 1, n);
+        const int h = (m + 1) >> 1;
+        C dpart = zero;                   // this lane's share of p^H v
+        for (int qb = 0; qb < h; qb += kMidThreads / kMidGroup) {
+            const int q = qb + grp;
+            const bool act = q < h;
+            const int r1 = q, r2 = m - 1 - q;
+            const bool two = act && r2 != r1;
+            C lo1 = zero, lo2 = lo1, up1 = lo1, up2 = lo1;
+            if (act) {
+                // lower row walk: row r1's r1 terms, then row r2's r2 terms
+                const int tot = two ? r1 + r2 : r1;
+                const int t0 = sub * tot / kMidGroup, t1 = (sub + 1) * tot / kMidGroup;
+                int jj = t0 < r1 ? t0 : t0 - r1;
+                const C* a = c0 + mid_off(jj, m) + (t0 < r1 ? r1 : r2);
+                for (int t = t0; t < t1; ++t) {
+                    if (t == r1) { jj = 0; a = c0 + r2; }
+                    if (t < r1) lo1 = cfma(*a, vb[jj], lo1); else lo2 = cfma(*a, vb[jj], lo2);
+                    a += m - jj - 1;
+                    ++jj;
+                }
+                // mirrored column walk: column r1 below the diagonal (m-1-r1 terms), then column r2's
+                const int sw = m - 1 - r1;
+                const int tot2 = two ? m - 1 : sw;
+                const int u0 = sub * tot2 / kMidGroup, u1 = (sub + 1) * tot2 / kMidGroup;
+                const C* d1 = c0 + mid_off(r1, m) + r1;
+                const C* d2 = c0 + mid_off(r2, m) + r2;
+                for (int t = u0; t < u1; ++t) {
+                    if (t < sw) up1 = cfmac(d1[t + 1], vb[r1 + t + 1], up1);
+                    else up2 = cfmac(d2[t - sw + 1], vb[r2 + t - sw + 1], up2);
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < kMidGroup; o <<= 1) {
+                lo1.x += shfl_xor(lo1.x, o); lo1.y += shfl_xor(lo1.y, o);
+                lo2.x += shfl_xor(lo2.x, o); lo2.y += shfl_xor(lo2.y, o);
+                up1.x += shfl_xor(up1.x, o); up1.y += shfl_xor(up1.y, o);
+                up2.x += shfl_xor(up2.x, o); up2.y += shfl_xor(up2.y, o);
+            }
+            if (act && sub == 0) {
+                const C* d1 = c0 + mid_off(r1, m) + r1;
+                C s = cadd(lo1, up1);
+                s.x = fma(d1[0].x, vb[r1].x, s.x);
+                s.y = fma(d1[0].x, vb[r1].y, s.y);
+                const C p1 = cmul(tk, s);
+                pb[r1] = p1;
+                dpart = cfmac(p1, vb[r1], dpart);
+                if (two) {
+                    const C* d2 = c0 + mid_off(r2, m) + r2;
+                    C s2v = cadd(lo2, up2);
+                    s2v.x = fma(d2[0].x, vb[r2].x, s2v.x);
+                    s2v.y = fma(d2[0].x, vb[r2].y, s2v.y);
+                    const C p2 = cmul(tk, s2v);
+                    pb[r2] = p2;
+                    dpart = cfmac(p2, vb[r2], dpart);
+                }
+            }
+        }
+        dpart.x = warp_sum(dpart.x);
+        dpart.y = warp_sum(dpart.y);
+        if (lane == 0) { red[2 * warp] = dpart.x; red[2 * warp + 1] = dpart.y; }
+        __syncthreads();
+        // w = p - tau/2 (p^H v) v
+        C dot = zero;
+#pragma unroll
+        for (int w8 = 0; w8 < kBigWarps; ++w8) { dot.x += red[2 * w8]; dot.y += red[2 * w8 + 1]; }
+        const C a2 = cscale(cmul(tk, dot), R(-0.5));
+        for (int i = tid; i < m; i += kMidThreads) wb[i] = cfma(a2, vb[i], pb[i]);
+        __syncthreads();
+        // A22 -= v w^H + w v^H (lower)
+        mid_pair_walk(c0, m, [&](C* a, int row, int j) {
+            C v = cfmsc(vb[row], wb[j], *a);
+            v = cfmsc(wb[row], vb[j], v);
+            if (row == j) v.y = R(0);
+            *a = v;
+        });
+        __syncthreads();
+    }
+    if (tid == 0) {
+        dout[n - 1] = P[pk(n - 1, n)].x;
+        eout[n - 1] = R(0);
+        tout[n - 1] = zero;
+    }
+}
+
 template <int RM>
 __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __restrict__ A,
                                                             const double2* __restrict__ B, int n, int batch,
                                                             Workspace ws, double2* __restrict__ X,
-                                                            int* __restrict__ info) {
+                                                            int* __restrict__ info, int hegst_only) {
     const int b = blockIdx.x;
-    if (b >= batch) return;
+    if (b >= batch || !pair_selected(ws, b)) return;
     extern __shared__ __align__(16) unsigned char smem[];
     const MidSmem lay(n);
     double2* P = reinterpret_cast<double2*>(smem + lay.P);
@@ -564,136 +701,102 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
     }
     __syncthreads();
 
-    // ---- hetrd: four CTA barriers per step (reflector and v by warp 0 | matvec with the dot
-    // product's per-warp partials | w | rank-2 update)
-    const int grp = tid / kMidGroup, sub = tid % kMidGroup;
-    for (int k = 0; k + 1 < n; ++k) {
-        const int m = n - k - 1;
-        double2* x = P + pk(k, n) + 1;                            // x[i] = A(k+1+i, k)
-        if (warp == 0) {
-            double s2 = 0.0;
-            for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
-            s2 = warp_sum(s2);
-            const double2 alpha = x[0];
-            double2 tk, scale;
-            double beta;
-            if (s2 == 0.0 && alpha.y == 0.0) {
-                tk = make_double2(0.0, 0.0); beta = alpha.x; scale = make_double2(0.0, 0.0);
-            } else {
-                const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
-                beta = alpha.x >= 0.0 ? -nrm : nrm;
-                tk = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
-                const double ar = alpha.x - beta, ai = alpha.y, den = ar * ar + ai * ai;
-                scale = make_double2(ar / den, -ai / den);
-            }
-            if (tk.x != 0.0 || tk.y != 0.0) {
-                __syncwarp();                                     // every lane has read alpha
-                for (int i = lane; i < m; i += 32) {
-                    const double2 v = (i == 0) ? make_double2(1.0, 0.0) : cmul(x[i], scale);
-                    vb[i] = v;
-                    x[i] = v;
-                }
-            }
-            if (lane == 0) {
-                s_tk[k & 1] = tk;
-                db[k] = P[pk(k, n)].x;
-                eb[k] = beta;
-                taub[k] = tk;
-            }
-        }
-        __syncthreads();
-        const double2 tk = s_tk[k & 1];
-        if (tk.x == 0.0 && tk.y == 0.0) continue;                 // H_k = I (uniform)
-        // p = tau A22 v over the row pairs; warp-uniform loop (the group shuffles need whole warps)
-        double2* c0 = P + pk(k + 1, n);
-        const int h = (m + 1) >> 1;
-        double2 dpart = make_double2(0.0, 0.0);                   // this lane's share of p^H v
-        for (int qb = 0; qb < h; qb += kMidThreads / kMidGroup) {
-            const int q = qb + grp;
-            const bool act = q < h;
-            const int r1 = q, r2 = m - 1 - q;
-            const bool two = act && r2 != r1;
-            double2 lo1 = make_double2(0.0, 0.0), lo2 = lo1, up1 = lo1, up2 = lo1;
-            if (act) {
-                // lower row walk: row r1's r1 terms, then row r2's r2 terms
-                const int tot = two ? r1 + r2 : r1;
-                const int t0 = sub * tot / kMidGroup, t1 = (sub + 1) * tot / kMidGroup;
-                int jj = t0 < r1 ? t0 : t0 - r1;
-                const double2* a = c0 + mid_off(jj, m) + (t0 < r1 ? r1 : r2);
-                for (int t = t0; t < t1; ++t) {
-                    if (t == r1) { jj = 0; a = c0 + r2; }
-                    if (t < r1) lo1 = cfma(*a, vb[jj], lo1); else lo2 = cfma(*a, vb[jj], lo2);
-                    a += m - jj - 1;
-                    ++jj;
-                }
-                // mirrored column walk: column r1 below the diagonal (m-1-r1 terms), then column r2's
-                const int sw = m - 1 - r1;
-                const int tot2 = two ? m - 1 : sw;
-                const int u0 = sub * tot2 / kMidGroup, u1 = (sub + 1) * tot2 / kMidGroup;
-                const double2* d1 = c0 + mid_off(r1, m) + r1;
-                const double2* d2 = c0 + mid_off(r2, m) + r2;
-                for (int t = u0; t < u1; ++t) {
-                    if (t < sw) up1 = cfmac(d1[t + 1], vb[r1 + t + 1], up1);
-                    else up2 = cfmac(d2[t - sw + 1], vb[r2 + t - sw + 1], up2);
-                }
-            }
-#pragma unroll
-            for (int o = 1; o < kMidGroup; o <<= 1) {
-                lo1.x += shfl_xor(lo1.x, o); lo1.y += shfl_xor(lo1.y, o);
-                lo2.x += shfl_xor(lo2.x, o); lo2.y += shfl_xor(lo2.y, o);
-                up1.x += shfl_xor(up1.x, o); up1.y += shfl_xor(up1.y, o);
-                up2.x += shfl_xor(up2.x, o); up2.y += shfl_xor(up2.y, o);
-            }
-            if (act && sub == 0) {
-                const double2* d1 = c0 + mid_off(r1, m) + r1;
-                double2 s = cadd(lo1, up1);
-                s.x = fma(d1[0].x, vb[r1].x, s.x);
-                s.y = fma(d1[0].x, vb[r1].y, s.y);
-                const double2 p1 = cmul(tk, s);
-                pb[r1] = p1;
-                dpart = cfmac(p1, vb[r1], dpart);
-                if (two) {
-                    const double2* d2 = c0 + mid_off(r2, m) + r2;
-                    double2 s2v = cadd(lo2, up2);
-                    s2v.x = fma(d2[0].x, vb[r2].x, s2v.x);
-                    s2v.y = fma(d2[0].x, vb[r2].y, s2v.y);
-                    const double2 p2 = cmul(tk, s2v);
-                    pb[r2] = p2;
-                    dpart = cfmac(p2, vb[r2], dpart);
-                }
-            }
-        }
-        dpart.x = warp_sum(dpart.x);
-        dpart.y = warp_sum(dpart.y);
-        if (lane == 0) { red[2 * warp] = dpart.x; red[2 * warp + 1] = dpart.y; }
-        __syncthreads();
-        // w = p - tau/2 (p^H v) v
-        double2 dot = make_double2(0.0, 0.0);
-#pragma unroll
-        for (int w8 = 0; w8 < kBigWarps; ++w8) { dot.x += red[2 * w8]; dot.y += red[2 * w8 + 1]; }
-        const double2 a2 = cscale(cmul(tk, dot), -0.5);
-        for (int i = tid; i < m; i += kMidThreads) wb[i] = cfma(a2, vb[i], pb[i]);
-        __syncthreads();
-        // A22 -= v w^H + w v^H (lower)
-        mid_pair_walk(c0, m, [&](double2* a, int row, int j) {
-            double2 v = cfmsc(vb[row], wb[j], *a);
-            v = cfmsc(wb[row], vb[j], v);
-            if (row == j) v.y = 0.0;
-            *a = v;
-        });
-        __syncthreads();
+    if (hegst_only) {                                              // mixed form: C stays in X
+        if (tid == 0) info[b] = status;
+        return;
     }
-    if (tid == 0) {
-        db[n - 1] = P[pk(n - 1, n)].x;
-        eb[n - 1] = 0.0;
-        taub[n - 1] = make_double2(0.0, 0.0);
-    }
+    mid_hetrd<double>(P, n, vb, wb, pb, red, s_tk, db, eb, taub);
     // reflector k (rows k+1 .. n-1 of column k) -> LV(s, n-1-k), s = i - k - 1
     for (size_t idx = tid; idx < mat; idx += kMidThreads) {
         const int k = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(k) * n);
         if (i > k) LVb[(i - k - 1) + static_cast<size_t>(n - 1 - k) * n] = P[pk(k, n) + i - k];
     }
     if (tid == 0) info[b] = status;
+}
+
+// ----------------------------------------------------------------------------- k_hetrd_c64_big
+// Mixed form, kMixedMaxN < n <= kMixedBigMaxN: the Householder stage in complex64, one CTA per
+// pair.  C's lower triangle (FP64, left in X by the reduction) is rounded to complex64 into a
+// packed tile (8 B per entry: 66 KB at n = 128, half of what the FP64 tile takes) and
+// tridiagonalised by mid_hetrd<float>; C itself, full Hermitian and FP64, goes to ws.rfC for the
+// refinement (X is overwritten before it runs).  The outputs go where the FP64 kernels put theirs,
+// promoted to FP64, so the FP64 eigensolve of T and the back-transform run on them unchanged:
+// reflector k along LV's row k above the superdiagonal for n <= kSmallMaxN, along LV's column
+// n-1-k beyond (v_k(k+1) = 1 stored), d and e, and tau rescaled in FP64 so that each
+// H = I - tau v v^H is unitary to FP64 rounding for the promoted v (|tau|^2 ||v||^2 = 2 Re tau).
+struct C64BigSmem {
+    size_t P, vb, wb, pb, red, tk, d, e, tau, total;
+    __host__ __device__ explicit C64BigSmem(int n) {
+        size_t o = 0;
+        P = o;   o += big_align(8 * static_cast<size_t>(n) * (n + 1) / 2, 16);
+        vb = o;  o += big_align(8 * static_cast<size_t>(n), 16);
+        wb = o;  o += big_align(8 * static_cast<size_t>(n), 16);
+        pb = o;  o += big_align(8 * static_cast<size_t>(n), 16);
+        red = o; o += 8 * kBigWarps;
+        tk = o;  o += 16;
+        d = o;   o += big_align(4 * static_cast<size_t>(n), 16);
+        e = o;   o += big_align(4 * static_cast<size_t>(n), 16);
+        tau = o; o += big_align(8 * static_cast<size_t>(n), 16);
+        total = o;
+    }
+};
+
+__global__ void __launch_bounds__(kMidThreads) k_hetrd_c64_big(int n, int batch, const double2* __restrict__ C,
+                                                               Workspace ws, int* __restrict__ info) {
+    const int b = blockIdx.x;
+    if (b >= batch) return;
+    if (info[b] != 0) return;                                     // an earlier stage failed (uniform)
+    extern __shared__ __align__(16) unsigned char smem[];
+    const C64BigSmem lay(n);
+    float2* P = reinterpret_cast<float2*>(smem + lay.P);
+    float2* vb = reinterpret_cast<float2*>(smem + lay.vb);
+    float2* wb = reinterpret_cast<float2*>(smem + lay.wb);
+    float2* pb = reinterpret_cast<float2*>(smem + lay.pb);
+    float* red = reinterpret_cast<float*>(smem + lay.red);
+    float2* s_tk = reinterpret_cast<float2*>(smem + lay.tk);
+    float* d_s = reinterpret_cast<float*>(smem + lay.d);
+    float* e_s = reinterpret_cast<float*>(smem + lay.e);
+    float2* tau_s = reinterpret_cast<float2*>(smem + lay.tau);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const size_t mat = static_cast<size_t>(n) * n;
+    const double2* Cb = C + mat * b;
+    double2* Sb = ws.rfC + mat * b;
+    for (size_t idx = tid; idx < mat; idx += kMidThreads) {
+        const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
+        if (i < j) continue;
+        double2 v = Cb[idx];
+        if (i == j) v.y = 0.0;
+        P[pk(j, n) + i - j] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+        Sb[idx] = v;
+        if (i != j) Sb[j + static_cast<size_t>(i) * n] = make_double2(v.x, -v.y);
+    }
+    __syncthreads();
+    mid_hetrd<float>(P, n, vb, wb, pb, red, s_tk, d_s, e_s, tau_s);
+    __syncthreads();
+    const bool rows = n <= kSmallMaxN;                            // the small path's reflector layout
+    double2* LVb = ws.LV + mat * b;
+    for (int k = warp; k + 1 < n; k += kBigWarps) {              // one warp per reflector
+        const float2* col = P + pk(k, n) - k;                     // col[i] = v_k(i), i >= k + 2
+        double s2 = 0.0;
+        for (int i = k + 1 + lane; i < n; i += 32) {
+            const double2 v = (i == k + 1) ? make_double2(1.0, 0.0)
+                                           : make_double2(static_cast<double>(col[i].x), static_cast<double>(col[i].y));
+            if (rows) LVb[k + static_cast<size_t>(i) * n] = v;
+            else LVb[(i - k - 1) + static_cast<size_t>(n - 1 - k) * n] = v;
+            s2 = fma(v.x, v.x, fma(v.y, v.y, s2));
+        }
+        s2 = warp_sum(s2);
+        if (lane == 0) {
+            const double tr = tau_s[k].x, ti = tau_s[k].y, t2 = tr * tr + ti * ti;
+            const double sc = t2 > 0.0 ? 2.0 * tr / (t2 * s2) : 0.0;
+            ws.tau[static_cast<size_t>(n) * b + k] = make_double2(tr * sc, ti * sc);
+        }
+    }
+    for (int i = tid; i < n; i += kMidThreads) {
+        ws.d[static_cast<size_t>(n) * b + i] = d_s[i];
+        ws.e[static_cast<size_t>(n) * b + i] = (i + 1 < n) ? static_cast<double>(e_s[i]) : 0.0;
+        if (i + 1 == n) ws.tau[static_cast<size_t>(n) * b + i] = make_double2(0.0, 0.0);
+    }
 }
 
 // ----------------------------------------------------------------------------- k_ql_apply_rows
@@ -710,7 +813,7 @@ __global__ void __launch_bounds__(32) k_ql_apply_rows(int n, int batch, Workspac
     using C = cplx<R>;
     const int nrb = (n + 31) / 32;                     // row blocks per pair
     const int b = blockIdx.x / nrb, rb = blockIdx.x - b * nrb, lane = threadIdx.x;
-    if (b >= batch) return;
+    if (b >= batch || !pair_selected(ws, b)) return;
     if (redo && ws.flag[b] < 2) return;
     if (info[b] > n || info[b] < 0) return;            // B not positive definite: the back stage writes NaN
     extern __shared__ __align__(16) unsigned char smem[];
@@ -774,6 +877,7 @@ __global__ void __launch_bounds__(kBigThreads) k_back_big(int mode, int n, int b
     constexpr int GROUPS = kBigThreads / G;
     const int r = CS == 1 ? 0 : static_cast<int>(cg::this_cluster().block_rank());
     const int b = blockIdx.x / CS;
+    if (!pair_selected(ws, b)) return;                  // uniform over the pair's cluster
     extern __shared__ __align__(16) unsigned char smem[];
     const BigBackSmem lay(n);
     double2* panel = reinterpret_cast<double2*>(smem + lay.panel);
@@ -793,7 +897,11 @@ __global__ void __launch_bounds__(kBigThreads) k_back_big(int mode, int n, int b
 #pragma unroll
         for (int q = 0; q < RM; ++q) {
             const int i = g + G * q, lc = grp + GROUPS * w;
-            y[w][q] = make_double2((!bad && lc < nc && i < n) ? Zg[i + static_cast<size_t>(c0 + lc) * n] : 0.0, 0.0);
+            const bool in = !bad && lc < nc && i < n;
+            if (mode == kBackLOnly)                     // complex Y in the X buffer
+                y[w][q] = in ? Xb[i + static_cast<size_t>(c0 + lc) * n] : make_double2(0.0, 0.0);
+            else                                        // real Z in the X buffer
+                y[w][q] = make_double2(in ? Zg[i + static_cast<size_t>(c0 + lc) * n] : 0.0, 0.0);
         }
     if (!bad) {
         for (int k = tid; k < n; k += kBigThreads) {
@@ -808,8 +916,8 @@ __global__ void __launch_bounds__(kBigThreads) k_back_big(int mode, int n, int b
             Xb[static_cast<size_t>(c0) * n + idx] = make_double2(nan, nan);
         return;
     }
-    // ---- Y = Q Z: H_k for k = n-2 .. 0
-    for (int k0 = n - 2; k0 >= 0; k0 -= kBigPanel) {
+    // ---- Y = Q Z: H_k for k = n-2 .. 0 (kBackLOnly: Y given)
+    for (int k0 = mode == kBackLOnly ? -1 : n - 2; k0 >= 0; k0 -= kBigPanel) {
         __syncthreads();
         for (int p = 0; p < kBigPanel && k0 - p >= 0; ++p) {
             const int k = k0 - p;
@@ -846,7 +954,7 @@ __global__ void __launch_bounds__(kBigThreads) k_back_big(int mode, int n, int b
         }
     }
     // ---- X = L^{-H} Y: x_k = (y_k - sum_{i > k} conj(L(i, k)) x_i) / L(k, k), k = n-1 .. 0
-    if (mode == kBackFull) {
+    if (mode == kBackFull || mode == kBackLOnly) {
         for (int k0 = n - 1; k0 >= 0; k0 -= kBigPanel) {
             __syncthreads();
             for (int p = 0; p < kBigPanel && k0 - p >= 0; ++p) {
@@ -954,10 +1062,11 @@ constexpr int kMidMaxN = 160;             // the packed tile + buffers fit 227 K
 
 template <int RM>
 void run_reduce_mid(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X, int* info,
-                    cudaStream_t stream) {
+                    cudaStream_t stream, bool hegst_only) {
     static SmemOptIn f;
     set_big_smem_once(k_reduce_mid<RM>, f, static_cast<size_t>(max_smem_optin()));
-    k_reduce_mid<RM><<<batch, kMidThreads, MidSmem(n).total, stream>>>(A, B, n, batch, ws, X, info);
+    k_reduce_mid<RM><<<batch, kMidThreads, MidSmem(n).total, stream>>>(A, B, n, batch, ws, X, info,
+                                                                       hegst_only ? 1 : 0);
 }
 
 }  // namespace
@@ -972,19 +1081,35 @@ size_t big_reduce_smem_bytes(int n) {
 }
 
 cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
-                              int* info, cudaStream_t stream) {
+                              int* info, cudaStream_t stream, bool hegst_only) {
     if (batch <= 0) return cudaSuccess;
     if (!A || !B || !X || !info || !ws.LV || !ws.d || !ws.e || !ws.tau) return cudaErrorInvalidValue;
     if (!big_path(n)) return cudaErrorInvalidValue;
     if (n <= kMidMaxN) {                     // one CTA per pair: no cluster barriers
-        if (n <= 96) run_reduce_mid<12>(A, B, n, batch, ws, X, info, stream);
-        else if (n <= 128) run_reduce_mid<16>(A, B, n, batch, ws, X, info, stream);
-        else run_reduce_mid<20>(A, B, n, batch, ws, X, info, stream);
+        if (n <= 96) run_reduce_mid<12>(A, B, n, batch, ws, X, info, stream, hegst_only);
+        else if (n <= 128) run_reduce_mid<16>(A, B, n, batch, ws, X, info, stream, hegst_only);
+        else run_reduce_mid<20>(A, B, n, batch, ws, X, info, stream, hegst_only);
         return cudaGetLastError();
     }
+    if (hegst_only) return cudaErrorInvalidValue;    // the cluster kernel always tridiagonalises
     cudaError_t err = cudaSuccess;
     SBG_BIG_DISPATCH(n, run_reduce_big, &err, A, B, n, batch, ws, X, info, stream);
     return err != cudaSuccess ? err : cudaGetLastError();
+}
+
+size_t hetrd_c64_big_smem_bytes(int n) { return C64BigSmem(n).total; }
+
+cudaError_t launch_hetrd_c64_big(int n, int batch, const double2* C, const Workspace& ws, int* info,
+                                 cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    if (n <= kMixedMaxN || n > kMixedBigMaxN || n > kMidMaxN) return cudaErrorInvalidValue;
+    if (!C || !info || !ws.LV || !ws.d || !ws.e || !ws.tau || !ws.rfC) return cudaErrorInvalidValue;
+    const size_t smem = C64BigSmem(n).total;
+    if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+    static SmemOptIn f;
+    set_big_smem_once(k_hetrd_c64_big, f, smem);
+    k_hetrd_c64_big<<<batch, kMidThreads, smem, stream>>>(n, batch, C, ws, info);
+    return cudaGetLastError();
 }
 
 size_t ql_rows_smem_bytes(int n, bool single) { return single ? ql_rows_bytes<float>(n) : ql_rows_bytes<double>(n); }

@@ -33,10 +33,14 @@ int supported_max_n(int precision) {
     int best = 0;
     const bool single = precision == SBG_PRECISION_MIXED;
     for (int n = 1; n <= sbg::kBigMaxN; ++n) {
+        // the mixed form above kMixedMaxN: the FP64 kernels (its own re-solve) plus the complex64
+        // Householder (one CTA per pair); the refinement's shared memory is fixed and small
+        if (single && n > sbg::kMixedBigMaxN) break;
+        const bool big_mixed = single && n > sbg::kMixedMaxN;
         if (n > sbg::kSmallMaxN) {          // cluster kernels
-            if (single) break;
             size_t need = std::max(sbg::big_reduce_smem_bytes(n), sbg::ql_rows_smem_bytes(n, false));
             need = std::max(need, sbg::ql_chain_smem_bytes(n, 32, false));
+            if (big_mixed) need = std::max(need, sbg::hetrd_c64_big_smem_bytes(n));
             if (sbg::big_path(n) && need <= lim) best = n;
             continue;
         }
@@ -44,8 +48,9 @@ int supported_max_n(int precision) {
         need = std::max(need, sbg::hetrd_smem_bytes(n, 128));
         need = std::max(need, sbg::ql_apply_smem_bytes(n, 1, false));
         need = std::max(need, sbg::ql_chain_smem_bytes(n, 32, false));
-        if (single) {                       // complex64 Householder + FP64 tensor-core refinement
-            if (n > sbg::kMixedMaxN) break;
+        if (big_mixed) {
+            need = std::max(need, sbg::hetrd_c64_big_smem_bytes(n));
+        } else if (single) {                // complex64 Householder + FP64 tensor-core refinement
             need = std::max(need, sbg::refine_c_smem_bytes(n));
             need = std::max(need, sbg::mixed_fallback_smem_bytes(n));
             need = std::max(need, sbg::hetrd_c64_smem_bytes(n));
@@ -78,7 +83,8 @@ void sbgi::create_solver(int n, int device, const sbg_solver_options* o, sbg_sol
     s->device = device;
     s->precision = opts.precision;
     s->refine_steps = opts.refine_steps > 0 ? opts.refine_steps : 5;
-    s->chunk_pairs = opts.workspace_pairs > 0 ? opts.workspace_pairs : default_chunk_pairs(n);
+    s->chunk_pairs = opts.workspace_pairs > 0 ? opts.workspace_pairs
+                                              : default_chunk_pairs(n, opts.precision == SBG_PRECISION_MIXED);
     sbg::TuneRequest req;
     req.n = n;
     req.device = device;
@@ -240,8 +246,8 @@ int sbg_solver_reserve(sbg_solver* s, int pairs, int stream_slots) {
     });
 }
 
-size_t sbg_workspace_bytes_per_pair(int n, int /*precision*/) {
-    return n > 0 ? sbg::workspace_bytes_per_pair(n) : 0;
+size_t sbg_workspace_bytes_per_pair(int n, int precision) {
+    return n > 0 ? sbg::workspace_bytes_per_pair(n, precision == SBG_PRECISION_MIXED) : 0;
 }
 
 int sbg_selftest_reciprocal(const double* d_u, double* d_r, int count, cudaStream_t stream) {
@@ -259,8 +265,8 @@ int sbg_selftest_fp64_fma(double* d_out, int blocks, int iters, cudaStream_t str
     });
 }
 
-size_t sbg_workspace_bytes(int n, int /*precision*/, int pairs) {
-    return n > 0 && pairs > 0 ? sbg::workspace_bytes(n, pairs) : 0;
+size_t sbg_workspace_bytes(int n, int precision, int pairs) {
+    return n > 0 && pairs > 0 ? sbg::workspace_bytes(n, pairs, precision == SBG_PRECISION_MIXED) : 0;
 }
 
 int sbg_solver_matrix_size(const sbg_solver* s) { return s ? s->n : 0; }

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_reduce(int mode, const d
                                               Workspace ws, double2* __restrict__ out,
                                               int* __restrict__ info) {
     const int b = blockIdx.x;
-    if (b >= batch) return;
+    if (b >= batch || !pair_selected(ws, b)) return;
     extern __shared__ __align__(16) unsigned char smem[];
     const ReduceSmem lay(n);
     const int ld = tile_ld(n);
@@ -409,7 +409,7 @@ template <int T>
 __global__ void __launch_bounds__(T) k_hetrd(int n, int batch, const double2* __restrict__ C, Workspace ws,
                                              int* __restrict__ info) {
     const int b = blockIdx.x;
-    if (b >= batch) return;
+    if (b >= batch || !pair_selected(ws, b)) return;
     if (info[b] != 0) return;
     extern __shared__ __align__(16) unsigned char smem[];
     const HetrdSmem lay(n, T);
@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(32 * kMaxPairWarps) k_hetrd_warp(int n, int ba
                                                                   Workspace ws, int* __restrict__ info) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (b >= batch) return;
+    if (b >= batch || !pair_selected(ws, b)) return;
     if (info[b] != 0) return;
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char* base = smem + hetrd_warp_bytes(n) * warp;
@@ -590,7 +590,7 @@ __global__ void k_ql_chain(int n, int batch, Workspace ws, double* __restrict__ 
     extern __shared__ __align__(16) unsigned char smem[];
     R* d = reinterpret_cast<R*>(smem) + tid;
     R* e = reinterpret_cast<R*>(smem) + static_cast<size_t>(n) * T + tid;
-    if (b >= batch) return;
+    if (b >= batch || !pair_selected(ws, b)) return;
     if (redo) {
         if (ws.flag[b] != 2) return;
         if (info[b] > 0 && info[b] <= n) info[b] = 0;          // QL non-convergence: run it again here
@@ -645,7 +645,7 @@ __global__ void k_ql_apply(int n, int batch, Workspace ws, double* __restrict__ 
     R* dd = reinterpret_cast<R*>(base + align_up(sizeof(R) * static_cast<size_t>(n) * ldz, 16) +
                                  static_cast<size_t>(wpp) * 2 * 32 * sizeof(C));
     R* ee = dd + n;
-    const bool live = b < batch && !(info[min(b, batch - 1)] > n || info[min(b, batch - 1)] < 0);
+    const bool live = b < batch && pair_selected(ws, b) && !(info[b] > n || info[b] < 0);
     const int row = wip * 32 + lane;
     const bool own = live && row < n;
     R* zrow = Z + row * ldz;
@@ -794,7 +794,7 @@ __global__ void k_ql_values(int n, int batch, Workspace ws, double* __restrict__
     extern __shared__ __align__(16) unsigned char smem[];
     double* d = reinterpret_cast<double*>(smem) + tid;
     double* e = reinterpret_cast<double*>(smem) + static_cast<size_t>(n) * T + tid;
-    if (b >= batch) return;
+    if (b >= batch || !pair_selected(ws, b)) return;
     double* Wb = W + static_cast<size_t>(n) * b;
     if (info[b] != 0) {
         for (int i = 0; i < n; ++i) Wb[i] = __longlong_as_double(0x7ff8000000000000ll);
@@ -932,7 +932,7 @@ __global__ void __launch_bounds__(32) k_tridiag_invit(int n, int batch, Workspac
                                                       double2* __restrict__ X, int* __restrict__ info,
                                                       int flag_redo) {
     const int b = blockIdx.x, lane = threadIdx.x & 31;
-    if (b >= batch) return;
+    if (b >= batch || !pair_selected(ws, b)) return;
     if (flag_redo && lane == 0) ws.flag[b] = 0;
     const int inf = info[b];
     if (inf > n || inf < 0) return;                   // an earlier stage failed: W and X are NaN
@@ -1085,7 +1085,7 @@ template <int T, int G, int RM>
 __global__ void __launch_bounds__(T, RM <= 8 ? 2 : 1) k_back(int mode, int n, int batch, Workspace ws,
                                             double2* __restrict__ X, int* __restrict__ info) {
     const int b = blockIdx.x;
-    if (b >= batch) return;
+    if (b >= batch || !pair_selected(ws, b)) return;
     const size_t mat = static_cast<size_t>(n) * n;
     double2* Xb = X + mat * b;
     const int tid = threadIdx.x;
@@ -1161,22 +1161,26 @@ int ql_log_capacity(int n) {
     return dflt;
 }
 
-size_t workspace_bytes_per_pair(int n) {
+size_t workspace_bytes_per_pair(int n, bool mixed) {
     const size_t nn = static_cast<size_t>(n) * n;
     // the default (largest) rotation-log capacity, or the mixed form's stash if that is larger
     const size_t cap = static_cast<size_t>(std::max((3 * n * n) / 2 + 8 * n + 16, refine_stash_entries(n)));
-    return 16 * nn + 16 * n + 8 * n * 2 + 16 * cap + 4 * n + 4;
+    const size_t refine = mixed_big(n, mixed) ? 5 * 16 * nn + 4 : 0;
+    return 16 * nn + 16 * n + 8 * n * 2 + 16 * cap + 4 * n + 4 + refine;
 }
 
 namespace {
-// Byte offsets of the workspace's seven regions from its base, each rounded up to 256 bytes.
+// Byte offsets of the workspace's regions from its base, each rounded up to 256 bytes: seven,
+// and for the mixed form above kMixedMaxN six more (the refinement's matrices and status).
 struct WorkspaceLayout {
-    size_t LV, tau, d, e, log, perm, flag, end;
+    size_t LV, tau, d, e, log, perm, flag, rfC = 0, rfY = 0, rfP = 0, rfG = 0, rfS = 0, rstat = 0, end;
     int log_cap, log_stride;
-    WorkspaceLayout(int n, int capacity) {
+    bool refine;
+    WorkspaceLayout(int n, int capacity, bool mixed) {
         const size_t nn = static_cast<size_t>(n) * n, cap = static_cast<size_t>(capacity);
         log_cap = ql_log_capacity(n);
         log_stride = std::max(log_cap, refine_stash_entries(n));
+        refine = mixed_big(n, mixed);
         size_t o = 0;
         auto take = [&](size_t bytes) { const size_t q = o; o += align_up(bytes, 256); return q; };
         LV = take(16 * nn * cap);
@@ -1186,15 +1190,23 @@ struct WorkspaceLayout {
         log = take(16 * static_cast<size_t>(log_stride) * cap);
         perm = take(4 * n * cap);
         flag = take(4 * cap);
+        if (refine) {
+            rfC = take(16 * nn * cap);
+            rfY = take(16 * nn * cap);
+            rfP = take(16 * nn * cap);
+            rfG = take(16 * nn * cap);
+            rfS = take(16 * nn * cap);
+            rstat = take(4 * cap);
+        }
         end = o;
     }
 };
 }  // namespace
 
-size_t workspace_bytes(int n, int capacity) { return WorkspaceLayout(n, capacity).end; }
+size_t workspace_bytes(int n, int capacity, bool mixed) { return WorkspaceLayout(n, capacity, mixed).end; }
 
-Workspace carve_workspace(void* base, int n, int capacity) {
-    const WorkspaceLayout lay(n, capacity);
+Workspace carve_workspace(void* base, int n, int capacity, bool mixed) {
+    const WorkspaceLayout lay(n, capacity, mixed);
     char* p = static_cast<char*>(base);
     Workspace w;
     w.n = n;
@@ -1208,6 +1220,14 @@ Workspace carve_workspace(void* base, int n, int capacity) {
     w.log = p + lay.log;
     w.perm = reinterpret_cast<int*>(p + lay.perm);
     w.flag = reinterpret_cast<int*>(p + lay.flag);
+    if (lay.refine) {
+        w.rfC = reinterpret_cast<double2*>(p + lay.rfC);
+        w.rfY = reinterpret_cast<double2*>(p + lay.rfY);
+        w.rfP = reinterpret_cast<double2*>(p + lay.rfP);
+        w.rfG = reinterpret_cast<double2*>(p + lay.rfG);
+        w.rfS = reinterpret_cast<double2*>(p + lay.rfS);
+        w.rstat = reinterpret_cast<int*>(p + lay.rstat);
+    }
     return w;
 }
 
@@ -1281,13 +1301,17 @@ void run_hegst_col(int mode, const double2* A, const Workspace& ws, double2* out
 cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, int batch,
                           const Workspace& ws, double2* out, int* info, const LaunchShape& shape, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
+    // kReduceMixed is kReduceFull that, above kSmallMaxN, stops before the tridiagonalisation
+    // (below it the reduction never tridiagonalises)
+    const bool hegst_only = mode == kReduceMixed;
+    if (hegst_only) mode = kReduceFull;
     if (!B || !info) return cudaErrorInvalidValue;
     if ((mode == kReduceChol || mode == kReduceHegst || mode == kReduceFull) && !out) return cudaErrorInvalidValue;
     if ((mode == kReduceHegst || mode == kReduceFull) && !A) return cudaErrorInvalidValue;
     if ((mode == kReduceFull || mode == kReduceFromLM) && !ws.LV) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) {
         if (mode != kReduceFull) return cudaErrorInvalidValue;
-        return launch_reduce_big(A, B, n, batch, ws, out, info, stream);
+        return launch_reduce_big(A, B, n, batch, ws, out, info, stream, hegst_only);
     }
     // The two-kernel path hands L from k_potrf_warp to k_hegst_col through ws.LV, so it
     // needs a workspace (the staged Cholesky alone does not).
@@ -1510,7 +1534,6 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
                         const LaunchShape& shape, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
-    if (mode == kBackLOnly && n > kSmallMaxN) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) return launch_back_big(mode, n, batch, ws, X, info, stream);
     const size_t smem = back_smem_bytes(n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;

@@ -32,7 +32,37 @@ struct Workspace {
     int log_stride = 0; // entries per pair of the log region (>= log_cap; the mixed form's stash lives there)
     int capacity = 0;   // pairs
     int n = 0;
+    // Mixed form for kMixedMaxN < n <= kMixedBigMaxN only (null otherwise): the refinement's
+    // per-pair n x n complex matrices (column-major, ld = n) -- the FP64 copy of C, the second
+    // eigenvector buffer, P = C Y (then the correction E), G = Y^H Y, S = Y^H P -- and its per-pair
+    // outcome rstat (kRefine* below).
+    double2* rfC = nullptr;
+    double2* rfY = nullptr;
+    double2* rfP = nullptr;
+    double2* rfG = nullptr;
+    double2* rfS = nullptr;
+    int* rstat = nullptr;
+    // Pair selection: when sel is set, the stage kernels that honour it (the FP64 kernels for
+    // 57 <= n <= 160) run pair b only if bit sel[b] of sel_mask is set, and leave every other
+    // pair's outputs and scratch untouched.  The mixed form uses it to re-solve in FP64 only the
+    // pairs its refinement gave up on.
+    const int* sel = nullptr;
+    int sel_mask = 0;
 };
+
+// Outcome of the mixed form's refinement for kMixedMaxN < n <= kMixedBigMaxN (Workspace::rstat).
+enum RefineStatus : int {
+    kRefineActive = 0,     // not decided yet (only while the refinement runs)
+    kRefineDone = 1,       // converged: W and Y (in X) final, X = L^{-H} Y still to come
+    kRefineRedo = 2,       // to be solved again by the FP64 kernels
+    kRefineSkip = 3,       // an earlier stage failed (B not positive definite, copy timeout)
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ bool pair_selected(const Workspace& ws, int b) {
+    return ws.sel == nullptr || ((ws.sel_mask >> ws.sel[b]) & 1) != 0;
+}
+#endif
 
 // Rotation-log capacity per pair: ~1.1 n^2 rotations are typical (about two QL sweeps per
 // eigenvalue); pairs that need more fall back to the warp-per-pair QL.  The environment
@@ -47,25 +77,33 @@ __host__ __device__ constexpr int refine_np(int n) { return (n + 7) / 8 * 8; }
 __host__ __device__ constexpr int refine_ld(int n) { return refine_np(n) + 4; }
 __host__ __device__ constexpr int refine_stash_entries(int n) { return refine_np(n) * refine_ld(n); }
 constexpr int kMixedMaxN = 63;       // inverse iteration (no rotation log, so the stash is free)
+// Mixed form above kMixedMaxN: the refinement runs on per-pair matrices in the workspace
+// (csrc/mixed_big.cu), up to the largest n the one-CTA reduction kernel takes.
+constexpr int kMixedBigMaxN = 160;
+inline bool mixed_big(int n, bool mixed) { return mixed && n > kMixedMaxN; }
 
-size_t workspace_bytes_per_pair(int n);
+// Bytes per pair of the workspace of a solver of order n (mixed: the mixed form's).
+size_t workspace_bytes_per_pair(int n, bool mixed = false);
 // Carves a Workspace for `capacity` pairs of size n out of `base` (256-byte aligned).  Each of
-// its seven regions starts on a 256-byte boundary.
-Workspace carve_workspace(void* base, int n, int capacity);
-// Exact bytes carve_workspace(base, n, capacity) spans from base: every allocation that backs a
-// workspace is sized by this (at most workspace_bytes_per_pair(n) * capacity + 7 * 256).
-size_t workspace_bytes(int n, int capacity);
+// its regions (seven; thirteen for the mixed form above kMixedMaxN) starts on a 256-byte boundary.
+Workspace carve_workspace(void* base, int n, int capacity, bool mixed = false);
+// Exact bytes carve_workspace(base, n, capacity, mixed) spans from base: every allocation that
+// backs a workspace is sized by this (at most workspace_bytes_per_pair(n, mixed) * capacity +
+// 13 * 256).
+size_t workspace_bytes(int n, int capacity, bool mixed = false);
 
 enum ReduceMode : int {
     kReduceFull = 0,      // potrf + hegst          -> L into ws.LV (lower), C lower into out
     kReduceChol = 1,      // potrf only             -> out (L, strict upper zeroed)
     kReduceHegst = 2,     // potrf + hegst          -> out (M lower, strict upper zeroed)
     kReduceFromLM = 3,    // given L                -> L copied into ws.LV (lower)
+    kReduceMixed = 4,     // potrf + hegst          -> as kReduceFull, but for n > kSmallMaxN the
+                          //                           reduction stops before the tridiagonalisation
 };
 enum BackMode : int {
     kBackFull = 0,        // X = L^{-H} Q Z
     kBackQOnly = 1,       // V = Q Z (eigenvectors of the reduced matrix)
-    kBackLOnly = 2,       // X = L^{-H} Y, Y complex in the X buffer (mixed form; n <= 84)
+    kBackLOnly = 2,       // X = L^{-H} Y, Y complex in the X buffer (mixed form)
 };
 
 // Launch shape of the stage kernels, the part of a schedule the autotuner varies:
@@ -134,8 +172,23 @@ constexpr int kBigMaxN = 256;
 bool big_path(int n);
 size_t big_reduce_smem_bytes(int n);
 size_t ql_rows_smem_bytes(int n, bool single);
+// hegst_only (n <= 160): stop after C = L^{-1} A L^{-H} (C's lower triangle in X, L in LV).
 cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
-                              int* info, cudaStream_t stream);
+                              int* info, cudaStream_t stream, bool hegst_only = false);
+// Mixed form for kMixedMaxN < n <= kMixedBigMaxN (csrc/mixed_big.cu), after
+// launch_reduce(kReduceMixed) left L in LV and C's lower triangle in X:
+//   launch_hetrd_c64_big   complex64 Householder, one CTA per pair: FP64-promoted reflectors (in the
+//                          layout launch_back expects for n), tau made unitary in FP64, d, e; C
+//                          (FP64, full Hermitian) into ws.rfC;
+//   launch_refine_big      after the FP64 eigenpairs of that T and Y = Q Z in X: Ogita-Aishima
+//                          refinement of (W, Y) against rfC, every product on the FP64 tensor
+//                          cores; ws.rstat gets each pair's outcome.
+cudaError_t launch_hetrd_c64_big(int n, int batch, const double2* C, const Workspace& ws, int* info,
+                                 cudaStream_t stream);
+cudaError_t launch_refine_big(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
+                              int refine_steps, cudaStream_t stream);
+size_t hetrd_c64_big_smem_bytes(int n);
+size_t refine_big_smem_bytes();
 cudaError_t launch_ql_rows(int n, int batch, const Workspace& ws, double* W, double2* X, int* info, bool single,
                            int chain_threads, cudaStream_t stream);
 cudaError_t launch_back_big(int mode, int n, int batch, const Workspace& ws, double2* X, const int* info,

@@ -81,9 +81,9 @@ struct Bucket {
 };
 
 // Device bytes one pair of order n takes in a bucket: staging plus solver workspace.
-size_t bucket_bytes_per_pair(int n) {
+size_t bucket_bytes_per_pair(int n, bool mixed) {
     const size_t nn = static_cast<size_t>(n) * n;
-    return 48 * nn + 8 * static_cast<size_t>(n) + 4 + sbg::workspace_bytes_per_pair(n);
+    return 48 * nn + 8 * static_cast<size_t>(n) + 4 + sbg::workspace_bytes_per_pair(n, mixed);
 }
 
 }  // namespace
@@ -242,12 +242,12 @@ void create_queue(const int* n_host, int count, int device, const sbg_solver_opt
         b.n = kv.first;
         b.pairs = std::move(kv.second);
         b.count = static_cast<int>(b.pairs.size());
-        const size_t per = bucket_bytes_per_pair(b.n);
+        b.precision = (opts.precision == SBG_PRECISION_MIXED && b.n <= max_mixed) ? SBG_PRECISION_MIXED
+                                                                                  : SBG_PRECISION_FP64;
+        const size_t per = bucket_bytes_per_pair(b.n, b.precision == SBG_PRECISION_MIXED);
         int chunk = static_cast<int>(std::max<size_t>(256, budget / per));
         if (opts.workspace_pairs > 0) chunk = opts.workspace_pairs;
         b.chunk = std::min(chunk, b.count);
-        b.precision = (opts.precision == SBG_PRECISION_MIXED && b.n <= max_mixed) ? SBG_PRECISION_MIXED
-                                                                                  : SBG_PRECISION_FP64;
         sbg_solver_options so = opts;
         so.precision = b.precision;
         so.workspace_pairs = b.chunk;

@@ -53,8 +53,8 @@ struct Slot {
     int capacity = 0;
 };
 
-inline int default_chunk_pairs(int n) {
-    const size_t per = sbg::workspace_bytes_per_pair(n);
+inline int default_chunk_pairs(int n, bool mixed = false) {
+    const size_t per = sbg::workspace_bytes_per_pair(n, mixed);
     const size_t target = size_t(1) << 30;     // about 1 GiB of scratch per stream slot
     size_t pairs = target / std::max<size_t>(per, 1);
     pairs = std::min<size_t>(std::max<size_t>(pairs, 1024), 65536);
@@ -197,17 +197,58 @@ struct sbg_solver {
                 throw Error(SBG_ERR_CAPTURING, "workspace must grow while the stream is capturing; "
                                                "call sbg_solver_reserve before capture");
             if (s.ptr) { check_cuda(cudaFree(s.ptr), "cudaFree"); s.ptr = nullptr; s.capacity = 0; }
-            const size_t bytes = sbg::workspace_bytes(n, pairs);
+            const size_t bytes = sbg::workspace_bytes(n, pairs, precision == SBG_PRECISION_MIXED);
             check_cuda(cudaMalloc(&s.ptr, bytes), "cudaMalloc(workspace)");
             s.bytes = bytes;
             s.capacity = pairs;
         }
-        return sbg::carve_workspace(s.ptr, n, s.capacity);
+        return sbg::carve_workspace(s.ptr, n, s.capacity, precision == SBG_PRECISION_MIXED);
+    }
+
+    // The mixed form above kMixedMaxN: FP64 reduction, complex64 Householder (one CTA per pair),
+    // FP64 eigenpairs of that T and Y = Q Z, the FP64 refinement on the pair's matrices in the
+    // workspace, X = L^{-H} Y for the pairs it converged; then the pairs it gave up on (ws.rstat ==
+    // kRefineRedo) are solved again by the FP64 stage kernels, every other pair left untouched.
+    void run_chunk_mixed_big(const double2* A, const double2* B, double* W, double2* X, int* info, int cnt,
+                             const sbg::Workspace& ws, cudaStream_t stream) {
+        cudaEvent_t ev;
+        stage_begin(stream, &ev);
+        check_cuda(sbg::launch_reduce(sbg::kReduceMixed, A, B, n, cnt, ws, X, info, sched.shape(), stream),
+                   "reduce kernel");
+        stage_end(stream, ev, 0, 1);
+        stage_begin(stream, &ev);
+        check_cuda(sbg::launch_hetrd_c64_big(n, cnt, X, ws, info, stream), "complex64 hetrd kernel");
+        stage_end(stream, ev, 1, 1);
+        stage_begin(stream, &ev);
+        check_cuda(sbg::launch_ql_logged(n, cnt, ws, W, X, info, false, sched.chain_threads, sched.ql_warps, stream),
+                   "QL kernels");
+        check_cuda(sbg::launch_back(sbg::kBackQOnly, n, cnt, ws, X, info, sched.shape(), stream), "Q-apply kernel");
+        check_cuda(sbg::launch_refine_big(n, cnt, ws, W, X, info, refine_steps, stream), "refinement kernel");
+        stage_end(stream, ev, 2, sbg::eig_kernel_count(n, false) + 2);
+        stage_begin(stream, &ev);
+        sbg::Workspace sel = ws;
+        sel.sel = ws.rstat;
+        sel.sel_mask = (1 << sbg::kRefineDone) | (1 << sbg::kRefineSkip);
+        check_cuda(sbg::launch_back(sbg::kBackLOnly, n, cnt, sel, X, info, sched.shape(), stream),
+                   "back-transform kernel");
+        sel.sel_mask = 1 << sbg::kRefineRedo;                   // the FP64 solve of the pairs left over
+        check_cuda(sbg::launch_reduce(sbg::kReduceFull, A, B, n, cnt, sel, X, info, sched.shape(), stream),
+                   "reduce kernel (FP64 redo)");
+        check_cuda(sbg::launch_hetrd(n, cnt, X, sel, info, sched.shape(), stream), "hetrd kernel (FP64 redo)");
+        check_cuda(sbg::launch_ql_logged(n, cnt, sel, W, X, info, false, sched.chain_threads, sched.ql_warps, stream),
+                   "QL kernels (FP64 redo)");
+        check_cuda(sbg::launch_back(sbg::kBackFull, n, cnt, sel, X, info, sched.shape(), stream),
+                   "back-transform kernel (FP64 redo)");
+        stage_end(stream, ev, 3, 1 + 1 + (n > sbg::kSmallMaxN ? 0 : 1) + sbg::eig_kernel_count(n, false) + 1);
     }
 
     // One chunk of at most chunk_pairs pairs through the three stages.
     void run_chunk(const double2* A, const double2* B, double* W, double2* X, int* info, int cnt,
                    const sbg::Workspace& ws, cudaStream_t stream) {
+        if (sbg::mixed_big(n, precision == SBG_PRECISION_MIXED)) {
+            run_chunk_mixed_big(A, B, W, X, info, cnt, ws, stream);
+            return;
+        }
         cudaEvent_t ev;
         stage_begin(stream, &ev);
         check_cuda(sbg::launch_reduce(sbg::kReduceFull, A, B, n, cnt, ws, X, info, sched.shape(), stream),

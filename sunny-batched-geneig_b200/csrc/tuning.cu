@@ -34,6 +34,12 @@ std::map<std::tuple<int, int, int>, Schedule> g_in_process;   // (device, n, pre
 
 bool fits(int n, int precision, const Schedule& s) {
     const size_t lim = static_cast<size_t>(max_smem_optin());
+    if (precision == SBG_PRECISION_MIXED && n > kMixedMaxN) {
+        // the mixed form above kMixedMaxN: the complex64 Householder, a refinement without
+        // schedule knobs, and otherwise the FP64 kernels (which the schedule shapes)
+        if (n > kMixedBigMaxN || hetrd_c64_big_smem_bytes(n) > lim) return false;
+        precision = SBG_PRECISION_FP64;
+    }
     if (n > kSmallMaxN) {                 // cluster kernels (FP64 only)
         if (precision == SBG_PRECISION_MIXED || !big_path(n)) return false;
         return big_reduce_smem_bytes(n) <= lim && ql_rows_smem_bytes(n, false) <= lim &&
@@ -252,7 +258,8 @@ double host_residual(int n, const std::complex<double>* A, const std::complex<do
 
 bool sweep(int n, int precision, const TuneRequest& req, Schedule& best, double& best_us) {
     const int count = std::max(512, std::min(4096, (1 << 22) / (n * n)));
-    Bench bench(n, precision, count);
+    // above kMixedMaxN the mixed form's schedule shapes only its FP64 kernels: time those
+    Bench bench(n, mixed_big(n, precision == SBG_PRECISION_MIXED) ? SBG_PRECISION_FP64 : precision, count);
     if (!bench.ok()) return false;
     std::vector<std::complex<double>> hA, hB;
     make_pairs(n, count, hA, hB);

@@ -94,8 +94,9 @@ class Solver:
     block_dim: threads per CTA of the CTA-per-pair stages, 128 or 256 (0 = auto).
     tuning: "suggested" (built-in schedule) or "autotune" (measured, persisted).
     cache: "auto" | "no_disk" | "none" (the autotune table's layers).
-    precision: "fp64" (the plain drop-in) or "mixed" (FP32 tridiagonal eigensolve +
-    FP64 Ogita-Aishima refinement).
+    precision: "fp64" (the plain drop-in) or "mixed" (complex64 tridiagonalisation and FP64
+    eigensolve of that T, then FP64 Ogita-Aishima refinement against C on the FP64 tensor cores;
+    n <= max_n("mixed") = 160).
     """
 
     def __init__(self, n: int, device: int = 0, *, precision: str = "fp64", batches_per_block: int = 0,

@@ -119,5 +119,6 @@ def test_big_limits():
     assert sbg.max_n("fp64") == 256
     with pytest.raises(sbg.SolverError):
         sbg.Solver(257)
+    assert sbg.max_n("mixed") == 160
     with pytest.raises(sbg.SolverError):
-        sbg.Solver(96, precision="mixed")
+        sbg.Solver(161, precision="mixed")

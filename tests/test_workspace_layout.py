@@ -37,6 +37,33 @@ def test_workspace_bytes_covers_the_carve_for_every_n_and_capacity(monkeypatch):
     assert lib.sbg_workspace_bytes(0, 0, 10) == 0 and lib.sbg_workspace_bytes(54, 0, 0) == 0
 
 
+def carve_end_mixed(n, pairs):
+    """The mixed form's layout: above n = 63 six more regions follow the seven of carve_end -- five
+    n x n complex matrices per pair (the refinement's C, second Y buffer, P / E, G, S) and one int
+    per pair (its status); at n <= 63 the layout is the plain one."""
+    end = carve_end(n, pairs)
+    if n > 63:
+        end += 5 * _align(16 * n * n * pairs) + _align(4 * pairs)
+    return end
+
+
+def test_mixed_workspace_bytes_cover_the_carve(monkeypatch):
+    monkeypatch.delenv("SBG_QL_LOG_CAPACITY", raising=False)
+    import sbg
+    lib = sbg.load()
+    pairs = np.arange(1, 2049)
+    for n in range(1, 161):
+        per = lib.sbg_workspace_bytes_per_pair(n, 1)
+        got = np.array([lib.sbg_workspace_bytes(n, 1, int(p)) for p in pairs], dtype=np.int64)
+        want = np.array([carve_end_mixed(n, int(p)) for p in pairs], dtype=np.int64)
+        assert (got >= want).all(), (n, pairs[got < want][:5])
+        assert (got <= per * pairs + 13 * 256).all(), n
+        if n <= 63:
+            assert lib.sbg_workspace_bytes_per_pair(n, 1) == lib.sbg_workspace_bytes_per_pair(n, 0)
+        else:
+            assert per == lib.sbg_workspace_bytes_per_pair(n, 0) + 80 * n * n + 4
+
+
 def test_old_slack_was_short_somewhere():
     """The sizing this replaced (per-pair bytes x pairs + 5 x 256) fell short of the carve for
     some orders and capacities: the exact size matters."""
