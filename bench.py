@@ -703,9 +703,13 @@ def run_other(args):
             ref = (a, b, Wr, Xr, time.perf_counter() - t0)
         forms_out = {}
         for f in forms:
-            s = sbg.Solver(n, local, precision=f, workspace_pairs=chunk)
+            # chunks of at most 65,536 pairs and ~16 GB of workspace (the mixed form above n = 63
+            # keeps five more n x n matrices per pair)
+            per = int(sbg.load().sbg_workspace_bytes_per_pair(n, sbg.PRECISIONS[f]))
+            s = sbg.Solver(n, local, precision=f, workspace_pairs=max(1024, min(chunk, int(16e9 // per))))
             s.launch(A, B, W, X, info, stream)
             torch.cuda.synchronize()
+            redo = s.refine_redo_pairs(reset=True)          # mixed: pairs its refinement handed to FP64
             acc = None
             if ref is not None:
                 idx = torch.as_tensor(sample_idx, device=device)
@@ -735,7 +739,7 @@ def run_other(args):
             st = {k: (v[0] / 2, v[1] / 2) for k, v in s.read_stage_times().items()}
             s.enable_stage_timing(False)
             forms_out[f] = dict(value=world * pairs / (ms / 1e3), ms=ms, accuracy=acc, clocks=clocks, stages=st,
-                                info_nonzero=int((info != 0).sum().item()), solver=s)
+                                info_nonzero=int((info != 0).sum().item()), solver=s, redo=redo)
         best = max(forms_out, key=lambda f: forms_out[f]["value"])
         R = forms_out[best]
         fl = stage_flops(n)
@@ -753,7 +757,9 @@ def run_other(args):
                                 "whole_solve": {"achieved_tflops": 32.0 * n ** 3 * R["value"] / world / 1e12,
                                                 "frac": 32.0 * n ** 3 * R["value"] / world / 1e12 / peak["tflops"]}},
                       forms={f: {"value": r["value"], "ms_per_step": r["ms"], "accuracy": r["accuracy"],
-                                 "stage_ms_per_step": {k: v[0] for k, v in r["stages"].items()}}
+                                 "stage_ms_per_step": {k: v[0] for k, v in r["stages"].items()},
+                                 **({"fp64_resolved_pairs": r["redo"], "fp64_resolved_fraction": r["redo"] / pairs}
+                                    if f == "mixed" else {})}
                              for f, r in forms_out.items()}, form=best)
         if ref is not None:
             result["cpu"] = {"value": len(sample_idx) / ref[4], "unit": "solves/s", "cores": threads, "kind": "port",

@@ -159,6 +159,12 @@ int sbg_solver_solve_host(sbg_solver* s, const cuDoubleComplex* h_A, const cuDou
 /* Bytes the solver's last sbg_solver_solve_host moved host -> device and device -> host. */
 int sbg_solver_host_transfer_bytes(const sbg_solver* s, long long* h2d_bytes, long long* d2h_bytes);
 
+/* Mixed form: the number of pairs its refinement handed to the FP64 re-solve (did not reach the
+ * gates within refine_steps updates, or the eigensolve of the complex64 T failed) over all launches
+ * since the solver was created or the count last reset (reset != 0 clears it after reading).
+ * Synchronous (waits for the device); 0 for an FP64 solver.  No counterpart in the reference. */
+int sbg_solver_refine_redo_pairs(sbg_solver* s, long long* count, int reset);
+
 /* Per-stage timing: when enabled, every launch records CUDA events around each stage
  * kernel on the launch stream.  sbg_solver_read_stage_times synchronizes on them and
  * returns, per stage (0 = Cholesky + two-sided reduction, 1 = Householder

@@ -208,6 +208,19 @@ int sbg_solver_host_transfer_bytes(const sbg_solver* s, long long* h2d_bytes, lo
     });
 }
 
+int sbg_solver_refine_redo_pairs(sbg_solver* s, long long* count, int reset) {
+    return guarded([&] {
+        if (!s || !count) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
+        *count = 0;
+        if (!s->d_redo) return;                 // FP64 solver, or no launch yet
+        DeviceGuard g(s->device);
+        unsigned long long v = 0;
+        check_cuda(cudaMemcpy(&v, s->d_redo, sizeof(v), cudaMemcpyDeviceToHost), "D2H redo counter");
+        *count = static_cast<long long>(v);
+        if (reset) check_cuda(cudaMemset(s->d_redo, 0, sizeof(v)), "cudaMemset(redo counter)");
+    });
+}
+
 int sbg_solver_enable_stage_timing(sbg_solver* s, int enable) {
     return guarded([&] {
         if (!s) throw Error(SBG_ERR_INVALID_VALUE, "solver == NULL");

@@ -48,6 +48,9 @@ struct Workspace {
     // pairs its refinement gave up on.
     const int* sel = nullptr;
     int sel_mask = 0;
+    // Mixed form: running count of the pairs its refinement handed to the FP64 re-solve (the
+    // solver's; null for workspaces without one).
+    unsigned long long* redo_count = nullptr;
 };
 
 // Outcome of the mixed form's refinement for kMixedMaxN < n <= kMixedBigMaxN (Workspace::rstat).

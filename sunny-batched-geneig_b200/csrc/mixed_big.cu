@@ -222,7 +222,11 @@ __global__ void __launch_bounds__(kRfThreads, 3) k_refine_big(int n, int batch, 
         return;
     }
     if (inf != 0) {                                           // the FP64 eigensolve of the complex64 T failed
-        if (tid == 0) { ws.rstat[b] = kRefineRedo; info[b] = 0; }
+        if (tid == 0) {
+            ws.rstat[b] = kRefineRedo;
+            info[b] = 0;
+            if (ws.redo_count) atomicAdd(ws.redo_count, 1ull);
+        }
         return;
     }
     const size_t mat = static_cast<size_t>(n) * n;
@@ -303,7 +307,10 @@ __global__ void __launch_bounds__(kRfThreads, 3) k_refine_big(int n, int batch, 
         const bool orth_ok = acc3[2] <= kRfOrthTol;
         if (res_ok && orth_ok) break;
         if (it >= max_updates) {
-            if (tid == 0) ws.rstat[b] = kRefineRedo;          // the FP64 kernels solve it again
+            if (tid == 0) {                                   // the FP64 kernels solve it again
+                ws.rstat[b] = kRefineRedo;
+                if (ws.redo_count) atomicAdd(ws.redo_count, 1ull);
+            }
             return;
         }
         const double floor_rel = res_ok ? 1e-2 : 0.0;

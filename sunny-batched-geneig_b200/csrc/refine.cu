@@ -324,7 +324,11 @@ __global__ void __launch_bounds__(NP * 4, 1) k_refine_c(int n, int batch, Worksp
     const int inf = info[b];
     if (inf > n || inf < 0) return;            // B not positive definite (or a copy timed out)
     if (inf != 0) {                            // the FP64 eigensolve of the complex64 T did not converge
-        if (tid == 0) { ws.flag[b] = 2; info[b] = 0; }
+        if (tid == 0) {
+            ws.flag[b] = 2;
+            info[b] = 0;
+            if (ws.redo_count) atomicAdd(ws.redo_count, 1ull);
+        }
         return;
     }
     extern __shared__ __align__(16) unsigned char smem[];
@@ -367,7 +371,10 @@ __global__ void __launch_bounds__(NP * 4, 1) k_refine_c(int n, int batch, Worksp
     block_sum4<NB>(cn, red);
     const double cnorm = sqrt(cn[0]);
     if (!refine<NP>(n, Cre, Cim, Yre, Yim, Pre, Pim, lam, red, cnorm, max_updates)) {
-        if (tid == 0) ws.flag[b] = 2;          // the FP64 fallback redoes this pair
+        if (tid == 0) {                        // the FP64 fallback redoes this pair
+            ws.flag[b] = 2;
+            if (ws.redo_count) atomicAdd(ws.redo_count, 1ull);
+        }
         return;
     }
     if (tid == 0) ws.flag[b] = 0;

@@ -122,6 +122,7 @@ struct sbg_solver {
     int precision = SBG_PRECISION_FP64;
     int refine_steps = 5;
     int chunk_pairs = 0;
+    unsigned long long* d_redo = nullptr;   // mixed form: pairs handed to the FP64 re-solve
     sbg::Schedule sched;
     bool autotuned = false;
     bool sweep_ran = false;
@@ -152,6 +153,7 @@ struct sbg_solver {
         cudaGetDevice(&prev);
         cudaSetDevice(device);
         for (auto& s : slots) if (s.ptr) cudaFree(s.ptr);
+        if (d_redo) cudaFree(d_redo);
         for (auto& st : staging) {
             if (st.stream) cudaStreamDestroy(st.stream);
             if (st.pull) cudaStreamDestroy(st.pull);
@@ -202,7 +204,15 @@ struct sbg_solver {
             s.bytes = bytes;
             s.capacity = pairs;
         }
-        return sbg::carve_workspace(s.ptr, n, s.capacity, precision == SBG_PRECISION_MIXED);
+        sbg::Workspace w = sbg::carve_workspace(s.ptr, n, s.capacity, precision == SBG_PRECISION_MIXED);
+        if (precision == SBG_PRECISION_MIXED) {
+            if (!d_redo) {
+                check_cuda(cudaMalloc(&d_redo, sizeof(unsigned long long)), "cudaMalloc(redo counter)");
+                check_cuda(cudaMemset(d_redo, 0, sizeof(unsigned long long)), "cudaMemset(redo counter)");
+            }
+            w.redo_count = d_redo;
+        }
+        return w;
     }
 
     // The mixed form above kMixedMaxN: FP64 reduction, complex64 Householder (one CTA per pair),

@@ -164,6 +164,14 @@ class Solver:
                "sbg_solver_host_transfer_bytes")
         return h2d.value, d2h.value
 
+    def refine_redo_pairs(self, reset: bool = False) -> int:
+        """Mixed form: pairs the refinement handed to the FP64 re-solve since creation (or the last
+        reset); 0 for the FP64 form.  Waits for the device."""
+        c = ctypes.c_longlong()
+        _check(self._lib.sbg_solver_refine_redo_pairs(self._h, ctypes.byref(c), 1 if reset else 0),
+               "sbg_solver_refine_redo_pairs")
+        return c.value
+
     def enable_stage_timing(self, enable: bool = True) -> None:
         _check(self._lib.sbg_solver_enable_stage_timing(self._h, int(enable)), "sbg_solver_enable_stage_timing")
 

@@ -52,6 +52,7 @@ SIGNATURES = {
     "sbg_solver_solve_host": (I, [P, P, P, P, P, P, I, I, I]),
     "sbg_solver_host_transfer_bytes": (I, [P, P, P]),
     "sbg_solver_enable_stage_timing": (I, [P, I]),
+    "sbg_solver_refine_redo_pairs": (I, [P, P, I]),
     "sbg_solver_read_stage_times": (I, [P, P, P]),
     "sbg_workspace_bytes_per_pair": (SZ, [I, I]),
     "sbg_workspace_bytes": (SZ, [I, I, I]),

@@ -65,12 +65,16 @@ def test_mixed_big_redo_path(n, oracle_mod):
     N = n // 2
     A, B = wl.bogoliubov(N, 16, seed=5, frac=1e-3)
     A, B = A.numpy(), B.numpy()
-    W, X, info = run(sbg.Solver(n, precision="mixed", refine_steps=1), A, B)
+    s = sbg.Solver(n, precision="mixed", refine_steps=1)
+    W, X, info = run(s, A, B)
     Wr, Xr, _ = oracle_mod.hegv(A, B, n, nthreads=8)
     check(A, B, W, X, info, Wr, Xr, n, relative=True)
     W64, X64, _ = run(n, A, B, "fp64")
     same = [(W[p] == W64[p]).all() and (X[p] == X64[p]).all() for p in range(len(W))]
     assert sum(same) >= 1, "no pair went through the FP64 re-solve"
+    assert s.refine_redo_pairs() == sum(same)            # the counter names exactly those pairs
+    assert s.refine_redo_pairs(reset=True) == sum(same) and s.refine_redo_pairs() == 0
+    assert sbg.Solver(n).refine_redo_pairs() == 0        # FP64 form: nothing to count
 
 
 def test_mixed_big_near_goldstone(oracle_mod):
