@@ -56,16 +56,14 @@ STAGE_BYTES = {"reduce": 32 * N * N, "tridiag": 0, "eig": 16 * N, "back": 16 * N
 
 # DRAM bytes (read + write) per pair of each FP64 stage at n = 54: ncu's dram__bytes_read.sum +
 # dram__bytes_write.sum of each stage kernel, one capture of a 16,384-pair solve of this workload
-#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none \
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none \
 #       -k regex:"k_potrf_warp|k_hegst_col|k_hetrd_warp|k_ql_values|k_tridiag_invit|k_back_col" -s 6 -c 6 \
 #       python bench.py --pairs 16384 --steps 1 --warmup 1 --no-e2e --no-cpu --forms fp64 --sample 64
 # divided by the pairs.  Traffic grows in proportion to the pairs a launch processes, so traffic per
-# launch = this x pairs per launch.  TRAFFIC_SOURCE says when the figures were taken.
-TRAFFIC_PER_PAIR_N54 = {"reduce": 51.4e3 + 120.0e3, "tridiag": 52.19e3, "eig": 0.9e3 + 21.4e3, "back": 114.4e3}
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per pair of a 16,384-pair solve, scaled to the "
-                  "launch's pairs: the Householder (k_hetrd_warp) from a capture of the current kernels "
-                  "(29.9 + 22.3 KB); the other stages from the same capture of their unchanged kernels one "
-                  "build earlier")
+# launch = this x pairs per launch.
+TRAFFIC_PER_PAIR_N54 = {"reduce": 51.4e3 + 119.8e3, "tridiag": 51.9e3, "eig": 0.9e3 + 21.1e3, "back": 157.3e3}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum per pair of a 16,384-pair solve of this "
+                  "workload by the current stage kernels (one capture of all six), scaled to the launch's pairs")
 
 # The other configurations (bench.py --workload NAME): fixed-n Bogoliubov / q-sweep batches and the
 # uneven-n batch through the queue.  Each prints one JSON line of the same shape as the headline.
