@@ -157,10 +157,11 @@ template <int CS, int RM>
 __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __restrict__ A,
                                                             const double2* __restrict__ B, int n, int batch,
                                                             Workspace ws, double2* __restrict__ X,
-                                                            int* __restrict__ info) {
+                                                            int* __restrict__ info, int hegst_only) {
     constexpr int NCW = ((32 * RM + CS - 1) / CS + kBigWarps - 1) / kBigWarps;   // own columns per warp (max)
     const int r = CS == 1 ? 0 : static_cast<int>(cg::this_cluster().block_rank());
     const int b = blockIdx.x / CS;                     // grid = batch * CS: b < batch
+    if (!pair_selected(ws, b)) return;                 // uniform over the pair's cluster
     extern __shared__ __align__(16) unsigned char smem[];
     const BigReduceSmem lay(n, CS);
     double2* Lp = reinterpret_cast<double2*>(smem + lay.Lp);
@@ -278,6 +279,16 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
                 if (c < ncw && i < n) Cc[static_cast<size_t>(t) * n + i] = v;
             }
         __syncthreads();
+        if (hegst_only) {                               // mixed form: C's lower triangle and L out
+            cluster_barrier<CS>();                      // every CTA has read its rows of W from X
+            for_own_lower(n, CS, r, 0, nc, [&](int t, int j, int i) {
+                LVb[i + static_cast<size_t>(j) * n] = Lp[own_off(t, n, CS, r) + (i - j)];
+                Xb[i + static_cast<size_t>(j) * n] = Cc[static_cast<size_t>(t) * n + i];
+            });
+            if (r == 0 && tid == 0) info[b] = status;
+            cluster_barrier<CS>();                      // no CTA leaves while a peer may read its memory
+            return;
+        }
 
         // ---- hetrd (LAPACK zhetd2's steps, lower)
         double2* vl = panel;                 // v_k(k+1+i'), i' < m
@@ -1037,12 +1048,12 @@ cudaError_t launch_clustered(void (*kernel)(KArgs...), int cs, int grid, int thr
 
 template <int CS, int RM>
 void run_reduce_big(cudaError_t* err, const double2* A, const double2* B, int n, int batch, const Workspace& ws,
-                    double2* X, int* info, cudaStream_t stream) {
+                    double2* X, int* info, cudaStream_t stream, int hegst_only) {
     const size_t smem = BigReduceSmem(n, CS).total;
     static SmemOptIn f;
     set_big_smem_once(k_reduce_big<CS, RM>, f, static_cast<size_t>(max_smem_optin()));
     *err = launch_clustered(k_reduce_big<CS, RM>, CS, batch * CS, kBigThreads, smem, stream, A, B, n, batch, ws, X,
-                            info);
+                            info, hegst_only);
 }
 
 template <int CS, int G, int RM, int NCW>
@@ -1091,9 +1102,8 @@ cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int bat
         else run_reduce_mid<20>(A, B, n, batch, ws, X, info, stream, hegst_only);
         return cudaGetLastError();
     }
-    if (hegst_only) return cudaErrorInvalidValue;    // the cluster kernel always tridiagonalises
     cudaError_t err = cudaSuccess;
-    SBG_BIG_DISPATCH(n, run_reduce_big, &err, A, B, n, batch, ws, X, info, stream);
+    SBG_BIG_DISPATCH(n, run_reduce_big, &err, A, B, n, batch, ws, X, info, stream, hegst_only ? 1 : 0);
     return err != cudaSuccess ? err : cudaGetLastError();
 }
 
@@ -1102,7 +1112,7 @@ size_t hetrd_c64_big_smem_bytes(int n) { return C64BigSmem(n).total; }
 cudaError_t launch_hetrd_c64_big(int n, int batch, const double2* C, const Workspace& ws, int* info,
                                  cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
-    if (n <= kMixedMaxN || n > kMixedBigMaxN || n > kMidMaxN) return cudaErrorInvalidValue;
+    if (n <= kMixedMaxN || n > kMixedBigMaxN) return cudaErrorInvalidValue;
     if (!C || !info || !ws.LV || !ws.d || !ws.e || !ws.tau || !ws.rfC) return cudaErrorInvalidValue;
     const size_t smem = C64BigSmem(n).total;
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;

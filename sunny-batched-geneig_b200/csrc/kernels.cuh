@@ -43,7 +43,7 @@ struct Workspace {
     double2* rfS = nullptr;
     int* rstat = nullptr;
     // Pair selection: when sel is set, the stage kernels that honour it (the FP64 kernels for
-    // 57 <= n <= 160) run pair b only if bit sel[b] of sel_mask is set, and leave every other
+    // 57 <= n <= 256) run pair b only if bit sel[b] of sel_mask is set, and leave every other
     // pair's outputs and scratch untouched.  The mixed form uses it to re-solve in FP64 only the
     // pairs its refinement gave up on.
     const int* sel = nullptr;
@@ -81,8 +81,9 @@ __host__ __device__ constexpr int refine_ld(int n) { return refine_np(n) + 4; }
 __host__ __device__ constexpr int refine_stash_entries(int n) { return refine_np(n) * refine_ld(n); }
 constexpr int kMixedMaxN = 63;       // inverse iteration (no rotation log, so the stash is free)
 // Mixed form above kMixedMaxN: the refinement runs on per-pair matrices in the workspace
-// (csrc/mixed_big.cu), up to the largest n the one-CTA reduction kernel takes.
-constexpr int kMixedBigMaxN = 160;
+// (csrc/mixed_big.cu); the largest n is where the complex64 Householder's packed tile still fits one
+// CTA's shared memory (sbg_max_n reports it: 235 with B200's 227 KB per CTA).
+constexpr int kMixedBigMaxN = 256;
 inline bool mixed_big(int n, bool mixed) { return mixed && n > kMixedMaxN; }
 
 // Bytes per pair of the workspace of a solver of order n (mixed: the mixed form's).
@@ -175,7 +176,7 @@ constexpr int kBigMaxN = 256;
 bool big_path(int n);
 size_t big_reduce_smem_bytes(int n);
 size_t ql_rows_smem_bytes(int n, bool single);
-// hegst_only (n <= 160): stop after C = L^{-1} A L^{-H} (C's lower triangle in X, L in LV).
+// hegst_only: stop after C = L^{-1} A L^{-H} (C's lower triangle in X, L in LV).
 cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
                               int* info, cudaStream_t stream, bool hegst_only = false);
 // Mixed form for kMixedMaxN < n <= kMixedBigMaxN (csrc/mixed_big.cu), after

@@ -119,6 +119,7 @@ def test_big_limits():
     assert sbg.max_n("fp64") == 256
     with pytest.raises(sbg.SolverError):
         sbg.Solver(257)
-    assert sbg.max_n("mixed") == 160
+    mx = sbg.max_n("mixed")                  # the complex64 Householder's tile: 235 on B200
+    assert 192 <= mx < 256
     with pytest.raises(sbg.SolverError):
-        sbg.Solver(161, precision="mixed")
+        sbg.Solver(mx + 1, precision="mixed")

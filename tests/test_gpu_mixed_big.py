@@ -1,4 +1,4 @@
-"""The mixed form above n = 63 (63 < n <= 160) against LAPACK zhegv, through the C ABI.
+"""The mixed form above n = 63 (63 < n <= sbg.max_n("mixed")) against LAPACK zhegv, through the C ABI.
 
 There the complex64 Householder runs one CTA per pair, the FP64 eigenpairs of its T and
 Y = Q Z come from the FP64 kernels, and the Ogita-Aishima refinement works on the pair's
@@ -21,12 +21,15 @@ from test_gpu_parity import check, run
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("n", [64, 65, 72, 84, 85, 96, 100, 128, 129, 160])
+@pytest.mark.parametrize("n", [64, 65, 72, 84, 85, 96, 100, 128, 129, 160, 161, 192, 235])
 def test_mixed_big_sizes(n, oracle_mod):
     """Both sides of every boundary the path crosses: the small-path reflector layout (n <= 84)
     and the cluster back-transform's (n > 84), partial and whole 32-wide refinement tiles, the
-    inverse-iteration (85..128) and rotation-log (64..84, 129..160) eigenvectors of T."""
-    H, S = oracle_mod.gen_fixture_pairs(n, 6, 13, "random")
+    inverse-iteration (85..128) and rotation-log (64..84, 129..) eigenvectors of T, the one-CTA
+    (85..160) and cluster (161..) FP64 reductions, and the largest n."""
+    if n > sbg.max_n("mixed"):
+        pytest.skip(f"the mixed form covers n <= {sbg.max_n('mixed')}")
+    H, S = oracle_mod.gen_fixture_pairs(n, 6 if n <= 160 else 3, 13, "random")
     W, X, info = run(n, H, S, "mixed")
     Wr, Xr, _ = oracle_mod.hegv(H, S, n, nthreads=8)
     check(H, S, W, X, info, Wr, Xr, n)
@@ -77,13 +80,14 @@ def test_mixed_big_redo_path(n, oracle_mod):
     assert sbg.Solver(n).refine_redo_pairs() == 0        # FP64 form: nothing to count
 
 
-def test_mixed_big_near_goldstone(oracle_mod):
-    """kappa(B) ~ 1e8 at n = 96: complex64 cannot resolve the O(1) eigenvalues of a C whose norm
-    is ~1e8, the refinement gives those pairs up, and the FP64 re-solve meets the same gates as the
-    FP64 form (eigenvalues against |l_i| kappa_i + ||C||; residual and orthogonality within 4x of
-    LAPACK's own)."""
-    n = 96
-    A, B = wl.bogoliubov(48, 6, seed=11, frac=1e-3, goldstone=1e-8)
+@pytest.mark.parametrize("N", [48, 96])
+def test_mixed_big_near_goldstone(N, oracle_mod):
+    """kappa(B) ~ 1e8 at n = 96 and 192 (config 5's sizes): C's norm is ~1e8 against O(1)
+    eigenvalues, so complex64 resolves them only coarsely; the refinement against the FP64 C brings
+    most pairs to the gates and hands the rest to the FP64 re-solve.  Gates as for the FP64 form:
+    eigenvalues against |l_i| kappa_i + ||C||, residual and orthogonality within 4x of LAPACK's."""
+    n = 2 * N
+    A, B = wl.bogoliubov(N, 6 if N <= 48 else 3, seed=11, frac=1e-3, goldstone=1e-8)
     A, B = A.numpy(), B.numpy()
     Wr, Xr, _ = oracle_mod.hegv(A, B, n, nthreads=8)
     normB = np.linalg.norm(Mx.as_mats(B, n), ord=2, axis=(1, 2))

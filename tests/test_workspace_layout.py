@@ -52,7 +52,7 @@ def test_mixed_workspace_bytes_cover_the_carve(monkeypatch):
     import sbg
     lib = sbg.load()
     pairs = np.arange(1, 2049)
-    for n in range(1, 161):
+    for n in range(1, 257):
         per = lib.sbg_workspace_bytes_per_pair(n, 1)
         got = np.array([lib.sbg_workspace_bytes(n, 1, int(p)) for p in pairs], dtype=np.int64)
         want = np.array([carve_end_mixed(n, int(p)) for p in pairs], dtype=np.int64)
