@@ -96,7 +96,7 @@ class Solver:
     cache: "auto" | "no_disk" | "none" (the autotune table's layers).
     precision: "fp64" (the plain drop-in) or "mixed" (complex64 tridiagonalisation and FP64
     eigensolve of that T, then FP64 Ogita-Aishima refinement against C on the FP64 tensor cores;
-    n <= max_n("mixed") = 160).
+    n <= max_n("mixed") = 235 on B200).
     """
 
     def __init__(self, n: int, device: int = 0, *, precision: str = "fp64", batches_per_block: int = 0,
