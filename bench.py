@@ -76,6 +76,11 @@ OTHER_WORKLOADS = {
                         desc="near-Goldstone Bogoliubov pairs n=96, kappa(B)~1e8 (null mode 1e-8||B|| injected)"),
     "goldstone192": dict(kind="bogoliubov", N=96, pairs=10000, frac=1e-3, goldstone=1e-8,
                          desc="near-Goldstone Bogoliubov pairs n=192, kappa(B)~1e8 (cluster/DSMEM path)"),
+    "bogoliubov128": dict(kind="bogoliubov", N=64, pairs=25000, frac=1e-3, goldstone=None,
+                          desc="Bogoliubov pairs n=128 (N=64), lambda_min(B)=1e-3||B||, A=diag(I,-I), seed 0"),
+    "bogoliubov192": dict(kind="bogoliubov", N=96, pairs=10000, frac=1e-3, goldstone=None,
+                          desc="Bogoliubov pairs n=192 (N=96), lambda_min(B)=1e-3||B||, A=diag(I,-I), seed 0 "
+                               "(the near-Goldstone n=192 line without its null mode)"),
     "spinwave54": dict(kind="spinwave", N=27, pairs=GRID ** 3, frac=1e-3,
                        desc="spin-wave q-sweep n=54 (N=27 sites, 4 bonds/site, 64^3 grid): A(q), B(q) assembled "
                             "on the GPU from the bond table, one field for the sweep with "
