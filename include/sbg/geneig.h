@@ -181,16 +181,17 @@ size_t sbg_workspace_bytes_per_pair(int n, int precision);
  * 7 * 256 bytes more). */
 size_t sbg_workspace_bytes(int n, int precision, int pairs);
 
-/* The solver's schedule as seven ints (no counterpart in the reference, whose schedule is its
+/* The solver's schedule as eight ints (no counterpart in the reference, whose schedule is its
  * (batches per block, block size) pair): [0] threads per CTA of the CTA-per-pair Householder,
  * [1] pairs per CTA of the warp-per-pair Cholesky / Householder kernels, [2] 1 = the exact-n
  * column kernels where they exist (n = 32, 54), [3] lanes per column of the column back-transform
  * (1 or 2), [4] pairs per CTA of the QL rotation stage, [5] pairs per CTA of the QL scalar
- * chain, [6] reflectors per pass of the column back-transform's Q application (1 or 2).
+ * chain, [6] reflectors per pass of the column back-transform's Q application (1 or 2), [7] 1 = the
+ * mixed form's Cholesky and reduction above n = 84 by the blocked tensor-core kernel (0 or 1).
  * set_schedule replaces it (values checked against their ranges and the device's shared memory;
  * SBG_ERR_INVALID_VALUE otherwise), for callers that tune outside the library. */
-int sbg_solver_schedule(const sbg_solver* s, int* out7);
-int sbg_solver_set_schedule(sbg_solver* s, const int* in7);
+int sbg_solver_schedule(const sbg_solver* s, int* out8);
+int sbg_solver_set_schedule(sbg_solver* s, const int* in8);
 
 /* Getters (nvrtc_solver.hpp:128-145). */
 int sbg_solver_matrix_size(const sbg_solver* s);

@@ -157,11 +157,12 @@ template <int CS, int RM>
 __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __restrict__ A,
                                                             const double2* __restrict__ B, int n, int batch,
                                                             Workspace ws, double2* __restrict__ X,
-                                                            int* __restrict__ info, int hegst_only) {
+                                                            int* __restrict__ info, int mode) {
     constexpr int NCW = ((32 * RM + CS - 1) / CS + kBigWarps - 1) / kBigWarps;   // own columns per warp (max)
     const int r = CS == 1 ? 0 : static_cast<int>(cg::this_cluster().block_rank());
     const int b = blockIdx.x / CS;                     // grid = batch * CS: b < batch
     if (!pair_selected(ws, b)) return;                 // uniform over the pair's cluster
+    if (mode == kBigHetrdOnly && info[b] != 0) return; // the Cholesky failed (read before any write)
     extern __shared__ __align__(16) unsigned char smem[];
     const BigReduceSmem lay(n, CS);
     double2* Lp = reinterpret_cast<double2*>(smem + lay.Lp);
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
     // ---- stage own columns: lower part of B (packed) and all of A
     if (tid == 0) { *s_fail = 0; mbar_init(bar, 1); fence_mbar_init(); }
     __syncthreads();
-    if (warp == 0) {
+    if (warp == 0 && mode != kBigHetrdOnly) {
         if (lane == 0) mbar_arrive_expect_tx(bar, 16u * static_cast<uint32_t>(own_off(nc, n, CS, r) + n * nc));
         __syncwarp();
         for (int t = lane; t < nc; t += 32) {
@@ -197,15 +198,19 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
         }
     }
     int status = 0;
-    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+    if (mode != kBigHetrdOnly && !mbar_wait_bounded(bar, 0, kMaxPolls)) {
         status = kInfoCopyTimeout;
         mbar_wait_bounded(bar, 0, kMaxPolls);
     }
+    if (mode == kBigHetrdOnly)                         // C's lower triangle from X (k_reduce_tc's output)
+        for_own_lower(n, CS, r, 0, nc, [&](int t, int j, int i) {
+            Cc[static_cast<size_t>(t) * n + i] = Xb[i + static_cast<size_t>(j) * n];
+        });
     cluster_barrier<CS>();                             // every CTA of the cluster is running
 
     // ---- potrf (right-looking, cyclic columns)
     int fail = 0;
-    for (int k = 0; k < n; ++k) {
+    for (int k = 0; k < n && mode != kBigHetrdOnly; ++k) {
         const int o = k % CS;
         if (r == o) {
             double2* col = Lp + own_off(k / CS, n, CS, r);             // col[i - k] = B(i, k)
@@ -236,50 +241,52 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
     }
 
     if (!fail) {
-        for (int k = tid; k < n; k += kBigThreads) {
-            const int o = k % CS;
-            invd[k] = 1.0 / peer(Lp, o)[own_off(k / CS, n, CS, o)].x;
+        if (mode != kBigHetrdOnly) {                    // Cholesky done: W and C here
+            for (int k = tid; k < n; k += kBigThreads) {
+                const int o = k % CS;
+                invd[k] = 1.0 / peer(Lp, o)[own_off(k / CS, n, CS, o)].x;
+            }
+            // ---- W = L^{-1} A on own columns (warp w: own columns t = w + 8 c)
+            const int ncw = nc > warp ? (nc - warp + kBigWarps - 1) / kBigWarps : 0;
+            double2 y[NCW][RM];
+    #pragma unroll
+            for (int c = 0; c < NCW; ++c)
+    #pragma unroll
+                for (int q = 0; q < RM; ++q) {
+                    const int i = lane + 32 * q, t = warp + kBigWarps * c;
+                    y[c][q] = (c < ncw && i < n) ? Cc[static_cast<size_t>(t) * n + i] : make_double2(0.0, 0.0);
+                }
+            big_lower_solve<CS, RM, NCW>(y, ncw, n, Lp, panel, invd);
+    #pragma unroll
+            for (int c = 0; c < NCW; ++c)
+    #pragma unroll
+                for (int q = 0; q < RM; ++q) {
+                    const int i = lane + 32 * q, j = (warp + kBigWarps * c) * CS + r;
+                    if (c < ncw && i < n) Xb[i + static_cast<size_t>(j) * n] = y[c][q];
+                }
+            __threadfence();
+            cluster_barrier<CS>();                          // all of W is in X
+            // ---- C = L^{-1} W^H: column j of W^H is conj(row j of W)
+    #pragma unroll
+            for (int c = 0; c < NCW; ++c)
+    #pragma unroll
+                for (int q = 0; q < RM; ++q) {
+                    const int i = lane + 32 * q, j = (warp + kBigWarps * c) * CS + r;
+                    y[c][q] = (c < ncw && i < n) ? cconj(Xb[j + static_cast<size_t>(i) * n]) : make_double2(0.0, 0.0);
+                }
+            big_lower_solve<CS, RM, NCW>(y, ncw, n, Lp, panel, invd);
+    #pragma unroll
+            for (int c = 0; c < NCW; ++c)
+    #pragma unroll
+                for (int q = 0; q < RM; ++q) {
+                    const int i = lane + 32 * q, t = warp + kBigWarps * c, j = t * CS + r;
+                    double2 v = y[c][q];
+                    if (i == j) v.y = 0.0;
+                    if (c < ncw && i < n) Cc[static_cast<size_t>(t) * n + i] = v;
+                }
+            __syncthreads();
         }
-        // ---- W = L^{-1} A on own columns (warp w: own columns t = w + 8 c)
-        const int ncw = nc > warp ? (nc - warp + kBigWarps - 1) / kBigWarps : 0;
-        double2 y[NCW][RM];
-#pragma unroll
-        for (int c = 0; c < NCW; ++c)
-#pragma unroll
-            for (int q = 0; q < RM; ++q) {
-                const int i = lane + 32 * q, t = warp + kBigWarps * c;
-                y[c][q] = (c < ncw && i < n) ? Cc[static_cast<size_t>(t) * n + i] : make_double2(0.0, 0.0);
-            }
-        big_lower_solve<CS, RM, NCW>(y, ncw, n, Lp, panel, invd);
-#pragma unroll
-        for (int c = 0; c < NCW; ++c)
-#pragma unroll
-            for (int q = 0; q < RM; ++q) {
-                const int i = lane + 32 * q, j = (warp + kBigWarps * c) * CS + r;
-                if (c < ncw && i < n) Xb[i + static_cast<size_t>(j) * n] = y[c][q];
-            }
-        __threadfence();
-        cluster_barrier<CS>();                          // all of W is in X
-        // ---- C = L^{-1} W^H: column j of W^H is conj(row j of W)
-#pragma unroll
-        for (int c = 0; c < NCW; ++c)
-#pragma unroll
-            for (int q = 0; q < RM; ++q) {
-                const int i = lane + 32 * q, j = (warp + kBigWarps * c) * CS + r;
-                y[c][q] = (c < ncw && i < n) ? cconj(Xb[j + static_cast<size_t>(i) * n]) : make_double2(0.0, 0.0);
-            }
-        big_lower_solve<CS, RM, NCW>(y, ncw, n, Lp, panel, invd);
-#pragma unroll
-        for (int c = 0; c < NCW; ++c)
-#pragma unroll
-            for (int q = 0; q < RM; ++q) {
-                const int i = lane + 32 * q, t = warp + kBigWarps * c, j = t * CS + r;
-                double2 v = y[c][q];
-                if (i == j) v.y = 0.0;
-                if (c < ncw && i < n) Cc[static_cast<size_t>(t) * n + i] = v;
-            }
-        __syncthreads();
-        if (hegst_only) {                               // mixed form: C's lower triangle and L out
+        if (mode == kBigHegstOnly) {                    // mixed form: C's lower triangle and L out
             cluster_barrier<CS>();                      // every CTA has read its rows of W from X
             for_own_lower(n, CS, r, 0, nc, [&](int t, int j, int i) {
                 LVb[i + static_cast<size_t>(j) * n] = Lp[own_off(t, n, CS, r) + (i - j)];
@@ -391,7 +398,7 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
         }
         // ---- L -> LV lower; reflector k -> LV(s, n-1-k), s = i - k - 1
         for_own_lower(n, CS, r, 0, nc, [&](int t, int j, int i) {
-            LVb[i + static_cast<size_t>(j) * n] = Lp[own_off(t, n, CS, r) + (i - j)];
+            if (mode != kBigHetrdOnly) LVb[i + static_cast<size_t>(j) * n] = Lp[own_off(t, n, CS, r) + (i - j)];
             if (i > j) LVb[(i - j - 1) + static_cast<size_t>(n - 1 - j) * n] = Cc[static_cast<size_t>(t) * n + i];
         });
     }
@@ -598,9 +605,10 @@ template <int RM>
 __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __restrict__ A,
                                                             const double2* __restrict__ B, int n, int batch,
                                                             Workspace ws, double2* __restrict__ X,
-                                                            int* __restrict__ info, int hegst_only) {
+                                                            int* __restrict__ info, int mode) {
     const int b = blockIdx.x;
     if (b >= batch || !pair_selected(ws, b)) return;
+    if (mode == kBigHetrdOnly && info[b] != 0) return;          // the Cholesky failed (uniform)
     extern __shared__ __align__(16) unsigned char smem[];
     const MidSmem lay(n);
     double2* P = reinterpret_cast<double2*>(smem + lay.P);
@@ -622,97 +630,99 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
     double* eb = ws.e + static_cast<size_t>(n) * b;
     double2* taub = ws.tau + static_cast<size_t>(n) * b;
 
-    if (tid == 0) { *s_fail = 0; mbar_init(bar, 1); fence_mbar_init(); }
-    __syncthreads();
-    if (warp == 0) {
-        if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(16 * (static_cast<size_t>(n) * (n + 1) / 2)));
-        __syncwarp();
-        for (int j = lane; j < n; j += 32)
-            bulk_g2s(P + pk(j, n), Bb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
-    }
     int status = 0;
-    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
-        status = kInfoCopyTimeout;
-        mbar_wait_bounded(bar, 0, kMaxPolls);
-    }
-
-    // ---- potrf
-    for (int k = 0; k < n; ++k) {
-        double2* col = P + pk(k, n);                              // col[i - k] = A(i, k)
-        const double dkk = col[0].x;
-        __syncthreads();                                          // every thread has read dkk
-        if (!(dkk > 0.0)) { if (tid == 0) *s_fail = k + 1; break; }     // uniform
-        const double dsq = sqrt(dkk), inv = 1.0 / dsq;
-        const int m = n - k - 1;
-        for (int i = 1 + tid; i <= m; i += kMidThreads) col[i] = cscale(col[i], inv);
-        if (tid == 0) { col[0] = make_double2(dsq, 0.0); invd[k] = inv; }
+    if (mode != kBigHetrdOnly) {                                  // Cholesky and reduction here
+        if (tid == 0) { *s_fail = 0; mbar_init(bar, 1); fence_mbar_init(); }
         __syncthreads();
-        if (m == 0) break;
-        const double2* l = col + 1;                               // l[r] = L(k+1+r, k)
-        mid_pair_walk(P + pk(k + 1, n), m, [&](double2* a, int row, int j) { *a = cfmsc(l[row], l[j], *a); });
-        __syncthreads();
-    }
-    __syncthreads();
-    const int fail = *s_fail;
-    if (fail) {
-        if (tid == 0) info[b] = (n + fail) | status;
-        return;
-    }
+        if (warp == 0) {
+            if (lane == 0) mbar_arrive_expect_tx(bar, static_cast<uint32_t>(16 * (static_cast<size_t>(n) * (n + 1) / 2)));
+            __syncwarp();
+            for (int j = lane; j < n; j += 32)
+                bulk_g2s(P + pk(j, n), Bb + j + static_cast<size_t>(j) * n, 16u * (n - j), bar);
+        }
+        if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
+            status = kInfoCopyTimeout;
+            mbar_wait_bounded(bar, 0, kMaxPolls);
+        }
 
-    // ---- hegst: 8 lanes per column, 32 columns per pass
-    {
-        const int g = tid % kMidLanes;
-        const int cpp = kMidThreads / kMidLanes;
-        for (int c0 = 0; c0 < n; c0 += cpp) {                     // W = L^{-1} A -> LV slot
-            const int j = c0 + tid / kMidLanes;
-            const bool own = j < n;
-            double2 y[RM];
-#pragma unroll
-            for (int r = 0; r < RM; ++r) {
-                const int i = g + kMidLanes * r;
-                y[r] = (own && i < n) ? Ab[i + static_cast<size_t>(j) * n] : make_double2(0.0, 0.0);
-            }
-            grp_trsm_lower_packed<kMidLanes, RM, double>(P, invd, y, n, g);
-#pragma unroll
-            for (int r = 0; r < RM; ++r) {
-                const int i = g + kMidLanes * r;
-                if (own && i < n) LVb[i + static_cast<size_t>(j) * n] = y[r];
-            }
+        // ---- potrf
+        for (int k = 0; k < n; ++k) {
+            double2* col = P + pk(k, n);                              // col[i - k] = A(i, k)
+            const double dkk = col[0].x;
+            __syncthreads();                                          // every thread has read dkk
+            if (!(dkk > 0.0)) { if (tid == 0) *s_fail = k + 1; break; }     // uniform
+            const double dsq = sqrt(dkk), inv = 1.0 / dsq;
+            const int m = n - k - 1;
+            for (int i = 1 + tid; i <= m; i += kMidThreads) col[i] = cscale(col[i], inv);
+            if (tid == 0) { col[0] = make_double2(dsq, 0.0); invd[k] = inv; }
+            __syncthreads();
+            if (m == 0) break;
+            const double2* l = col + 1;                               // l[r] = L(k+1+r, k)
+            mid_pair_walk(P + pk(k + 1, n), m, [&](double2* a, int row, int j) { *a = cfmsc(l[row], l[j], *a); });
+            __syncthreads();
         }
         __syncthreads();
-        for (int c0 = 0; c0 < n; c0 += cpp) {                     // C = L^{-1} W^H -> X slot (lower)
-            const int j = c0 + tid / kMidLanes;
-            const bool own = j < n;
-            double2 y[RM];
-#pragma unroll
-            for (int r = 0; r < RM; ++r) {
-                const int i = g + kMidLanes * r;
-                y[r] = (own && i < n) ? cconj(LVb[j + static_cast<size_t>(i) * n]) : make_double2(0.0, 0.0);
+        const int fail = *s_fail;
+        if (fail) {
+            if (tid == 0) info[b] = (n + fail) | status;
+            return;
+        }
+
+        // ---- hegst: 8 lanes per column, 32 columns per pass
+        {
+            const int g = tid % kMidLanes;
+            const int cpp = kMidThreads / kMidLanes;
+            for (int c0 = 0; c0 < n; c0 += cpp) {                     // W = L^{-1} A -> LV slot
+                const int j = c0 + tid / kMidLanes;
+                const bool own = j < n;
+                double2 y[RM];
+    #pragma unroll
+                for (int r = 0; r < RM; ++r) {
+                    const int i = g + kMidLanes * r;
+                    y[r] = (own && i < n) ? Ab[i + static_cast<size_t>(j) * n] : make_double2(0.0, 0.0);
+                }
+                grp_trsm_lower_packed<kMidLanes, RM, double>(P, invd, y, n, g);
+    #pragma unroll
+                for (int r = 0; r < RM; ++r) {
+                    const int i = g + kMidLanes * r;
+                    if (own && i < n) LVb[i + static_cast<size_t>(j) * n] = y[r];
+                }
             }
-            grp_trsm_lower_packed<kMidLanes, RM, double>(P, invd, y, n, g);
-#pragma unroll
-            for (int r = 0; r < RM; ++r) {
-                const int i = g + kMidLanes * r;
-                double2 v = y[r];
-                if (i == j) v.y = 0.0;
-                if (own && i < n && i >= j) Xb[i + static_cast<size_t>(j) * n] = v;
+            __syncthreads();
+            for (int c0 = 0; c0 < n; c0 += cpp) {                     // C = L^{-1} W^H -> X slot (lower)
+                const int j = c0 + tid / kMidLanes;
+                const bool own = j < n;
+                double2 y[RM];
+    #pragma unroll
+                for (int r = 0; r < RM; ++r) {
+                    const int i = g + kMidLanes * r;
+                    y[r] = (own && i < n) ? cconj(LVb[j + static_cast<size_t>(i) * n]) : make_double2(0.0, 0.0);
+                }
+                grp_trsm_lower_packed<kMidLanes, RM, double>(P, invd, y, n, g);
+    #pragma unroll
+                for (int r = 0; r < RM; ++r) {
+                    const int i = g + kMidLanes * r;
+                    double2 v = y[r];
+                    if (i == j) v.y = 0.0;
+                    if (own && i < n && i >= j) Xb[i + static_cast<size_t>(j) * n] = v;
+                }
             }
+            __syncthreads();
+        }
+        // L -> LV lower (W is no longer needed), then C's lower triangle -> the tile
+        for (size_t idx = tid; idx < mat; idx += kMidThreads) {
+            const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
+            if (i >= j) LVb[idx] = P[pk(j, n) + i - j];
         }
         __syncthreads();
     }
-    // L -> LV lower (W is no longer needed), then C's lower triangle -> the tile
-    for (size_t idx = tid; idx < mat; idx += kMidThreads) {
-        const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
-        if (i >= j) LVb[idx] = P[pk(j, n) + i - j];
-    }
-    __syncthreads();
     for (size_t idx = tid; idx < mat; idx += kMidThreads) {
         const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
         if (i >= j) P[pk(j, n) + i - j] = Xb[idx];
     }
     __syncthreads();
 
-    if (hegst_only) {                                              // mixed form: C stays in X
+    if (mode == kBigHegstOnly) {                                   // mixed form: C stays in X
         if (tid == 0) info[b] = status;
         return;
     }
@@ -1048,12 +1058,12 @@ cudaError_t launch_clustered(void (*kernel)(KArgs...), int cs, int grid, int thr
 
 template <int CS, int RM>
 void run_reduce_big(cudaError_t* err, const double2* A, const double2* B, int n, int batch, const Workspace& ws,
-                    double2* X, int* info, cudaStream_t stream, int hegst_only) {
+                    double2* X, int* info, cudaStream_t stream, int mode) {
     const size_t smem = BigReduceSmem(n, CS).total;
     static SmemOptIn f;
     set_big_smem_once(k_reduce_big<CS, RM>, f, static_cast<size_t>(max_smem_optin()));
     *err = launch_clustered(k_reduce_big<CS, RM>, CS, batch * CS, kBigThreads, smem, stream, A, B, n, batch, ws, X,
-                            info, hegst_only);
+                            info, mode);
 }
 
 template <int CS, int G, int RM, int NCW>
@@ -1073,11 +1083,10 @@ constexpr int kMidMaxN = 160;             // the packed tile + buffers fit 227 K
 
 template <int RM>
 void run_reduce_mid(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X, int* info,
-                    cudaStream_t stream, bool hegst_only) {
+                    cudaStream_t stream, int mode) {
     static SmemOptIn f;
     set_big_smem_once(k_reduce_mid<RM>, f, static_cast<size_t>(max_smem_optin()));
-    k_reduce_mid<RM><<<batch, kMidThreads, MidSmem(n).total, stream>>>(A, B, n, batch, ws, X, info,
-                                                                       hegst_only ? 1 : 0);
+    k_reduce_mid<RM><<<batch, kMidThreads, MidSmem(n).total, stream>>>(A, B, n, batch, ws, X, info, mode);
 }
 
 }  // namespace
@@ -1092,18 +1101,18 @@ size_t big_reduce_smem_bytes(int n) {
 }
 
 cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
-                              int* info, cudaStream_t stream, bool hegst_only) {
+                              int* info, cudaStream_t stream, int mode) {
     if (batch <= 0) return cudaSuccess;
     if (!A || !B || !X || !info || !ws.LV || !ws.d || !ws.e || !ws.tau) return cudaErrorInvalidValue;
-    if (!big_path(n)) return cudaErrorInvalidValue;
+    if (!big_path(n) || mode < kBigFull || mode > kBigHetrdOnly) return cudaErrorInvalidValue;
     if (n <= kMidMaxN) {                     // one CTA per pair: no cluster barriers
-        if (n <= 96) run_reduce_mid<12>(A, B, n, batch, ws, X, info, stream, hegst_only);
-        else if (n <= 128) run_reduce_mid<16>(A, B, n, batch, ws, X, info, stream, hegst_only);
-        else run_reduce_mid<20>(A, B, n, batch, ws, X, info, stream, hegst_only);
+        if (n <= 96) run_reduce_mid<12>(A, B, n, batch, ws, X, info, stream, mode);
+        else if (n <= 128) run_reduce_mid<16>(A, B, n, batch, ws, X, info, stream, mode);
+        else run_reduce_mid<20>(A, B, n, batch, ws, X, info, stream, mode);
         return cudaGetLastError();
     }
     cudaError_t err = cudaSuccess;
-    SBG_BIG_DISPATCH(n, run_reduce_big, &err, A, B, n, batch, ws, X, info, stream, hegst_only ? 1 : 0);
+    SBG_BIG_DISPATCH(n, run_reduce_big, &err, A, B, n, batch, ws, X, info, stream, mode);
     return err != cudaSuccess ? err : cudaGetLastError();
 }
 

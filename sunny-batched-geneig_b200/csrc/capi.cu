@@ -283,28 +283,30 @@ size_t sbg_workspace_bytes(int n, int precision, int pairs) {
 }
 
 int sbg_solver_matrix_size(const sbg_solver* s) { return s ? s->n : 0; }
-int sbg_solver_schedule(const sbg_solver* s, int* out7) {
+int sbg_solver_schedule(const sbg_solver* s, int* out8) {
     return guarded([&] {
-        if (!s || !out7) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
+        if (!s || !out8) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
         const sbg::Schedule& c = s->sched;
-        const int v[7] = {c.hetrd_threads, c.pair_warps, c.col_exact, c.back_lanes, c.ql_warps, c.chain_threads,
-                          c.back_qpass};
-        for (int i = 0; i < 7; ++i) out7[i] = v[i];
+        const int v[8] = {c.hetrd_threads, c.pair_warps, c.col_exact, c.back_lanes, c.ql_warps, c.chain_threads,
+                          c.back_qpass, c.reduce_tc};
+        for (int i = 0; i < 8; ++i) out8[i] = v[i];
     });
 }
 
-int sbg_solver_set_schedule(sbg_solver* s, const int* in7) {
+int sbg_solver_set_schedule(sbg_solver* s, const int* in8) {
     return guarded([&] {
-        if (!s || !in7) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
+        if (!s || !in8) throw Error(SBG_ERR_INVALID_VALUE, "null argument");
         sbg::Schedule c;
-        c.hetrd_threads = in7[0];
-        c.pair_warps = in7[1];
-        c.col_exact = in7[2];
-        c.back_lanes = in7[3];
-        c.ql_warps = in7[4];
-        c.chain_threads = in7[5];
-        c.back_qpass = in7[6];
+        c.hetrd_threads = in8[0];
+        c.pair_warps = in8[1];
+        c.col_exact = in8[2];
+        c.back_lanes = in8[3];
+        c.ql_warps = in8[4];
+        c.chain_threads = in8[5];
+        c.back_qpass = in8[6];
+        c.reduce_tc = in8[7];
         const bool ok = (c.hetrd_threads == 128 || c.hetrd_threads == 256) &&
+                        (c.reduce_tc == 0 || c.reduce_tc == 1) &&
                         (c.pair_warps == 1 || c.pair_warps == 2 || c.pair_warps == 4) &&
                         (c.col_exact == 0 || c.col_exact == 1) && (c.back_lanes == 1 || c.back_lanes == 2) &&
                         (c.back_qpass == 1 || c.back_qpass == 2) &&

@@ -1311,7 +1311,12 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
     if ((mode == kReduceFull || mode == kReduceFromLM) && !ws.LV) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) {
         if (mode != kReduceFull) return cudaErrorInvalidValue;
-        return launch_reduce_big(A, B, n, batch, ws, out, info, stream, hegst_only);
+        if (shape.reduce_tc) {                       // tensor-core Cholesky + reduction, then the Householder
+            cudaError_t err = launch_reduce_tc(A, B, n, batch, ws, out, info, stream);
+            if (err != cudaSuccess || hegst_only) return err;
+            return launch_reduce_big(A, B, n, batch, ws, out, info, stream, kBigHetrdOnly);
+        }
+        return launch_reduce_big(A, B, n, batch, ws, out, info, stream, hegst_only ? kBigHegstOnly : kBigFull);
     }
     // The two-kernel path hands L from k_potrf_warp to k_hegst_col through ws.LV, so it
     // needs a workspace (the staged Cholesky alone does not).

@@ -118,12 +118,16 @@ enum BackMode : int {
 //               instead of the one for the next larger NMAX
 //   back_lanes  lanes per column of k_back_col (n <= 56): 1 or 2
 //   back_qpass  reflectors per pass of k_back_col's Q application (n <= 56): 1 or 2
+//   reduce_tc   n > kSmallMaxN: Cholesky and reduction by the blocked tensor-core kernel
+//               (k_reduce_tc), then (FP64 form) the Householder alone by k_reduce_mid / k_reduce_big,
+//               instead of those kernels doing all three
 struct LaunchShape {
     int threads = 256;
     int pair_warps = 2;
     int col_exact = 1;
     int back_lanes = 1;
     int back_qpass = 1;
+    int reduce_tc = 0;
 };
 
 // Launchers (asynchronous on `stream`; return cudaSuccess or the launch error).
@@ -176,9 +180,12 @@ constexpr int kBigMaxN = 256;
 bool big_path(int n);
 size_t big_reduce_smem_bytes(int n);
 size_t ql_rows_smem_bytes(int n, bool single);
-// hegst_only: stop after C = L^{-1} A L^{-H} (C's lower triangle in X, L in LV).
+// mode: kBigFull (Cholesky, reduction, Householder), kBigHegstOnly (stop after C = L^{-1} A L^{-H}:
+// C's lower triangle in X, L in LV) or kBigHetrdOnly (the Householder alone, from C's lower triangle
+// in X with L already in LV, as k_reduce_tc leaves them; pairs with info != 0 are skipped).
+enum BigReduceMode : int { kBigFull = 0, kBigHegstOnly = 1, kBigHetrdOnly = 2 };
 cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
-                              int* info, cudaStream_t stream, bool hegst_only = false);
+                              int* info, cudaStream_t stream, int mode = kBigFull);
 // Mixed form for kMixedMaxN < n <= kMixedBigMaxN (csrc/mixed_big.cu), after
 // launch_reduce(kReduceMixed) left L in LV and C's lower triangle in X:
 //   launch_hetrd_c64_big   complex64 Householder, one CTA per pair: FP64-promoted reflectors (in the
@@ -189,6 +196,12 @@ cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int bat
 //                          cores; ws.rstat gets each pair's outcome.
 cudaError_t launch_hetrd_c64_big(int n, int batch, const double2* C, const Workspace& ws, int* info,
                                  cudaStream_t stream);
+// Blocked FP64 Cholesky and reduction on the FP64 tensor cores (csrc/reduce_tc.cu), one CTA per
+// pair: L into LV's lower triangle, C = L^{-1} A L^{-H} (lower triangle) into X, info as the other
+// reduce kernels (n + i for a leading minor i that is not positive definite).  Uses the pair's
+// rotation-log region as scratch.  Honours the pair selection.
+cudaError_t launch_reduce_tc(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
+                             int* info, cudaStream_t stream);
 cudaError_t launch_refine_big(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
                               int refine_steps, cudaStream_t stream);
 size_t hetrd_c64_big_smem_bytes(int n);
@@ -204,8 +217,9 @@ cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, in
                             int chain_threads, cudaStream_t stream, bool redo = false);
 
 // Kernels one full reduce launch (kReduceFull) issues for order n: the warp Cholesky and the
-// column hegst kernel for n <= 56, one kernel otherwise.
-inline int reduce_kernel_count(int n) { return n <= 56 ? 2 : 1; }
+// column hegst kernel for n <= 56; above kSmallMaxN with the tensor-core reduction (tc), k_reduce_tc
+// and the Householder kernel; one kernel otherwise.
+inline int reduce_kernel_count(int n, bool tc = false) { return n <= 56 || (n > kSmallMaxN && tc) ? 2 : 1; }
 // FP64 eigenvectors by inverse iteration (k_ql_values + k_tridiag_invit) for n <= kInvitMaxN, with
 // the warp QL inside the kernel for pairs it cannot take, and for kSmallMaxN < n <= kInvitBigMaxN,
 // where such pairs are flagged and the rotation-log QL (k_ql_chain + k_ql_apply_rows) redone for

@@ -15,171 +15,38 @@
 //                  kRefineSkip).
 #include "kernels.cuh"
 #include "stages.cuh"
+#include "tiles.cuh"
 
 namespace sbg {
 
 namespace {
 
-constexpr int kRfThreads = 128;          // 4 warps, 2 x 2 over a 32 x 32 output tile
-constexpr int kRfTile = 32;
-constexpr int kRfKP = 16;                // k values per staged panel
-constexpr int kRfLDA = kRfTile + 2;      // As: A(r, k) at k * kRfLDA + r (16-byte entries)
-constexpr int kRfLDB = kRfKP + 4;        // Bs: B(k, c) at c * kRfLDB + k
-constexpr int kRfWarps = kRfThreads / 32;
+constexpr int kRfThreads = kTileThreads;
+constexpr int kRfTile = kTile;
+constexpr int kRfWarps = kTileWarps;
 constexpr double kRfEps = 1.1102230246251565e-16;
 constexpr double kRfOrthTol = 1e-13;     // max |(Y^H Y - I)_ij| accepted
 
-// Strides keep the fragment loads free of bank conflicts: a quarter-warp phase of 16-byte loads
-// covers lanes (g, t), g in {0, 1}, t in 0..3, at entries t * kRfLDA + g (A: 2t + g mod 8 distinct)
-// and g * kRfLDB + t (B: 4g + t mod 8 distinct).
-static_assert(kRfLDA % 8 == 2 && kRfLDB % 8 == 4, "fragment strides");
-
 struct RfSmem {
-    double2 As[kRfKP * kRfLDA];
-    double2 Bs[2][kRfTile * kRfLDB];
+    TileSmem t;
     double lam[kMixedBigMaxN];
     double red[4 * kRfWarps];
     int order[kMixedBigMaxN];
 };
 
-// D(8x8) += A(8x4) B(4x8), FP64, one warp: lane (g, t) = (lane / 4, lane % 4) holds a = A(g, t),
-// b = B(t, g) and d0, d1 = D(g, 2t), D(g, 2t + 1).
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-        : "+d"(d0), "+d"(d1)
-        : "d"(a), "d"(b));
-}
-
-// A warp's 16 x 16 quarter of a 32 x 32 complex tile: 2 x 2 blocks of 8 x 8 in the MMA
-// accumulator layout.  Block (br, bc) holds rows 16 wr + 8 br + g, columns 16 wc + 8 bc + 2t + q.
-struct Quarter {
-    double re[2][2][2], im[2][2][2];
-    __device__ __forceinline__ void zero() {
-#pragma unroll
-        for (int br = 0; br < 2; ++br)
-#pragma unroll
-            for (int bc = 0; bc < 2; ++bc)
-#pragma unroll
-                for (int q = 0; q < 2; ++q) re[br][bc][q] = im[br][bc][q] = 0.0;
-    }
-};
-
-__device__ __forceinline__ double2 ldcg2(const double2* p) { return __ldcg(p); }
-
-// Position of this lane's accumulator entry (br, bc, q) within the tile at (r0, c0).
-__device__ __forceinline__ void quarter_pos(int r0, int c0, int br, int bc, int q, int& row, int& col) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
-    row = r0 + 16 * (w >> 1) + 8 * br + g;
-    col = c0 + 16 * (w & 1) + 8 * bc + 2 * t + q;
-}
-
-__device__ __forceinline__ void quarter_load(Quarter& acc, const double2* M, int n, int r0, int c0) {
-#pragma unroll
-    for (int br = 0; br < 2; ++br)
-#pragma unroll
-        for (int bc = 0; bc < 2; ++bc)
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                int row, col;
-                quarter_pos(r0, c0, br, bc, q, row, col);
-                const double2 v = (row < n && col < n) ? ldcg2(M + row + static_cast<size_t>(col) * n)
-                                                       : make_double2(0.0, 0.0);
-                acc.re[br][bc][q] = v.x;
-                acc.im[br][bc][q] = v.y;
-            }
-}
-
-__device__ __forceinline__ void quarter_store(const Quarter& acc, double2* M, int n, int r0, int c0) {
-#pragma unroll
-    for (int br = 0; br < 2; ++br)
-#pragma unroll
-        for (int bc = 0; bc < 2; ++bc)
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                int row, col;
-                quarter_pos(r0, c0, br, bc, q, row, col);
-                if (row < n && col < n)
-                    __stcg(M + row + static_cast<size_t>(col) * n, make_double2(acc.re[br][bc][q], acc.im[br][bc][q]));
-            }
-}
-
-// acc[o] += op(A)(r0 .. r0+31, :) B_o(:, c0 .. c0+31), o < NOUT, over k < n.  op(A)(r, k) is
-// A(r, k), or conj(A(k, r)) when CONJA.  Entries beyond n read as zero.  All threads of the CTA
-// take part (the panel staging is shared); the caller synchronises before reusing the outputs.
+// The tile at (r0, c0) of products of the pair's n x n matrices: acc[o] += op(A) B_o with op(A) = A
+// or A^H (CONJA), summed over all of k.
 template <bool CONJA, int NOUT>
-__device__ void tile_mm(Quarter (&acc)[NOUT], const double2* A, const double2* B0, const double2* B1, int n, int r0,
-                        int c0, RfSmem& sm) {
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = lane >> 2, t = lane & 3;
-    const int wr = w >> 1, wc = w & 1;
-    constexpr int kPer = kRfKP * kRfTile / kRfThreads;       // entries per thread per operand panel
-    double2 ra[kPer], rb[NOUT][kPer];
-    auto fetch = [&](int kb) {
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-            const int e = tid + kRfThreads * u;
-            if (CONJA) {                                     // A(k, r): a 16-row run of column r
-                const int r = e / kRfKP, k = e % kRfKP, ra_ = r0 + r, ka = kb + k;
-                const double2 v = (ra_ < n && ka < n) ? ldcg2(A + ka + static_cast<size_t>(ra_) * n)
-                                                      : make_double2(0.0, 0.0);
-                ra[u] = make_double2(v.x, -v.y);
-            } else {                                         // A(r, k): a 32-row run of column k
-                const int k = e / kRfTile, r = e % kRfTile, ra_ = r0 + r, ka = kb + k;
-                ra[u] = (ra_ < n && ka < n) ? ldcg2(A + ra_ + static_cast<size_t>(ka) * n) : make_double2(0.0, 0.0);
-            }
-            const int c = e / kRfKP, k = e % kRfKP, ca = c0 + c, ka = kb + k;
-#pragma unroll
-            for (int o = 0; o < NOUT; ++o) {
-                const double2* B = o == 0 ? B0 : B1;
-                rb[o][u] = (ca < n && ka < n) ? ldcg2(B + ka + static_cast<size_t>(ca) * n) : make_double2(0.0, 0.0);
-            }
-        }
-    };
-    auto stash = [&]() {
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-            const int e = tid + kRfThreads * u;
-            if (CONJA) {
-                const int r = e / kRfKP, k = e % kRfKP;
-                sm.As[k * kRfLDA + r] = ra[u];
-            } else {
-                const int k = e / kRfTile, r = e % kRfTile;
-                sm.As[k * kRfLDA + r] = ra[u];
-            }
-            const int c = e / kRfKP, k = e % kRfKP;
-#pragma unroll
-            for (int o = 0; o < NOUT; ++o) sm.Bs[o][c * kRfLDB + k] = rb[o][u];
-        }
-    };
-    fetch(0);
-    for (int kb = 0; kb < n; kb += kRfKP) {
-        __syncthreads();                                     // the previous panel is consumed
-        stash();
-        __syncthreads();
-        if (kb + kRfKP < n) fetch(kb + kRfKP);               // in flight while this panel is multiplied
-#pragma unroll
-        for (int k0 = 0; k0 < kRfKP; k0 += 4) {
-            double2 a[2], bf[NOUT][2];
-#pragma unroll
-            for (int br = 0; br < 2; ++br) a[br] = sm.As[(k0 + t) * kRfLDA + 16 * wr + 8 * br + g];
-#pragma unroll
-            for (int o = 0; o < NOUT; ++o)
-#pragma unroll
-                for (int bc = 0; bc < 2; ++bc) bf[o][bc] = sm.Bs[o][(16 * wc + 8 * bc + g) * kRfLDB + k0 + t];
-#pragma unroll
-            for (int o = 0; o < NOUT; ++o)
-#pragma unroll
-                for (int br = 0; br < 2; ++br)
-#pragma unroll
-                    for (int bc = 0; bc < 2; ++bc) {
-                        double* dr = acc[o].re[br][bc];
-                        double* di = acc[o].im[br][bc];
-                        dmma(dr[0], dr[1], a[br].x, bf[o][bc].x);
-                        dmma(dr[0], dr[1], -a[br].y, bf[o][bc].y);
-                        dmma(di[0], di[1], a[br].x, bf[o][bc].y);
-                        dmma(di[0], di[1], a[br].y, bf[o][bc].x);
-                    }
-        }
-    }
+__device__ __forceinline__ void rf_tile_mm(Quarter (&acc)[NOUT], const double2* A, const double2* B0,
+                                           const double2* B1, int n, int r0, int c0, RfSmem& sm) {
+    const MatView a = CONJA ? sub_view(A, n, n, n, 0, r0) : sub_view(A, n, n, n, r0, 0);
+    const MatView b0 = sub_view(B0, n, n, n, 0, c0);
+    const MatView b1 = NOUT == 2 ? sub_view(B1, n, n, n, 0, c0) : b0;
+    tile_mm<CONJA ? kOpC : kOpN, kOpN, NOUT>(acc, a, b0, b1, n, sm.t);
+}
+
+__device__ __forceinline__ void rf_store(const Quarter& acc, double2* M, int n, int r0, int c0) {
+    quarter_store(acc, M + r0 + static_cast<size_t>(c0) * n, n, n - r0, n - c0);
 }
 
 // Block-wide sums of v[0], v[1] and the max of v[2]; every thread gets them.
@@ -251,8 +118,8 @@ __global__ void __launch_bounds__(kRfThreads, 3) k_refine_big(int n, int batch, 
             const int r0 = kRfTile * (tile % nt), c0 = kRfTile * (tile / nt);
             Quarter acc[1];
             acc[0].zero();
-            tile_mm<false, 1>(acc, Cb, Y, nullptr, n, r0, c0, sm);
-            quarter_store(acc[0], Pb, n, r0, c0);
+            rf_tile_mm<false, 1>(acc, Cb, Y, nullptr, n, r0, c0, sm);
+            rf_store(acc[0], Pb, n, r0, c0);
         }
         __syncthreads();                                      // P complete (global, this CTA's writes)
         // ---- G = Y^H Y and S = Y^H P, lower tiles
@@ -261,9 +128,9 @@ __global__ void __launch_bounds__(kRfThreads, 3) k_refine_big(int n, int batch, 
                 Quarter acc[2];
                 acc[0].zero();
                 acc[1].zero();
-                tile_mm<true, 2>(acc, Y, Y, Pb, n, kRfTile * tr, kRfTile * tc, sm);
-                quarter_store(acc[0], Gb, n, kRfTile * tr, kRfTile * tc);
-                quarter_store(acc[1], Sb, n, kRfTile * tr, kRfTile * tc);
+                rf_tile_mm<true, 2>(acc, Y, Y, Pb, n, kRfTile * tr, kRfTile * tc, sm);
+                rf_store(acc[0], Gb, n, kRfTile * tr, kRfTile * tc);
+                rf_store(acc[1], Sb, n, kRfTile * tr, kRfTile * tc);
             }
         __syncthreads();
         // ---- Rayleigh quotients
@@ -342,9 +209,9 @@ __global__ void __launch_bounds__(kRfThreads, 3) k_refine_big(int n, int batch, 
         for (int tile = 0; tile < nt * nt; ++tile) {
             const int r0 = kRfTile * (tile % nt), c0 = kRfTile * (tile / nt);
             Quarter acc[1];
-            quarter_load(acc[0], Y, n, r0, c0);
-            tile_mm<false, 1>(acc, Y, Pb, nullptr, n, r0, c0, sm);
-            quarter_store(acc[0], Yn, n, r0, c0);
+            quarter_load<kOpN>(acc[0], sub_view(Y, n, n, n, r0, c0));
+            rf_tile_mm<false, 1>(acc, Y, Pb, nullptr, n, r0, c0, sm);
+            rf_store(acc[0], Yn, n, r0, c0);
         }
         __syncthreads();
         double2* tmp = Y;

@@ -263,7 +263,7 @@ struct sbg_solver {
         stage_begin(stream, &ev);
         check_cuda(sbg::launch_reduce(sbg::kReduceFull, A, B, n, cnt, ws, X, info, sched.shape(), stream),
                    "reduce kernel");
-        stage_end(stream, ev, 0, sbg::reduce_kernel_count(n));
+        stage_end(stream, ev, 0, sbg::reduce_kernel_count(n, sched.reduce_tc != 0));
         const bool mixed = precision == SBG_PRECISION_MIXED;
         stage_begin(stream, &ev);
         if (mixed)

@@ -27,6 +27,7 @@ struct Schedule {
     int col_exact = 1;          // exact-n column kernels (k_hegst_col, k_back_col) where they exist
     int back_lanes = 1;         // lanes per column of k_back_col (n <= 56)
     int back_qpass = 1;         // reflectors per pass of k_back_col's Q application (n <= 56): 1 or 2
+    int reduce_tc = 0;          // n > 84, mixed form: Cholesky + reduction by k_reduce_tc (0 or 1)
     int ql_warps = 4;           // pairs (warps) per CTA of the QL rotation-application kernel
     int chain_threads = 128;    // pairs (threads) per CTA of the QL scalar-chain kernels
     LaunchShape shape() const {
@@ -36,12 +37,13 @@ struct Schedule {
         l.col_exact = col_exact;
         l.back_lanes = back_lanes;
         l.back_qpass = back_qpass;
+        l.reduce_tc = reduce_tc;
         return l;
     }
     bool operator==(const Schedule& o) const {
         return hetrd_threads == o.hetrd_threads && pair_warps == o.pair_warps && col_exact == o.col_exact &&
                back_lanes == o.back_lanes && back_qpass == o.back_qpass && ql_warps == o.ql_warps &&
-               chain_threads == o.chain_threads;
+               chain_threads == o.chain_threads && reduce_tc == o.reduce_tc;
     }
 };
 

@@ -190,7 +190,7 @@ class Solver:
         _check(self._lib.sbg_solver_reserve(self._h, pairs, stream_slots), "sbg_solver_reserve")
 
     SCHEDULE_FIELDS = ("hetrd_threads", "pairs_per_cta", "col_exact", "back_lanes", "ql_warps", "chain_threads",
-                       "back_qpass")
+                       "back_qpass", "reduce_tc")
 
     @property
     def schedule(self) -> dict:

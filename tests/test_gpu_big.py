@@ -123,3 +123,20 @@ def test_big_limits():
     assert 192 <= mx < 256
     with pytest.raises(sbg.SolverError):
         sbg.Solver(mx + 1, precision="mixed")
+
+
+@pytest.mark.parametrize("n", [96, 160, 192])
+def test_big_scalar_reduction_schedule(n, oracle_mod):
+    """The one-CTA and cluster kernels doing Cholesky, reduction and Householder together (schedule
+    reduce_tc = 0; the default above n = 84 is the blocked tensor-core reduction followed by the
+    Householder alone) against zhegv, and equal to the default schedule's results to 1e-12."""
+    H, S = oracle_mod.gen_fixture_pairs(n, 4, 29, "random")
+    s = sbg.Solver(n)
+    assert s.schedule["reduce_tc"] == 1
+    W1, X1, info1 = run(s, H, S)
+    s.schedule = dict(reduce_tc=0)
+    W0, X0, info0 = run(s, H, S)
+    Wr, Xr, _ = oracle_mod.hegv(H, S, n, nthreads=8)
+    check(H, S, W0, X0, info0, Wr, Xr, n)
+    check(H, S, W1, X1, info1, Wr, Xr, n)
+    assert Mx.eig_rel_norm(W0, W1).max() <= 1e-12

@@ -134,3 +134,59 @@ def test_mixed_big_chunks_and_determinism(oracle_mod):
         assert np.array_equal(x, y, equal_nan=True) and np.array_equal(y, z, equal_nan=True)
     Wr, Xr, _ = oracle_mod.hegv(H, S, n, nthreads=8)
     check(H, S, a[0], a[1], a[2], Wr, Xr, n)
+
+
+def _tc_solver(n, **kw):
+    s = sbg.Solver(n, precision="mixed", **kw)
+    s.schedule = dict(reduce_tc=1)
+    assert s.schedule["reduce_tc"] == 1
+    return s
+
+
+@pytest.mark.parametrize("n", [85, 96, 100, 128, 160, 161, 192, 235])
+def test_mixed_big_tensor_core_reduction(n, oracle_mod):
+    """The blocked Cholesky and reduction on the FP64 tensor cores (schedule reduce_tc = 1): whole
+    and partial 32-blocks, one to eight block rows, against zhegv with the parity gates."""
+    if n > sbg.max_n("mixed"):
+        pytest.skip(f"the mixed form covers n <= {sbg.max_n('mixed')}")
+    H, S = oracle_mod.gen_fixture_pairs(n, 6 if n <= 160 else 3, 17, "random")
+    W, X, info = run(_tc_solver(n), H, S)
+    Wr, Xr, _ = oracle_mod.hegv(H, S, n, nthreads=8)
+    check(H, S, W, X, info, Wr, Xr, n)
+
+
+@pytest.mark.parametrize("N", [48, 96])
+def test_mixed_big_tensor_core_reduction_near_goldstone(N, oracle_mod):
+    """kappa(B) ~ 1e8 through the blocked reduction (its diagonal blocks inverted explicitly): the
+    same gates as the FP64 form's near-Goldstone tests."""
+    n = 2 * N
+    A, B = wl.bogoliubov(N, 6 if N <= 48 else 3, seed=23, frac=1e-3, goldstone=1e-8)
+    A, B = A.numpy(), B.numpy()
+    Wr, Xr, _ = oracle_mod.hegv(A, B, n, nthreads=8)
+    normB = np.linalg.norm(Mx.as_mats(B, n), ord=2, axis=(1, 2))
+    cond = normB[:, None] * np.linalg.norm(Mx.as_mats(Xr, n), axis=1) ** 2
+    scale = np.abs(Wr) * cond + np.abs(Wr).max(axis=1, keepdims=True)
+    res_ref = float(Mx.residual(A, B, Xr, Wr, n).max())
+    orth_ref = float(Mx.orth(B, Xr, n).max())
+    W, X, info = run(_tc_solver(n), A, B)
+    assert (info == 0).all()
+    assert (np.abs(W - Wr) / scale).max() < 1e-12
+    assert Mx.residual(A, B, X, W, n).max() < max(1e-12, 4 * res_ref)
+    assert Mx.orth(B, X, n).max() < max(1e-9, 4 * orth_ref)
+
+
+@pytest.mark.parametrize("n", [96, 192])
+def test_mixed_big_tensor_core_reduction_not_positive_definite(n, oracle_mod):
+    """zpotrf's info through the blocked Cholesky: n + i for the first leading minor i that is not
+    positive definite, in the first block and in a later one; NaN outputs for those pairs only."""
+    H, S = oracle_mod.gen_fixture_pairs(n, 3, 4, "random")
+    Sm = Mx.as_mats(S.copy(), n).copy()
+    Sm[0] -= 1e4 * np.eye(n)                       # the first minor
+    Sm[1, 70, 70] = -1.0                           # a minor in the third block
+    W, X, info = run(_tc_solver(n), H, Mx.from_mats(Sm))
+    W64, X64, info64 = run(n, H, Mx.from_mats(Sm), "fp64")
+    assert info[0] == n + 1 and info64[0] == n + 1
+    assert info[1] == info64[1] and n + 32 < info[1] <= n + 71
+    assert np.isnan(W[:2]).all() and np.isnan(X[:2]).all()
+    Wr, Xr, _ = oracle_mod.hegv(H[2:], S[2:], n, nthreads=8)
+    check(H[2:], S[2:], W[2:], X[2:], info[2:], Wr, Xr, n)
