@@ -1539,7 +1539,16 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
                         const LaunchShape& shape, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;
     if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
-    if (n > kSmallMaxN) return launch_back_big(mode, n, batch, ws, X, info, stream);
+    if (n > kSmallMaxN) {
+        if (shape.reduce_tc && mode != kBackQOnly) {    // Q Z on the cluster, L^{-H} on the tensor cores
+            if (mode == kBackFull) {
+                cudaError_t err = launch_back_big(kBackQOnly, n, batch, ws, X, info, stream);
+                if (err != cudaSuccess) return err;
+            }
+            return launch_back_tc(n, batch, ws, X, info, stream);
+        }
+        return launch_back_big(mode, n, batch, ws, X, info, stream);
+    }
     const size_t smem = back_smem_bytes(n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     if (n <= kColMaxN) {

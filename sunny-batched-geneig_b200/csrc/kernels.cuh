@@ -118,9 +118,10 @@ enum BackMode : int {
 //               instead of the one for the next larger NMAX
 //   back_lanes  lanes per column of k_back_col (n <= 56): 1 or 2
 //   back_qpass  reflectors per pass of k_back_col's Q application (n <= 56): 1 or 2
-//   reduce_tc   n > kSmallMaxN: Cholesky and reduction by the blocked tensor-core kernel
-//               (k_reduce_tc), then (FP64 form) the Householder alone by k_reduce_mid / k_reduce_big,
-//               instead of those kernels doing all three
+//   reduce_tc   n > kSmallMaxN: the triangular stages on the FP64 tensor cores -- Cholesky and
+//               reduction by the blocked kernel k_reduce_tc, then (FP64 form) the Householder alone
+//               by k_reduce_mid / k_reduce_big, instead of those kernels doing all three; and
+//               X = L^{-H} Y by k_back_tc after the Q-only cluster back-transform
 struct LaunchShape {
     int threads = 256;
     int pair_warps = 2;
@@ -202,6 +203,10 @@ cudaError_t launch_hetrd_c64_big(int n, int batch, const double2* C, const Works
 // rotation-log region as scratch.  Honours the pair selection.
 cudaError_t launch_reduce_tc(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
                              int* info, cudaStream_t stream);
+// X = L^{-H} Y in place (Y complex in X) by the blocked backward substitution on the FP64 tensor
+// cores (csrc/reduce_tc.cu), one CTA per pair; NaN for pairs whose B was not positive definite.
+// Uses the pair's rotation-log region as scratch.  Honours the pair selection.
+cudaError_t launch_back_tc(int n, int batch, const Workspace& ws, double2* X, const int* info, cudaStream_t stream);
 cudaError_t launch_refine_big(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
                               int refine_steps, cudaStream_t stream);
 size_t hetrd_c64_big_smem_bytes(int n);

@@ -198,6 +198,72 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_reduce_tc(const double2* A,
     if (tid == 0) info[b] = 0;
 }
 
+// X = L^{-H} Y in place over the X buffer (Y complex there), one CTA per pair, for n > kSmallMaxN:
+// the backward substitution by blocks of 32, from the last block row up,
+//   T(I, :) = Y(I, :) - L(>I, I)^H X(>I, :),   X(I, :) = L(I, I)^{-H} T(I, :),
+// every product a tile product on the FP64 tensor cores; the diagonal blocks of L (LV's lower
+// triangle) inverted in shared memory into the pair's rotation-log region (free again after the
+// eigensolve).  Pairs with info outside 0..n get NaN (B was not positive definite); pairs not
+// selected are left alone.
+__global__ void __launch_bounds__(kTileThreads, 3) k_back_tc(int n, int batch, Workspace ws, double2* X,
+                                                             const int* info) {
+    __shared__ TcSmem sm;
+    const int b = blockIdx.x;
+    if (b >= batch || !pair_selected(ws, b)) return;
+    const int tid = threadIdx.x;
+    const size_t mat = static_cast<size_t>(n) * n;
+    double2* Xb = X + mat * b;
+    if (info[b] > n || info[b] < 0) {                         // uniform
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        for (size_t idx = tid; idx < mat; idx += kTileThreads) Xb[idx] = make_double2(nan, nan);
+        return;
+    }
+    const double2* L = ws.LV + mat * b;
+    double2* Linv = static_cast<double2*>(ws.log) + static_cast<size_t>(ws.log_stride) * b;
+    const int nbk = (n + kNB - 1) / kNB;
+    const MatView none{nullptr, 1, 0, 0};
+    for (int K = 0; K < nbk; ++K) {                           // the diagonal blocks of L, inverted
+        const int c0 = kNB * K, bs = min(kNB, n - c0);
+        for (int e = tid; e < kNB * kNB; e += kTileThreads) {
+            const int i = e % kNB, j = e / kNB;
+            double2 v = make_double2(i == j ? 1.0 : 0.0, 0.0);
+            if (i < bs && j < bs && i >= j) v = ldcg2(L + (c0 + i) + static_cast<size_t>(c0 + j) * n);
+            sm.D[i + j * kDLD] = v;
+        }
+        __syncthreads();
+        invert_diag(sm);
+        double2* LiK = Linv + static_cast<size_t>(K) * kNB * kNB;
+        for (int e = tid; e < kNB * kNB; e += kTileThreads) {
+            const int i = e % kNB, j = e / kNB;
+            LiK[e] = i >= j ? sm.D[i + j * kDLD] : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+    }
+    for (int I = nbk - 1; I >= 0; --I) {
+        const int r0 = kNB * I, bs = min(kNB, n - r0), below = n - r0 - bs;
+        if (below > 0) {
+            for (int C = 0; C < nbk; ++C) {                   // T(I, :) = Y(I, :) - L(>I, I)^H X(>I, :)
+                const int cc = kNB * C;
+                Quarter acc[1];
+                quarter_load<kOpN>(acc[0], sub_view(Xb, n, n, n, r0, cc));
+                tile_mm<kOpC, kOpN, 1>(acc, sub_view(L, n, n, n, r0 + bs, r0), sub_view(Xb, n, n, n, r0 + bs, cc),
+                                       none, below, sm.t, true);
+                store_tile(acc[0], Xb, n, r0, cc, false);
+            }
+            __syncthreads();
+        }
+        const MatView inv{Linv + static_cast<size_t>(I) * kNB * kNB, kNB, kNB, kNB};
+        for (int C = 0; C < nbk; ++C) {                       // X(I, :) = L(I, I)^{-H} T(I, :), in place
+            const int cc = kNB * C;
+            Quarter acc[1];
+            acc[0].zero();
+            tile_mm<kOpC, kOpN, 1>(acc, inv, sub_view(Xb, n, n, n, r0, cc), none, bs, sm.t);
+            store_tile(acc[0], Xb, n, r0, cc, false);
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_reduce_tc(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
@@ -208,6 +274,15 @@ cudaError_t launch_reduce_tc(const double2* A, const double2* B, int n, int batc
     if (static_cast<size_t>(ws.log_stride) < static_cast<size_t>((n + kNB - 1) / kNB) * kNB * kNB)
         return cudaErrorInvalidValue;
     k_reduce_tc<<<batch, kTileThreads, 0, stream>>>(A, B, n, batch, ws, X, info);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_back_tc(int n, int batch, const Workspace& ws, double2* X, const int* info, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    if (n < 1 || n > kBigMaxN || !X || !info || !ws.LV || !ws.log) return cudaErrorInvalidValue;
+    if (static_cast<size_t>(ws.log_stride) < static_cast<size_t>((n + kNB - 1) / kNB) * kNB * kNB)
+        return cudaErrorInvalidValue;
+    k_back_tc<<<batch, kTileThreads, 0, stream>>>(n, batch, ws, X, info);
     return cudaGetLastError();
 }
 

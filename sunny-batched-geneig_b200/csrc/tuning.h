@@ -27,7 +27,7 @@ struct Schedule {
     int col_exact = 1;          // exact-n column kernels (k_hegst_col, k_back_col) where they exist
     int back_lanes = 1;         // lanes per column of k_back_col (n <= 56)
     int back_qpass = 1;         // reflectors per pass of k_back_col's Q application (n <= 56): 1 or 2
-    int reduce_tc = 0;          // n > 84, mixed form: Cholesky + reduction by k_reduce_tc (0 or 1)
+    int reduce_tc = 0;          // n > 84: the triangular stages on the tensor cores (k_reduce_tc, k_back_tc)
     int ql_warps = 4;           // pairs (warps) per CTA of the QL rotation-application kernel
     int chain_threads = 128;    // pairs (threads) per CTA of the QL scalar-chain kernels
     LaunchShape shape() const {
