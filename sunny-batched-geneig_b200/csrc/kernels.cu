@@ -1334,6 +1334,9 @@ cudaError_t launch_reduce(int mode, const double2* A, const double2* B, int n, i
         else run_hegst_col<56>(mode, A, ws, out, n, batch, info, stream);
         return cudaGetLastError();
     }
+    // 57 <= n <= 84 with the tensor-core triangular stages: the blocked Cholesky and reduction
+    // (the Householder is a separate kernel here anyway)
+    if (shape.reduce_tc && mode == kReduceFull) return launch_reduce_tc(A, B, n, batch, ws, out, info, stream);
     const size_t smem = reduce_smem_bytes(mode, n);
     if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
     SBG_DISPATCH_BY_N(n, run_reduce, mode, A, B, n, batch, ws, out, info, smem, stream);
@@ -1571,6 +1574,14 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
             else run_back_col_g<56, 1>(mode, n, batch, ws, X, info, smem, stream, qp);
         }
         return cudaGetLastError();
+    }
+    if (shape.reduce_tc && mode != kBackQOnly) {        // Q Z by the CTA kernel, L^{-H} on the tensor cores
+        if (mode == kBackFull) {
+            SBG_DISPATCH_BY_N(n, run_back, kBackQOnly, n, batch, ws, X, info, smem, stream);
+            const cudaError_t err = cudaGetLastError();
+            if (err != cudaSuccess) return err;
+        }
+        return launch_back_tc(n, batch, ws, X, info, stream);
     }
     SBG_DISPATCH_BY_N(n, run_back, mode, n, batch, ws, X, info, smem, stream);
     return cudaGetLastError();

@@ -118,10 +118,10 @@ enum BackMode : int {
 //               instead of the one for the next larger NMAX
 //   back_lanes  lanes per column of k_back_col (n <= 56): 1 or 2
 //   back_qpass  reflectors per pass of k_back_col's Q application (n <= 56): 1 or 2
-//   reduce_tc   n > kSmallMaxN: the triangular stages on the FP64 tensor cores -- Cholesky and
-//               reduction by the blocked kernel k_reduce_tc, then (FP64 form) the Householder alone
-//               by k_reduce_mid / k_reduce_big, instead of those kernels doing all three; and
-//               X = L^{-H} Y by k_back_tc after the Q-only cluster back-transform
+//   reduce_tc   n > 56: the triangular stages on the FP64 tensor cores -- Cholesky and reduction by
+//               the blocked kernel k_reduce_tc (above kSmallMaxN, FP64 form, then the Householder
+//               alone by k_reduce_mid / k_reduce_big instead of those kernels doing all three), and
+//               X = L^{-H} Y by k_back_tc after the Q-only back-transform
 struct LaunchShape {
     int threads = 256;
     int pair_warps = 2;
@@ -225,6 +225,7 @@ cudaError_t launch_ql_chain(int n, int batch, const Workspace& ws, double* W, in
 // column hegst kernel for n <= 56; above kSmallMaxN with the tensor-core reduction (tc), k_reduce_tc
 // and the Householder kernel; one kernel otherwise.
 inline int reduce_kernel_count(int n, bool tc = false) { return n <= 56 || (n > kSmallMaxN && tc) ? 2 : 1; }
+// (57 <= n <= 84 with tc: k_reduce_tc alone, the Householder being its own stage there.)
 // FP64 eigenvectors by inverse iteration (k_ql_values + k_tridiag_invit) for n <= kInvitMaxN, with
 // the warp QL inside the kernel for pairs it cannot take, and for kSmallMaxN < n <= kInvitBigMaxN,
 // where such pairs are flagged and the rotation-log QL (k_ql_chain + k_ql_apply_rows) redone for

@@ -283,7 +283,7 @@ struct sbg_solver {
         stage_begin(stream, &ev);
         check_cuda(sbg::launch_back(mixed ? sbg::kBackLOnly : sbg::kBackFull, n, cnt, ws, X, info, sched.shape(),
                                     stream), "back-transform kernel");
-        stage_end(stream, ev, 3, !mixed && n > sbg::kSmallMaxN && sched.reduce_tc ? 2 : 1);
+        stage_end(stream, ev, 3, !mixed && n > 56 && sched.reduce_tc ? 2 : 1);
     }
 
     // Host buffers in, host buffers out, chunks round-robin over nstreams internal streams.  A goes

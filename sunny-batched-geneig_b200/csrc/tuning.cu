@@ -388,9 +388,9 @@ Schedule default_schedule(int n, int precision) {
     s.back_qpass = n > 32 ? 2 : 1;
     s.ql_warps = n <= 32 ? 8 : (n <= 64 ? 4 : 2);
     s.chain_threads = 128;
-    // above kSmallMaxN the blocked tensor-core Cholesky and reduction: measured 2.5x (n = 96) to 12.7x
-    // (n = 192) faster than the scalar one-CTA and cluster kernels
-    s.reduce_tc = n > kSmallMaxN ? 1 : 0;
+    // above n = 56 the triangular stages on the tensor cores: the whole solve measured 1.14x (n = 58)
+    // to 1.59x (n = 192) faster than with the scalar CTA-per-pair and cluster kernels
+    s.reduce_tc = n > 56 ? 1 : 0;
     while (s.chain_threads > 32 && !fits(n, precision, s)) s.chain_threads /= 2;
     while (s.ql_warps > 1 && !fits(n, precision, s)) s.ql_warps /= 2;
     return s;

@@ -125,11 +125,12 @@ def test_big_limits():
         sbg.Solver(mx + 1, precision="mixed")
 
 
-@pytest.mark.parametrize("n", [96, 160, 192])
+@pytest.mark.parametrize("n", [72, 96, 160, 192])
 def test_big_scalar_reduction_schedule(n, oracle_mod):
-    """The one-CTA and cluster kernels doing Cholesky, reduction and Householder together (schedule
-    reduce_tc = 0; the default above n = 84 is the blocked tensor-core reduction followed by the
-    Householder alone) against zhegv, and equal to the default schedule's results to 1e-12."""
+    """The scalar triangular stages (schedule reduce_tc = 0: the CTA-per-pair kernels for n <= 84,
+    above that the one-CTA and cluster kernels doing Cholesky, reduction and Householder together;
+    the default above n = 56 is the blocked tensor-core Cholesky, reduction and L^{-H}) against
+    zhegv, and equal to the default schedule's results to 1e-12."""
     H, S = oracle_mod.gen_fixture_pairs(n, 4, 29, "random")
     s = sbg.Solver(n)
     assert s.schedule["reduce_tc"] == 1
