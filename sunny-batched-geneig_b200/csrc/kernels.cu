@@ -1179,7 +1179,7 @@ struct WorkspaceLayout {
     WorkspaceLayout(int n, int capacity, bool mixed) {
         const size_t nn = static_cast<size_t>(n) * n, cap = static_cast<size_t>(capacity);
         log_cap = ql_log_capacity(n);
-        log_stride = std::max(log_cap, refine_stash_entries(n));
+        log_stride = std::max(std::max(log_cap, refine_stash_entries(n)), tc_scratch_entries(n));
         refine = mixed_big(n, mixed);
         size_t o = 0;
         auto take = [&](size_t bytes) { const size_t q = o; o += align_up(bytes, 256); return q; };
@@ -1543,10 +1543,10 @@ cudaError_t launch_back(int mode, int n, int batch, const Workspace& ws, double2
     if (batch <= 0) return cudaSuccess;
     if (!X || !info || !ws.LV || !ws.tau) return cudaErrorInvalidValue;
     if (n > kSmallMaxN) {
-        if (shape.reduce_tc && mode != kBackQOnly) {    // Q Z on the cluster, L^{-H} on the tensor cores
-            if (mode == kBackFull) {
-                cudaError_t err = launch_back_big(kBackQOnly, n, batch, ws, X, info, stream);
-                if (err != cudaSuccess) return err;
+        if (shape.reduce_tc) {                          // Q Z and L^{-H} on the tensor cores
+            if (mode != kBackLOnly) {
+                const cudaError_t err = launch_back_q_tc(n, batch, ws, X, info, stream);
+                if (err != cudaSuccess || mode == kBackQOnly) return err;
             }
             return launch_back_tc(n, batch, ws, X, info, stream);
         }

@@ -80,6 +80,18 @@ __host__ __device__ constexpr int refine_np(int n) { return (n + 7) / 8 * 8; }
 __host__ __device__ constexpr int refine_ld(int n) { return refine_np(n) + 4; }
 __host__ __device__ constexpr int refine_stash_entries(int n) { return refine_np(n) * refine_ld(n); }
 constexpr int kMixedMaxN = 63;       // inverse iteration (no rotation log, so the stash is free)
+// Entries of the rotation-log region the tensor-core kernels of n > 56 use as scratch between the
+// eigensolves (csrc/reduce_tc.cu): the inverted 32 x 32 diagonal blocks of L, and above n = 84 the
+// Q application's copy of Z (n^2 doubles), block of reflectors (n x 32), T (32 x 32) and V^H Y
+// (32 x n).  Never more than the default rotation-log capacity (3 n^2 / 2 + 8 n + 16); the region
+// is kept at least this large when a smaller log capacity is asked for.
+__host__ __device__ constexpr int tc_scratch_entries(int n) {
+    return n <= 56 ? 0
+                   : (n <= 84 ? (n + 31) / 32 * 1024
+                              : ((n + 31) / 32 * 1024 > (n * n + 1) / 2 + (2 * n + 32) * 32
+                                     ? (n + 31) / 32 * 1024
+                                     : (n * n + 1) / 2 + (2 * n + 32) * 32));
+}
 // Mixed form above kMixedMaxN: the refinement runs on per-pair matrices in the workspace
 // (csrc/mixed_big.cu); the largest n is where the complex64 Householder's packed tile still fits one
 // CTA's shared memory (sbg_max_n reports it: 235 with B200's 227 KB per CTA).
@@ -121,7 +133,8 @@ enum BackMode : int {
 //   reduce_tc   n > 56: the triangular stages on the FP64 tensor cores -- Cholesky and reduction by
 //               the blocked kernel k_reduce_tc (above kSmallMaxN, FP64 form, then the Householder
 //               alone by k_reduce_mid / k_reduce_big instead of those kernels doing all three), and
-//               X = L^{-H} Y by k_back_tc after the Q-only back-transform
+//               X = L^{-H} Y by k_back_tc after the Q-only back-transform, which above kSmallMaxN is
+//               the compact-WY tensor-core kernel k_back_q_tc
 struct LaunchShape {
     int threads = 256;
     int pair_warps = 2;
@@ -207,6 +220,12 @@ cudaError_t launch_reduce_tc(const double2* A, const double2* B, int n, int batc
 // cores (csrc/reduce_tc.cu), one CTA per pair; NaN for pairs whose B was not positive definite.
 // Uses the pair's rotation-log region as scratch.  Honours the pair selection.
 cudaError_t launch_back_tc(int n, int batch, const Workspace& ws, double2* X, const int* info, cudaStream_t stream);
+// Y = Q Z in place (Z real in X, Y complex over it) for n > kSmallMaxN: the reflectors of the big-n
+// Householder applied in compact-WY blocks of 32 (zlarft's T) as tile products on the FP64 tensor
+// cores (csrc/reduce_tc.cu), one CTA per pair; NaN for pairs whose B was not positive definite.
+// Uses the pair's rotation-log region as scratch.  Honours the pair selection.
+cudaError_t launch_back_q_tc(int n, int batch, const Workspace& ws, double2* X, const int* info,
+                             cudaStream_t stream);
 cudaError_t launch_refine_big(int n, int batch, const Workspace& ws, double* W, double2* X, int* info,
                               int refine_steps, cudaStream_t stream);
 size_t hetrd_c64_big_smem_bytes(int n);

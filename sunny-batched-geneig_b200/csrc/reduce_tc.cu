@@ -264,6 +264,117 @@ __global__ void __launch_bounds__(kTileThreads, 3) k_back_tc(int n, int batch, W
     }
 }
 
+// Y = Q Z for n > kSmallMaxN (Z real in the X buffer, Y complex over it), Q = H_0 H_1 ... H_{n-2}
+// from the reflectors the big-n Householder stores (v_k(k+1+s) = LV(s, n-1-k), v_k(k+1) = 1) and
+// tau: blocks of 32 reflectors in compact WY form, Q_blk = I - V T V^H with T upper triangular
+// (LAPACK zlarft, forward, columnwise: T(i, i) = tau_i, T(0:i, i) = -tau_i T(0:i, 0:i) V^H v_i),
+// applied from the last block to the first, Y(rows below the block) -= V (T (V^H Y)), every product
+// a tile product on the FP64 tensor cores.  One CTA per pair; the pair's rotation-log region (free
+// after the eigensolve) holds a copy of Z, the block's V (n x 32), T (32 x 32) and V^H Y (32 x n).
+// Pairs with info outside 0..n get NaN; pairs not selected are left alone.
+__global__ void __launch_bounds__(kTileThreads, 3) k_back_q_tc(int n, int batch, Workspace ws, double2* X,
+                                                               const int* info) {
+    __shared__ TcSmem sm;
+    __shared__ double2 s_tau[kNB];
+    const int b = blockIdx.x;
+    if (b >= batch || !pair_selected(ws, b)) return;
+    const int tid = threadIdx.x;
+    const size_t mat = static_cast<size_t>(n) * n;
+    double2* Xb = X + mat * b;
+    if (info[b] > n || info[b] < 0) {                         // uniform
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        for (size_t idx = tid; idx < mat; idx += kTileThreads) Xb[idx] = make_double2(nan, nan);
+        return;
+    }
+    const double2* LV = ws.LV + mat * b;
+    const double2* taub = ws.tau + static_cast<size_t>(n) * b;
+    double2* scr = static_cast<double2*>(ws.log) + static_cast<size_t>(ws.log_stride) * b;
+    double* Zc = reinterpret_cast<double*>(scr);                              // n^2 doubles
+    double2* Vb = scr + (mat + 1) / 2;                                        // n x 32, ld n
+    double2* Tb = Vb + static_cast<size_t>(n) * kNB;                          // 32 x 32
+    double2* Wb = Tb + kNB * kNB;                                             // 32 x n, ld 32
+    const MatView none{nullptr, 1, 0, 0};
+    // ---- Y = Z as complex (through a copy of Z: the complex Y overwrites the real Z it is made of)
+    const double* Zg = reinterpret_cast<const double*>(Xb);
+    for (size_t idx = tid; idx < mat; idx += kTileThreads) Zc[idx] = Zg[idx];
+    __syncthreads();
+    for (size_t idx = tid; idx < mat; idx += kTileThreads) Xb[idx] = make_double2(Zc[idx], 0.0);
+    __syncthreads();
+    const int nref = n - 1;                                   // reflectors 0 .. n-2
+    const int nblk = (nref + kNB - 1) / kNB;
+    for (int blk = nblk - 1; blk >= 0; --blk) {
+        const int j0 = kNB * blk, kb = min(kNB, nref - j0), r0 = j0 + 1, m = n - r0;
+        // V: rows r0 .. n-1 of reflectors j0 .. j0 + kb - 1 (zero above each one's leading 1)
+        for (int e = tid; e < m * kNB; e += kTileThreads) {
+            const int r = e % m, jj = e / m, k = j0 + jj, i = r0 + r;
+            double2 v = make_double2(0.0, 0.0);
+            if (jj < kb) {
+                if (i == k + 1) v = make_double2(1.0, 0.0);
+                else if (i > k + 1) v = ldcg2(LV + (i - k - 1) + static_cast<size_t>(n - 1 - k) * n);
+            }
+            Vb[r + static_cast<size_t>(jj) * n] = v;
+        }
+        if (tid < kNB) s_tau[tid] = tid < kb ? ldcg2(taub + j0 + tid) : make_double2(0.0, 0.0);
+        __syncthreads();
+        const MatView vview{Vb, n, m, kNB};
+        {                                                     // G = V^H V into D
+            Quarter acc[1];
+            acc[0].zero();
+            tile_mm<kOpC, kOpN, 1>(acc, vview, vview, none, m, sm.t);
+            quarter_store(acc[0], Tb, kNB, kNB, kNB);
+        }
+        __syncthreads();
+        for (int e = tid; e < kNB * kNB; e += kTileThreads) sm.D[(e % kNB) + (e / kNB) * kDLD] = ldcg2(Tb + e);
+        __syncthreads();
+        // T over G's strict upper part (G(l, j) is read only for l < j, T(i, l) only for i <= l < j)
+        for (int j = 0; j < kNB; ++j) {
+            double2 t = make_double2(0.0, 0.0);
+            if (tid < j) {
+                for (int l = tid; l < j; ++l) {
+                    const double2 til = l == tid ? s_tau[tid] : sm.D[l + tid * kDLD];    // T(tid, l), stored transposed
+                    t = cfma(til, sm.D[l + j * kDLD], t);
+                }
+                t = cmul(t, make_double2(-s_tau[j].x, -s_tau[j].y));
+            }
+            __syncthreads();                                  // column j of G is read
+            if (tid < j) sm.D[j + tid * kDLD] = t;            // T(tid, j) kept at D(j, tid), below the diagonal
+            __syncthreads();
+        }
+        for (int e = tid; e < kNB * kNB; e += kTileThreads) {
+            const int i = e % kNB, j = e / kNB;
+            double2 v = make_double2(0.0, 0.0);
+            if (i == j) v = s_tau[i];
+            else if (i < j) v = sm.D[j + i * kDLD];
+            Tb[e] = v;                                        // T(i, j), upper triangular
+        }
+        __syncthreads();
+        const MatView tview{Tb, kNB, kNB, kNB};
+        for (int cc = 0; cc < n; cc += kTile) {               // W = V^H Y(r0:, :)
+            Quarter acc[1];
+            acc[0].zero();
+            tile_mm<kOpC, kOpN, 1>(acc, vview, sub_view(Xb, n, n, n, r0, cc), none, m, sm.t);
+            quarter_store(acc[0], Wb + static_cast<size_t>(cc) * kNB, kNB, kNB, n - cc);
+        }
+        __syncthreads();
+        for (int cc = 0; cc < n; cc += kTile) {               // W = T W, in place
+            Quarter acc[1];
+            acc[0].zero();
+            tile_mm<kOpN, kOpN, 1>(acc, tview, sub_view(Wb, kNB, kNB, n, 0, cc), none, kb, sm.t);
+            quarter_store(acc[0], Wb + static_cast<size_t>(cc) * kNB, kNB, kNB, n - cc);
+        }
+        __syncthreads();
+        for (int rr = 0; rr < m; rr += kTile)                 // Y(r0:, :) -= V W
+            for (int cc = 0; cc < n; cc += kTile) {
+                Quarter acc[1];
+                quarter_load<kOpN>(acc[0], sub_view(Xb, n, n, n, r0 + rr, cc));
+                tile_mm<kOpN, kOpN, 1>(acc, sub_view(Vb, n, m, kNB, rr, 0), sub_view(Wb, kNB, kNB, n, 0, cc), none,
+                                       kb, sm.t, true);
+                store_tile(acc[0], Xb, n, r0 + rr, cc, false);
+            }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_reduce_tc(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
@@ -283,6 +394,17 @@ cudaError_t launch_back_tc(int n, int batch, const Workspace& ws, double2* X, co
     if (static_cast<size_t>(ws.log_stride) < static_cast<size_t>((n + kNB - 1) / kNB) * kNB * kNB)
         return cudaErrorInvalidValue;
     k_back_tc<<<batch, kTileThreads, 0, stream>>>(n, batch, ws, X, info);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_back_q_tc(int n, int batch, const Workspace& ws, double2* X, const int* info,
+                             cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    if (n <= kSmallMaxN || n > kBigMaxN || !X || !info || !ws.LV || !ws.tau || !ws.log) return cudaErrorInvalidValue;
+    // Z's copy, V, T and V^H Y in the rotation-log region
+    const size_t need = (static_cast<size_t>(n) * n + 1) / 2 + static_cast<size_t>(2 * n + kNB) * kNB;
+    if (static_cast<size_t>(ws.log_stride) < need) return cudaErrorInvalidValue;
+    k_back_q_tc<<<batch, kTileThreads, 0, stream>>>(n, batch, ws, X, info);
     return cudaGetLastError();
 }
 
