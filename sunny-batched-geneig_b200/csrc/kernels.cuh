@@ -196,7 +196,8 @@ size_t big_reduce_smem_bytes(int n);
 size_t ql_rows_smem_bytes(int n, bool single);
 // mode: kBigFull (Cholesky, reduction, Householder), kBigHegstOnly (stop after C = L^{-1} A L^{-H}:
 // C's lower triangle in X, L in LV) or kBigHetrdOnly (the Householder alone, from C's lower triangle
-// in X with L already in LV, as k_reduce_tc leaves them; pairs with info != 0 are skipped).
+// in X with L already in LV, as k_reduce_tc leaves them; pairs with info != 0 are skipped; above
+// n = 160 by k_hetrd_l2 rather than the cluster).
 enum BigReduceMode : int { kBigFull = 0, kBigHegstOnly = 1, kBigHetrdOnly = 2 };
 cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
                               int* info, cudaStream_t stream, int mode = kBigFull);
@@ -210,6 +211,11 @@ cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int bat
 //                          cores; ws.rstat gets each pair's outcome.
 cudaError_t launch_hetrd_c64_big(int n, int batch, const double2* C, const Workspace& ws, int* info,
                                  cudaStream_t stream);
+// The FP64 Householder alone for n > kSmallMaxN after launch_reduce_tc (C's lower triangle in X),
+// one CTA per pair with the packed triangle in the pair's rotation-log region (L2-resident global
+// memory): reflectors to LV's columns, d, e, tau; pairs with info != 0 are skipped.
+cudaError_t launch_hetrd_l2(int n, int batch, const double2* C, const Workspace& ws, int* info,
+                           cudaStream_t stream);
 // Blocked FP64 Cholesky and reduction on the FP64 tensor cores (csrc/reduce_tc.cu), one CTA per
 // pair: L into LV's lower triangle, C = L^{-1} A L^{-H} (lower triangle) into X, info as the other
 // reduce kernels (n + i for a leading minor i that is not positive definite).  Uses the pair's
