@@ -826,7 +826,10 @@ __global__ void __launch_bounds__(kMidThreads) k_hetrd_c64_big(int n, int batch,
 // memory: mid_hetrd's steps unchanged, every walk an L2 access.  No shared-memory tile limits how
 // many pairs an SM holds or how large n may be (the FP64 tile no longer fits one SM above n = 160).
 // Reflector k goes to LV's column n-1-k (the big path's layout), d, e, tau as k_reduce_mid's.
-__global__ void __launch_bounds__(kMidThreads) k_hetrd_l2(int n, int batch, const double2* __restrict__ C,
+// The walks are bound by L2 round trips, so resident pairs count: 4 CTAs per SM (64 registers)
+// measured 6 % faster than the 3 that 75 registers allow at n = 192, and 1 or 2 (shared memory
+// reserved) 1.6x and 1.2x slower.
+__global__ void __launch_bounds__(kMidThreads, 4) k_hetrd_l2(int n, int batch, const double2* __restrict__ C,
                                                           Workspace ws, int* __restrict__ info) {
     __shared__ double2 vb[kBigMaxN], wb[kBigMaxN], pb[kBigMaxN], s_tk[2];
     __shared__ double red[2 * kBigWarps];
