@@ -162,7 +162,6 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
     const int r = CS == 1 ? 0 : static_cast<int>(cg::this_cluster().block_rank());
     const int b = blockIdx.x / CS;                     // grid = batch * CS: b < batch
     if (!pair_selected(ws, b)) return;                 // uniform over the pair's cluster
-    if (mode == kBigHetrdOnly && info[b] != 0) return; // the Cholesky failed (read before any write)
     extern __shared__ __align__(16) unsigned char smem[];
     const BigReduceSmem lay(n, CS);
     double2* Lp = reinterpret_cast<double2*>(smem + lay.Lp);
@@ -188,7 +187,7 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
     // ---- stage own columns: lower part of B (packed) and all of A
     if (tid == 0) { *s_fail = 0; mbar_init(bar, 1); fence_mbar_init(); }
     __syncthreads();
-    if (warp == 0 && mode != kBigHetrdOnly) {
+    if (warp == 0) {
         if (lane == 0) mbar_arrive_expect_tx(bar, 16u * static_cast<uint32_t>(own_off(nc, n, CS, r) + n * nc));
         __syncwarp();
         for (int t = lane; t < nc; t += 32) {
@@ -198,19 +197,15 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
         }
     }
     int status = 0;
-    if (mode != kBigHetrdOnly && !mbar_wait_bounded(bar, 0, kMaxPolls)) {
+    if (!mbar_wait_bounded(bar, 0, kMaxPolls)) {
         status = kInfoCopyTimeout;
         mbar_wait_bounded(bar, 0, kMaxPolls);
     }
-    if (mode == kBigHetrdOnly)                         // C's lower triangle from X (k_reduce_tc's output)
-        for_own_lower(n, CS, r, 0, nc, [&](int t, int j, int i) {
-            Cc[static_cast<size_t>(t) * n + i] = Xb[i + static_cast<size_t>(j) * n];
-        });
     cluster_barrier<CS>();                             // every CTA of the cluster is running
 
     // ---- potrf (right-looking, cyclic columns)
     int fail = 0;
-    for (int k = 0; k < n && mode != kBigHetrdOnly; ++k) {
+    for (int k = 0; k < n; ++k) {
         const int o = k % CS;
         if (r == o) {
             double2* col = Lp + own_off(k / CS, n, CS, r);             // col[i - k] = B(i, k)
@@ -241,7 +236,7 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
     }
 
     if (!fail) {
-        if (mode != kBigHetrdOnly) {                    // Cholesky done: W and C here
+        {                                               // Cholesky done: W and C here
             for (int k = tid; k < n; k += kBigThreads) {
                 const int o = k % CS;
                 invd[k] = 1.0 / peer(Lp, o)[own_off(k / CS, n, CS, o)].x;
@@ -398,7 +393,7 @@ __global__ void __launch_bounds__(kBigThreads) k_reduce_big(const double2* __res
         }
         // ---- L -> LV lower; reflector k -> LV(s, n-1-k), s = i - k - 1
         for_own_lower(n, CS, r, 0, nc, [&](int t, int j, int i) {
-            if (mode != kBigHetrdOnly) LVb[i + static_cast<size_t>(j) * n] = Lp[own_off(t, n, CS, r) + (i - j)];
+            LVb[i + static_cast<size_t>(j) * n] = Lp[own_off(t, n, CS, r) + (i - j)];
             if (i > j) LVb[(i - j - 1) + static_cast<size_t>(n - 1 - j) * n] = Cc[static_cast<size_t>(t) * n + i];
         });
     }
@@ -608,7 +603,6 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
                                                             int* __restrict__ info, int mode) {
     const int b = blockIdx.x;
     if (b >= batch || !pair_selected(ws, b)) return;
-    if (mode == kBigHetrdOnly && info[b] != 0) return;          // the Cholesky failed (uniform)
     extern __shared__ __align__(16) unsigned char smem[];
     const MidSmem lay(n);
     double2* P = reinterpret_cast<double2*>(smem + lay.P);
@@ -631,7 +625,7 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
     double2* taub = ws.tau + static_cast<size_t>(n) * b;
 
     int status = 0;
-    if (mode != kBigHetrdOnly) {                                  // Cholesky and reduction here
+    {                                                             // Cholesky and reduction
         if (tid == 0) { *s_fail = 0; mbar_init(bar, 1); fence_mbar_init(); }
         __syncthreads();
         if (warp == 0) {
@@ -716,16 +710,15 @@ __global__ void __launch_bounds__(kMidThreads) k_reduce_mid(const double2* __res
         }
         __syncthreads();
     }
+    if (mode == kBigHegstOnly) {                                   // mixed form: C stays in X
+        if (tid == 0) info[b] = status;
+        return;
+    }
     for (size_t idx = tid; idx < mat; idx += kMidThreads) {
         const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
         if (i >= j) P[pk(j, n) + i - j] = Xb[idx];
     }
     __syncthreads();
-
-    if (mode == kBigHegstOnly) {                                   // mixed form: C stays in X
-        if (tid == 0) info[b] = status;
-        return;
-    }
     mid_hetrd<double>(P, n, vb, wb, pb, red, s_tk, db, eb, taub);
     // reflector k (rows k+1 .. n-1 of column k) -> LV(s, n-1-k), s = i - k - 1
     for (size_t idx = tid; idx < mat; idx += kMidThreads) {
@@ -823,38 +816,208 @@ __global__ void __launch_bounds__(kMidThreads) k_hetrd_c64_big(int n, int batch,
 // ----------------------------------------------------------------------------- k_hetrd_l2
 // The FP64 Householder alone (after k_reduce_tc), one CTA per pair, with the packed lower triangle
 // in global memory -- the pair's rotation-log region, free until the eigensolve -- instead of shared
-// memory: mid_hetrd's steps unchanged, every walk an L2 access.  No shared-memory tile limits how
-// many pairs an SM holds or how large n may be (the FP64 tile no longer fits one SM above n = 160).
+// memory, so no shared-memory tile limits how large n may be (the FP64 tile no longer fits one SM
+// above n = 160).  zhetd2's steps, with ONE pass over the trailing triangle per step instead of a
+// matvec walk that reads it twice and an update walk that reads and writes it: step k-1's rank-2
+// update is applied lazily, to column k by warp 0 just before it forms reflector k from that
+// column, and to columns k+1.. by all warps in the same walk that forms the Hermitian matvec with
+// reflector k.  The walk goes down columns (pairs of a long and a short column per warp), a warp
+// reading 32 consecutive rows at a time; lane l owns the rows i = l (mod 32), so the matvec's
+// row sums stay in its registers and only the column sums need a warp reduction.
 // Reflector k goes to LV's column n-1-k (the big path's layout), d, e, tau as k_reduce_mid's.
-// The walks are bound by L2 round trips, so resident pairs count: 4 CTAs per SM (64 registers)
-// measured 6 % faster than the 3 that 75 registers allow at n = 192, and 1 or 2 (shared memory
-// reserved) 1.6x and 1.2x slower.
-__global__ void __launch_bounds__(kMidThreads, 4) k_hetrd_l2(int n, int batch, const double2* __restrict__ C,
-                                                          Workspace ws, int* __restrict__ info) {
-    __shared__ double2 vb[kBigMaxN], wb[kBigMaxN], pb[kBigMaxN], s_tk[2];
-    __shared__ double red[2 * kBigWarps];
+// 3 CTAs per SM (80 registers; 92 unbounded, 2 CTAs) measured fastest: 1.12x over 2 and 4.
+constexpr int kL2Slots = kBigMaxN / 32;         // 32-row chunks of a column
+
+struct L2HetrdSmem {
+    size_t v, w, p, col, rows, red, tk, total;
+    __host__ __device__ explicit L2HetrdSmem(int n) {
+        size_t o = 0;
+        v = o;    o += 16 * 2 * static_cast<size_t>(n);            // reflectors k and k-1, by absolute row
+        w = o;    o += 16 * static_cast<size_t>(n);                // w of the pending update
+        p = o;    o += 16 * static_cast<size_t>(n);
+        col = o;  o += 16 * static_cast<size_t>(n);                // column sums of the matvec
+        rows = o; o += 16 * static_cast<size_t>(kBigWarps) * n;    // row sums, per warp
+        red = o;  o += 16 * kBigWarps;
+        tk = o;   o += 32;
+        total = o;
+    }
+};
+
+__global__ void __launch_bounds__(kMidThreads, 3) k_hetrd_l2(int n, int batch, const double2* __restrict__ C,
+                                                             Workspace ws, int* __restrict__ info) {
     const int b = blockIdx.x;
     if (b >= batch || !pair_selected(ws, b)) return;
     if (info[b] != 0) return;                                     // the Cholesky failed (uniform)
-    const int tid = threadIdx.x;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const L2HetrdSmem L(n);
+    double2* vbuf = reinterpret_cast<double2*>(smem + L.v);
+    double2* wb = reinterpret_cast<double2*>(smem + L.w);
+    double2* pb = reinterpret_cast<double2*>(smem + L.p);
+    double2* colp = reinterpret_cast<double2*>(smem + L.col);
+    double2* prow = reinterpret_cast<double2*>(smem + L.rows);
+    double* red = reinterpret_cast<double*>(smem + L.red);
+    double2* s_tk = reinterpret_cast<double2*>(smem + L.tk);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const size_t mat = static_cast<size_t>(n) * n;
     const double2* Cb = C + mat * b;
     double2* P = static_cast<double2*>(ws.log) + static_cast<size_t>(ws.log_stride) * b;
-    for (size_t idx = tid; idx < mat; idx += kMidThreads) {
-        const int j = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(j) * n);
-        if (i < j) continue;
-        double2 v = Cb[idx];
-        if (i == j) v.y = 0.0;
-        P[pk(j, n) + i - j] = v;
+    double* dout = ws.d + static_cast<size_t>(n) * b;
+    double* eout = ws.e + static_cast<size_t>(n) * b;
+    double2* tout = ws.tau + static_cast<size_t>(n) * b;
+    for (int j = warp; j < n; j += kBigWarps)                     // C's lower triangle, packed by columns
+        for (int i = j + lane; i < n; i += 32) {
+            double2 v = Cb[i + static_cast<size_t>(j) * n];
+            if (i == j) v.y = 0.0;
+            P[pk(j, n) + i - j] = v;
+        }
+    __syncthreads();
+    const double2 zero = make_double2(0.0, 0.0);
+    bool upd = false;                                             // step k-1's update pending (uniform)
+    for (int k = 0; k + 1 < n; ++k) {
+        double2* vb = vbuf + (k & 1) * n;                         // reflector k, vb[i] for rows i > k
+        const double2* vp = vbuf + ((k + 1) & 1) * n;             // reflector k-1 (while upd)
+        const int m = n - k - 1;
+        double2* ck = P + pk(k, n) - k;                           // ck[i] = A(i, k), i >= k
+        if (warp == 0) {
+            if (upd) {
+                const double2 wk = wb[k], vk = vp[k];
+                for (int i = k + lane; i < n; i += 32) {
+                    double2 a = cfmsc(vp[i], wk, ck[i]);
+                    a = cfmsc(wb[i], vk, a);
+                    if (i == k) a.y = 0.0;
+                    ck[i] = a;
+                }
+                __syncwarp();
+            }
+            double2* x = ck + k + 1;                              // x[i] = A(k+1+i, k)
+            double s2 = 0.0;
+            for (int i = 1 + lane; i < m; i += 32) s2 += cabs2(x[i]);
+            s2 = warp_sum(s2);
+            const double2 alpha = x[0];
+            double2 tk, scale;
+            double beta;
+            if (s2 == 0.0 && alpha.y == 0.0) {
+                tk = zero; beta = alpha.x; scale = zero;
+            } else {
+                const double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + s2);
+                beta = alpha.x >= 0.0 ? -nrm : nrm;
+                tk = make_double2((beta - alpha.x) / beta, -alpha.y / beta);
+                const double ar = alpha.x - beta, ai = alpha.y, den = ar * ar + ai * ai;
+                scale = make_double2(ar / den, -ai / den);
+            }
+            if (tk.x != 0.0 || tk.y != 0.0) {
+                __syncwarp();                                     // every lane has read alpha
+                for (int i = lane; i < m; i += 32) {
+                    const double2 v = (i == 0) ? make_double2(1.0, 0.0) : cmul(x[i], scale);
+                    vb[k + 1 + i] = v;
+                    x[i] = v;
+                }
+            }
+            if (lane == 0) {
+                s_tk[k & 1] = tk;
+                dout[k] = ck[k].x;
+                eout[k] = beta;
+                tout[k] = tk;
+            }
+        }
+        __syncthreads();
+        const double2 tk = s_tk[k & 1];
+        const bool mv = tk.x != 0.0 || tk.y != 0.0;
+        if (!upd && !mv) continue;                                // nothing to apply or form (uniform)
+        double2 acc[kL2Slots];
+#pragma unroll
+        for (int s = 0; s < kL2Slots; ++s) acc[s] = zero;
+        const int npair = (m + 1) >> 1;                           // columns k+1+q and n-1-q
+        for (int q = warp; q < npair; q += kBigWarps) {
+            for (int h = 0; h < 2; ++h) {
+                const int j = h == 0 ? k + 1 + q : n - 1 - q;
+                if (h == 1 && j == k + 1 + q) break;              // the middle column, once
+                double2* cj = P + pk(j, n) - j;                   // cj[i] = A(i, j), i >= j
+                const double2 vj = vb[j];
+                double2 wj = zero, vpj = zero;
+                if (upd) { wj = wb[j]; vpj = vp[j]; }
+                double2 cs = zero;
+#pragma unroll
+                for (int s = 0; s < kL2Slots; ++s) {
+                    if (32 * s >= n) break;                       // uniform
+                    if (32 * s + 31 < j) continue;                // uniform: the chunk is above the diagonal
+                    const int i = 32 * s + lane;
+                    if (i >= j && i < n) {
+                        double2 a = cj[i];
+                        if (upd) {
+                            a = cfmsc(vp[i], wj, a);
+                            a = cfmsc(wb[i], vpj, a);
+                            if (i == j) a.y = 0.0;
+                            cj[i] = a;
+                        }
+                        if (mv) {
+                            if (i == j) {
+                                acc[s].x = fma(a.x, vj.x, acc[s].x);
+                                acc[s].y = fma(a.x, vj.y, acc[s].y);
+                            } else {
+                                acc[s] = cfma(a, vj, acc[s]);
+                                cs = cfmac(a, vb[i], cs);
+                            }
+                        }
+                    }
+                }
+                if (mv) {
+                    cs.x = warp_sum(cs.x);
+                    cs.y = warp_sum(cs.y);
+                    if (lane == 0) colp[j] = cs;
+                }
+            }
+        }
+        if (mv) {
+#pragma unroll
+            for (int s = 0; s < kL2Slots; ++s) {
+                const int i = 32 * s + lane;
+                if (i > k && i < n) prow[warp * n + i] = acc[s];
+            }
+        }
+        __syncthreads();
+        if (!mv) { upd = false; continue; }                       // H_k = I: nothing pending (uniform)
+        // p = tau A22 v, then w = p - tau/2 (p^H v) v
+        double2 dpart = zero;
+        for (int i = k + 1 + tid; i < n; i += kMidThreads) {
+            double2 sum = colp[i];
+#pragma unroll
+            for (int w8 = 0; w8 < kBigWarps; ++w8) sum = cadd(sum, prow[w8 * n + i]);
+            const double2 p = cmul(tk, sum);
+            pb[i] = p;
+            dpart = cfmac(p, vb[i], dpart);
+        }
+        dpart.x = warp_sum(dpart.x);
+        dpart.y = warp_sum(dpart.y);
+        if (lane == 0) { red[2 * warp] = dpart.x; red[2 * warp + 1] = dpart.y; }
+        __syncthreads();
+        double2 dot = zero;
+#pragma unroll
+        for (int w8 = 0; w8 < kBigWarps; ++w8) { dot.x += red[2 * w8]; dot.y += red[2 * w8 + 1]; }
+        const double2 a2 = cscale(cmul(tk, dot), -0.5);
+        for (int i = k + 1 + tid; i < n; i += kMidThreads) wb[i] = cfma(a2, vb[i], pb[i]);
+        __syncthreads();
+        upd = true;
+    }
+    if (tid == 0) {
+        double2* cl = P + pk(n - 1, n);
+        double2 a = cl[0];
+        if (upd) {                                                // step n-2's update of A(n-1, n-1)
+            const double2* vl = vbuf + ((n - 2) & 1) * n;
+            a = cfmsc(vl[n - 1], wb[n - 1], a);
+            a = cfmsc(wb[n - 1], vl[n - 1], a);
+            a.y = 0.0;
+            cl[0] = a;
+        }
+        dout[n - 1] = a.x;
+        eout[n - 1] = 0.0;
+        tout[n - 1] = zero;
     }
     __syncthreads();
-    mid_hetrd<double>(P, n, vb, wb, pb, red, s_tk, ws.d + static_cast<size_t>(n) * b,
-                      ws.e + static_cast<size_t>(n) * b, ws.tau + static_cast<size_t>(n) * b);
-    __syncthreads();
     double2* LVb = ws.LV + mat * b;
-    for (size_t idx = tid; idx < mat; idx += kMidThreads) {
-        const int k = static_cast<int>(idx / n), i = static_cast<int>(idx - static_cast<size_t>(k) * n);
-        if (i > k) LVb[(i - k - 1) + static_cast<size_t>(n - 1 - k) * n] = P[pk(k, n) + i - k];
+    for (int k = warp; k + 1 < n; k += kBigWarps) {               // reflector k below the diagonal of column k
+        const double2* ck = P + pk(k, n) - k;
+        for (int i = k + 1 + lane; i < n; i += 32) LVb[(i - k - 1) + static_cast<size_t>(n - 1 - k) * n] = ck[i];
     }
 }
 
@@ -1143,10 +1306,10 @@ cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int bat
     if (batch <= 0) return cudaSuccess;
     if (!A || !B || !X || !info || !ws.LV || !ws.d || !ws.e || !ws.tau) return cudaErrorInvalidValue;
     if (!big_path(n) || mode < kBigFull || mode > kBigHetrdOnly) return cudaErrorInvalidValue;
-    // the Householder alone above kMidMaxN: one CTA per pair on the L2-resident packed triangle, measured
-    // 2.2x (n = 192) and 1.5x (n = 256) faster than the 8-CTA cluster; up to kMidMaxN the shared-memory
-    // tile of k_reduce_mid is faster (1.2x to 1.5x)
-    if (mode == kBigHetrdOnly && n > kMidMaxN) return launch_hetrd_l2(n, batch, X, ws, info, stream);
+    // the Householder alone: one CTA per pair, one pass over the L2-resident packed triangle per step
+    // (k_hetrd_l2), measured faster than both the shared-memory tile of k_reduce_mid (1.04x at
+    // n = 96, 1.3x at n = 128 and 160, whole reduce stage) and the 8-CTA cluster (4.7x at n = 192)
+    if (mode == kBigHetrdOnly) return launch_hetrd_l2(n, batch, X, ws, info, stream);
     if (n <= kMidMaxN) {                     // one CTA per pair: no cluster barriers
         if (n <= 96) run_reduce_mid<12>(A, B, n, batch, ws, X, info, stream, mode);
         else if (n <= 128) run_reduce_mid<16>(A, B, n, batch, ws, X, info, stream, mode);
@@ -1179,7 +1342,11 @@ cudaError_t launch_hetrd_l2(int n, int batch, const double2* C, const Workspace&
     if (n <= kSmallMaxN || n > kBigMaxN || !C || !info || !ws.LV || !ws.d || !ws.e || !ws.tau || !ws.log)
         return cudaErrorInvalidValue;
     if (static_cast<size_t>(ws.log_stride) < static_cast<size_t>(n) * (n + 1) / 2) return cudaErrorInvalidValue;
-    k_hetrd_l2<<<batch, kMidThreads, 0, stream>>>(n, batch, C, ws, info);
+    const size_t smem = L2HetrdSmem(n).total;
+    if (smem > static_cast<size_t>(max_smem_optin())) return cudaErrorInvalidValue;
+    static SmemOptIn f;
+    set_big_smem_once(k_hetrd_l2, f, smem);
+    k_hetrd_l2<<<batch, kMidThreads, smem, stream>>>(n, batch, C, ws, info);
     return cudaGetLastError();
 }
 

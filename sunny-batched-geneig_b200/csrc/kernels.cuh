@@ -194,10 +194,10 @@ constexpr int kBigMaxN = 256;
 bool big_path(int n);
 size_t big_reduce_smem_bytes(int n);
 size_t ql_rows_smem_bytes(int n, bool single);
-// mode: kBigFull (Cholesky, reduction, Householder), kBigHegstOnly (stop after C = L^{-1} A L^{-H}:
-// C's lower triangle in X, L in LV) or kBigHetrdOnly (the Householder alone, from C's lower triangle
-// in X with L already in LV, as k_reduce_tc leaves them; pairs with info != 0 are skipped; above
-// n = 160 by k_hetrd_l2 rather than the cluster).
+// mode: kBigFull (Cholesky, reduction, Householder: k_reduce_mid / k_reduce_big), kBigHegstOnly (the
+// same kernels, stopping after C = L^{-1} A L^{-H}: C's lower triangle in X, L in LV) or kBigHetrdOnly
+// (the Householder alone by k_hetrd_l2, from C's lower triangle in X with L already in LV, as
+// k_reduce_tc leaves them; pairs with info != 0 are skipped).
 enum BigReduceMode : int { kBigFull = 0, kBigHegstOnly = 1, kBigHetrdOnly = 2 };
 cudaError_t launch_reduce_big(const double2* A, const double2* B, int n, int batch, const Workspace& ws, double2* X,
                               int* info, cudaStream_t stream, int mode = kBigFull);
