@@ -187,8 +187,9 @@ size_t sbg_workspace_bytes(int n, int precision, int pairs);
  * column kernels where they exist (n = 32, 54), [3] lanes per column of the column back-transform
  * (1 or 2), [4] pairs per CTA of the QL rotation stage, [5] pairs per CTA of the QL scalar
  * chain, [6] reflectors per pass of the column back-transform's Q application (1 or 2), [7] 1 = the
- * triangular stages above n = 84 (Cholesky, reduction, X = L^{-H} Y) by the blocked kernels on the
- * FP64 tensor cores, 0 = by the one-CTA / cluster kernels that also do the Householder (0 or 1).
+ * triangular stages above n = 56 (Cholesky, reduction, X = L^{-H} Y) by the blocked kernels on the
+ * FP64 tensor cores, and above n = 84 the Householder by its own one-pass kernel, 0 = by the
+ * one-CTA / cluster kernels that also do the Householder (0 or 1).
  * set_schedule replaces it (values checked against their ranges and the device's shared memory;
  * SBG_ERR_INVALID_VALUE otherwise), for callers that tune outside the library. */
 int sbg_solver_schedule(const sbg_solver* s, int* out8);

@@ -132,7 +132,7 @@ enum BackMode : int {
 //   back_qpass  reflectors per pass of k_back_col's Q application (n <= 56): 1 or 2
 //   reduce_tc   n > 56: the triangular stages on the FP64 tensor cores -- Cholesky and reduction by
 //               the blocked kernel k_reduce_tc (above kSmallMaxN, FP64 form, then the Householder
-//               alone by k_reduce_mid / k_reduce_big instead of those kernels doing all three), and
+//               alone by k_hetrd_l2 instead of k_reduce_mid / k_reduce_big doing all three), and
 //               X = L^{-H} Y by k_back_tc after the Q-only back-transform, which above kSmallMaxN is
 //               the compact-WY tensor-core kernel k_back_q_tc
 struct LaunchShape {
