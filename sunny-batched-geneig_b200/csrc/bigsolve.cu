@@ -825,7 +825,8 @@ __global__ void __launch_bounds__(kMidThreads) k_hetrd_c64_big(int n, int batch,
 // reading 32 consecutive rows at a time; lane l owns the rows i = l (mod 32), so the matvec's
 // row sums stay in its registers and only the column sums need a warp reduction.
 // Reflector k goes to LV's column n-1-k (the big path's layout), d, e, tau as k_reduce_mid's.
-// 3 CTAs per SM (80 registers; 92 unbounded, 2 CTAs) measured fastest: 1.12x over 2 and 4.
+// 3 CTAs per SM (80 registers; 92 unbounded, 2 CTAs) measured fastest: 1.12x over 2, 1.06x over 4
+// (64 registers, with spills), at n = 192.
 constexpr int kL2Slots = kBigMaxN / 32;         // 32-row chunks of a column
 
 struct L2HetrdSmem {
