@@ -44,7 +44,8 @@ REF_DRIVERS = ("test_full_batched_n54", "test_full_n54", "test_chol_n54", "test_
 
 def build(quiet: bool = True) -> None:
     """Compile libsbg_oracle.so and, when the reference tree is present, _ref/: the reference's
-    fixture generator and its own n = 54 test drivers linked against libsbg_geneig.so (which
+    fixture generator, its own n = 54 test drivers and its runtime-n solver tests (the latter
+    through include/sbg/compat/nvrtc/nvrtc_solver.hpp), linked against libsbg_geneig.so (which
     must be built first)."""
     targets = ["all"]
     ref = reference_dir()
@@ -52,7 +53,7 @@ def build(quiet: bool = True) -> None:
         targets.append("ref")
         lib_so = os.path.join(os.path.dirname(HERE), "sunny-batched-geneig_b200", "sbg", "libsbg_geneig.so")
         if os.path.exists(lib_so):
-            targets.append("drivers")
+            targets += ["drivers", "nvrtc-drivers"]
     subprocess.run(["make", "-C", HERE, f"SBG_REFERENCE_DIR={ref}", *targets], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
 
