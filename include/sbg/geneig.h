@@ -199,6 +199,8 @@ int sbg_solver_set_schedule(sbg_solver* s, const int* in8);
 int sbg_solver_matrix_size(const sbg_solver* s);
 int sbg_solver_batches_per_block(const sbg_solver* s);
 int sbg_solver_block_dim_x(const sbg_solver* s);
+/* The largest dynamic shared memory per CTA among the stage kernels this solver launches (the
+ * reference's was its one fused kernel's). */
 unsigned int sbg_solver_shared_mem_bytes(const sbg_solver* s);
 int sbg_solver_was_autotuned(const sbg_solver* s);
 int sbg_solver_autotune_sweep_ran(const sbg_solver* s);

@@ -1353,6 +1353,13 @@ cudaError_t launch_hetrd_l2(int n, int batch, const double2* C, const Workspace&
 
 size_t ql_rows_smem_bytes(int n, bool single) { return single ? ql_rows_bytes<float>(n) : ql_rows_bytes<double>(n); }
 
+size_t big_stage_smem_bytes(int n, bool tc, int chain_threads) {
+    size_t m = std::max(ql_rows_smem_bytes(n, false), ql_chain_smem_bytes(n, chain_threads, false));
+    if (eig_by_inverse_iteration(n, false)) m = std::max(m, invit_smem_bytes(n, false));
+    if (tc) return std::max(m, L2HetrdSmem(n).total);       // k_reduce_tc / k_back_*_tc: static only
+    return std::max(m, std::max(big_reduce_smem_bytes(n), BigBackSmem(n).total));
+}
+
 cudaError_t launch_ql_rows(int n, int batch, const Workspace& ws, double* W, double2* X, int* info, bool single,
                            int chain_threads, cudaStream_t stream) {
     if (batch <= 0) return cudaSuccess;

@@ -328,7 +328,11 @@ int sbg_solver_batches_per_block(const sbg_solver* s) {
 int sbg_solver_block_dim_x(const sbg_solver* s) { return s ? s->sched.hetrd_threads : 0; }
 unsigned int sbg_solver_shared_mem_bytes(const sbg_solver* s) {
     if (!s) return 0;
-    size_t m = std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, s->n), sbg::back_smem_bytes(s->n));
+    size_t m = s->n > sbg::kSmallMaxN
+                   ? sbg::big_stage_smem_bytes(s->n, s->sched.reduce_tc != 0, s->sched.chain_threads)
+                   : std::max(sbg::reduce_smem_bytes(sbg::kReduceFull, s->n), sbg::back_smem_bytes(s->n));
+    if (sbg::mixed_big(s->n, s->precision == SBG_PRECISION_MIXED))
+        m = std::max(m, std::max(sbg::hetrd_c64_big_smem_bytes(s->n), sbg::refine_big_smem_bytes()));
     return static_cast<unsigned>(m);
 }
 int sbg_solver_was_autotuned(const sbg_solver* s) { return s ? s->autotuned : 0; }

@@ -1264,6 +1264,7 @@ void set_smem_limit(const void* kernel, SmemOptIn& rec, int bytes) {
 
 size_t reduce_smem_bytes(int, int n) { return ReduceSmem(n).total; }
 size_t back_smem_bytes(int n) { return BackSmem(n).total; }
+size_t invit_smem_bytes(int n, bool with_tile) { return InvitSmem(n, with_tile).per_warp; }
 
 // The register-segment kernels: (threads T, lanes per column G, rows per lane RM) by
 // size: n <= 32 -> (256, 8, 4), n <= 64 -> (512, 8, 8), else (512, 4, 22) (n <= 88).

@@ -194,6 +194,9 @@ constexpr int kBigMaxN = 256;
 bool big_path(int n);
 size_t big_reduce_smem_bytes(int n);
 size_t ql_rows_smem_bytes(int n, bool single);
+// Largest dynamic shared memory per CTA among the FP64 kernels a solve of order n > kSmallMaxN
+// launches: tc = the schedule's reduce_tc, chain_threads its QL chain width.
+size_t big_stage_smem_bytes(int n, bool tc, int chain_threads);
 // mode: kBigFull (Cholesky, reduction, Householder: k_reduce_mid / k_reduce_big), kBigHegstOnly (the
 // same kernels, stopping after C = L^{-1} A L^{-H}: C's lower triangle in X, L in LV) or kBigHetrdOnly
 // (the Householder alone by k_hetrd_l2, from C's lower triangle in X with L already in LV, as
@@ -275,6 +278,7 @@ size_t reduce_smem_bytes(int mode, int n);
 size_t ql_chain_smem_bytes(int n, int threads, bool single);
 size_t ql_apply_smem_bytes(int n, int warps_per_cta, bool single);
 size_t back_smem_bytes(int n);
+size_t invit_smem_bytes(int n, bool with_tile);
 // r[i] = recip_nr(u[i]) for i < count (device self-test of the inverse iteration's reciprocal).
 cudaError_t launch_selftest_recip(const double* u, double* r, int count, cudaStream_t stream);
 // FP64 FMA throughput probe: `blocks` CTAs of 256 threads, each thread 8 chains x 4 x iters FMAs;
