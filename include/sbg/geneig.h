@@ -209,7 +209,8 @@ const char* sbg_solver_cache_layer_used(const sbg_solver* s);
 int sbg_solver_precision(const sbg_solver* s);
 
 /* Largest n each form supports on this device (shared-memory bound).  FP64: 256 (n <= 84
- * one CTA or warp per pair, 84 < n <= 256 one thread-block cluster per pair); mixed: 235 (the
+ * one CTA or warp per pair; 84 < n <= 256 one CTA per pair with the pair's matrices in device
+ * memory, or thread-block clusters in the scalar schedule); mixed: 235 (the
  * complex64 Householder takes one CTA per pair: n <= 63 one warp per pair and the refinement on
  * shared-memory tiles, 63 < n <= 235 one CTA per pair and the refinement on the pair's matrices in
  * the workspace, which then holds five more n x n complex matrices per pair). */
